@@ -1,0 +1,102 @@
+"""Extract the reference's own golden vectors into small numpy fixtures.
+
+Run in a container where the reference source tree is mounted (default
+/root/reference, override with ABACUS_REF).  Reads the literal arrays of the
+reference's unit tests as text and writes ``tests/golden/*.npz``:
+
+  ekinetic_op.npz  <- source/module_hamilt_pw/hamilt_pwdft/kernels/test/ekinetic_op_test.cpp
+  nonlocal_op.npz  <- .../kernels/test/nonlocal_op_test.cpp
+  veff_op.npz      <- .../kernels/test/veff_op_test.cpp
+  pw_op.npz        <- source/module_basis/module_pw/kernels/test/pw_op_test.cpp
+  pyabacus_si2.npz <- python/pyabacus/tests/test_diag/Si2.mat (sparse H, CSC arrays)
+
+The fixtures are committed; tests never read the reference tree.
+"""
+from __future__ import annotations
+
+import os
+import re
+import sys
+from pathlib import Path
+
+import numpy as np
+
+REF = Path(os.environ.get("ABACUS_REF", "/root/reference"))
+OUT = Path(__file__).resolve().parent
+
+_num = r"[-+]?(?:\d+\.?\d*|\.\d+)(?:[eE][-+]?\d+)?"
+
+
+def _parse_block(text: str):
+    """Parse the body of a C++ initializer list: complex pairs {a,b} or plain numbers."""
+    pairs = re.findall(r"\{\s*(" + _num + r")\s*,\s*(" + _num + r")\s*\}", text)
+    if pairs:
+        return np.array([complex(float(a), float(b)) for a, b in pairs])
+    return np.array([float(x) for x in re.findall(_num, text)])
+
+
+def _vectors(path: Path) -> dict:
+    src = path.read_text()
+    out = {}
+    for m in re.finditer(r"std::vector<[^=;{]*?>\s+(\w+)\s*=\s*\{", src):
+        name = m.group(1)
+        i = m.end()
+        depth = 1
+        while depth:
+            c = src[i]
+            depth += (c == "{") - (c == "}")
+            i += 1
+        out[name] = _parse_block(src[m.end():i - 1])
+    return out
+
+
+def _scalars(path: Path, names):
+    src = path.read_text()
+    res = {}
+    for n in names:
+        m = re.search(r"\b" + n + r"\s*=\s*(" + _num + r")\s*[;,]", src)
+        res[n] = float(m.group(1))
+    return res
+
+
+def main():
+    kt = REF / "source/module_hamilt_pw/hamilt_pwdft/kernels/test"
+    v = _vectors(kt / "ekinetic_op_test.cpp")
+    s = _scalars(kt / "ekinetic_op_test.cpp", ["dim", "band", "tpiba2"])
+    np.savez(OUT / "ekinetic_op.npz", gk2=v["gk2"], psi=v["psi"], expected_hpsi=v["expected_hpsi"],
+             dim=int(s["dim"]), band=int(s["band"]), tpiba2=s["tpiba2"])
+
+    v = _vectors(kt / "nonlocal_op_test.cpp")
+    s = _scalars(kt / "nonlocal_op_test.cpp",
+                 ["l1", "l2", "l2_spin", "l3", "spin", "nkb", "deeq_x", "deeq_y", "deeq_z", "expected_sum", "expected_iat"])
+    np.savez(OUT / "nonlocal_op.npz", deeq=v["deeq"], deeq_spin=v["deeq_spin"], becp=v["becp"],
+             becp_spin=v["becp_spin"], expected_ps=v["expected_ps"], expected_ps_spin=v["expected_ps_spin"],
+             **{k: int(x) for k, x in s.items()})
+
+    v = _vectors(kt / "veff_op_test.cpp")
+    s = _scalars(kt / "veff_op_test.cpp", ["size"])
+    np.savez(OUT / "veff_op.npz", vin=v["in"], out=v["out"], expected_out=v["expected_out"],
+             out_spin=v["out_spin"], in_spin=v["in_spin"], expected_out_spin=v["expected_out_spin"],
+             size=int(s["size"]))
+
+    pt = REF / "source/module_basis/module_pw/kernels/test/pw_op_test.cpp"
+    v = _vectors(pt)
+    s = _scalars(pt, ["npwk", "nxyz", "factor"])
+    np.savez(OUT / "pw_op.npz", box_index=v["box_index"].astype(np.int64), in_1=v["in_1"], out_1=v["out_1"],
+             in_2=v["in_2"], out_2=v["out_2"], in_3=v["in_3"], out_3=v["out_3"], out_3_init=v["out_3_init"],
+             npwk=int(s["npwk"]), nxyz=int(s["nxyz"]), factor=s["factor"])
+
+    try:
+        import scipy.io
+        import scipy.sparse
+        mat = scipy.io.loadmat(REF / "python/pyabacus/tests/test_diag/Si2.mat")["Problem"]["A"][0, 0]
+        csc = scipy.sparse.csc_matrix(mat)
+        np.savez_compressed(OUT / "pyabacus_si2.npz", data=csc.data, indices=csc.indices, indptr=csc.indptr,
+                            shape=np.array(csc.shape))
+    except Exception as exc:  # pragma: no cover
+        print("Si2.mat skipped:", exc, file=sys.stderr)
+    print("golden fixtures written to", OUT)
+
+
+if __name__ == "__main__":
+    main()
