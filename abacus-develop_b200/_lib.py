@@ -1,0 +1,113 @@
+"""ctypes binding of libabacus_b200.so (the C-ABI in include/abacus_b200.h).
+
+The library is loaded from this directory; a missing library or a failing call
+raises -- there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import re
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "libabacus_b200.so"
+HEADER = HERE.parent / "include" / "abacus_b200.h"
+
+vp = C.c_void_p
+i32 = C.c_int
+f64 = C.c_double
+f32 = C.c_float
+pi32 = C.POINTER(C.c_int)
+pf64 = C.POINTER(C.c_double)
+
+HPSI_CB = C.CFUNCTYPE(None, vp, vp, vp, i32, i32, i32, i32)
+
+_SIGS = {
+    "b200_last_error": ([], C.c_char_p),
+    "b200_version": ([], C.c_char_p),
+    "b200_ekinetic_pw_op_f64": ([i32, i32, i32, f64, vp, vp, vp, vp], i32),
+    "b200_ekinetic_pw_op_f32": ([i32, i32, i32, f32, vp, vp, vp, vp], i32),
+    "b200_veff_pw_op_f64": ([i32, vp, vp, vp], i32),
+    "b200_veff_pw_op_f32": ([i32, vp, vp, vp], i32),
+    "b200_veff_pw_op_npol2_f64": ([i32, vp, vp, vp, vp, vp, vp, vp], i32),
+    "b200_veff_pw_op_npol2_f32": ([i32, vp, vp, vp, vp, vp, vp, vp], i32),
+    "b200_nonlocal_pw_op_f64": ([i32, i32, i32, pi32, pi32, i32, i32, i32, i32, i32, vp, vp, vp, vp], i32),
+    "b200_nonlocal_pw_op_f32": ([i32, i32, i32, pi32, pi32, i32, i32, i32, i32, i32, vp, vp, vp, vp], i32),
+    "b200_nonlocal_pw_op_nc_f64": ([i32, i32, i32, pi32, pi32, i32, i32, i32, i32, vp, vp, vp, vp], i32),
+    "b200_nonlocal_pw_op_nc_f32": ([i32, i32, i32, pi32, pi32, i32, i32, i32, i32, vp, vp, vp, vp], i32),
+    "b200_set_3d_fft_box_op_f64": ([i32, vp, vp, vp, vp], i32),
+    "b200_set_3d_fft_box_op_f32": ([i32, vp, vp, vp, vp], i32),
+    "b200_set_recip_to_real_output_op_f64": ([i32, i32, f64, vp, vp, vp], i32),
+    "b200_set_recip_to_real_output_op_f32": ([i32, i32, f32, vp, vp, vp], i32),
+    "b200_set_real_to_recip_output_op_f64": ([i32, i32, i32, f64, vp, vp, vp, vp], i32),
+    "b200_set_real_to_recip_output_op_f32": ([i32, i32, i32, f32, vp, vp, vp, vp], i32),
+    "b200_pw_basis_create": ([f64, pf64, f64, f64, i32, i32, i32, i32, pf64, C.POINTER(vp)], i32),
+    "b200_pw_basis_destroy": ([vp], i32),
+    "b200_pw_basis_dims": ([vp, pi32], i32),
+    "b200_pw_basis_scalars": ([vp, pf64], i32),
+    "b200_pw_basis_kpoint": ([vp, i32, pi32, vp, vp, vp], i32),
+    "b200_pw_basis_kvec_c": ([vp, i32, pf64], i32),
+    "b200_pw_basis_device_maps": ([vp, i32, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp)], i32),
+    "b200_recip_to_real_f64": ([vp, vp, vp, i32, i32, f64, vp], i32),
+    "b200_recip_to_real_f32": ([vp, vp, vp, i32, i32, f32, vp], i32),
+    "b200_real_to_recip_f64": ([vp, vp, vp, i32, i32, f64, vp], i32),
+    "b200_real_to_recip_f32": ([vp, vp, vp, i32, i32, f32, vp], i32),
+    "b200_hamilt_create": ([vp, i32, C.POINTER(vp)], i32),
+    "b200_hamilt_destroy": ([vp], i32),
+    "b200_hamilt_set_veff": ([vp, vp], i32),
+    "b200_hamilt_set_vkb": ([vp, i32, i32, i32, vp], i32),
+    "b200_hamilt_set_deeq": ([vp, i32, pi32, pi32, i32, i32, i32, i32, vp], i32),
+    "b200_hamilt_hpsi": ([vp, i32, i32, i32, i32, vp, vp, vp], i32),
+    "b200_hamilt_hpsi_part": ([vp, i32, i32, i32, i32, vp, vp, i32, vp], i32),
+    "b200_david_create": ([i32, i32, i32, i32, vp, C.POINTER(vp)], i32),
+    "b200_david_destroy": ([vp], i32),
+    "b200_david_diag": ([vp, HPSI_CB, vp, i32, vp, pf64, f64, i32, i32, i32, pi32], i32),
+    "b200_david_diag_hamilt": ([vp, vp, i32, i32, i32, vp, pf64, f64, i32, i32, i32, pi32], i32),
+}
+
+_lib = None
+
+
+class B200Error(RuntimeError):
+    def __init__(self, fn: str, code: int, msg: str):
+        super().__init__(f"{fn} failed with status {code}: {msg}")
+        self.code = code
+
+
+def header_symbols() -> list[str]:
+    """Entry points declared in include/abacus_b200.h."""
+    txt = HEADER.read_text()
+    return sorted(set(re.findall(r"^\s*(?:int|const char\*)\s+(b200_\w+)\s*\(", txt, re.M)))
+
+
+def load() -> C.CDLL:
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise ImportError(f"{LIB_PATH} is missing: run abacus-develop_b200/build.py (no CPU fallback exists)")
+    lib = C.CDLL(str(LIB_PATH))
+    for name, (args, res) in _SIGS.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = res
+    _lib = lib
+    return lib
+
+
+def call(name: str, *args) -> None:
+    lib = load()
+    rc = getattr(lib, name)(*args)
+    if rc != 0:
+        raise B200Error(name, rc, lib.b200_last_error().decode())
+
+
+def ptr(t) -> int:
+    """Device pointer of a torch tensor (or None)."""
+    return None if t is None else t.data_ptr()
+
+
+def stream_ptr(stream=None):
+    import torch
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return s.cuda_stream

@@ -1,0 +1,363 @@
+// C-ABI entry points (include/abacus_b200.h).  Every call catches library
+// errors and returns a status; the message is kept per thread.
+#include <cstring>
+#include <memory>
+#include <string>
+
+#include "../../include/abacus_b200.h"
+#include "david.h"
+#include "functors.h"
+#include "hamilt.h"
+#include "pw_grid.h"
+
+struct b200_pw_basis {
+    b200::PWGrid grid;
+    b200::DeviceArray<double2> aux64;
+    b200::DeviceArray<float2> aux32;
+};
+struct b200_hamilt {
+    std::unique_ptr<b200::Hamilt> h;
+};
+struct b200_david {
+    std::unique_ptr<b200::DavidBase> d;
+};
+
+namespace b200 {
+namespace {
+thread_local std::string g_last_error;
+}
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+const char* last_error() { return g_last_error.c_str(); }
+}  // namespace b200
+
+namespace {
+template <typename F> int guarded(F&& f) {
+    try {
+        f();
+        b200::set_last_error("");
+        return B200_STATUS_OK;
+    } catch (const b200::Error& e) {
+        b200::set_last_error(e.what());
+        return e.code;
+    } catch (const std::exception& e) {
+        b200::set_last_error(e.what());
+        return B200_STATUS_INVALID_ARGUMENT;
+    }
+}
+inline cudaStream_t S(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+}  // namespace
+
+namespace {
+template <typename T> T* aux_of(b200_pw_basis* b);
+// device maps are uploaded on first device use, so basis set-up works without a GPU
+template <> double2* aux_of<double2>(b200_pw_basis* b) {
+    b->aux64.resize(size_t(b->grid.nxyz()));
+    return b->aux64.ptr;
+}
+template <> float2* aux_of<float2>(b200_pw_basis* b) {
+    b->aux32.resize(size_t(b->grid.nxyz()));
+    return b->aux32.ptr;
+}
+template <typename T> int r2r_impl(b200_pw_basis* b, const void* in, void* out, int ik, int add, double f, void* st) {
+    return guarded([&] {
+        B200_CHECK(b && in && out, b200::kInvalidArgument, "NULL argument");
+        B200_CHECK(ik >= 0 && ik < int(b->grid.kmaps.size()), b200::kInvalidArgument, "k-point index out of range");
+        b->grid.ensure_device();
+        b200::launch_recip_to_real<T>(b->grid, ik, (const T*)in, (T*)out, aux_of<T>(b), add, f, S(st));
+    });
+}
+template <typename T> int r2g_impl(b200_pw_basis* b, const void* in, void* out, int ik, int add, double f, void* st) {
+    return guarded([&] {
+        B200_CHECK(b && in && out, b200::kInvalidArgument, "NULL argument");
+        B200_CHECK(ik >= 0 && ik < int(b->grid.kmaps.size()), b200::kInvalidArgument, "k-point index out of range");
+        b->grid.ensure_device();
+        b200::launch_real_to_recip<T>(b->grid, ik, (const T*)in, (T*)out, aux_of<T>(b), add, f, S(st));
+    });
+}
+}  // namespace
+
+extern "C" {
+
+const char* b200_last_error(void) { return b200::last_error(); }
+const char* b200_version(void) { return "abacus_b200 0.1 (sm_100a)"; }
+
+// ------------------------------------------------------------------ functors
+int b200_ekinetic_pw_op_f64(int nband, int npw, int max_npw, double tpiba2, const double* gk2, void* hpsi,
+                            const void* psi, void* stream) {
+    return guarded([&] {
+        B200_CHECK(max_npw >= npw, b200::kInvalidArgument, "max_npw < npw");
+        b200::ekinetic_pw<double2, double>(nband, npw, max_npw, tpiba2, gk2, (double2*)hpsi, (const double2*)psi, S(stream));
+    });
+}
+int b200_ekinetic_pw_op_f32(int nband, int npw, int max_npw, float tpiba2, const float* gk2, void* hpsi, const void* psi,
+                            void* stream) {
+    return guarded([&] {
+        B200_CHECK(max_npw >= npw, b200::kInvalidArgument, "max_npw < npw");
+        b200::ekinetic_pw<float2, float>(nband, npw, max_npw, tpiba2, gk2, (float2*)hpsi, (const float2*)psi, S(stream));
+    });
+}
+int b200_veff_pw_op_f64(int size, void* out, const double* in, void* stream) {
+    return guarded([&] { b200::veff_pw<double2, double>(size, (double2*)out, in, S(stream)); });
+}
+int b200_veff_pw_op_f32(int size, void* out, const float* in, void* stream) {
+    return guarded([&] { b200::veff_pw<float2, float>(size, (float2*)out, in, S(stream)); });
+}
+int b200_veff_pw_op_npol2_f64(int size, void* out, void* out1, const double* in0, const double* in1, const double* in2,
+                              const double* in3, void* stream) {
+    return guarded([&] {
+        const double* in[4] = {in0, in1, in2, in3};
+        b200::veff_pw_npol2<double2, double>(size, (double2*)out, (double2*)out1, in, S(stream));
+    });
+}
+int b200_veff_pw_op_npol2_f32(int size, void* out, void* out1, const float* in0, const float* in1, const float* in2,
+                              const float* in3, void* stream) {
+    return guarded([&] {
+        const float* in[4] = {in0, in1, in2, in3};
+        b200::veff_pw_npol2<float2, float>(size, (float2*)out, (float2*)out1, in, S(stream));
+    });
+}
+int b200_nonlocal_pw_op_f64(int l1, int l2, int l3, int* sum, int* iat, int spin, int nkb, int dx, int dy, int dz,
+                            const double* deeq, void* ps, const void* becp, void* stream) {
+    return guarded([&] {
+        B200_CHECK(sum && iat, b200::kInvalidArgument, "sum/iat must not be NULL");
+        b200::nonlocal_pw<double2, double>(l1, l2, l3, *sum, *iat, spin, nkb, dx, dy, dz, deeq, (double2*)ps,
+                                           (const double2*)becp, S(stream));
+    });
+}
+int b200_nonlocal_pw_op_f32(int l1, int l2, int l3, int* sum, int* iat, int spin, int nkb, int dx, int dy, int dz,
+                            const float* deeq, void* ps, const void* becp, void* stream) {
+    return guarded([&] {
+        B200_CHECK(sum && iat, b200::kInvalidArgument, "sum/iat must not be NULL");
+        b200::nonlocal_pw<float2, float>(l1, l2, l3, *sum, *iat, spin, nkb, dx, dy, dz, deeq, (float2*)ps,
+                                         (const float2*)becp, S(stream));
+    });
+}
+int b200_nonlocal_pw_op_nc_f64(int l1, int l2, int l3, int* sum, int* iat, int nkb, int dx, int dy, int dz,
+                               const void* deeq_nc, void* ps, const void* becp, void* stream) {
+    return guarded([&] {
+        B200_CHECK(sum && iat, b200::kInvalidArgument, "sum/iat must not be NULL");
+        b200::nonlocal_pw_nc<double2>(l1, l2, l3, *sum, *iat, nkb, dx, dy, dz, (const double2*)deeq_nc, (double2*)ps,
+                                      (const double2*)becp, S(stream));
+    });
+}
+int b200_nonlocal_pw_op_nc_f32(int l1, int l2, int l3, int* sum, int* iat, int nkb, int dx, int dy, int dz,
+                               const void* deeq_nc, void* ps, const void* becp, void* stream) {
+    return guarded([&] {
+        B200_CHECK(sum && iat, b200::kInvalidArgument, "sum/iat must not be NULL");
+        b200::nonlocal_pw_nc<float2>(l1, l2, l3, *sum, *iat, nkb, dx, dy, dz, (const float2*)deeq_nc, (float2*)ps,
+                                     (const float2*)becp, S(stream));
+    });
+}
+int b200_set_3d_fft_box_op_f64(int npwk, const int* idx, const void* in, void* out, void* stream) {
+    return guarded([&] { b200::set_3d_fft_box<double2>(npwk, idx, (const double2*)in, (double2*)out, S(stream)); });
+}
+int b200_set_3d_fft_box_op_f32(int npwk, const int* idx, const void* in, void* out, void* stream) {
+    return guarded([&] { b200::set_3d_fft_box<float2>(npwk, idx, (const float2*)in, (float2*)out, S(stream)); });
+}
+int b200_set_recip_to_real_output_op_f64(int nrxx, int add, double factor, const void* in, void* out, void* stream) {
+    return guarded([&] {
+        b200::set_recip_to_real_output<double2, double>(nrxx, add, factor, (const double2*)in, (double2*)out, S(stream));
+    });
+}
+int b200_set_recip_to_real_output_op_f32(int nrxx, int add, float factor, const void* in, void* out, void* stream) {
+    return guarded([&] {
+        b200::set_recip_to_real_output<float2, float>(nrxx, add, factor, (const float2*)in, (float2*)out, S(stream));
+    });
+}
+int b200_set_real_to_recip_output_op_f64(int npw_k, int nxyz, int add, double factor, const int* idx, const void* in,
+                                         void* out, void* stream) {
+    return guarded([&] {
+        b200::set_real_to_recip_output<double2, double>(npw_k, nxyz, add, factor, idx, (const double2*)in, (double2*)out,
+                                                        S(stream));
+    });
+}
+int b200_set_real_to_recip_output_op_f32(int npw_k, int nxyz, int add, float factor, const int* idx, const void* in,
+                                         void* out, void* stream) {
+    return guarded([&] {
+        b200::set_real_to_recip_output<float2, float>(npw_k, nxyz, add, factor, idx, (const float2*)in, (float2*)out,
+                                                      S(stream));
+    });
+}
+
+// ------------------------------------------------------------------ basis
+int b200_pw_basis_create(double lat0, const double* latvec, double ecutwfc, double ecutrho, int nx, int ny, int nz,
+                         int nks, const double* kvec_d, b200_pw_basis** out) {
+    return guarded([&] {
+        B200_CHECK(out != nullptr, b200::kInvalidArgument, "out must not be NULL");
+        b200::PWBasisK b;
+        const int rc = b.setup(lat0, latvec, ecutwfc, ecutrho, nx, ny, nz, nks, kvec_d);
+        B200_CHECK(rc == 0, b200::kInvalidArgument,
+                   rc == 2 ? "a k-point has no plane waves" : "invalid lattice, cut-off or k-points");
+        auto p = std::make_unique<b200_pw_basis>();
+        p->grid.build(b);
+        *out = p.release();
+    });
+}
+int b200_pw_basis_destroy(b200_pw_basis* b) {
+    return guarded([&] { delete b; });
+}
+int b200_pw_basis_dims(const b200_pw_basis* b, int* dims) {
+    return guarded([&] {
+        B200_CHECK(b && dims, b200::kInvalidArgument, "NULL argument");
+        const auto& g = b->grid;
+        dims[0] = g.nx;
+        dims[1] = g.ny;
+        dims[2] = g.nz;
+        dims[3] = g.nst;
+        dims[4] = g.basis.npw;
+        dims[5] = g.basis.npwk_max;
+        dims[6] = g.basis.nks;
+        dims[7] = g.nxc;
+    });
+}
+int b200_pw_basis_scalars(const b200_pw_basis* b, double* scal) {
+    return guarded([&] {
+        B200_CHECK(b && scal, b200::kInvalidArgument, "NULL argument");
+        scal[0] = b->grid.basis.tpiba2;
+        scal[1] = b->grid.basis.omega;
+        scal[2] = b->grid.basis.gk_ecut;
+    });
+}
+int b200_pw_basis_kpoint(const b200_pw_basis* b, int ik, int* npwk, int* ig2ixyz, double* gk2, double* gcar) {
+    return guarded([&] {
+        B200_CHECK(b != nullptr, b200::kInvalidArgument, "NULL basis");
+        const auto& B = b->grid.basis;
+        B200_CHECK(ik >= 0 && ik < B.nks, b200::kInvalidArgument, "k-point index out of range");
+        const int n = B.npwk[ik];
+        const size_t off = size_t(ik) * B.npwk_max;
+        if (npwk) *npwk = n;
+        if (ig2ixyz) std::memcpy(ig2ixyz, &B.ig2ixyz_k[off], n * sizeof(int));
+        if (gk2) std::memcpy(gk2, &B.gk2[off], n * sizeof(double));
+        if (gcar) std::memcpy(gcar, &B.gcar[off * 3], n * 3 * sizeof(double));
+    });
+}
+int b200_pw_basis_kvec_c(const b200_pw_basis* b, int ik, double* kvec_c) {
+    return guarded([&] {
+        B200_CHECK(b && kvec_c, b200::kInvalidArgument, "NULL argument");
+        const auto& B = b->grid.basis;
+        B200_CHECK(ik >= 0 && ik < B.nks, b200::kInvalidArgument, "k-point index out of range");
+        for (int j = 0; j < 3; ++j) kvec_c[j] = B.kvec_c[3 * ik + j];
+    });
+}
+int b200_pw_basis_device_maps(const b200_pw_basis* b, int ik, const double** gk2_d, const float** gk2f_d,
+                              const int** ig2ixyz_d) {
+    return guarded([&] {
+        B200_CHECK(b != nullptr, b200::kInvalidArgument, "NULL basis");
+        B200_CHECK(ik >= 0 && ik < int(b->grid.kmaps.size()), b200::kInvalidArgument, "k-point index out of range");
+        const_cast<b200::PWGrid&>(b->grid).ensure_device();
+        const auto& k = b->grid.kmaps[ik];
+        if (gk2_d) *gk2_d = k.gk2.ptr;
+        if (gk2f_d) *gk2f_d = k.gk2f.ptr;
+        if (ig2ixyz_d) *ig2ixyz_d = k.ig2ixyz.ptr;
+    });
+}
+
+int b200_recip_to_real_f64(b200_pw_basis* b, const void* in, void* out, int ik, int add, double factor, void* stream) {
+    return r2r_impl<double2>(b, in, out, ik, add, factor, stream);
+}
+int b200_recip_to_real_f32(b200_pw_basis* b, const void* in, void* out, int ik, int add, float factor, void* stream) {
+    return r2r_impl<float2>(b, in, out, ik, add, factor, stream);
+}
+int b200_real_to_recip_f64(b200_pw_basis* b, const void* in, void* out, int ik, int add, double factor, void* stream) {
+    return r2g_impl<double2>(b, in, out, ik, add, factor, stream);
+}
+int b200_real_to_recip_f32(b200_pw_basis* b, const void* in, void* out, int ik, int add, float factor, void* stream) {
+    return r2g_impl<float2>(b, in, out, ik, add, factor, stream);
+}
+
+// ------------------------------------------------------------------ Hamiltonian
+int b200_hamilt_create(b200_pw_basis* b, int precision, b200_hamilt** out) {
+    return guarded([&] {
+        B200_CHECK(b && out, b200::kInvalidArgument, "NULL argument");
+        B200_CHECK(precision == B200_PREC_FP64 || precision == B200_PREC_MIXED, b200::kInvalidArgument, "bad precision");
+        b->grid.ensure_device();
+        auto p = std::make_unique<b200_hamilt>();
+        p->h = std::make_unique<b200::Hamilt>(&b->grid, precision);
+        *out = p.release();
+    });
+}
+int b200_hamilt_destroy(b200_hamilt* h) {
+    return guarded([&] { delete h; });
+}
+int b200_hamilt_set_veff(b200_hamilt* h, const double* veff) {
+    return guarded([&] {
+        B200_CHECK(h && veff, b200::kInvalidArgument, "NULL argument");
+        h->h->set_veff(veff);
+    });
+}
+int b200_hamilt_set_vkb(b200_hamilt* h, int ik, int nkb, int npwx, const void* vkb) {
+    return guarded([&] {
+        B200_CHECK(h != nullptr && (nkb == 0 || vkb != nullptr), b200::kInvalidArgument, "NULL argument");
+        h->h->set_vkb(ik, nkb, npwx, (const double2*)vkb);
+    });
+}
+int b200_hamilt_set_deeq(b200_hamilt* h, int ntype, const int* na, const int* nh, int nspin, int dx, int dy, int dz,
+                         const double* deeq) {
+    return guarded([&] {
+        B200_CHECK(h && na && nh && deeq, b200::kInvalidArgument, "NULL argument");
+        h->h->set_deeq(ntype, na, nh, nspin, dx, dy, dz, deeq);
+    });
+}
+static int hpsi_impl(b200_hamilt* h, int ik, int spin, int nb, int ld, const void* psi, void* hpsi, int mode, void* st) {
+    return guarded([&] {
+        B200_CHECK(h && psi && hpsi, b200::kInvalidArgument, "NULL argument");
+        if (h->h->precision == B200_PREC_FP64)
+            h->h->hpsi<double2>(ik, spin, nb, ld, (const double2*)psi, (double2*)hpsi, mode, S(st));
+        else
+            h->h->hpsi<float2>(ik, spin, nb, ld, (const float2*)psi, (float2*)hpsi, mode, S(st));
+    });
+}
+int b200_hamilt_hpsi(b200_hamilt* h, int ik, int spin, int nbands, int ld, const void* psi, void* hpsi, void* stream) {
+    return hpsi_impl(h, ik, spin, nbands, ld, psi, hpsi, 0, stream);
+}
+int b200_hamilt_hpsi_part(b200_hamilt* h, int ik, int spin, int nbands, int ld, const void* psi, void* hpsi, int mode,
+                          void* stream) {
+    if (mode != 1 && mode != 2) {
+        b200::set_last_error("mode must be 1 (local) or 2 (nonlocal)");
+        return B200_STATUS_INVALID_ARGUMENT;
+    }
+    return hpsi_impl(h, ik, spin, nbands, ld, psi, hpsi, mode, stream);
+}
+
+// ------------------------------------------------------------------ Davidson
+int b200_david_create(int nband, int dim, int david_ndim, int precision, const double* precond, b200_david** out) {
+    return guarded([&] {
+        B200_CHECK(out && precond, b200::kInvalidArgument, "NULL argument");
+        auto p = std::make_unique<b200_david>();
+        p->d = b200::make_david(nband, dim, david_ndim, precision, precond);
+        *out = p.release();
+    });
+}
+int b200_david_destroy(b200_david* d) {
+    return guarded([&] { delete d; });
+}
+int b200_david_diag(b200_david* d, b200_hpsi_cb hpsi, void* user, int ldpsi, void* psi, double* eig, double thr,
+                    int maxiter, int ntry_max, int notconv_max, int* iters) {
+    return guarded([&] {
+        B200_CHECK(d && hpsi && psi && eig, b200::kInvalidArgument, "NULL argument");
+        b200::HPsiDevice f = [hpsi, user](const void* x, void* hx, int nvec, int dim, int i0, int i1, cudaStream_t) {
+            hpsi(user, x, hx, nvec, dim, i0, i1);
+        };
+        const int it = d->d->diag(f, ldpsi, psi, eig, thr, maxiter, ntry_max, notconv_max);
+        if (iters) *iters = it;
+    });
+}
+int b200_david_diag_hamilt(b200_david* d, b200_hamilt* h, int ik, int spin, int ldpsi, void* psi, double* eig,
+                           double thr, int maxiter, int ntry_max, int notconv_max, int* iters) {
+    return guarded([&] {
+        B200_CHECK(d && h && psi && eig, b200::kInvalidArgument, "NULL argument");
+        b200::Hamilt* H = h->h.get();
+        b200::HPsiDevice f64 = [H, ik, spin](const void* x, void* hx, int, int dim, int i0, int i1, cudaStream_t s) {
+            const double2* X = (const double2*)x + size_t(i0) * dim;
+            H->hpsi<double2>(ik, spin, i1 - i0 + 1, dim, X, (double2*)hx, 0, s);
+        };
+        b200::HPsiDevice f32 = [H, ik, spin](const void* x, void* hx, int, int dim, int i0, int i1, cudaStream_t s) {
+            const float2* X = (const float2*)x + size_t(i0) * dim;
+            H->hpsi<float2>(ik, spin, i1 - i0 + 1, dim, X, (float2*)hx, 0, s);
+        };
+        const int it = d->d->diag_hamilt(f64, f32, H->precision, ldpsi, psi, eig, thr, maxiter, ntry_max, notconv_max);
+        if (iters) *iters = it;
+    });
+}
+
+}  // extern "C"

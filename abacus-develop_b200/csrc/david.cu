@@ -1,0 +1,429 @@
+// Block Davidson on the device, restating hsolver::DiagoDavid (diago_david.cpp:151-1240).
+//
+// Same iteration as the reference: Rayleigh-Ritz on the basis, residuals
+// r_m = H x_m - lambda_m x_m of the unconverged bands (cal_grad :359-611),
+// preconditioned by h_diag, orthogonalised and appended; the projected rows of
+// hcc = basis^H H basis (cal_elem :626-717); the lowest nband eigenpairs of its
+// lower triangle (diag_zhegvx :731-777); convergence |lambda_new - lambda_old|
+// < thr per band (:270-280); restart through refresh (:797-934) when the basis
+// would overflow nbase_x = david_ndim * nband; diag() retries (:1173-1240).
+//
+// B200 differences (same mathematics):
+//  * the per-vector Gram-Schmidt (SchmidtOrth, :950-1075) becomes a block
+//    classical Gram-Schmidt against the basis (two GEMMs) followed by
+//    Cholesky-QR (twice) of the new block, with the Cholesky in FP64;
+//  * S = I for norm-conserving pseudopotentials, so spsi aliases the basis and
+//    scc (never read by the eigensolver) is not formed;
+//  * no per-band cudaMalloc / host round trip; one small device-to-host copy of
+//    the eigenvalues per iteration drives the host-side convergence test.
+//  * mixed precision: the same iteration with FP32 vectors and FP32 GEMMs
+//    (FP64 Cholesky and FP64 subspace eigensolve), then an FP64 Davidson from
+//    the FP32 eigenvectors to the requested threshold.
+#include <cublas_v2.h>
+#include <cusolverDn.h>
+
+#include <cmath>
+#include <vector>
+
+#include "common.h"
+#include "david.h"
+#include "fft_core.cuh"
+
+namespace b200 {
+
+#define B200_CUSOLVER(call)                                                                                   \
+    do {                                                                                                      \
+        cusolverStatus_t st_ = (call);                                                                        \
+        if (st_ != CUSOLVER_STATUS_SUCCESS)                                                                   \
+            throw ::b200::Error(::b200::kCusolverError, std::string(#call) + " failed with status " +       \
+                                                            std::to_string(int(st_)));                       \
+    } while (0)
+#define B200_CUBLAS_D(call)                                                                                   \
+    do {                                                                                                      \
+        cublasStatus_t st_ = (call);                                                                          \
+        if (st_ != CUBLAS_STATUS_SUCCESS)                                                                     \
+            throw ::b200::Error(::b200::kCublasError, std::string(#call) + " failed with status " +         \
+                                                          std::to_string(int(st_)));                         \
+    } while (0)
+
+namespace {
+
+constexpr int kT = 256;
+inline int grid_of(long n) {
+    long b = (n + kT - 1) / kT;
+    if (b > 148L * 8) b = 148L * 8;
+    return int(b < 1 ? 1 : b);
+}
+
+template <typename T, typename R>
+__global__ void k_precond(long dim, int nc, T* __restrict__ v, const R* __restrict__ pc) {
+    const long n = dim * nc;
+    for (long i = blockIdx.x * long(blockDim.x) + threadIdx.x; i < n; i += long(gridDim.x) * blockDim.x) {
+        const R p = pc[i % dim];
+        v[i] = cmake<T>(v[i].x / p, v[i].y / p);
+    }
+}
+
+// vc(:, m) = vcc(:nbase, unconv[m]); vcl(:, m) = -lambda_{unconv[m]} vc(:, m)
+template <typename T>
+__global__ void k_gather_cols(int nbase, int nbase_x, int nc, const int* __restrict__ unconv, const T* __restrict__ vcc,
+                              const double* __restrict__ w, T* __restrict__ vc, T* __restrict__ vcl) {
+    using R = typename RealOf<T>::type;
+    const long n = long(nbase) * nc;
+    for (long i = blockIdx.x * long(blockDim.x) + threadIdx.x; i < n; i += long(gridDim.x) * blockDim.x) {
+        const int m = int(i / nbase);
+        const int r = int(i - long(m) * nbase);
+        const int col = unconv[m];
+        const T v = vcc[long(col) * nbase_x + r];
+        vc[i] = v;
+        vcl[i] = cscale(v, R(-w[col]));
+    }
+}
+
+template <typename T>
+__global__ void k_refresh_diag(int nband, int nbase_x, const double* __restrict__ e, T* __restrict__ hcc,
+                               T* __restrict__ vcc) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nband; i += gridDim.x * blockDim.x) {
+        hcc[long(i) * nbase_x + i] = cmake<T>(e[i], 0);
+        vcc[long(i) * nbase_x + i] = cmake<T>(1, 0);
+    }
+}
+
+template <typename A, typename B> __global__ void k_convert(long n, const A* __restrict__ a, B* __restrict__ b) {
+    for (long i = blockIdx.x * long(blockDim.x) + threadIdx.x; i < n; i += long(gridDim.x) * blockDim.x)
+        b[i] = cmake<B>(a[i].x, a[i].y);
+}
+
+template <typename R> __global__ void k_convert_real(long n, const double* __restrict__ a, R* __restrict__ b) {
+    for (long i = blockIdx.x * long(blockDim.x) + threadIdx.x; i < n; i += long(gridDim.x) * blockDim.x) b[i] = R(a[i]);
+}
+
+template <typename T> struct Lin;
+template <> struct Lin<double2> {
+    static void gemm(cublasHandle_t h, cublasOperation_t a, cublasOperation_t b, int m, int n, int k, double2 al,
+                     const double2* A, int lda, const double2* B, int ldb, double2 be, double2* C, int ldc) {
+        B200_CUBLAS_D(cublasZgemm(h, a, b, m, n, k, (const cuDoubleComplex*)&al, (const cuDoubleComplex*)A, lda,
+                                  (const cuDoubleComplex*)B, ldb, (const cuDoubleComplex*)&be, (cuDoubleComplex*)C, ldc));
+    }
+    static void herk(cublasHandle_t h, int n, int k, const double2* A, int lda, double2* C, int ldc) {
+        const double one = 1.0, zero = 0.0;
+        B200_CUBLAS_D(cublasZherk(h, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_C, n, k, &one, (const cuDoubleComplex*)A, lda, &zero,
+                                  (cuDoubleComplex*)C, ldc));
+    }
+    static void trsm(cublasHandle_t h, int m, int n, const double2* U, int ldu, double2* X, int ldx) {
+        const double2 one = make_double2(1.0, 0.0);
+        B200_CUBLAS_D(cublasZtrsm(h, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, m, n,
+                                  (const cuDoubleComplex*)&one, (const cuDoubleComplex*)U, ldu, (cuDoubleComplex*)X, ldx));
+    }
+};
+template <> struct Lin<float2> {
+    static void gemm(cublasHandle_t h, cublasOperation_t a, cublasOperation_t b, int m, int n, int k, float2 al,
+                     const float2* A, int lda, const float2* B, int ldb, float2 be, float2* C, int ldc) {
+        B200_CUBLAS_D(cublasCgemm(h, a, b, m, n, k, (const cuComplex*)&al, (const cuComplex*)A, lda, (const cuComplex*)B,
+                                  ldb, (const cuComplex*)&be, (cuComplex*)C, ldc));
+    }
+    static void herk(cublasHandle_t h, int n, int k, const float2* A, int lda, float2* C, int ldc) {
+        const float one = 1.f, zero = 0.f;
+        B200_CUBLAS_D(cublasCherk(h, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_C, n, k, &one, (const cuComplex*)A, lda, &zero,
+                                  (cuComplex*)C, ldc));
+    }
+    static void trsm(cublasHandle_t h, int m, int n, const float2* U, int ldu, float2* X, int ldx) {
+        const float2 one = make_float2(1.f, 0.f);
+        B200_CUBLAS_D(cublasCtrsm(h, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, m, n,
+                                  (const cuComplex*)&one, (const cuComplex*)U, ldu, (cuComplex*)X, ldx));
+    }
+};
+
+template <typename T> struct Engine {
+    using R = typename RealOf<T>::type;
+    int nband, dim, nbase_x;
+    cudaStream_t s = 0;
+    cublasHandle_t cb = nullptr;
+    cusolverDnHandle_t cs = nullptr;
+    DeviceArray<T> basis, hp, newv, hcc, vcc, vc, vcl, lag, gram;
+    DeviceArray<double2> A64, gram64, work;
+    DeviceArray<double> w, ein;
+    DeviceArray<R> pc;
+    DeviceArray<int> unconv_d, info;
+    int lwork = 0;
+    std::vector<double> eig_h;
+    std::vector<int> unconv_h;
+    bool ref_refresh = true;
+    int hpsi_bands = 0;
+
+    Engine(int nb, int d, int ndim, const double* precond_d) : nband(nb), dim(d), nbase_x(ndim * nb) {
+        B200_CHECK(ndim > 1 && nb > 0 && ndim * nb < d, kInvalidArgument, "need david_ndim > 1 and david_ndim*nband < dim");
+        B200_CUBLAS_D(cublasCreate(&cb));
+        B200_CUSOLVER(cusolverDnCreate(&cs));
+        B200_CUBLAS_D(cublasSetStream(cb, s));
+        B200_CUSOLVER(cusolverDnSetStream(cs, s));
+        basis.resize(size_t(nbase_x) * dim);
+        hp.resize(size_t(nbase_x) * dim);
+        newv.resize(size_t(nband) * dim);
+        hcc.resize(size_t(nbase_x) * nbase_x);
+        vcc.resize(size_t(nbase_x) * nbase_x);
+        vc.resize(size_t(nbase_x) * nband);
+        vcl.resize(size_t(nbase_x) * nband);
+        lag.resize(size_t(nbase_x) * nband);
+        gram.resize(size_t(nband) * nband);
+        A64.resize(size_t(nbase_x) * nbase_x);
+        gram64.resize(size_t(nband) * nband);
+        w.resize(nbase_x);
+        ein.resize(nband);
+        pc.resize(dim);
+        unconv_d.resize(nband);
+        info.resize(4);
+        B200_CUDA(cudaMemsetAsync(hcc.ptr, 0, hcc.n * sizeof(T), s));
+        B200_CUDA(cudaMemsetAsync(vcc.ptr, 0, vcc.n * sizeof(T), s));
+        B200_CUDA(cudaMemsetAsync(basis.ptr, 0, basis.n * sizeof(T), s));
+        B200_CUDA(cudaMemsetAsync(info.ptr, 0, 4 * sizeof(int), s));
+        if constexpr (std::is_same<R, double>::value) {
+            B200_CUDA(cudaMemcpyAsync(pc.ptr, precond_d, dim * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        } else {
+            k_convert_real<R><<<grid_of(dim), kT, 0, s>>>(dim, precond_d, pc.ptr);
+            B200_CUDA(cudaGetLastError());
+        }
+        int l1 = 0, l2 = 0;
+        B200_CUSOLVER(cusolverDnZheevd_bufferSize(cs, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, nbase_x,
+                                                  (cuDoubleComplex*)A64.ptr, nbase_x, w.ptr, &l1));
+        B200_CUSOLVER(cusolverDnZpotrf_bufferSize(cs, CUBLAS_FILL_MODE_UPPER, nband, (cuDoubleComplex*)gram64.ptr, nband, &l2));
+        lwork = l1 > l2 ? l1 : l2;
+        work.resize(size_t(lwork > 0 ? lwork : 1));
+        eig_h.assign(nbase_x, 0.0);
+        unconv_h.assign(nband, 0);
+        B200_CUDA(cudaStreamSynchronize(s));
+    }
+    ~Engine() {
+        if (cb) cublasDestroy(cb);
+        if (cs) cusolverDnDestroy(cs);
+    }
+
+    void gemm(cublasOperation_t a, cublasOperation_t b, int m, int n, int k, T al, const T* A, int lda, const T* B,
+              int ldb, T be, T* C, int ldc) {
+        if (m <= 0 || n <= 0) return;
+        Lin<T>::gemm(cb, a, b, m, n, k, al, A, lda, B, ldb, be, C, ldc);
+    }
+
+    // X (dim x nc) <- X U^-1 with X^H X = U^H U, U from an FP64 Cholesky
+    void cholqr(T* X, int nc) {
+        Lin<T>::herk(cb, nc, dim, X, dim, gram.ptr, nc);
+        const long n2 = long(nc) * nc;
+        double2* G = gram64.ptr;
+        if constexpr (std::is_same<T, double2>::value) {
+            B200_CUDA(cudaMemcpyAsync(G, gram.ptr, n2 * sizeof(double2), cudaMemcpyDeviceToDevice, s));
+        } else {
+            k_convert<T, double2><<<grid_of(n2), kT, 0, s>>>(n2, gram.ptr, G);
+            B200_CUDA(cudaGetLastError());
+        }
+        B200_CUSOLVER(cusolverDnZpotrf(cs, CUBLAS_FILL_MODE_UPPER, nc, (cuDoubleComplex*)G, nc, (cuDoubleComplex*)work.ptr,
+                                       lwork, info.ptr + 1));
+        const T* U;
+        if constexpr (std::is_same<T, double2>::value) {
+            U = G;
+        } else {
+            k_convert<double2, T><<<grid_of(n2), kT, 0, s>>>(n2, G, gram.ptr);
+            B200_CUDA(cudaGetLastError());
+            U = gram.ptr;
+        }
+        Lin<T>::trsm(cb, dim, nc, U, nc, X, dim);
+    }
+
+    // orthonormalise X (dim x nc) against basis[:, :nprev] and within itself
+    void orth_block(T* X, int nc, int nprev) {
+        const T one = cmake<T>(1, 0), zero = cmake<T>(0, 0), mone = cmake<T>(-1, 0);
+        for (int pass = 0; pass < 2; ++pass) {
+            if (nprev > 0) {
+                gemm(CUBLAS_OP_C, CUBLAS_OP_N, nprev, nc, dim, one, basis.ptr, dim, X, dim, zero, lag.ptr, nprev);
+                gemm(CUBLAS_OP_N, CUBLAS_OP_N, dim, nc, nprev, mone, basis.ptr, dim, lag.ptr, nprev, one, X, dim);
+            }
+            cholqr(X, nc);
+        }
+    }
+
+    void cal_elem(int nbase, int nc) {
+        const T one = cmake<T>(1, 0), zero = cmake<T>(0, 0);
+        gemm(CUBLAS_OP_C, CUBLAS_OP_N, nc, nbase + nc, dim, one, basis.ptr + size_t(nbase) * dim, dim, hp.ptr, dim, zero,
+             hcc.ptr + nbase, nbase_x);
+    }
+
+    void eigsolve(int nbase) {
+        const long n = long(nbase_x) * nbase;
+        if constexpr (std::is_same<T, double2>::value) {
+            B200_CUDA(cudaMemcpyAsync(A64.ptr, hcc.ptr, n * sizeof(double2), cudaMemcpyDeviceToDevice, s));
+        } else {
+            k_convert<T, double2><<<grid_of(n), kT, 0, s>>>(n, hcc.ptr, A64.ptr);
+            B200_CUDA(cudaGetLastError());
+        }
+        B200_CUSOLVER(cusolverDnZheevd(cs, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, nbase,
+                                       (cuDoubleComplex*)A64.ptr, nbase_x, w.ptr, (cuDoubleComplex*)work.ptr, lwork,
+                                       info.ptr));
+        const long nv = long(nbase_x) * nband;
+        if constexpr (std::is_same<T, double2>::value) {
+            B200_CUDA(cudaMemcpyAsync(vcc.ptr, A64.ptr, nv * sizeof(double2), cudaMemcpyDeviceToDevice, s));
+        } else {
+            k_convert<double2, T><<<grid_of(nv), kT, 0, s>>>(nv, A64.ptr, vcc.ptr);
+            B200_CUDA(cudaGetLastError());
+        }
+        int hinfo[4];
+        B200_CUDA(cudaMemcpyAsync(eig_h.data(), w.ptr, nband * sizeof(double), cudaMemcpyDeviceToHost, s));
+        B200_CUDA(cudaMemcpyAsync(hinfo, info.ptr, 4 * sizeof(int), cudaMemcpyDeviceToHost, s));
+        B200_CUDA(cudaStreamSynchronize(s));
+        B200_CHECK(hinfo[1] == 0, kNumericalError,
+                   "Cholesky of the new block failed (linearly dependent search directions), info " + std::to_string(hinfo[1]));
+        B200_CHECK(hinfo[0] == 0, kNumericalError, "subspace eigensolver failed, info " + std::to_string(hinfo[0]));
+        for (int m = 0; m < nband; ++m)
+            B200_CHECK(std::isfinite(eig_h[m]), kNumericalError, "non-finite eigenvalue (NaN/Inf in H|psi> or psi)");
+    }
+
+    void cal_grad(const HPsiDevice& f, int nbase, int nc) {
+        const T one = cmake<T>(1, 0), zero = cmake<T>(0, 0);
+        B200_CUDA(cudaMemcpyAsync(unconv_d.ptr, unconv_h.data(), nc * sizeof(int), cudaMemcpyHostToDevice, s));
+        k_gather_cols<T><<<grid_of(long(nbase) * nc), kT, 0, s>>>(nbase, nbase_x, nc, unconv_d.ptr, vcc.ptr, w.ptr, vc.ptr,
+                                                                  vcl.ptr);
+        B200_CUDA(cudaGetLastError());
+        T* X = basis.ptr + size_t(nbase) * dim;
+        gemm(CUBLAS_OP_N, CUBLAS_OP_N, dim, nc, nbase, one, hp.ptr, dim, vc.ptr, nbase, zero, X, dim);
+        gemm(CUBLAS_OP_N, CUBLAS_OP_N, dim, nc, nbase, one, basis.ptr, dim, vcl.ptr, nbase, one, X, dim);
+        k_precond<T, R><<<grid_of(long(dim) * nc), kT, 0, s>>>(dim, nc, X, pc.ptr);
+        B200_CUDA(cudaGetLastError());
+        orth_block(X, nc, nbase);
+        f(basis.ptr, hp.ptr + size_t(nbase) * dim, nbase_x, dim, nbase, nbase + nc - 1, s);
+        hpsi_bands += nc;
+    }
+
+    void refresh(int nbase, const double* eig_in, T* psi, int ldpsi) {
+        const T one = cmake<T>(1, 0), zero = cmake<T>(0, 0);
+        gemm(CUBLAS_OP_N, CUBLAS_OP_N, dim, nband, nbase, one, hp.ptr, dim, vcc.ptr, nbase_x, zero, newv.ptr, dim);
+        B200_CUDA(cudaMemcpyAsync(hp.ptr, newv.ptr, size_t(nband) * dim * sizeof(T), cudaMemcpyDeviceToDevice, s));
+        B200_CUDA(cudaMemcpy2DAsync(basis.ptr, dim * sizeof(T), psi, size_t(ldpsi) * sizeof(T), dim * sizeof(T), nband,
+                                    cudaMemcpyDeviceToDevice, s));
+        B200_CUDA(cudaMemsetAsync(hcc.ptr, 0, hcc.n * sizeof(T), s));
+        if (!ref_refresh) B200_CUDA(cudaMemsetAsync(vcc.ptr, 0, vcc.n * sizeof(T), s));
+        B200_CUDA(cudaMemcpyAsync(ein.ptr, eig_in, nband * sizeof(double), cudaMemcpyHostToDevice, s));
+        k_refresh_diag<T><<<grid_of(nband), kT, 0, s>>>(nband, nbase_x, ein.ptr, hcc.ptr, vcc.ptr);
+        B200_CUDA(cudaGetLastError());
+    }
+
+    int diag_once(const HPsiDevice& f, int ldpsi, T* psi, double* eig_in, double thr, int maxiter, int& notconv) {
+        const T one = cmake<T>(1, 0), zero = cmake<T>(0, 0);
+        B200_CUDA(cudaMemsetAsync(info.ptr, 0, 4 * sizeof(int), s));
+        B200_CUDA(cudaMemcpy2DAsync(basis.ptr, dim * sizeof(T), psi, size_t(ldpsi) * sizeof(T), dim * sizeof(T), nband,
+                                    cudaMemcpyDeviceToDevice, s));
+        orth_block(basis.ptr, nband, 0);
+        f(basis.ptr, hp.ptr, nbase_x, dim, 0, nband - 1, s);
+        hpsi_bands += nband;
+        cal_elem(0, nband);
+        int nbase = nband;
+        eigsolve(nbase);
+        for (int m = 0; m < nband; ++m) eig_in[m] = eig_h[m];
+        notconv = nband;
+        for (int m = 0; m < nband; ++m) unconv_h[m] = m;
+        int iter = 0;
+        while (true) {
+            ++iter;
+            cal_grad(f, nbase, notconv);
+            cal_elem(nbase, notconv);
+            nbase += notconv;
+            eigsolve(nbase);
+            notconv = 0;
+            for (int m = 0; m < nband; ++m) {
+                if (!(std::fabs(eig_h[m] - eig_in[m]) < thr)) unconv_h[notconv++] = m;
+                eig_in[m] = eig_h[m];
+            }
+            if (notconv == 0 || nbase + notconv > nbase_x || iter == maxiter) {
+                B200_CUDA(cudaMemsetAsync(psi, 0, size_t(nband) * ldpsi * sizeof(T), s));
+                gemm(CUBLAS_OP_N, CUBLAS_OP_N, dim, nband, nbase, one, basis.ptr, dim, vcc.ptr, nbase_x, zero, psi, ldpsi);
+                if (notconv == 0 || iter == maxiter) break;
+                refresh(nbase, eig_in, psi, ldpsi);
+                nbase = nband;
+            }
+        }
+        B200_CUDA(cudaStreamSynchronize(s));
+        return iter;
+    }
+
+    int diag(const HPsiDevice& f, int ldpsi, T* psi, double* eig, double thr, int maxiter, int ntry_max, int notconv_max,
+             int& notconv) {
+        int ntry = 0, total = 0;
+        notconv = 0;
+        do {
+            total += diag_once(f, ldpsi, psi, eig, thr, maxiter, notconv);
+            ++ntry;
+        } while (!(ntry > ntry_max || notconv <= notconv_max));
+        return total;
+    }
+};
+
+class David : public DavidBase {
+  public:
+    David(int nband, int dim, int ndim, int precision, const double* precond_d)
+        : nband_(nband), dim_(dim), ndim_(ndim), precision_(precision) {
+        B200_CHECK(precision == 0 || precision == 1, kInvalidArgument, "bad precision");
+        pc_.resize(dim);
+        B200_CUDA(cudaMemcpy(pc_.ptr, precond_d, dim * sizeof(double), cudaMemcpyDeviceToDevice));
+        e64_ = std::make_unique<Engine<double2>>(nband, dim, ndim, pc_.ptr);
+    }
+    int diag(const HPsiDevice& f64, int ldpsi, void* psi, double* eig, double thr, int maxiter, int ntry_max,
+             int notconv_max) override {
+        B200_CHECK(precision_ == 0, kInvalidArgument, "a mixed-precision solve needs a Hamiltonian handle");
+        stats_ = DavidStats{};
+        e64_->hpsi_bands = 0;
+        int nc = 0;
+        const int it = e64_->diag(f64, ldpsi, (double2*)psi, eig, thr, maxiter, ntry_max, notconv_max, nc);
+        stats_.iters_fp64 = it;
+        stats_.hpsi_bands = e64_->hpsi_bands;
+        notconv_ = nc;
+        return it;
+    }
+    int diag_hamilt(const HPsiDevice& f64, const HPsiDevice& f32, int precision, int ldpsi, void* psi, double* eig,
+                    double thr, int maxiter, int ntry_max, int notconv_max) override {
+        stats_ = DavidStats{};
+        int total = 0, nc = 0;
+        if (precision == 1) {
+            if (!e32_) e32_ = std::make_unique<Engine<float2>>(nband_, dim_, ndim_, pc_.ptr);
+            e32_->ref_refresh = e64_->ref_refresh;
+            e32_->hpsi_bands = 0;
+            psi32_.resize(size_t(nband_) * ldpsi);
+            const long n = long(nband_) * ldpsi;
+            k_convert<double2, float2><<<grid_of(n), kT>>>(n, (const double2*)psi, psi32_.ptr);
+            B200_CUDA(cudaGetLastError());
+            const double t32 = thr > mixed_thr_ ? thr : mixed_thr_;
+            const int it32 = e32_->diag(f32, ldpsi, psi32_.ptr, eig, t32, maxiter, 0, nband_, nc);
+            k_convert<float2, double2><<<grid_of(n), kT>>>(n, psi32_.ptr, (double2*)psi);
+            B200_CUDA(cudaGetLastError());
+            stats_.iters_low = it32;
+            stats_.hpsi_bands += e32_->hpsi_bands;
+            total += it32;
+        }
+        e64_->hpsi_bands = 0;
+        const int it64 = e64_->diag(f64, ldpsi, (double2*)psi, eig, thr, maxiter, ntry_max, notconv_max, nc);
+        stats_.iters_fp64 = it64;
+        stats_.hpsi_bands += e64_->hpsi_bands;
+        notconv_ = nc;
+        return total + it64;
+    }
+    const DavidStats& stats() const override { return stats_; }
+    void set_mixed_thr(double thr) override { mixed_thr_ = thr; }
+    void set_reference_refresh(bool on) override {
+        e64_->ref_refresh = on;
+        if (e32_) e32_->ref_refresh = on;
+    }
+
+  private:
+    int nband_, dim_, ndim_, precision_;
+    int notconv_ = 0;
+    double mixed_thr_ = 1e-5;
+    DeviceArray<double> pc_;
+    DeviceArray<float2> psi32_;
+    std::unique_ptr<Engine<double2>> e64_;
+    std::unique_ptr<Engine<float2>> e32_;
+    DavidStats stats_;
+};
+
+}  // namespace
+
+std::unique_ptr<DavidBase> make_david(int nband, int dim, int david_ndim, int precision, const double* precond_d) {
+    return std::make_unique<David>(nband, dim, david_ndim, precision, precond_d);
+}
+
+}  // namespace b200

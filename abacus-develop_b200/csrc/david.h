@@ -1,0 +1,35 @@
+// Block Davidson on the device: hsolver::DiagoDavid<T, DEVICE_GPU> (diago_david.h:19-84).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <functional>
+#include <memory>
+
+namespace b200 {
+
+// H applied to vectors id_start..id_end of the block starting at x (vectors of length dim, stride dim);
+// hx points at the output of vector id_start (the reference's HPsiFunc contract, diago_david.h:40-57).
+using HPsiDevice = std::function<void(const void* x, void* hx, int nvec, int dim, int id_start, int id_end, cudaStream_t s)>;
+
+struct DavidStats {
+    int iters_low = 0;     // Davidson iterations in the low-precision stage (mixed only)
+    int iters_fp64 = 0;    // Davidson iterations in FP64
+    int hpsi_bands = 0;    // band applications of H (all stages)
+};
+
+struct DavidBase {
+    virtual ~DavidBase() = default;
+    // FP64 solve with a user H|psi> (psi: complex128, nband vectors at psi + m*ldpsi)
+    virtual int diag(const HPsiDevice& f64, int ldpsi, void* psi, double* eig, double thr, int maxiter, int ntry_max,
+                     int notconv_max) = 0;
+    // Solve with built-in H|psi> callbacks for both precisions; precision 0 = FP64, 1 = mixed + FP64 refinement
+    virtual int diag_hamilt(const HPsiDevice& f64, const HPsiDevice& f32, int precision, int ldpsi, void* psi,
+                            double* eig, double thr, int maxiter, int ntry_max, int notconv_max) = 0;
+    virtual const DavidStats& stats() const = 0;
+    virtual void set_mixed_thr(double thr) = 0;
+    virtual void set_reference_refresh(bool on) = 0;
+};
+
+std::unique_ptr<DavidBase> make_david(int nband, int dim, int david_ndim, int precision, const double* precond_d);
+
+}  // namespace b200

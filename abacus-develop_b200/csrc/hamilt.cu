@@ -1,0 +1,165 @@
+// Device Hamiltonian: the Ekinetic -> Veff -> Nonlocal chain of HamiltPW
+// (hamilt_pw.cpp:21-114) as one fused local pass plus the projector GEMMs.
+#include "functors.h"
+#include "hamilt.h"
+
+namespace b200 {
+
+__global__ void k_d2f(long n, const double* __restrict__ a, float* __restrict__ b) {
+    for (long i = blockIdx.x * long(blockDim.x) + threadIdx.x; i < n; i += long(gridDim.x) * blockDim.x) b[i] = float(a[i]);
+}
+__global__ void k_z2c(long n, const double2* __restrict__ a, float2* __restrict__ b) {
+    for (long i = blockIdx.x * long(blockDim.x) + threadIdx.x; i < n; i += long(gridDim.x) * blockDim.x)
+        b[i] = make_float2(float(a[i].x), float(a[i].y));
+}
+
+Hamilt::Hamilt(PWGrid* g, int prec) : grid(g), precision(prec) {
+    B200_CUBLAS(cublasCreate(&cublas));
+    nl.resize(g->kmaps.size());
+}
+
+Hamilt::~Hamilt() {
+    if (cublas) cublasDestroy(cublas);
+}
+
+void Hamilt::set_veff(const double* veff_d) {
+    const size_t N = size_t(grid->nxyz());
+    veff_zyx.resize(N);
+    launch_transpose_veff<double>(*grid, veff_d, veff_zyx.ptr, 0);
+    veff_zyxf.resize(N);
+    launch_transpose_veff<float>(*grid, veff_d, veff_zyxf.ptr, 0);
+    B200_CUDA(cudaStreamSynchronize(0));
+    has_veff = true;
+}
+
+void Hamilt::set_vkb(int ik, int nkb, int npwx, const double2* vkb_d) {
+    B200_CHECK(ik >= 0 && ik < int(nl.size()), kInvalidArgument, "k-point index out of range");
+    NonlocalK& k = nl[ik];
+    k.nkb = nkb;
+    k.npwx = npwx;
+    if (nkb <= 0) return;
+    B200_CHECK(npwx >= grid->kmaps[ik].npw, kInvalidArgument, "npwx smaller than npwk");
+    const long n = long(nkb) * npwx;
+    k.vkb.resize(n);
+    B200_CUDA(cudaMemcpyAsync(k.vkb.ptr, vkb_d, n * sizeof(double2), cudaMemcpyDeviceToDevice, 0));
+    k.vkbf.resize(n);
+    k_z2c<<<592, 256>>>(n, vkb_d, k.vkbf.ptr);
+    B200_CUDA(cudaGetLastError());
+    B200_CUDA(cudaStreamSynchronize(0));
+}
+
+void Hamilt::set_deeq(int ntype_, const int* na_, const int* nh_, int nspin_, int dx_, int dy_, int dz_,
+                      const double* deeq_d) {
+    B200_CHECK(ntype_ >= 0 && nspin_ >= 1, kInvalidArgument, "bad deeq shape");
+    ntype = ntype_;
+    na.assign(na_, na_ + ntype);
+    nh.assign(nh_, nh_ + ntype);
+    nspin = nspin_;
+    dx = dx_;
+    dy = dy_;
+    dz = dz_;
+    const long n = long(nspin) * dx * dy * dz;
+    deeq.resize(n);
+    B200_CUDA(cudaMemcpyAsync(deeq.ptr, deeq_d, n * sizeof(double), cudaMemcpyDeviceToDevice, 0));
+    deeqf.resize(n);
+    k_d2f<<<592, 256>>>(n, deeq_d, deeqf.ptr);
+    B200_CUDA(cudaGetLastError());
+    B200_CUDA(cudaStreamSynchronize(0));
+}
+
+int Hamilt::band_chunk(size_t elem) const {
+    // keep one chunk's stick buffer (nst*nz per band) inside ~48 MB so the three passes hit L2
+    const size_t per_band = size_t(grid->nst) * grid->nz * elem;
+    size_t c = (size_t(48) << 20) / (per_band ? per_band : 1);
+    if (c < 1) c = 1;
+    if (c > 4096) c = 4096;
+    return int(c);
+}
+
+namespace {
+template <typename T> struct Blas;
+template <> struct Blas<double2> {
+    static cublasStatus_t gemm(cublasHandle_t h, cublasOperation_t ta, cublasOperation_t tb, int m, int n, int k,
+                               const double2* alpha, const double2* A, int lda, const double2* B, int ldb,
+                               const double2* beta, double2* C, int ldc) {
+        return cublasZgemm(h, ta, tb, m, n, k, reinterpret_cast<const cuDoubleComplex*>(alpha),
+                           reinterpret_cast<const cuDoubleComplex*>(A), lda, reinterpret_cast<const cuDoubleComplex*>(B),
+                           ldb, reinterpret_cast<const cuDoubleComplex*>(beta), reinterpret_cast<cuDoubleComplex*>(C), ldc);
+    }
+};
+template <> struct Blas<float2> {
+    static cublasStatus_t gemm(cublasHandle_t h, cublasOperation_t ta, cublasOperation_t tb, int m, int n, int k,
+                               const float2* alpha, const float2* A, int lda, const float2* B, int ldb,
+                               const float2* beta, float2* C, int ldc) {
+        return cublasCgemm(h, ta, tb, m, n, k, reinterpret_cast<const cuComplex*>(alpha),
+                           reinterpret_cast<const cuComplex*>(A), lda, reinterpret_cast<const cuComplex*>(B), ldb,
+                           reinterpret_cast<const cuComplex*>(beta), reinterpret_cast<cuComplex*>(C), ldc);
+    }
+};
+}  // namespace
+
+template <typename T> void Hamilt::hpsi(int ik, int spin, int nb, int ld, const T* psi, T* hpsi, int mode, cudaStream_t s) {
+    using R = typename RealOf<T>::type;
+    constexpr bool f64 = std::is_same<T, double2>::value;
+    B200_CHECK(ik >= 0 && ik < int(grid->kmaps.size()), kInvalidArgument, "k-point index out of range");
+    const int npw = grid->kmaps[ik].npw;
+    B200_CHECK(nb >= 0 && ld >= npw, kInvalidArgument, "ld smaller than npwk or negative band count");
+    if (nb == 0) return;
+    if (mode != 2) {
+        B200_CHECK(has_veff, kInvalidArgument, "V_eff not set");
+        const R* veff = f64 ? (const R*)veff_zyx.ptr : (const R*)veff_zyxf.ptr;
+        const int chunk = band_chunk(sizeof(T));
+        const int nbc0 = nb < chunk ? nb : chunk;
+        const size_t sbn = size_t(nbc0) * grid->nst * grid->nz;
+        T* sb;
+        if constexpr (f64) {
+            sb64.resize(sbn);
+            sb = sb64.ptr;
+        } else {
+            sb32.resize(sbn);
+            sb = sb32.ptr;
+        }
+        for (int b0 = 0; b0 < nb; b0 += chunk) {
+            const int nbc = nb - b0 < chunk ? nb - b0 : chunk;
+            launch_hpsi_local<T, R>(*grid, ik, veff, nbc, ld, psi + size_t(b0) * ld, hpsi + size_t(b0) * ld, sb,
+                                    grid->basis.tpiba2, 0, s);
+        }
+    }
+    if (mode == 1) return;
+    const NonlocalK& k = nl[ik];
+    if (k.nkb <= 0) return;
+    const int nkb = k.nkb;
+    T* becp;
+    T* ps;
+    if constexpr (f64) {
+        becp64.resize(size_t(nkb) * nb);
+        ps64.resize(size_t(nkb) * nb);
+        becp = becp64.ptr;
+        ps = ps64.ptr;
+    } else {
+        becp32.resize(size_t(nkb) * nb);
+        ps32.resize(size_t(nkb) * nb);
+        becp = becp32.ptr;
+        ps = ps32.ptr;
+    }
+    const T* vkb = f64 ? (const T*)k.vkb.ptr : (const T*)k.vkbf.ptr;
+    const T one = cmake<T>(1, 0), zero = cmake<T>(0, 0);
+    B200_CUBLAS(cublasSetStream(cublas, s));
+    // becp = vkb^H psi (Nonlocal::act, nonlocal_pw.cpp:261-276)
+    B200_CUBLAS(Blas<T>::gemm(cublas, CUBLAS_OP_C, CUBLAS_OP_N, nkb, nb, npw, &one, vkb, k.npwx, psi, ld, &zero, becp, nkb));
+    // ps = D becp per atom type (add_nonlocal_pp, nonlocal_pw.cpp:64-110)
+    B200_CUDA(cudaMemsetAsync(ps, 0, size_t(nkb) * nb * sizeof(T), s));
+    int sum = 0, iat = 0;
+    const R* d = f64 ? (const R*)deeq.ptr : (const R*)deeqf.ptr;
+    B200_CHECK(d != nullptr, kInvalidArgument, "deeq not set");
+    B200_CHECK(spin >= 0 && spin < nspin, kInvalidArgument, "spin out of range");
+    for (int it = 0; it < ntype; ++it) nonlocal_pw<T, R>(na[it], nb, nh[it], sum, iat, spin, nkb, dx, dy, dz, d, ps, becp, s);
+    B200_CHECK(sum == nkb, kInvalidArgument, "sum of na*nh over types differs from nkb");
+    // hpsi += vkb ps^T (nonlocal_pw.cpp:190-205)
+    B200_CUBLAS(Blas<T>::gemm(cublas, CUBLAS_OP_N, CUBLAS_OP_T, npw, nb, nkb, &one, vkb, k.npwx, ps, nb, &one, hpsi, ld));
+}
+
+template void Hamilt::hpsi<double2>(int, int, int, int, const double2*, double2*, int, cudaStream_t);
+template void Hamilt::hpsi<float2>(int, int, int, int, const float2*, float2*, int, cudaStream_t);
+
+}  // namespace b200

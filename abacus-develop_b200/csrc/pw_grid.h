@@ -1,0 +1,104 @@
+// Device-resident plane-wave grid: FFT plans, stick maps and per-k sphere maps.
+//
+// Layouts in HBM (one pool, one GPU):
+//  * psi / hpsi: band b at psi + b*ld, G in the order of the basis (ABACUS's
+//    igl2isz_k order: sticks by ixy = x*ny + y, z ascending from the bottom).
+//  * stick buffer (fused H|psi>): per band nz planes of nst sticks,
+//    element (band, z, s) at band*nz*nst + z*nst + s.  A z-plane is contiguous,
+//    so the plane pass reads and writes whole planes with coalesced accesses.
+//  * r box (drop-in transforms): ABACUS's order r = (ix*ny + iy)*nz + iz.
+//  * V_eff for the fused path: transposed once to (z, y, x) so a plane row is
+//    contiguous.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <memory>
+#include <vector>
+
+#include "common.h"
+#include "fft_core.cuh"
+#include "pw_basis.h"
+
+namespace b200 {
+
+// One FFT axis: plan plus twiddles in both precisions.
+struct FftAxis {
+    FftPlan1D plan{};
+    std::vector<double2> h_tw64;
+    DeviceArray<double2> tw64;
+    DeviceArray<float2> tw32;
+    void build(int n);  // host plan + twiddles
+    void upload();
+};
+
+// Sphere -> stick maps for one k-point.
+struct KMap {
+    int npw = 0;
+    std::vector<int> h_gofs, h_gpk, h_glist;
+    std::vector<double> h_precond;
+    DeviceArray<int> gofs;   // nst+1 offsets of each stick's entries in the sorted list
+    DeviceArray<int> gpk;    // packed (stick << 10) | z per sorted entry
+    DeviceArray<int> glist;  // G index (position in psi) per sorted entry
+    DeviceArray<int> ig2ixyz;
+    DeviceArray<double> gk2;
+    DeviceArray<float> gk2f;
+    DeviceArray<double> precond;  // Davidson preconditioner 1 + g2 + sqrt(1 + (g2-1)^2)
+};
+
+// Index maps handed to kernels by value.
+struct StickMapView {
+    int nst, nz;
+    const int* gofs;
+    const int* gpk;
+    const int* glist;
+};
+struct PlaneMapView {
+    int nst, nxc;
+    const int* xc;    // per stick: compact x-column index
+    const int* sy;    // per stick: y
+    const int* xpos;  // per compact column: x
+};
+
+struct PWGrid {
+    PWBasisK basis;
+    int nx = 0, ny = 0, nz = 0, nst = 0, nxc = 0;
+    FftAxis ax, ay, az;
+    DeviceArray<int> st_xc, st_y, xpos, st_ixy;
+    std::vector<int> h_xpos, h_xc, h_sy, h_sixy;
+    std::vector<KMap> kmaps;
+    bool on_device = false;
+
+    void build(const PWBasisK& b);  // host-side plans and maps only (no GPU needed)
+    void ensure_device();           // uploads plans and maps on first device use
+    StickMapView stick_view(int ik) const {
+        const KMap& k = kmaps[ik];
+        return StickMapView{nst, nz, k.gofs.ptr, k.gpk.ptr, k.glist.ptr};
+    }
+    PlaneMapView plane_view() const { return PlaneMapView{nst, nxc, st_xc.ptr, st_y.ptr, xpos.ptr}; }
+    long nxyz() const { return long(nx) * ny * nz; }
+};
+
+// Shared-memory footprint helpers (bytes) for the launch shapes used by the kernels.
+constexpr int kStickTile = 16;   // sticks per CTA in the z passes
+constexpr int kPlaneCols = 8;    // y-FFT column chunk in the plane pass
+constexpr int kPlaneRows = 8;    // x-FFT row chunk in the plane pass
+constexpr int kBoxTile = 16;     // z-columns per CTA in the box x/y passes
+inline int odd_ld(int n) { return n | 1; }
+size_t zpass_smem(const PWGrid& g, size_t elem);
+size_t plane_smem(const PWGrid& g, size_t elem);
+
+// ---- launchers (fft_kernels.cu); all asynchronous on `s` ----
+// Fused local part of H|psi> for nb bands (one chunk): hpsi = Ekin psi + V_loc psi (accumulate==0 zeroes padding).
+template <typename T, typename R>
+void launch_hpsi_local(const PWGrid& g, int ik, const R* veff_zyx, int nb, int ld, const T* psi, T* hpsi, T* stickbuf,
+                       double tpiba2, int accumulate, cudaStream_t s);
+// Drop-in transforms (PW_Basis_K::recip_to_real / real_to_recip on the GPU), one band.
+template <typename T>
+void launch_recip_to_real(const PWGrid& g, int ik, const T* in, T* out, T* aux, int add, double factor, cudaStream_t s);
+template <typename T>
+void launch_real_to_recip(const PWGrid& g, int ik, const T* in, T* out, T* aux, int add, double factor, cudaStream_t s);
+// V_eff (ABACUS r order) -> (z, y, x) transposed copy, in precision R.
+template <typename R>
+void launch_transpose_veff(const PWGrid& g, const double* veff, R* out, cudaStream_t s);
+
+}  // namespace b200

@@ -1,0 +1,317 @@
+"""Python face of the plane-wave H|psi> / Davidson C-ABI.
+
+Names, argument order and meaning follow the reference's op functors,
+PW_Basis_K and DiagoDavid (abacus-develop v3.8.0) so that tests read like the
+reference's own.  Device buffers are torch CUDA tensors (torch is used for
+device memory and streams only; every computation runs in libabacus_b200.so).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib
+from ._lib import call, ptr, stream_ptr
+
+PREC_FP64 = 0
+PREC_MIXED = 1
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def _f64p(a: np.ndarray):
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    return a, a.ctypes.data_as(_lib.pf64)
+
+
+# ------------------------------------------------------------------ op functors
+def ekinetic_pw_op(nband, npw, max_npw, tpiba2, gk2_ik, tmhpsi, tmpsi_in, stream=None):
+    """ekinetic_pw_op<FP, DEVICE_GPU> (ekinetic_op.h:38-48); FP from the tensors' dtype."""
+    torch = _torch()
+    f = "b200_ekinetic_pw_op_f64" if tmhpsi.dtype == torch.complex128 else "b200_ekinetic_pw_op_f32"
+    call(f, nband, npw, max_npw, tpiba2, ptr(gk2_ik), ptr(tmhpsi), ptr(tmpsi_in), stream_ptr(stream))
+
+
+def veff_pw_op(size, out, vin, stream=None):
+    """veff_pw_op<FP, DEVICE_GPU>(dev, size, out, in) (veff_op.h:57-66)."""
+    torch = _torch()
+    f = "b200_veff_pw_op_f64" if out.dtype == torch.complex128 else "b200_veff_pw_op_f32"
+    call(f, size, ptr(out), ptr(vin), stream_ptr(stream))
+
+
+def veff_pw_op_npol2(size, out, out1, vin4, stream=None):
+    """veff_pw_op<FP, DEVICE_GPU>(dev, size, out, out1, in[4]) (veff_op.h:57-66)."""
+    torch = _torch()
+    f = "b200_veff_pw_op_npol2_f64" if out.dtype == torch.complex128 else "b200_veff_pw_op_npol2_f32"
+    call(f, size, ptr(out), ptr(out1), *(ptr(v) for v in vin4), stream_ptr(stream))
+
+
+def nonlocal_pw_op(l1, l2, l3, sum_, iat, spin, nkb, deeq_x, deeq_y, deeq_z, deeq, ps, becp, stream=None):
+    """nonlocal_pw_op<FP, DEVICE_GPU> (nonlocal_op.h:82-113). Returns the updated (sum, iat)."""
+    torch = _torch()
+    s, i = C.c_int(sum_), C.c_int(iat)
+    f = "b200_nonlocal_pw_op_f64" if ps.dtype == torch.complex128 else "b200_nonlocal_pw_op_f32"
+    call(f, l1, l2, l3, C.byref(s), C.byref(i), spin, nkb, deeq_x, deeq_y, deeq_z, ptr(deeq), ptr(ps), ptr(becp),
+         stream_ptr(stream))
+    return s.value, i.value
+
+
+def nonlocal_pw_op_nc(l1, l2, l3, sum_, iat, nkb, deeq_x, deeq_y, deeq_z, deeq_nc, ps, becp, stream=None):
+    torch = _torch()
+    s, i = C.c_int(sum_), C.c_int(iat)
+    f = "b200_nonlocal_pw_op_nc_f64" if ps.dtype == torch.complex128 else "b200_nonlocal_pw_op_nc_f32"
+    call(f, l1, l2, l3, C.byref(s), C.byref(i), nkb, deeq_x, deeq_y, deeq_z, ptr(deeq_nc), ptr(ps), ptr(becp),
+         stream_ptr(stream))
+    return s.value, i.value
+
+
+def set_3d_fft_box_op(npwk, box_index, inp, out, stream=None):
+    torch = _torch()
+    f = "b200_set_3d_fft_box_op_f64" if out.dtype == torch.complex128 else "b200_set_3d_fft_box_op_f32"
+    call(f, npwk, ptr(box_index), ptr(inp), ptr(out), stream_ptr(stream))
+
+
+def set_recip_to_real_output_op(nrxx, add, factor, inp, out, stream=None):
+    torch = _torch()
+    f = "b200_set_recip_to_real_output_op_f64" if out.dtype == torch.complex128 else "b200_set_recip_to_real_output_op_f32"
+    call(f, nrxx, int(add), factor, ptr(inp), ptr(out), stream_ptr(stream))
+
+
+def set_real_to_recip_output_op(npw_k, nxyz, add, factor, box_index, inp, out, stream=None):
+    torch = _torch()
+    f = "b200_set_real_to_recip_output_op_f64" if out.dtype == torch.complex128 else "b200_set_real_to_recip_output_op_f32"
+    call(f, npw_k, nxyz, int(add), factor, ptr(box_index), ptr(inp), ptr(out), stream_ptr(stream))
+
+
+# ------------------------------------------------------------------ basis
+class PWBasisK:
+    """ModulePW::PW_Basis_K for one pool: grid, G sphere, index maps, device transforms."""
+
+    def __init__(self, lat0, latvec, ecutwfc, kvec_d, ecutrho=None, grid=None):
+        lib = _lib.load()
+        lv, lvp = _f64p(np.asarray(latvec, dtype=np.float64).reshape(9))
+        kd, kdp = _f64p(np.atleast_2d(np.asarray(kvec_d, dtype=np.float64)).reshape(-1))
+        nks = kd.size // 3
+        gx, gy, gz = grid if grid is not None else (0, 0, 0)
+        h = _lib.vp()
+        call("b200_pw_basis_create", float(lat0), lvp, float(ecutwfc), float(ecutrho or 0.0), gx, gy, gz, nks, kdp,
+             C.byref(h))
+        self._h = h
+        self._lib = lib
+        dims = (C.c_int * 8)()
+        call("b200_pw_basis_dims", h, dims)
+        self.nx, self.ny, self.nz, self.nst, self.npw, self.npwk_max, self.nks, self.nxc = list(dims)
+        sc = (C.c_double * 3)()
+        call("b200_pw_basis_scalars", h, sc)
+        self.tpiba2, self.omega, self.gk_ecut = list(sc)
+        self.lat0 = float(lat0)
+        self.npwk = np.zeros(self.nks, dtype=np.int64)
+        self._kcache = {}
+        for ik in range(self.nks):
+            n = C.c_int()
+            call("b200_pw_basis_kpoint", h, ik, C.byref(n), None, None, None)
+            self.npwk[ik] = n.value
+
+    @property
+    def handle(self):
+        return self._h
+
+    @property
+    def nxyz(self):
+        return self.nx * self.ny * self.nz
+
+    def _k(self, ik):
+        if ik not in self._kcache:
+            n = int(self.npwk[ik])
+            idx = np.zeros(n, dtype=np.int32)
+            gk2 = np.zeros(n)
+            gcar = np.zeros((n, 3))
+            call("b200_pw_basis_kpoint", self._h, ik, None, idx.ctypes.data_as(_lib.vp), gk2.ctypes.data_as(_lib.vp),
+                 gcar.ctypes.data_as(_lib.vp))
+            kc = (C.c_double * 3)()
+            call("b200_pw_basis_kvec_c", self._h, ik, kc)
+            self._kcache[ik] = (idx, gk2, gcar, np.array(list(kc)))
+        return self._kcache[ik]
+
+    def ig2ixyz(self, ik):
+        return self._k(ik)[0].astype(np.int64)
+
+    def gk2_k(self, ik):
+        return self._k(ik)[1]
+
+    def gplusk_cart(self, ik):
+        """k+G cartesian in bohr^-1."""
+        _, _, gcar, kc = self._k(ik)
+        return (gcar + kc[None, :]) * np.sqrt(self.tpiba2)
+
+    def device_maps(self, ik):
+        g, gf, ix = _lib.vp(), _lib.vp(), _lib.vp()
+        call("b200_pw_basis_device_maps", self._h, ik, C.byref(g), C.byref(gf), C.byref(ix))
+        return g.value, gf.value, ix.value
+
+    def recip_to_real(self, inp, out, ik, add=False, factor=1.0, stream=None):
+        """PW_Basis_K::recip_to_real<FP, DEVICE_GPU> (pw_basis_k.h:140-153)."""
+        torch = _torch()
+        f = "b200_recip_to_real_f64" if out.dtype == torch.complex128 else "b200_recip_to_real_f32"
+        call(f, self._h, ptr(inp), ptr(out), ik, int(add), factor, stream_ptr(stream))
+
+    def real_to_recip(self, inp, out, ik, add=False, factor=1.0, stream=None):
+        """PW_Basis_K::real_to_recip<FP, DEVICE_GPU> (pw_basis_k.h:140-153)."""
+        torch = _torch()
+        f = "b200_real_to_recip_f64" if out.dtype == torch.complex128 else "b200_real_to_recip_f32"
+        call(f, self._h, ptr(inp), ptr(out), ik, int(add), factor, stream_ptr(stream))
+
+    def __del__(self):
+        try:
+            if getattr(self, "_h", None):
+                self._lib.b200_pw_basis_destroy(self._h)
+                self._h = None
+        except Exception:
+            pass
+
+
+# ------------------------------------------------------------------ Hamiltonian
+class HamiltPW:
+    """Ekinetic -> Veff -> Nonlocal on the device (HamiltPW, hamilt_pw.cpp:21-114)."""
+
+    def __init__(self, basis: PWBasisK, precision=PREC_FP64):
+        self.basis = basis
+        self.precision = precision
+        h = _lib.vp()
+        call("b200_hamilt_create", basis.handle, precision, C.byref(h))
+        self._h = h
+        self._lib = _lib.load()
+        self._keep = []
+
+    @property
+    def handle(self):
+        return self._h
+
+    def set_veff(self, veff_d):
+        call("b200_hamilt_set_veff", self._h, ptr(veff_d))
+
+    def set_vkb(self, ik, vkb_d):
+        nkb, npwx = (0, 0) if vkb_d is None else (int(vkb_d.shape[0]), int(vkb_d.shape[1]))
+        call("b200_hamilt_set_vkb", self._h, ik, nkb, npwx, ptr(vkb_d))
+
+    def set_deeq(self, na, nh, deeq_d):
+        na_a = (C.c_int * len(na))(*na)
+        nh_a = (C.c_int * len(nh))(*nh)
+        ns, dx, dy, dz = (int(v) for v in deeq_d.shape)
+        call("b200_hamilt_set_deeq", self._h, len(na), na_a, nh_a, ns, dx, dy, dz, ptr(deeq_d))
+
+    def hpsi(self, ik, psi, hpsi, nbands, ld, spin=0, stream=None):
+        """Operator::hPsi: hpsi = H psi for bands [0, nbands)."""
+        call("b200_hamilt_hpsi", self._h, ik, spin, nbands, ld, ptr(psi), ptr(hpsi), stream_ptr(stream))
+
+    def hpsi_part(self, ik, psi, hpsi, nbands, ld, mode, spin=0, stream=None):
+        call("b200_hamilt_hpsi_part", self._h, ik, spin, nbands, ld, ptr(psi), ptr(hpsi), mode, stream_ptr(stream))
+
+    def __del__(self):
+        try:
+            if getattr(self, "_h", None):
+                self._lib.b200_hamilt_destroy(self._h)
+                self._h = None
+        except Exception:
+            pass
+
+
+# ------------------------------------------------------------------ Davidson
+class DiagoDavid:
+    """hsolver::DiagoDavid<T, DEVICE_GPU> (diago_david.h:19-84); S = I."""
+
+    def __init__(self, precondition_d, nband, dim, david_ndim=4, precision=PREC_FP64):
+        h = _lib.vp()
+        call("b200_david_create", nband, dim, david_ndim, precision, ptr(precondition_d), C.byref(h))
+        self._h = h
+        self._lib = _lib.load()
+        self.nband = nband
+        self.dim = dim
+
+    def diag(self, hpsi_func, ld_psi, psi, eigenvalue, thr, maxiter, ntry_max=5, notconv_max=0):
+        """hpsi_func(x_ptr, hx_ptr, nvec, dim, id_start, id_end) with raw device pointers (HPsiFunc contract).
+        eigenvalue: numpy float64 array of nband, filled on return. Returns the iteration count."""
+
+        def cb(user, x, hx, nvec, dim, i0, i1):
+            hpsi_func(x, hx, nvec, dim, i0, i1)
+
+        cfn = _lib.HPSI_CB(cb)
+        it = C.c_int()
+        call("b200_david_diag", self._h, cfn, None, ld_psi, ptr(psi), eigenvalue.ctypes.data_as(_lib.pf64), thr, maxiter,
+             ntry_max, notconv_max, C.byref(it))
+        return it.value
+
+    def diag_hamilt(self, hamilt: HamiltPW, ik, ld_psi, psi, eigenvalue, thr, maxiter, ntry_max=5, notconv_max=0,
+                    spin=0):
+        it = C.c_int()
+        call("b200_david_diag_hamilt", self._h, hamilt.handle, ik, spin, ld_psi, ptr(psi),
+             eigenvalue.ctypes.data_as(_lib.pf64), thr, maxiter, ntry_max, notconv_max, C.byref(it))
+        return it.value
+
+    def __del__(self):
+        try:
+            if getattr(self, "_h", None):
+                self._lib.b200_david_destroy(self._h)
+                self._h = None
+        except Exception:
+            pass
+
+
+# ------------------------------------------------------------------ workloads
+@dataclass
+class Workload:
+    spec: object
+    cell: object
+    basis: PWBasisK
+    veff_h: np.ndarray          # host V_eff (reference r order)
+    vkb_h: list                 # per k: (nkb, npwx) complex128
+    deeq_h: np.ndarray
+    psi0_h: list                # per k: (nbands, npwx) complex128
+
+    @property
+    def nkb(self):
+        return self.cell.nkb
+
+
+def build_workload(spec, kpts=None) -> Workload:
+    """Synthetic cell + basis + host inputs for a CellSpec (see synth.py)."""
+    from . import synth
+    cell = synth.make_cell(spec)
+    k = spec.kpts if kpts is None else kpts
+    if k is None:
+        k = np.zeros((1, 3))
+    basis = PWBasisK(spec.a, cell.latvec, spec.ecut, k, grid=spec.grid)
+    veff = cell.veff(basis.nx, basis.ny, basis.nz)
+    npwx = basis.npwk_max
+    vkbs, psis = [], []
+    for ik in range(basis.nks):
+        q = basis.gplusk_cart(ik)
+        vkbs.append(cell.vkb(q, npwx, basis.omega))
+        psis.append(cell.psi0(q, spec.nbands, npwx, seed_offset=ik))
+    return Workload(spec, cell, basis, veff, vkbs, cell.deeq(), psis)
+
+
+def device_hamilt(wl: Workload, precision=PREC_FP64) -> HamiltPW:
+    torch = _torch()
+    h = HamiltPW(wl.basis, precision)
+    h._veff_d = torch.from_numpy(wl.veff_h).cuda()
+    h.set_veff(h._veff_d)
+    h._deeq_d = torch.from_numpy(wl.deeq_h).cuda()
+    h.set_deeq([wl.cell.nat], [8], h._deeq_d)
+    for ik, v in enumerate(wl.vkb_h):
+        vd = torch.from_numpy(v).cuda()
+        h.set_vkb(ik, vd)
+    torch.cuda.synchronize()
+    return h
+
+
+def precondition_d(basis: PWBasisK, ik: int):
+    """h_diag = 1 + g2 + sqrt(1 + (g2-1)^2) (hsolver_pw.cpp:567-584) as a device FP64 tensor."""
+    torch = _torch()
+    g2 = basis.gk2_k(ik) * basis.tpiba2
+    return torch.from_numpy(1.0 + g2 + np.sqrt(1.0 + (g2 - 1.0) ** 2)).cuda()

@@ -1,0 +1,180 @@
+/*
+ * abacus_b200.h -- C-ABI of the B200-native plane-wave H|psi> / Davidson path.
+ *
+ * Every entry point takes plain pointers, sizes and a CUDA stream (as void*,
+ * NULL = legacy default stream, which is what ABACUS uses implicitly) and
+ * returns an int status (0 = success, see B200_STATUS_*).  On failure
+ * b200_last_error() returns a message for the calling thread.  No entry point
+ * calls exit(); the reference's cudaErrcheck / WARNING_QUIT become statuses.
+ *
+ * Device pointers (suffix _d in the comments) are CUDA device memory owned by
+ * the caller, exactly as in the reference where buffers come from
+ * resize_memory_op<T, DEVICE_GPU> (module_base/module_device/memory_op.h:16-93).
+ * Complex numbers are interleaved (re, im) pairs, layout-compatible with
+ * std::complex<double> / std::complex<float>.
+ *
+ * Reference = abacus-develop v3.8.0; paths are relative to its source/ tree.
+ */
+#ifndef ABACUS_B200_H
+#define ABACUS_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define B200_STATUS_OK 0
+#define B200_STATUS_INVALID_ARGUMENT 1
+#define B200_STATUS_CUDA_ERROR 2
+#define B200_STATUS_CUBLAS_ERROR 3
+#define B200_STATUS_CUSOLVER_ERROR 4
+#define B200_STATUS_NUMERICAL_ERROR 5
+#define B200_STATUS_CAPACITY_ERROR 6
+#define B200_STATUS_NOT_CONVERGED 7
+
+/* precision of a handle: plain FP64, or mixed (FP32 FFTs / split-precision GEMMs) */
+#define B200_PREC_FP64 0
+#define B200_PREC_MIXED 1
+
+typedef struct b200_pw_basis b200_pw_basis; /* host + device plane-wave basis of one pool */
+typedef struct b200_hamilt b200_hamilt;     /* V_eff, projectors, D and workspaces */
+typedef struct b200_david b200_david;       /* Davidson workspaces */
+
+/* Message of the last failed call on this thread ("" if none). */
+const char* b200_last_error(void);
+/* Library version string. */
+const char* b200_version(void);
+
+/* ------------------------------------------------------------------ op functors
+ * Each replaces the body of a DEVICE_GPU partial specialisation; arguments keep
+ * the reference's meaning and order. */
+
+/* ekinetic_pw_op<FP, DEVICE_GPU>::operator()
+ *   module_hamilt_pw/hamilt_pwdft/kernels/ekinetic_op.h:38-48
+ *   tmhpsi_d[ib*max_npw+ig] += gk2_ik_d[ig]*tpiba2*tmpsi_in_d[ib*max_npw+ig], ig < npw */
+int b200_ekinetic_pw_op_f64(int nband, int npw, int max_npw, double tpiba2, const double* gk2_ik_d, void* tmhpsi_d,
+                            const void* tmpsi_in_d, void* stream);
+int b200_ekinetic_pw_op_f32(int nband, int npw, int max_npw, float tpiba2, const float* gk2_ik_d, void* tmhpsi_d,
+                            const void* tmpsi_in_d, void* stream);
+
+/* veff_pw_op<FP, DEVICE_GPU>::operator()(dev, size, out, in)
+ *   module_hamilt_pw/hamilt_pwdft/kernels/veff_op.h:57-66 -- out_d[ir] *= in_d[ir] */
+int b200_veff_pw_op_f64(int size, void* out_d, const double* in_d, void* stream);
+int b200_veff_pw_op_f32(int size, void* out_d, const float* in_d, void* stream);
+/* npol = 2 form (dev, size, out, out1, const FP** in): in0..in3 are the four spin components */
+int b200_veff_pw_op_npol2_f64(int size, void* out_d, void* out1_d, const double* in0_d, const double* in1_d,
+                              const double* in2_d, const double* in3_d, void* stream);
+int b200_veff_pw_op_npol2_f32(int size, void* out_d, void* out1_d, const float* in0_d, const float* in1_d,
+                              const float* in2_d, const float* in3_d, void* stream);
+
+/* nonlocal_pw_op<FP, DEVICE_GPU>::operator()
+ *   module_hamilt_pw/hamilt_pwdft/kernels/nonlocal_op.h:82-113
+ *   l1 = na, l2 = nbands, l3 = nh; *sum += l1*l3 and *iat += l1 on return, as the reference does. */
+int b200_nonlocal_pw_op_f64(int l1, int l2, int l3, int* sum, int* iat, int spin, int nkb, int deeq_x, int deeq_y,
+                            int deeq_z, const double* deeq_d, void* ps_d, const void* becp_d, void* stream);
+int b200_nonlocal_pw_op_f32(int l1, int l2, int l3, int* sum, int* iat, int spin, int nkb, int deeq_x, int deeq_y,
+                            int deeq_z, const float* deeq_d, void* ps_d, const void* becp_d, void* stream);
+/* non-collinear form with complex deeq_nc (same header, second overload) */
+int b200_nonlocal_pw_op_nc_f64(int l1, int l2, int l3, int* sum, int* iat, int nkb, int deeq_x, int deeq_y,
+                               int deeq_z, const void* deeq_nc_d, void* ps_d, const void* becp_d, void* stream);
+int b200_nonlocal_pw_op_nc_f32(int l1, int l2, int l3, int* sum, int* iat, int nkb, int deeq_x, int deeq_y,
+                               int deeq_z, const void* deeq_nc_d, void* ps_d, const void* becp_d, void* stream);
+
+/* set_3d_fft_box_op / set_recip_to_real_output_op / set_real_to_recip_output_op <FP, DEVICE_GPU>
+ *   module_basis/module_pw/kernels/pw_op.h (CPU bodies pw_op.cpp:6-68) */
+int b200_set_3d_fft_box_op_f64(int npwk, const int* box_index_d, const void* in_d, void* out_d, void* stream);
+int b200_set_3d_fft_box_op_f32(int npwk, const int* box_index_d, const void* in_d, void* out_d, void* stream);
+int b200_set_recip_to_real_output_op_f64(int nrxx, int add, double factor, const void* in_d, void* out_d, void* stream);
+int b200_set_recip_to_real_output_op_f32(int nrxx, int add, float factor, const void* in_d, void* out_d, void* stream);
+int b200_set_real_to_recip_output_op_f64(int npw_k, int nxyz, int add, double factor, const int* box_index_d,
+                                         const void* in_d, void* out_d, void* stream);
+int b200_set_real_to_recip_output_op_f32(int npw_k, int nxyz, int add, float factor, const int* box_index_d,
+                                         const void* in_d, void* out_d, void* stream);
+
+/* ------------------------------------------------------------------ plane-wave basis
+ * Replaces PW_Basis_K set-up for one pool: initgrids (module_basis/module_pw/pw_init.cpp:24-170),
+ * initparameters (pw_basis_k.cpp:53-116), setuptransform + setupIndGk (pw_basis_k.cpp:118-187),
+ * collect_local_pw (:189-265) and get_ig2ixyz_k (:319-344).  Builds the host maps and
+ * uploads the device stick maps.  nx = ny = nz = 0 selects the reference's 2,3,5-smooth
+ * grid rule; ecutrho <= 0 means 4*ecutwfc.  latvec is row-major (rows = a1, a2, a3 in
+ * units of lat0), kvec_d is nks x 3 direct coordinates. */
+int b200_pw_basis_create(double lat0, const double* latvec, double ecutwfc, double ecutrho, int nx, int ny, int nz,
+                         int nks, const double* kvec_d, b200_pw_basis** out);
+int b200_pw_basis_destroy(b200_pw_basis* b);
+/* dims[0..7] = nx, ny, nz, nst, npw (ggecut sphere), npwk_max, nks, nxc (occupied x columns) */
+int b200_pw_basis_dims(const b200_pw_basis* b, int* dims);
+/* scal[0..2] = tpiba2, omega, gk_ecut */
+int b200_pw_basis_scalars(const b200_pw_basis* b, double* scal);
+/* host copies for k-point ik: npwk, ig2ixyz (npwk ints), gk2 (npwk), gcar (npwk x 3, units of tpiba);
+ * any output pointer may be NULL */
+int b200_pw_basis_kpoint(const b200_pw_basis* b, int ik, int* npwk, int* ig2ixyz, double* gk2, double* gcar);
+/* kvec_c (3 doubles, units of tpiba) of k-point ik */
+int b200_pw_basis_kvec_c(const b200_pw_basis* b, int ik, double* kvec_c);
+/* device pointers of gk2 (FP64 and FP32 copies, npwk) and ig2ixyz for k-point ik -- the
+ * arrays ABACUS keeps as d_gk2 / s_gk2 / ig2ixyz_k (pw_basis_k.h). */
+int b200_pw_basis_device_maps(const b200_pw_basis* b, int ik, const double** gk2_d, const float** gk2f_d,
+                              const int** ig2ixyz_d);
+
+/* PW_Basis_K::recip_to_real<FP, DEVICE_GPU>(ctx, in, out, ik, add, factor)
+ *   module_basis/module_pw/pw_basis_k.h:140-153, GPU bodies pw_transform_k.cpp:404-476.
+ *   in_d: npwk coefficients of k-point ik; out_d: nx*ny*nz box in r = (ix*ny+iy)*nz+iz order.
+ *   out = r (add = 0) or out += factor*r (add = 1); r is the un-normalised exp(+iGr) sum. */
+int b200_recip_to_real_f64(b200_pw_basis* b, const void* in_d, void* out_d, int ik, int add, double factor,
+                           void* stream);
+int b200_recip_to_real_f32(b200_pw_basis* b, const void* in_d, void* out_d, int ik, int add, float factor,
+                           void* stream);
+/* PW_Basis_K::real_to_recip<FP, DEVICE_GPU>(ctx, in, out, ik, add, factor)
+ *   GPU bodies pw_transform_k.cpp:336-401: out = box/nxyz (add = 0) or out += factor/nxyz*box. */
+int b200_real_to_recip_f64(b200_pw_basis* b, const void* in_d, void* out_d, int ik, int add, double factor,
+                           void* stream);
+int b200_real_to_recip_f32(b200_pw_basis* b, const void* in_d, void* out_d, int ik, int add, float factor,
+                           void* stream);
+
+/* ------------------------------------------------------------------ Hamiltonian
+ * One handle holds what the operator chain Ekinetic -> Veff -> Nonlocal of
+ * HamiltPW (module_hamilt_pw/hamilt_pwdft/hamilt_pw.cpp:21-114) holds on the
+ * device: V_eff, the projectors vkb per k (Nonlocal::init, nonlocal_pw.cpp:42-58)
+ * and deeq.  npol = 1, one spin channel per call. */
+int b200_hamilt_create(b200_pw_basis* b, int precision, b200_hamilt** out);
+int b200_hamilt_destroy(b200_hamilt* h);
+/* veff_d: nx*ny*nz FP64 in ABACUS's r order (the row this->veff + spin*veff_col of Veff::act) */
+int b200_hamilt_set_veff(b200_hamilt* h, const double* veff_d);
+/* vkb_d: nkb x npwx row-major complex128 (ABACUS's ppcell->vkb for k-point ik, VNL_in_pw.h:106);
+ * pass nkb = 0 for no projectors */
+int b200_hamilt_set_vkb(b200_hamilt* h, int ik, int nkb, int npwx, const void* vkb_d);
+/* deeq_d: (nspin, deeq_x = nat, deeq_y = nhm, deeq_z = nhm) FP64; na/nh per atom type (host arrays) */
+int b200_hamilt_set_deeq(b200_hamilt* h, int ntype, const int* na, const int* nh, int nspin, int deeq_x, int deeq_y,
+                         int deeq_z, const double* deeq_d);
+/* Operator::hPsi for bands [0, nbands) of k-point ik (module_hamilt_general/operator.cpp:39-88):
+ * hpsi = (T + V_loc + V_NL) psi, entries npwk..ld-1 of each band zeroed.
+ * psi_d / hpsi_d: complex128 (FP64 handle) or complex64 (mixed handle), band b at b*ld.
+ * spin selects the deeq spin channel (isk[ik]). */
+int b200_hamilt_hpsi(b200_hamilt* h, int ik, int spin, int nbands, int ld, const void* psi_d, void* hpsi_d,
+                     void* stream);
+/* Parts of H|psi>, for checking and for callers that compose their own chain:
+ * mode 1 = kinetic + local only, mode 2 = nonlocal only (accumulated into hpsi_d). */
+int b200_hamilt_hpsi_part(b200_hamilt* h, int ik, int spin, int nbands, int ld, const void* psi_d, void* hpsi_d,
+                          int mode, void* stream);
+
+/* ------------------------------------------------------------------ Davidson
+ * hsolver::DiagoDavid<T, DEVICE_GPU> (module_hsolver/diago_david.h:19-84):
+ * constructor (precondition, nband, dim, david_ndim, use_paw = false) and
+ * diag(hpsi_func, spsi_func, ldPsi, psi_in, eigenvalue_in, thr, maxiter, ntry_max, notconv_max)
+ * (diago_david.cpp:1173-1200).  S = I (norm-conserving).  precondition_d is a device array of dim. */
+int b200_david_create(int nband, int dim, int david_ndim, int precision, const double* precondition_d,
+                      b200_david** out);
+int b200_david_destroy(b200_david* d);
+/* HPsiFunc (diago_david.h:57): hpsi(X, HX, nvec, dim, id_start, id_end) with X the base pointer of
+ * the block (vectors of length dim at X + m*dim) and HX already offset to vector id_start. */
+typedef void (*b200_hpsi_cb)(void* user, const void* x_d, void* hx_d, int nvec, int dim, int id_start, int id_end);
+/* psi_d: nband vectors at psi_d + m*ldpsi (complex128 for FP64, complex128 for mixed: the solver
+ * demotes internally); eigenvalue: host array of nband doubles; returns iterations in *iters. */
+int b200_david_diag(b200_david* d, b200_hpsi_cb hpsi, void* user, int ldpsi, void* psi_d, double* eigenvalue,
+                    double thr, int maxiter, int ntry_max, int notconv_max, int* iters);
+/* Same, with H|psi> taken from a Hamiltonian handle at k-point ik (no host callback per block). */
+int b200_david_diag_hamilt(b200_david* d, b200_hamilt* h, int ik, int spin, int ldpsi, void* psi_d,
+                           double* eigenvalue, double thr, int maxiter, int ntry_max, int notconv_max, int* iters);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ABACUS_B200_H */
