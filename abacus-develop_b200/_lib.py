@@ -25,6 +25,7 @@ HPSI_CB = C.CFUNCTYPE(None, vp, vp, vp, i32, i32, i32, i32)
 _SIGS = {
     "b200_last_error": ([], C.c_char_p),
     "b200_version": ([], C.c_char_p),
+    "b200_kernel_launches": ([], C.c_ulonglong),
     "b200_ekinetic_pw_op_f64": ([i32, i32, i32, f64, vp, vp, vp, vp], i32),
     "b200_ekinetic_pw_op_f32": ([i32, i32, i32, f32, vp, vp, vp, vp], i32),
     "b200_veff_pw_op_f64": ([i32, vp, vp, vp], i32),
@@ -77,7 +78,7 @@ class B200Error(RuntimeError):
 def header_symbols() -> list[str]:
     """Entry points declared in include/abacus_b200.h."""
     txt = HEADER.read_text()
-    return sorted(set(re.findall(r"^\s*(?:int|const char\*)\s+(b200_\w+)\s*\(", txt, re.M)))
+    return sorted(set(re.findall(r"^\s*(?:int|const char\*|unsigned long long)\s+(b200_\w+)\s*\(", txt, re.M)))
 
 
 def load() -> C.CDLL:

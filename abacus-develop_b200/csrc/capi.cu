@@ -22,12 +22,17 @@ struct b200_david {
     std::unique_ptr<b200::DavidBase> d;
 };
 
+#include <atomic>
+
 namespace b200 {
 namespace {
 thread_local std::string g_last_error;
-}
+std::atomic<unsigned long long> g_launches{0};
+}  // namespace
 void set_last_error(const std::string& msg) { g_last_error = msg; }
 const char* last_error() { return g_last_error.c_str(); }
+void note_launch(unsigned n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+unsigned long long launches() { return g_launches.load(std::memory_order_relaxed); }
 }  // namespace b200
 
 namespace {
@@ -80,6 +85,7 @@ extern "C" {
 
 const char* b200_last_error(void) { return b200::last_error(); }
 const char* b200_version(void) { return "abacus_b200 0.1 (sm_100a)"; }
+unsigned long long b200_kernel_launches(void) { return b200::launches(); }
 
 // ------------------------------------------------------------------ functors
 int b200_ekinetic_pw_op_f64(int nband, int npw, int max_npw, double tpiba2, const double* gk2, void* hpsi,

@@ -30,6 +30,10 @@ struct Error : std::runtime_error {
 void set_last_error(const std::string& msg);
 const char* last_error();
 
+// Number of kernels this library has launched (all devices, all threads).
+void note_launch(unsigned n = 1);
+unsigned long long launches();
+
 #define B200_CUDA(call)                                                                                    \
     do {                                                                                                   \
         cudaError_t e_ = (call);                                                                           \

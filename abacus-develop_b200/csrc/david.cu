@@ -181,6 +181,7 @@ template <typename T> struct Engine {
             B200_CUDA(cudaMemcpyAsync(pc.ptr, precond_d, dim * sizeof(double), cudaMemcpyDeviceToDevice, s));
         } else {
             k_convert_real<R><<<grid_of(dim), kT, 0, s>>>(dim, precond_d, pc.ptr);
+            note_launch();
             B200_CUDA(cudaGetLastError());
         }
         int l1 = 0, l2 = 0;
@@ -213,6 +214,7 @@ template <typename T> struct Engine {
             B200_CUDA(cudaMemcpyAsync(G, gram.ptr, n2 * sizeof(double2), cudaMemcpyDeviceToDevice, s));
         } else {
             k_convert<T, double2><<<grid_of(n2), kT, 0, s>>>(n2, gram.ptr, G);
+            note_launch();
             B200_CUDA(cudaGetLastError());
         }
         B200_CUSOLVER(cusolverDnZpotrf(cs, CUBLAS_FILL_MODE_UPPER, nc, (cuDoubleComplex*)G, nc, (cuDoubleComplex*)work.ptr,
@@ -222,6 +224,7 @@ template <typename T> struct Engine {
             U = G;
         } else {
             k_convert<double2, T><<<grid_of(n2), kT, 0, s>>>(n2, G, gram.ptr);
+            note_launch();
             B200_CUDA(cudaGetLastError());
             U = gram.ptr;
         }
@@ -252,6 +255,7 @@ template <typename T> struct Engine {
             B200_CUDA(cudaMemcpyAsync(A64.ptr, hcc.ptr, n * sizeof(double2), cudaMemcpyDeviceToDevice, s));
         } else {
             k_convert<T, double2><<<grid_of(n), kT, 0, s>>>(n, hcc.ptr, A64.ptr);
+            note_launch();
             B200_CUDA(cudaGetLastError());
         }
         B200_CUSOLVER(cusolverDnZheevd(cs, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, nbase,
@@ -262,6 +266,7 @@ template <typename T> struct Engine {
             B200_CUDA(cudaMemcpyAsync(vcc.ptr, A64.ptr, nv * sizeof(double2), cudaMemcpyDeviceToDevice, s));
         } else {
             k_convert<double2, T><<<grid_of(nv), kT, 0, s>>>(nv, A64.ptr, vcc.ptr);
+            note_launch();
             B200_CUDA(cudaGetLastError());
         }
         int hinfo[4];
@@ -280,11 +285,13 @@ template <typename T> struct Engine {
         B200_CUDA(cudaMemcpyAsync(unconv_d.ptr, unconv_h.data(), nc * sizeof(int), cudaMemcpyHostToDevice, s));
         k_gather_cols<T><<<grid_of(long(nbase) * nc), kT, 0, s>>>(nbase, nbase_x, nc, unconv_d.ptr, vcc.ptr, w.ptr, vc.ptr,
                                                                   vcl.ptr);
+        note_launch();
         B200_CUDA(cudaGetLastError());
         T* X = basis.ptr + size_t(nbase) * dim;
         gemm(CUBLAS_OP_N, CUBLAS_OP_N, dim, nc, nbase, one, hp.ptr, dim, vc.ptr, nbase, zero, X, dim);
         gemm(CUBLAS_OP_N, CUBLAS_OP_N, dim, nc, nbase, one, basis.ptr, dim, vcl.ptr, nbase, one, X, dim);
         k_precond<T, R><<<grid_of(long(dim) * nc), kT, 0, s>>>(dim, nc, X, pc.ptr);
+        note_launch();
         B200_CUDA(cudaGetLastError());
         orth_block(X, nc, nbase);
         f(basis.ptr, hp.ptr + size_t(nbase) * dim, nbase_x, dim, nbase, nbase + nc - 1, s);
@@ -301,6 +308,7 @@ template <typename T> struct Engine {
         if (!ref_refresh) B200_CUDA(cudaMemsetAsync(vcc.ptr, 0, vcc.n * sizeof(T), s));
         B200_CUDA(cudaMemcpyAsync(ein.ptr, eig_in, nband * sizeof(double), cudaMemcpyHostToDevice, s));
         k_refresh_diag<T><<<grid_of(nband), kT, 0, s>>>(nband, nbase_x, ein.ptr, hcc.ptr, vcc.ptr);
+        note_launch();
         B200_CUDA(cudaGetLastError());
     }
 
@@ -386,10 +394,12 @@ class David : public DavidBase {
             psi32_.resize(size_t(nband_) * ldpsi);
             const long n = long(nband_) * ldpsi;
             k_convert<double2, float2><<<grid_of(n), kT>>>(n, (const double2*)psi, psi32_.ptr);
+            note_launch();
             B200_CUDA(cudaGetLastError());
             const double t32 = thr > mixed_thr_ ? thr : mixed_thr_;
             const int it32 = e32_->diag(f32, ldpsi, psi32_.ptr, eig, t32, maxiter, 0, nband_, nc);
             k_convert<float2, double2><<<grid_of(n), kT>>>(n, psi32_.ptr, (double2*)psi);
+            note_launch();
             B200_CUDA(cudaGetLastError());
             stats_.iters_low = it32;
             stats_.hpsi_bands += e32_->hpsi_bands;

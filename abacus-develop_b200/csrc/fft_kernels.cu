@@ -423,16 +423,19 @@ void launch_hpsi_local(const PWGrid& g, int ik, const R* veff_zyx, int nb, int l
     const dim3 gz(ceil_div(g.nst, kStickTile), nb);
     set_smem(k_zpass_inv<T>, zs);
     k_zpass_inv<T><<<gz, 256, zs, s>>>(sm, g.az.plan, tw_of<T>(g.az), psi, ld, stickbuf);
+    note_launch();
     B200_CUDA(cudaGetLastError());
     set_smem(k_plane<T, R>, ps);
     k_plane<T, R><<<dim3(nb, g.nz), 512, ps, s>>>(g.plane_view(), g.nx, g.ny, g.nz, g.ax.plan, g.ay.plan, tw_of<T>(g.ax),
                                                   tw_of<T>(g.ay), veff_zyx, stickbuf);
+    note_launch();
     B200_CUDA(cudaGetLastError());
     const KMap& km = g.kmaps[ik];
     const R* gk2 = std::is_same<R, double>::value ? (const R*)km.gk2.ptr : (const R*)km.gk2f.ptr;
     set_smem(k_zpass_fwd<T, R>, zs);
     k_zpass_fwd<T, R><<<gz, 256, zs, s>>>(sm, g.az.plan, tw_of<T>(g.az), stickbuf, psi, hpsi, ld, km.npw, gk2, R(tpiba2),
                                           R(1.0 / double(g.nxyz())), accumulate);
+    note_launch();
     B200_CUDA(cudaGetLastError());
 }
 
@@ -445,16 +448,19 @@ void launch_recip_to_real(const PWGrid& g, int ik, const T* in, T* out, T* aux, 
     set_smem(k_box_zinv<T>, zs);
     k_box_zinv<T><<<ceil_div(g.nst, kStickTile), 256, zs, s>>>(g.stick_view(ik), g.az.plan, tw_of<T>(g.az), g.st_ixy.ptr,
                                                                in, aux);
+    note_launch();
     B200_CUDA(cudaGetLastError());
     const size_t ys = size_t(2) * kBoxTile * odd_ld(g.ny) * sizeof(T);
     set_smem(k_box_y<T, +1>, ys);
     k_box_y<T, +1><<<dim3(g.nxc, ceil_div(g.nz, kBoxTile)), 256, ys, s>>>(g.ay.plan, tw_of<T>(g.ay), g.xpos.ptr, g.ny,
                                                                           g.nz, aux);
+    note_launch();
     B200_CUDA(cudaGetLastError());
     const size_t xsm = size_t(2) * kBoxTile * odd_ld(g.nx) * sizeof(T);
     set_smem(k_box_x<T, R, +1>, xsm);
     k_box_x<T, R, +1><<<dim3(g.ny, ceil_div(g.nz, kBoxTile)), 256, xsm, s>>>(g.ax.plan, tw_of<T>(g.ax), g.nx, g.ny, g.nz,
                                                                              aux, out, add, R(factor));
+    note_launch();
     B200_CUDA(cudaGetLastError());
 }
 
@@ -465,11 +471,13 @@ void launch_real_to_recip(const PWGrid& g, int ik, const T* in, T* out, T* aux, 
     set_smem(k_box_x<T, R, -1>, xsm);
     k_box_x<T, R, -1><<<dim3(g.ny, ceil_div(g.nz, kBoxTile)), 256, xsm, s>>>(g.ax.plan, tw_of<T>(g.ax), g.nx, g.ny, g.nz,
                                                                              in, aux, 0, R(1));
+    note_launch();
     B200_CUDA(cudaGetLastError());
     const size_t ys = size_t(2) * kBoxTile * odd_ld(g.ny) * sizeof(T);
     set_smem(k_box_y<T, -1>, ys);
     k_box_y<T, -1><<<dim3(g.nxc, ceil_div(g.nz, kBoxTile)), 256, ys, s>>>(g.ay.plan, tw_of<T>(g.ay), g.xpos.ptr, g.ny,
                                                                           g.nz, aux);
+    note_launch();
     B200_CUDA(cudaGetLastError());
     const size_t zs = zpass_smem(g, sizeof(T));
     set_smem(k_box_zfwd<T, R>, zs);
@@ -477,12 +485,14 @@ void launch_real_to_recip(const PWGrid& g, int ik, const T* in, T* out, T* aux, 
     const double scale = (add ? factor : 1.0) / double(g.nxyz());
     k_box_zfwd<T, R><<<ceil_div(g.nst, kStickTile), 256, zs, s>>>(g.stick_view(ik), g.az.plan, tw_of<T>(g.az),
                                                                   g.st_ixy.ptr, aux, out, add, R(scale));
+    note_launch();
     B200_CUDA(cudaGetLastError());
 }
 
 template <typename R>
 void launch_transpose_veff(const PWGrid& g, const double* veff, R* out, cudaStream_t s) {
     k_veff_zyx<R><<<1184, 256, 0, s>>>(g.nx, g.ny, g.nz, veff, out);
+    note_launch();
     B200_CUDA(cudaGetLastError());
 }
 

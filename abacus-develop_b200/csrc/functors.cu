@@ -121,12 +121,14 @@ template <typename T, typename R>
 void ekinetic_pw(int nband, int npw, int max_npw, R tpiba2, const R* gk2, T* hpsi, const T* psi, cudaStream_t s) {
     if (nband <= 0 || npw <= 0) return;
     k_ekinetic<T, R><<<grid_for(long(nband) * npw), kThreads, 0, s>>>(nband, npw, max_npw, tpiba2, gk2, hpsi, psi);
+    note_launch();
     B200_CUDA(cudaGetLastError());
 }
 
 template <typename T, typename R> void veff_pw(long size, T* out, const R* in, cudaStream_t s) {
     if (size <= 0) return;
     k_veff<T, R><<<grid_for(size), kThreads, 0, s>>>(size, out, in);
+    note_launch();
     B200_CUDA(cudaGetLastError());
 }
 
@@ -134,6 +136,7 @@ template <typename T, typename R>
 void veff_pw_npol2(long size, T* out, T* out1, const R* const in[4], cudaStream_t s) {
     if (size <= 0) return;
     k_veff_npol2<T, R><<<grid_for(size), kThreads, 0, s>>>(size, out, out1, in[0], in[1], in[2], in[3]);
+    note_launch();
     B200_CUDA(cudaGetLastError());
 }
 
@@ -143,6 +146,7 @@ void nonlocal_pw(int l1, int l2, int l3, int& sum, int& iat, int spin, int nkb, 
     const long total = long(l1) * l2 * l3;
     if (total > 0) {
         k_nonlocal<T, R><<<grid_for(total), kThreads, 0, s>>>(l1, l2, l3, sum, iat, spin, nkb, dx, dy, dz, deeq, ps, becp);
+        note_launch();
         B200_CUDA(cudaGetLastError());
     }
     sum += l1 * l3;
@@ -155,6 +159,7 @@ void nonlocal_pw_nc(int l1, int l2, int l3, int& sum, int& iat, int nkb, int dx,
     const long total = long(l1) * (l2 / 2) * l3;
     if (total > 0) {
         k_nonlocal_nc<T><<<grid_for(total), kThreads, 0, s>>>(l1, l2, l3, sum, iat, nkb, dx, dy, dz, dnc, ps, becp);
+        note_launch();
         B200_CUDA(cudaGetLastError());
     }
     iat += l1;
@@ -164,6 +169,7 @@ void nonlocal_pw_nc(int l1, int l2, int l3, int& sum, int& iat, int nkb, int dx,
 template <typename T> void set_3d_fft_box(int npwk, const int* idx, const T* in, T* out, cudaStream_t s) {
     if (npwk <= 0) return;
     k_set_box<T><<<grid_for(npwk), kThreads, 0, s>>>(npwk, idx, in, out);
+    note_launch();
     B200_CUDA(cudaGetLastError());
 }
 
@@ -171,6 +177,7 @@ template <typename T, typename R>
 void set_recip_to_real_output(long nrxx, int add, R factor, const T* in, T* out, cudaStream_t s) {
     if (nrxx <= 0) return;
     k_r2r_out<T, R><<<grid_for(nrxx), kThreads, 0, s>>>(nrxx, add, factor, in, out);
+    note_launch();
     B200_CUDA(cudaGetLastError());
 }
 
@@ -179,6 +186,7 @@ void set_real_to_recip_output(int npw, long nxyz, int add, R factor, const int* 
     if (npw <= 0) return;
     const R scale = add ? R(factor / R(nxyz)) : R(R(1) / R(nxyz));
     k_r2g_out<T, R><<<grid_for(npw), kThreads, 0, s>>>(npw, add, scale, idx, in, out);
+    note_launch();
     B200_CUDA(cudaGetLastError());
 }
 

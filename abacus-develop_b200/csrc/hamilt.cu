@@ -44,6 +44,7 @@ void Hamilt::set_vkb(int ik, int nkb, int npwx, const double2* vkb_d) {
     B200_CUDA(cudaMemcpyAsync(k.vkb.ptr, vkb_d, n * sizeof(double2), cudaMemcpyDeviceToDevice, 0));
     k.vkbf.resize(n);
     k_z2c<<<592, 256>>>(n, vkb_d, k.vkbf.ptr);
+    note_launch();
     B200_CUDA(cudaGetLastError());
     B200_CUDA(cudaStreamSynchronize(0));
 }
@@ -63,6 +64,7 @@ void Hamilt::set_deeq(int ntype_, const int* na_, const int* nh_, int nspin_, in
     B200_CUDA(cudaMemcpyAsync(deeq.ptr, deeq_d, n * sizeof(double), cudaMemcpyDeviceToDevice, 0));
     deeqf.resize(n);
     k_d2f<<<592, 256>>>(n, deeq_d, deeqf.ptr);
+    note_launch();
     B200_CUDA(cudaGetLastError());
     B200_CUDA(cudaStreamSynchronize(0));
 }

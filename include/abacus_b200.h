@@ -43,6 +43,9 @@ typedef struct b200_david b200_david;       /* Davidson workspaces */
 const char* b200_last_error(void);
 /* Library version string. */
 const char* b200_version(void);
+/* Number of kernels this library has launched so far in this process (its own
+ * kernels only; cuBLAS / cuSOLVER launches are not counted). */
+unsigned long long b200_kernel_launches(void);
 
 /* ------------------------------------------------------------------ op functors
  * Each replaces the body of a DEVICE_GPU partial specialisation; arguments keep

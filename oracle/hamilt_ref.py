@@ -11,7 +11,7 @@ Followed reference code (abacus-develop v3.8.0):
   * pw_op functors ............ source/module_basis/module_pw/kernels/pw_op.cpp:6-68
   * recip_to_real/real_to_recip source/module_basis/module_pw/pw_transform_k.cpp:336-476
     (FFTW/cuFFT convention: backward = exp(+iGr) un-normalised, forward =
-    exp(-iGr), the 1/N applied at the gather) -- numpy's pocketfft has the
+    exp(-iGr), the 1/N applied at the gather) -- scipy's pocketfft has the
     same convention (fftn = forward, ifftn * N = backward).
   * Veff::act ................. source/module_hamilt_pw/hamilt_pwdft/operator_pw/veff_pw.cpp:38-109
   * Ekinetic::act ............. source/module_hamilt_pw/hamilt_pwdft/operator_pw/ekinetic_pw.cpp:34-50
@@ -23,6 +23,10 @@ Followed reference code (abacus-develop v3.8.0):
 from __future__ import annotations
 
 import numpy as np
+import scipy.fft
+
+# threads for the oracle's FFTs (scipy's pocketfft; 1 = single thread)
+FFT_WORKERS = 1
 
 
 # ---------------------------------------------------------------- functors
@@ -113,7 +117,7 @@ def recip_to_real(basis, inp, ik, out=None, add=False, factor=1.0):
     box = np.zeros(N, dtype=np.complex128)
     npw = int(basis.npwk[ik])
     set_3d_fft_box_op(npw, basis.ig2ixyz(ik), inp, box)
-    r = np.fft.ifftn(box.reshape(nx, ny, nz)).reshape(-1) * N
+    r = scipy.fft.ifftn(box.reshape(nx, ny, nz), workers=FFT_WORKERS).reshape(-1) * N
     if out is None:
         out = np.zeros(N, dtype=np.complex128)
     set_recip_to_real_output_op(N, add, factor, r, out)
@@ -124,7 +128,7 @@ def real_to_recip(basis, inp, ik, out=None, add=False, factor=1.0):
     """PW_Basis_K::real_to_recip (pw_transform_k.cpp:336-401): full r box -> sphere."""
     nx, ny, nz = basis.nx, basis.ny, basis.nz
     N = nx * ny * nz
-    g = np.fft.fftn(np.asarray(inp, dtype=np.complex128).reshape(nx, ny, nz)).reshape(-1)
+    g = scipy.fft.fftn(np.asarray(inp, dtype=np.complex128).reshape(nx, ny, nz), workers=FFT_WORKERS).reshape(-1)
     npw = int(basis.npwk[ik])
     if out is None:
         out = np.zeros(npw, dtype=np.complex128)
