@@ -348,6 +348,15 @@ int b200_david_diag(b200_david* d, b200_hpsi_cb hpsi, void* user, int ldpsi, voi
         if (iters) *iters = it;
     });
 }
+int b200_david_stats(const b200_david* d, int* iters_low, int* iters_fp64, int* hpsi_bands) {
+    return guarded([&] {
+        B200_CHECK(d != nullptr, b200::kInvalidArgument, "NULL argument");
+        const auto& st = d->d->stats();
+        if (iters_low) *iters_low = st.iters_low;
+        if (iters_fp64) *iters_fp64 = st.iters_fp64;
+        if (hpsi_bands) *hpsi_bands = st.hpsi_bands;
+    });
+}
 int b200_david_diag_hamilt(b200_david* d, b200_hamilt* h, int ik, int spin, int ldpsi, void* psi, double* eig,
                            double thr, int maxiter, int ntry_max, int notconv_max, int* iters) {
     return guarded([&] {
@@ -361,7 +370,7 @@ int b200_david_diag_hamilt(b200_david* d, b200_hamilt* h, int ik, int spin, int 
             const float2* X = (const float2*)x + size_t(i0) * dim;
             H->hpsi<float2>(ik, spin, i1 - i0 + 1, dim, X, (float2*)hx, 0, s);
         };
-        const int it = d->d->diag_hamilt(f64, f32, H->precision, ldpsi, psi, eig, thr, maxiter, ntry_max, notconv_max);
+        const int it = d->d->diag_hamilt(f64, f32, d->d->precision(), ldpsi, psi, eig, thr, maxiter, ntry_max, notconv_max);
         if (iters) *iters = it;
     });
 }

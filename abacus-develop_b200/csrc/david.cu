@@ -414,6 +414,7 @@ class David : public DavidBase {
     }
     const DavidStats& stats() const override { return stats_; }
     void set_mixed_thr(double thr) override { mixed_thr_ = thr; }
+    int precision() const override { return precision_; }
     void set_reference_refresh(bool on) override {
         e64_->ref_refresh = on;
         if (e32_) e32_->ref_refresh = on;

@@ -28,6 +28,7 @@ struct DavidBase {
     virtual const DavidStats& stats() const = 0;
     virtual void set_mixed_thr(double thr) = 0;
     virtual void set_reference_refresh(bool on) = 0;
+    virtual int precision() const = 0;
 };
 
 std::unique_ptr<DavidBase> make_david(int nband, int dim, int david_ndim, int precision, const double* precond_d);

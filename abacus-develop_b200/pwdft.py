@@ -253,6 +253,12 @@ class DiagoDavid:
              eigenvalue.ctypes.data_as(_lib.pf64), thr, maxiter, ntry_max, notconv_max, C.byref(it))
         return it.value
 
+    def stats(self):
+        """(iterations in the FP32 stage, iterations in FP64, single-band H applications) of the last solve."""
+        a, b, c = C.c_int(), C.c_int(), C.c_int()
+        call("b200_david_stats", self._h, C.byref(a), C.byref(b), C.byref(c))
+        return a.value, b.value, c.value
+
     def __del__(self):
         try:
             if getattr(self, "_h", None):

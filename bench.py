@@ -359,13 +359,14 @@ def davidson_bench(P, wl, h64, h32):
         t0 = time.perf_counter()
         it = dav.diag_hamilt(h, 0, ld, x, e, thr, 200)
         torch.cuda.synchronize()
-        return time.perf_counter() - t0, e, it
+        return time.perf_counter() - t0, e, dav.stats()
 
     _, e_ref, it_ref = solve(h64, P.PREC_FP64, 1e-11)
     t64, e64, it64 = solve(h64, P.PREC_FP64, 1e-9)
     tmx, emx, itmx = solve(h64, P.PREC_MIXED, 1e-9)
     return {"fp64_s": t64, "mixed_s": tmx, "speedup": t64 / tmx,
-            "fp64_iters": it64, "mixed_iters": itmx, "ref_iters": it_ref,
+            "fp64_iters": it64[1], "mixed_iters_fp32": itmx[0], "mixed_iters_fp64": itmx[1],
+            "fp64_hpsi_bands": it64[2], "mixed_hpsi_bands": itmx[2], "ref_iters": it_ref[1],
             "fp64_max_err_ry": float(np.max(np.abs(e64 - e_ref))),
             "mixed_max_err_ry": float(np.max(np.abs(emx - e_ref))),
             "reference_solve": "FP64 Davidson to thr 1e-11 on the same device",

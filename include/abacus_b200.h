@@ -177,6 +177,10 @@ int b200_david_diag(b200_david* d, b200_hpsi_cb hpsi, void* user, int ldpsi, voi
 int b200_david_diag_hamilt(b200_david* d, b200_hamilt* h, int ik, int spin, int ldpsi, void* psi_d,
                            double* eigenvalue, double thr, int maxiter, int ntry_max, int notconv_max, int* iters);
 
+/* Statistics of the last solve: Davidson iterations in the FP32 stage (mixed only), in FP64,
+ * and the number of single-band H applications (all stages). */
+int b200_david_stats(const b200_david* d, int* iters_low, int* iters_fp64, int* hpsi_bands);
+
 #ifdef __cplusplus
 }
 #endif

@@ -84,6 +84,12 @@ def test_david_diamond8(pkg, diamond8, prec):
     e = np.zeros(nband)
     it = dav.diag_hamilt(h, 0, ld, psi, e, 1e-10, 100)
     assert np.max(np.abs(e - e_ref)) < 1e-8, (e - e_ref)
+    it_low, it64, nh = dav.stats()
+    assert it == it_low + it64 and nh > 0
+    if prec == "mixed":
+        assert it_low > 0  # the FP32 stage really ran
+    else:
+        assert it_low == 0
     if prec == "fp64":
         # same algorithm: iteration count within a couple of the restated reference
         assert abs(it - it_ref) <= 3, (it, it_ref)
