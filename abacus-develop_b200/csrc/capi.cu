@@ -10,17 +10,7 @@
 #include "hamilt.h"
 #include "pw_grid.h"
 
-struct b200_pw_basis {
-    b200::PWGrid grid;
-    b200::DeviceArray<double2> aux64;
-    b200::DeviceArray<float2> aux32;
-};
-struct b200_hamilt {
-    std::unique_ptr<b200::Hamilt> h;
-};
-struct b200_david {
-    std::unique_ptr<b200::DavidBase> d;
-};
+#include "capi_handles.h"
 
 #include <atomic>
 

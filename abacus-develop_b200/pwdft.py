@@ -212,6 +212,12 @@ class HamiltPW:
     def hpsi_part(self, ik, psi, hpsi, nbands, ld, mode, spin=0, stream=None):
         call("b200_hamilt_hpsi_part", self._h, ik, spin, nbands, ld, ptr(psi), ptr(hpsi), mode, stream_ptr(stream))
 
+    def hpsi_local_noalloc(self, ik, psi, hpsi, nbands, ld, stream=None):
+        """Kinetic + local part of H|psi> without any device allocation during the call, for callers that
+        cannot allocate (graph capture, externally owned memory pools); scratch is a fixed 32 MiB array
+        inside the library shared by all calls, so concurrent calls on one device must be serialised."""
+        call("b200_hamilt_hpsi_local_noalloc", self._h, ik, nbands, ld, ptr(psi), ptr(hpsi), stream_ptr(stream))
+
     def __del__(self):
         try:
             if getattr(self, "_h", None):

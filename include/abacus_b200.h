@@ -158,6 +158,20 @@ int b200_hamilt_hpsi(b200_hamilt* h, int ik, int spin, int nbands, int ld, const
 int b200_hamilt_hpsi_part(b200_hamilt* h, int ik, int spin, int nbands, int ld, const void* psi_d, void* hpsi_d,
                           int mode, void* stream);
 
+/* Allocation-free form of b200_hamilt_hpsi_part(mode = 1): kinetic + local part of
+ * H|psi> for bands [0, nbands) of k-point ik, written to hpsi_d (padding zeroed).
+ * No counterpart in the reference: it exists for callers that cannot allocate device
+ * memory during the call (inside a CUDA-graph capture, under a host framework that owns
+ * the device memory pool, or on paths that must not synchronise).  It calls no
+ * cudaMalloc/cudaFree; its scratch is a fixed 32 MiB device array inside the library,
+ * held by every GPU that loads the library until exit.  The first call on each device
+ * looks up that array's address (cudaGetSymbolAddress), so make it before any stream
+ * capture.  A grid whose one-band stick buffer (nst*nz complex values) exceeds 32 MiB is
+ * rejected with B200_STATUS_CAPACITY_ERROR.  All calls share the array: calls that
+ * overlap on the GPU race and must be serialised by the caller. */
+int b200_hamilt_hpsi_local_noalloc(b200_hamilt* h, int ik, int nbands, int ld, const void* psi_d, void* hpsi_d,
+                                   void* stream);
+
 /* ------------------------------------------------------------------ Davidson
  * hsolver::DiagoDavid<T, DEVICE_GPU> (module_hsolver/diago_david.h:19-84):
  * constructor (precondition, nband, dim, david_ndim, use_paw = false) and
