@@ -61,6 +61,8 @@ _SIGS = {
     "b200_hamilt_hpsi": ([vp, i32, i32, i32, i32, vp, vp, vp], i32),
     "b200_hamilt_hpsi_part": ([vp, i32, i32, i32, i32, vp, vp, i32, vp], i32),
     "b200_hamilt_hpsi_local_noalloc": ([vp, i32, i32, i32, vp, vp, vp], i32),
+    "b200_tc_cgemm": ([C.c_char, C.c_char, i32, i32, i32, f32, f32, vp, i32, vp, i32, f32, f32, vp, i32, vp], i32),
+    "b200_tc_cgemm_error": ([pi32], i32),
     "b200_david_create": ([i32, i32, i32, i32, vp, C.POINTER(vp)], i32),
     "b200_david_destroy": ([vp], i32),
     "b200_david_diag": ([vp, HPSI_CB, vp, i32, vp, pf64, f64, i32, i32, i32, pi32], i32),

@@ -11,6 +11,7 @@
 #include "pw_grid.h"
 
 #include "capi_handles.h"
+#include "gemm_tc.h"
 
 #include <atomic>
 
@@ -336,6 +337,24 @@ int b200_david_diag(b200_david* d, b200_hpsi_cb hpsi, void* user, int ldpsi, voi
         };
         const int it = d->d->diag(f, ldpsi, psi, eig, thr, maxiter, ntry_max, notconv_max);
         if (iters) *iters = it;
+    });
+}
+static thread_local b200::TcGemmWorkspace g_tc_ws;
+int b200_tc_cgemm(char transa, char transb, int m, int n, int k, float alpha_re, float alpha_im, const void* a, int lda,
+                  const void* b, int ldb, float beta_re, float beta_im, void* c, int ldc, void* stream) {
+    b200::TcGemmWorkspace& ws = g_tc_ws;
+    return guarded([&] {
+        B200_CHECK(transb == 'N' || transb == 'n', b200::kInvalidArgument, "transb must be 'N'");
+        const char opa = (transa == 'n' || transa == 'N') ? 'N' : ((transa == 'c' || transa == 'C') ? 'C' : '?');
+        B200_CHECK(opa != '?', b200::kInvalidArgument, "transa must be 'N' or 'C'");
+        b200::tc_cgemm(opa, m, n, k, make_float2(alpha_re, alpha_im), (const float2*)a, lda, (const float2*)b, ldb,
+                       make_float2(beta_re, beta_im), (float2*)c, ldc, ws, S(stream));
+    });
+}
+int b200_tc_cgemm_error(int* code) {
+    return guarded([&] {
+        B200_CHECK(code != nullptr, b200::kInvalidArgument, "NULL argument");
+        *code = g_tc_ws.read_error();
     });
 }
 int b200_david_stats(const b200_david* d, int* iters_low, int* iters_fp64, int* hpsi_bands) {

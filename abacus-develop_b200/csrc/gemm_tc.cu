@@ -1,0 +1,523 @@
+// Complex FP32 GEMM on the 5th-generation tensor cores (tcgen05, kind::tf32) with
+// split precision: every FP32 operand x is split into hi = tf32(x) (rounded) and
+// lo = x - hi, and C = A_hi*B_hi + A_hi*B_lo + A_lo*B_hi is accumulated in FP32 in
+// tensor memory (the hi/lo "3xTF32" scheme: about FP32 accuracy at tensor-core rate).
+//
+//   C (M x N, column-major, complex) = alpha * op(A) * B + beta * C
+//   op(A) = A   (A column-major M x K)            "N"
+//   op(A) = A^H (A column-major K x M)            "C"
+//   B column-major K x N.
+//
+// The complex product is done as one real GEMM of size 2M x N x 2K: with
+// interleaved (re, im) storage B is already the real 2K x N matrix, and op(A)
+// becomes the real 2M x 2K matrix whose 2x2 blocks are [[ar, -ai], [ai, ar]]
+// (for A^H: [[ar, ai], [-ai, ar]]).  Those blocks are built in shared memory from
+// the TMA-loaded tile: each 128-byte row of the raw tile (a column of A for "N",
+// MN-major; a row of A^H for "C", K-major) becomes two rows, the row itself and
+// the row multiplied by i (pairs (a, b) -> (-b, a)).  The same pass writes the
+// hi/lo split, so nothing is pre-processed in HBM.
+//
+// CTA: 6 warps.  warp 0 issues TMA loads (cp.async.bulk.tensor, no multicast),
+// warp 1 allocates TMEM and one lane issues tcgen05.mma, warps 2-5 split/expand
+// the tiles and then run the epilogue (tcgen05.ld -> alpha/beta -> global).
+// 3-stage mbarrier pipeline, two TMEM accumulators.  Every wait is bounded in time; a wait that runs out
+// sets an error word, the CTA drains its own copies in flight, frees TMEM and
+// returns.  Long K is split across CTAs (grid.z) with a deterministic reduction.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <mutex>
+
+#include "common.h"
+#include "gemm_tc.h"
+
+namespace b200 {
+namespace {
+
+constexpr int kBM = 128;     // real rows of C per tile
+constexpr int kBK = 32;      // real K per stage (one 128-byte swizzle row of fp32)
+constexpr int kStages = 3;
+constexpr int kThreads = 192;
+constexpr unsigned long long kWaitNs = 2000000000ull;  // 2 s bound on any single wait
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+    return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ unsigned long long gtimer() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+__device__ __forceinline__ void mbar_init(unsigned bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count));
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(unsigned bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(unsigned bar, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// bounded wait: true on success, false after kWaitNs
+__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity) {
+    if (mbar_try(bar, parity)) return true;
+    const unsigned long long t0 = gtimer();
+    while (true) {
+        if (mbar_try(bar, parity)) return true;
+        if (gtimer() - t0 > kWaitNs) return false;
+    }
+}
+__device__ __forceinline__ void tma_load_2d(unsigned dst, const CUtensorMap* map, int x, int y, unsigned bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(dst),
+        "l"(reinterpret_cast<unsigned long long>(map)), "r"(x), "r"(y), "r"(bar)
+        : "memory");
+}
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// Shared-memory matrix descriptor (Blackwell version 1).  layout: 2 = SWIZZLE_128B (16-byte chunks XOR the
+// row within 8-row / 1024-byte atoms), 1 = SWIZZLE_128B_BASE32B (32-byte chunks XOR the row within 4-row /
+// 512-byte atoms, the only layout for MN-major TF32 operands).
+__device__ __forceinline__ unsigned long long sdesc(unsigned addr, unsigned lbo, unsigned sbo, unsigned layout) {
+    unsigned long long d = 0;
+    d |= (unsigned long long)((addr >> 4) & 0x3FFF);
+    d |= (unsigned long long)((lbo >> 4) & 0x3FFF) << 16;
+    d |= (unsigned long long)((sbo >> 4) & 0x3FFF) << 32;
+    d |= 1ull << 46;                       // version
+    d |= (unsigned long long)(layout & 7) << 61;
+    return d;
+}
+__device__ __forceinline__ void mma_tf32(unsigned tmem_d, unsigned long long a, unsigned long long b, unsigned idesc,
+                                         unsigned accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(tmem_d),
+        "l"(a), "l"(b), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+}
+__device__ __forceinline__ void mma_commit(unsigned bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ void tmem_ld16(unsigned taddr, float* v) {
+    unsigned r[16];
+    // load and wait in one statement: the destination registers are only valid after tcgen05.wait::ld
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];\n\t"
+        "tcgen05.wait::ld.sync.aligned;"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+          "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr)
+        : "memory");
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// hi part of the split: x rounded to the nearest TF32 value (10 explicit mantissa bits); lo = x - hi is exact
+__device__ __forceinline__ float tf32_trunc(float x) {
+    return __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xFFFFE000u);
+}
+// physical byte offset of (row, 16-byte chunk) in a 1024-byte-aligned SW128 tile with 128-byte rows
+__device__ __forceinline__ unsigned sw128(unsigned row, unsigned chunk) {
+    return row * 128u + ((chunk ^ (row & 7u)) << 4);
+}
+// the same for the SW128_BASE32B pattern: 32-byte chunks XOR (row mod 4)
+__device__ __forceinline__ unsigned sw128_32b(unsigned row, unsigned chunk) {
+    return row * 128u + ((((chunk >> 1) ^ (row & 3u)) << 5) | ((chunk & 1u) << 4));
+}
+
+template <int BN> struct TileBytes {
+    static constexpr int a_raw = 8192;             // 64 rows x 128 B ("C")  or 4 x 16 x 128 B ("N")
+    static constexpr int a_exp = kBM * 128;        // 16 KB
+    static constexpr int b = BN * 128;
+    static constexpr int stage = a_raw + 2 * a_exp + 2 * b;
+    static constexpr int total = kStages * stage + 2048;  // + barriers / flags + 1024-byte alignment slack
+};
+
+// OPA: 0 = "N" (A column-major M x K, MN-major tiles), 1 = "C" (A^H of a column-major K x M, K-major tiles)
+//
+// Accumulation: the tensor-core accumulator truncates on every accumulate, so a long
+// chain of MMAs into one TMEM accumulator drifts (about 2e-8 relative per MMA).  Each
+// K stage therefore starts a fresh accumulator in one of two TMEM buffers; the
+// epilogue warps drain the finished buffer into FP32 registers (IEEE round-to-nearest
+// adds) while the next stage runs in the other buffer.
+template <int BN, int OPA>
+__global__ void __launch_bounds__(kThreads, 1)
+    k_tc_cgemm(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB, int M2, int N, int K2,
+               int kstages_per_split, float2 alpha, float2 beta, float* __restrict__ C, long ldc2,
+               float* __restrict__ ws, int* __restrict__ err) {
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    using TB = TileBytes<BN>;
+    // 1024-byte alignment of the tile area (the swizzle pattern depends on address bits 7..9)
+    unsigned char* base = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
+    unsigned char* bars = base + kStages * TB::stage;
+    unsigned long long* full = reinterpret_cast<unsigned long long*>(bars);
+    unsigned long long* ready = full + kStages;
+    unsigned long long* empty = ready + kStages;
+    unsigned long long* acc_full = empty + kStages;   // [2] MMA -> epilogue: stage result in TMEM buffer b
+    unsigned long long* acc_empty = acc_full + 2;     // [2] epilogue -> MMA: buffer b drained
+    unsigned* tmem_slot = reinterpret_cast<unsigned*>(acc_empty + 2);
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int tile_m = blockIdx.x, tile_n = blockIdx.y, split = blockIdx.z;
+    const int nk_total = (K2 + kBK - 1) / kBK;
+    const int k_begin = split * kstages_per_split;
+    const int k_end = min(nk_total, k_begin + kstages_per_split);
+    const int nk = max(0, k_end - k_begin);
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kStages; ++s) {
+            mbar_init(smem_u32(&full[s]), 1);
+            mbar_init(smem_u32(&ready[s]), 128);
+            mbar_init(smem_u32(&empty[s]), 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(smem_u32(&acc_full[b]), 1);
+            mbar_init(smem_u32(&acc_empty[b]), 128);
+        }
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(unsigned(2 * BN)));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const unsigned tmem = *tmem_slot;
+
+    auto fail = [&](int code) {
+        *abort_flag = 1;
+        atomicOr(err, code);
+    };
+
+    if (warp == 0) {
+        if (lane == 0) {
+            // producer
+            int issued = 0;
+            for (int i = 0; i < nk && !*abort_flag; ++i) {
+                const int s = i % kStages;
+                if (i >= kStages && !mbar_wait(smem_u32(&empty[s]), ((i / kStages) - 1) & 1)) {
+                    fail(1);
+                    break;
+                }
+                unsigned char* st = base + s * TB::stage;
+                const unsigned fb = smem_u32(&full[s]);
+                mbar_expect_tx(fb, unsigned(TB::a_raw + TB::b));
+                const int kr = (k_begin + i) * kBK;  // real K offset
+                if (OPA == 1) {
+                    tma_load_2d(smem_u32(st), &mapA, kr, tile_m * (kBM / 2), fb);
+                } else {
+                    for (int b = 0; b < 4; ++b)
+                        tma_load_2d(smem_u32(st + b * 2048), &mapA, tile_m * kBM + 32 * b, kr / 2, fb);
+                }
+                tma_load_2d(smem_u32(st + TB::a_raw + 2 * TB::a_exp), &mapB, kr, tile_n * BN, fb);
+                ++issued;
+            }
+            // drain: every load this thread issued must land before the CTA exits
+            for (int i = max(0, issued - kStages); i < issued; ++i) {
+                const int s = i % kStages;
+                if (!mbar_wait(smem_u32(&full[s]), (i / kStages) & 1)) atomicOr(err, 8);
+            }
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            // MMA issuer: stage i accumulates (fresh) into TMEM buffer i & 1
+            const unsigned idesc = (1u << 4) | (2u << 7) | (2u << 10) | (unsigned(OPA == 0) << 15) |
+                                   (unsigned(BN >> 3) << 17) | (unsigned(kBM >> 4) << 24);
+            for (int i = 0; i < nk && !*abort_flag; ++i) {
+                const int s = i % kStages;
+                const int bf = i & 1;
+                if (i >= 2 && !mbar_wait(smem_u32(&acc_empty[bf]), ((i >> 1) - 1) & 1)) {
+                    fail(32);
+                    break;
+                }
+                if (!mbar_wait(smem_u32(&ready[s]), (i / kStages) & 1)) {
+                    fail(2);
+                    break;
+                }
+                tc_fence_after();
+                unsigned char* st = base + s * TB::stage;
+                const unsigned a_hi = smem_u32(st + TB::a_raw);
+                const unsigned a_lo = a_hi + TB::a_exp;
+                const unsigned b_hi = smem_u32(st + TB::a_raw + 2 * TB::a_exp);
+                const unsigned b_lo = b_hi + TB::b;
+                const unsigned d = tmem + unsigned(bf * BN);
+#pragma unroll
+                for (int kk = 0; kk < kBK / 8; ++kk) {
+                    unsigned long long dah, dal;
+                    if (OPA == 1) {  // K-major SW128: 8-row groups 1024 B apart, K step of 8 = 32 B
+                        dah = sdesc(a_hi + kk * 32, 16, 1024, 2);
+                        dal = sdesc(a_lo + kk * 32, 16, 1024, 2);
+                    } else {  // MN-major SW128_BASE32B: 32-float MN blocks 4 KB apart, 4-row K groups 512 B apart
+                        dah = sdesc(a_hi + kk * 1024, 4096, 512, 1);
+                        dal = sdesc(a_lo + kk * 1024, 4096, 512, 1);
+                    }
+                    const unsigned long long dbh = sdesc(b_hi + kk * 32, 16, 1024, 2);
+                    const unsigned long long dbl = sdesc(b_lo + kk * 32, 16, 1024, 2);
+                    // small terms first, then the leading product
+                    mma_tf32(d, dah, dbl, idesc, kk > 0 ? 1u : 0u);
+                    mma_tf32(d, dal, dbh, idesc, 1u);
+                    mma_tf32(d, dah, dbh, idesc, 1u);
+                }
+                mma_commit(smem_u32(&empty[s]));
+                mma_commit(smem_u32(&acc_full[bf]));
+            }
+        }
+    } else {
+        // warps 2..5: split / expand stage i, drain stage i-1, finally store
+        const int t = threadIdx.x - 64;  // 0..127
+        const int q = warp & 3;          // TMEM lane quarter of this warp
+        float acc[BN];
+#pragma unroll
+        for (int j = 0; j < BN; ++j) acc[j] = 0.f;
+        bool ok = true;
+        auto drain = [&](int i) {
+            const int bf = i & 1;
+            ok = ok && mbar_wait(smem_u32(&acc_full[bf]), (i >> 1) & 1);
+            if (!ok) {
+                fail(16);
+                return;
+            }
+            tc_fence_after();
+            const unsigned ta = tmem + (unsigned(32 * q) << 16) + unsigned(bf * BN);
+#pragma unroll
+            for (int c0 = 0; c0 < BN; c0 += 16) {
+                float v[16];
+                tmem_ld16(ta + unsigned(c0), v);
+#pragma unroll
+                for (int j = 0; j < 16; ++j) acc[c0 + j] += v[j];
+            }
+            tc_fence_before();
+            mbar_arrive(smem_u32(&acc_empty[bf]));
+        };
+        for (int i = 0; i < nk && !*abort_flag; ++i) {
+            const int s = i % kStages;
+            if (!mbar_wait(smem_u32(&full[s]), (i / kStages) & 1)) {
+                fail(4);
+                break;
+            }
+            unsigned char* st = base + s * TB::stage;
+            unsigned char* araw = st;
+            unsigned char* ahi = st + TB::a_raw;
+            unsigned char* alo = ahi + TB::a_exp;
+            unsigned char* bhi = ahi + 2 * TB::a_exp;
+            unsigned char* blo = bhi + TB::b;
+            // A: 512 raw 16-byte chunks -> 2 expanded rows each (hi and lo)
+            for (int qq = t; qq < 512; qq += 128) {
+                unsigned src, d0, d1;
+                if (OPA == 1) {
+                    const unsigned r = qq >> 3, c = qq & 7;  // raw row r (one complex row of A^H), chunk c
+                    src = sw128(r, c);
+                    d0 = sw128(2 * r, c);
+                    d1 = sw128(2 * r + 1, c);
+                } else {
+                    const unsigned b = qq >> 7, k = (qq >> 3) & 15, c = qq & 7;  // MN block b, raw K-row k
+                    src = b * 2048 + sw128(k, c);
+                    d0 = b * 4096 + sw128_32b(2 * k, c);
+                    d1 = b * 4096 + sw128_32b(2 * k + 1, c);
+                }
+                const float4 x = *reinterpret_cast<const float4*>(araw + src);
+                const float4 h = make_float4(tf32_trunc(x.x), tf32_trunc(x.y), tf32_trunc(x.z), tf32_trunc(x.w));
+                const float4 l = make_float4(x.x - h.x, x.y - h.y, x.z - h.z, x.w - h.w);
+                *reinterpret_cast<float4*>(ahi + d0) = h;
+                *reinterpret_cast<float4*>(alo + d0) = l;
+                // times i: (a, b) -> (-b, a)
+                *reinterpret_cast<float4*>(ahi + d1) = make_float4(-h.y, h.x, -h.w, h.z);
+                *reinterpret_cast<float4*>(alo + d1) = make_float4(-l.y, l.x, -l.w, l.z);
+            }
+            // B: in-place hi, lo beside it (same layout)
+            for (int qq = t; qq < BN * 8; qq += 128) {
+                float4* p = reinterpret_cast<float4*>(bhi + qq * 16);
+                const float4 x = *p;
+                const float4 h = make_float4(tf32_trunc(x.x), tf32_trunc(x.y), tf32_trunc(x.z), tf32_trunc(x.w));
+                *p = h;
+                *reinterpret_cast<float4*>(blo + qq * 16) = make_float4(x.x - h.x, x.y - h.y, x.z - h.z, x.w - h.w);
+            }
+            fence_async_smem();
+            mbar_arrive(smem_u32(&ready[s]));
+            if (i > 0) drain(i - 1);
+            if (!ok) break;
+        }
+        if (ok && !*abort_flag && nk > 0) drain(nk - 1);
+        // store (warp-uniform: the shuffles are collective)
+        const bool go = __all_sync(0xffffffffu, ok && !*abort_flag && nk > 0);
+        if (go) {
+            const int row = tile_m * kBM + 32 * q + lane;  // real row of C
+            const bool row_ok = row < M2;
+            const bool im = row & 1;
+            const bool use_beta = (beta.x != 0.f || beta.y != 0.f);
+#pragma unroll
+            for (int j = 0; j < BN; ++j) {
+                const int n = tile_n * BN + j;
+                const bool valid = row_ok && n < N;
+                const float v = acc[j];
+                const float partner = __shfl_xor_sync(0xffffffffu, v, 1);
+                if (ws) {
+                    if (valid) ws[(size_t(split) * N + n) * size_t(M2) + row] = v;
+                    continue;
+                }
+                // (alpha * acc): re = ar*vr - ai*vi, im = ar*vi + ai*vr
+                float out = im ? alpha.x * v + alpha.y * partner : alpha.x * v - alpha.y * partner;
+                float* cp = C + size_t(n) * ldc2 + row;
+                const float cs = (use_beta && valid) ? *cp : 0.f;
+                const float cpart = __shfl_xor_sync(0xffffffffu, cs, 1);
+                if (use_beta) out += im ? beta.x * cs + beta.y * cpart : beta.x * cs - beta.y * cpart;
+                if (valid) *cp = out;
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(unsigned(2 * BN)));
+    }
+}
+
+// C (+)= sum over splits, with alpha / beta, deterministic order
+__global__ void k_splitk_reduce(int M2, int N, int splits, const float* __restrict__ ws, float2 alpha, float2 beta,
+                                float* __restrict__ C, long ldc2) {
+    const long total = long(M2 / 2) * N;
+    for (long t = blockIdx.x * long(blockDim.x) + threadIdx.x; t < total; t += long(gridDim.x) * blockDim.x) {
+        const int n = int(t / (M2 / 2));
+        const int a = int(t - long(n) * (M2 / 2));
+        float sr = 0.f, si = 0.f;
+        for (int s = 0; s < splits; ++s) {
+            const float* w = ws + (size_t(s) * N + n) * size_t(M2) + 2 * a;
+            sr += w[0];
+            si += w[1];
+        }
+        float* cp = C + size_t(n) * ldc2 + 2 * a;
+        float orr = alpha.x * sr - alpha.y * si, oi = alpha.x * si + alpha.y * sr;
+        if (beta.x != 0.f || beta.y != 0.f) {
+            const float cr = cp[0], ci = cp[1];
+            orr += beta.x * cr - beta.y * ci;
+            oi += beta.x * ci + beta.y * cr;
+        }
+        cp[0] = orr;
+        cp[1] = oi;
+    }
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    });
+    B200_CHECK(fn != nullptr, kCudaError, "cuTensorMapEncodeTiled entry point not available");
+    return fn;
+}
+
+// 2-D fp32 tensor map: inner extent `inner` floats, `outer` rows of pitch `pitch_floats`
+CUtensorMap make_map(const void* base, long inner, long outer, long pitch_floats, unsigned box_inner, unsigned box_outer) {
+    CUtensorMap m;
+    const cuuint64_t dims[2] = {cuuint64_t(inner), cuuint64_t(outer)};
+    const cuuint64_t strides[1] = {cuuint64_t(pitch_floats) * 4};
+    const cuuint32_t box[2] = {box_inner, box_outer};
+    const cuuint32_t estr[2] = {1, 1};
+    const CUresult r = get_encode()(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<void*>(base), dims, strides, box,
+                                    estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                                    CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    B200_CHECK(r == CUDA_SUCCESS, kInvalidArgument, "cuTensorMapEncodeTiled failed (code " + std::to_string(int(r)) + ")");
+    return m;
+}
+
+template <int BN, int OPA> void set_attr_once() {
+    static std::once_flag once;
+    std::call_once(once, [] {
+        B200_CUDA(cudaFuncSetAttribute(k_tc_cgemm<BN, OPA>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       TileBytes<BN>::total));
+    });
+}
+
+template <int BN, int OPA>
+void launch(int M, int N, int K, float2 alpha, const float2* A, int lda, const float2* B, int ldb, float2 beta, float2* C,
+            int ldc, TcGemmWorkspace& w, cudaStream_t s) {
+    const int M2 = 2 * M, K2 = 2 * K;
+    CUtensorMap mA = (OPA == 1) ? make_map(A, 2L * K, M, 2L * lda, 32, 64)   // rows of A^H = columns of A
+                                : make_map(A, 2L * M, K, 2L * lda, 32, 16);  // columns of A, MN-major
+    CUtensorMap mB = make_map(B, 2L * K, N, 2L * ldb, 32, BN);
+    const int tm = (M2 + kBM - 1) / kBM, tn = (N + BN - 1) / BN;
+    const int nk = (K2 + kBK - 1) / kBK;
+    // split K until the grid covers the 148 SMs (at least 4 stages per split)
+    int splits = 1;
+    while (tm * tn * splits < 148 && nk / (splits * 2) >= 4) splits *= 2;
+    const int per = (nk + splits - 1) / splits;
+    splits = (nk + per - 1) / per;
+    float* ws = nullptr;
+    if (splits > 1) {
+        w.ws.resize(size_t(splits) * N * M2);
+        ws = w.ws.ptr;
+    }
+    set_attr_once<BN, OPA>();
+    k_tc_cgemm<BN, OPA><<<dim3(tm, tn, splits), kThreads, TileBytes<BN>::total, s>>>(
+        mA, mB, M2, N, K2, per, alpha, beta, reinterpret_cast<float*>(C), 2L * ldc, ws, w.err.ptr);
+    note_launch();
+    B200_CUDA(cudaGetLastError());
+    if (splits > 1) {
+        const long total = long(M) * N;
+        int blocks = int((total + 255) / 256);
+        if (blocks > 148 * 8) blocks = 148 * 8;
+        k_splitk_reduce<<<blocks, 256, 0, s>>>(M2, N, splits, ws, alpha, beta, reinterpret_cast<float*>(C), 2L * ldc);
+        note_launch();
+        B200_CUDA(cudaGetLastError());
+    }
+}
+
+}  // namespace
+
+void TcGemmWorkspace::ensure() {
+    if (!err.ptr) {
+        err.resize(1);
+        B200_CUDA(cudaMemset(err.ptr, 0, sizeof(int)));
+    }
+}
+
+int TcGemmWorkspace::read_error() {
+    int h = 0;
+    if (err.ptr) B200_CUDA(cudaMemcpy(&h, err.ptr, sizeof(int), cudaMemcpyDeviceToHost));
+    return h;
+}
+
+void tc_cgemm(char opa, int M, int N, int K, float2 alpha, const float2* A, int lda, const float2* B, int ldb,
+              float2 beta, float2* C, int ldc, TcGemmWorkspace& w, cudaStream_t s) {
+    B200_CHECK(opa == 'N' || opa == 'C', kInvalidArgument, "tc_cgemm: op(A) must be 'N' or 'C'");
+    B200_CHECK(M > 0 && N > 0 && K > 0, kInvalidArgument, "tc_cgemm: empty problem");
+    B200_CHECK(lda % 2 == 0 && ldb % 2 == 0, kInvalidArgument,
+               "tc_cgemm: lda and ldb must be even (16-byte row pitch for TMA)");
+    B200_CHECK(ldc >= M, kInvalidArgument, "tc_cgemm: ldc < M");
+    B200_CHECK((reinterpret_cast<uintptr_t>(A) & 15) == 0 && (reinterpret_cast<uintptr_t>(B) & 15) == 0, kInvalidArgument,
+               "tc_cgemm: A and B must be 16-byte aligned");
+    B200_CHECK(opa == 'C' ? lda >= K : lda >= M, kInvalidArgument, "tc_cgemm: lda too small");
+    B200_CHECK(ldb >= K, kInvalidArgument, "tc_cgemm: ldb < K");
+    w.ensure();
+    if (N <= 64) {
+        if (opa == 'N') launch<64, 0>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, w, s);
+        else launch<64, 1>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, w, s);
+    } else {
+        if (opa == 'N') launch<128, 0>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, w, s);
+        else launch<128, 1>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, w, s);
+    }
+}
+
+}  // namespace b200

@@ -88,6 +88,21 @@ def set_real_to_recip_output_op(npw_k, nxyz, add, factor, box_index, inp, out, s
     call(f, npw_k, nxyz, int(add), factor, ptr(box_index), ptr(inp), ptr(out), stream_ptr(stream))
 
 
+def tc_cgemm(transa, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, stream=None):
+    """gemm_op<complex<float>, DEVICE_GPU> on the tensor cores (3xTF32 split precision):
+    C = alpha*op(A)*B + beta*C, column-major complex64, transa 'N' or 'C', transb 'N'."""
+    alpha = complex(alpha)
+    beta = complex(beta)
+    call("b200_tc_cgemm", transa.encode(), b"N", m, n, k, alpha.real, alpha.imag, ptr(a), lda, ptr(b), ldb,
+         beta.real, beta.imag, ptr(c), ldc, stream_ptr(stream))
+
+
+def tc_cgemm_error():
+    code = C.c_int()
+    call("b200_tc_cgemm_error", C.byref(code))
+    return code.value
+
+
 # ------------------------------------------------------------------ basis
 class PWBasisK:
     """ModulePW::PW_Basis_K for one pool: grid, G sphere, index maps, device transforms."""

@@ -172,6 +172,17 @@ int b200_hamilt_hpsi_part(b200_hamilt* h, int ik, int spin, int nbands, int ld, 
 int b200_hamilt_hpsi_local_noalloc(b200_hamilt* h, int ik, int nbands, int ld, const void* psi_d, void* hpsi_d,
                                    void* stream);
 
+/* gemm_op<std::complex<float>, DEVICE_GPU> (module_hsolver/kernels/math_kernel_op.h:240-265) on the
+ * tensor cores: C = alpha * op(A) * B + beta * C, complex64 column-major, transa 'N' or 'C', transb 'N'.
+ * Split precision (3xTF32: hi*hi + hi*lo + lo*hi, FP32 accumulate), about FP32 accuracy.
+ * lda and ldb must be even and A, B 16-byte aligned (TMA row pitch); other shapes return
+ * B200_STATUS_INVALID_ARGUMENT. */
+int b200_tc_cgemm(char transa, char transb, int m, int n, int k, float alpha_re, float alpha_im, const void* a_d,
+                  int lda, const void* b_d, int ldb, float beta_re, float beta_im, void* c_d, int ldc, void* stream);
+/* Error word of the calling thread's tensor-core GEMMs (synchronous read): nonzero if a bounded
+ * wait inside a kernel ran out (the kernel then returned without finishing its tile). */
+int b200_tc_cgemm_error(int* code);
+
 /* ------------------------------------------------------------------ Davidson
  * hsolver::DiagoDavid<T, DEVICE_GPU> (module_hsolver/diago_david.h:19-84):
  * constructor (precondition, nband, dim, david_ndim, use_paw = false) and
