@@ -1,0 +1,212 @@
+// Warp-synchronous forms of the three fused local H|psi> passes for the grid sizes
+// of the standard workloads (18, 36, 45, 90, 96, 125, 128 along z; square xy
+// planes of 18, 36, 45, 96, 125, 128).  Same data layouts and results as the
+// generic kernels in fft_kernels.cu; each 1-D transform is done by one warp with
+// compile-time radices (fft_warp.cuh), so a CTA needs only a handful of block
+// barriers.  Other sizes use the generic kernels.
+#include "fft_warp.cuh"
+#include "pw_grid.h"
+
+namespace b200 {
+
+namespace {
+
+template <typename T> __device__ __forceinline__ T zero_c() { return cmake<T>(0, 0); }
+
+constexpr int kZWarps = 8;       // z passes: 8 warps, 16 sticks per CTA
+constexpr int kPlaneWarps = 16;  // plane pass: 16 warps per (band, z)
+
+template <typename T, int NZ>
+__global__ void __launch_bounds__(kZWarps * 32) k_zinv_w(StickMapView sm, const T* __restrict__ twz,
+                                                        const T* __restrict__ psi, int ld, T* __restrict__ sb) {
+    constexpr int LDZ = NZ | 1;
+    __shared__ T A[kStickTile * LDZ];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int s0 = blockIdx.x * kStickTile;
+    const int ns = min(kStickTile, sm.nst - s0);
+    const int band = blockIdx.y;
+    for (int i = tid; i < kStickTile * LDZ; i += kZWarps * 32) A[i] = zero_c<T>();
+    __syncthreads();
+    const T* p = psi + size_t(band) * ld;
+    const int j0 = sm.gofs[s0], j1 = sm.gofs[s0 + ns];
+    for (int j = j0 + tid; j < j1; j += kZWarps * 32) {
+        const int pk = sm.gpk[j];
+        A[((pk >> 10) - s0) * LDZ + (pk & 1023)] = p[sm.glist[j]];
+    }
+    __syncthreads();
+    for (int sl = warp; sl < ns; sl += kZWarps) fft_warp<T, +1, NZ>(A + sl * LDZ, lane, twz);
+    __syncthreads();
+    T* out = sb + size_t(band) * NZ * sm.nst;
+    for (int i = tid; i < ns * NZ; i += kZWarps * 32) {
+        const int z = i / ns;
+        const int sl = i - z * ns;
+        out[size_t(z) * sm.nst + s0 + sl] = A[sl * LDZ + z];
+    }
+}
+
+template <typename T, typename R, int NZ>
+__global__ void __launch_bounds__(kZWarps * 32) k_zfwd_w(StickMapView sm, const T* __restrict__ twz,
+                                                        const T* __restrict__ sb, const T* __restrict__ psi,
+                                                        T* __restrict__ hpsi, int ld, int npw,
+                                                        const R* __restrict__ gk2, R tpiba2, R invn, int accumulate) {
+    constexpr int LDZ = NZ | 1;
+    __shared__ T A[kStickTile * LDZ];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int s0 = blockIdx.x * kStickTile;
+    const int ns = min(kStickTile, sm.nst - s0);
+    const int band = blockIdx.y;
+    const T* in = sb + size_t(band) * NZ * sm.nst;
+    for (int i = tid; i < ns * NZ; i += kZWarps * 32) {
+        const int z = i / ns;
+        const int sl = i - z * ns;
+        A[sl * LDZ + z] = in[size_t(z) * sm.nst + s0 + sl];
+    }
+    __syncthreads();
+    for (int sl = warp; sl < ns; sl += kZWarps) fft_warp<T, -1, NZ>(A + sl * LDZ, lane, twz);
+    __syncthreads();
+    const T* p = psi + size_t(band) * ld;
+    T* h = hpsi + size_t(band) * ld;
+    const int j0 = sm.gofs[s0], j1 = sm.gofs[s0 + ns];
+    for (int j = j0 + tid; j < j1; j += kZWarps * 32) {
+        const int pk = sm.gpk[j];
+        const int g = sm.glist[j];
+        T v = cscale(A[((pk >> 10) - s0) * LDZ + (pk & 1023)], invn);
+        v = cadd(v, cscale(p[g], gk2[g] * tpiba2));
+        if (accumulate) v = cadd(v, h[g]);
+        h[g] = v;
+    }
+    if (!accumulate && blockIdx.x == 0)
+        for (int g = npw + tid; g < ld; g += kZWarps * 32) h[g] = zero_c<T>();
+}
+
+template <typename T, typename R, int NX, int NY>
+__global__ void __launch_bounds__(kPlaneWarps * 32) k_plane_w(PlaneMapView pm, int nz, const T* __restrict__ twx,
+                                                             const T* __restrict__ twy, const R* __restrict__ veff_zyx,
+                                                             T* __restrict__ sb) {
+    constexpr int LDY = NY | 1;
+    constexpr int NT = kPlaneWarps * 32;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* rows = reinterpret_cast<T*>(smem_raw);  // kPlaneWarps private rows of NX
+    T* A = rows + kPlaneWarps * NX;            // nxc columns of LDY
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int band = blockIdx.x;
+    const int z = blockIdx.y;
+    const int nxc = pm.nxc;
+    for (int i = tid; i < nxc * LDY; i += NT) A[i] = zero_c<T>();
+    __syncthreads();
+    T* plane = sb + (size_t(band) * nz + z) * pm.nst;
+    for (int s = tid; s < pm.nst; s += NT) A[pm.xc[s] * LDY + pm.sy[s]] = plane[s];
+    __syncthreads();
+    for (int c = warp; c < nxc; c += kPlaneWarps) fft_warp<T, +1, NY>(A + c * LDY, lane, twy);
+    __syncthreads();
+    T* row = rows + warp * NX;
+    const R* vz = veff_zyx + size_t(z) * NY * NX;
+    for (int y = warp; y < NY; y += kPlaneWarps) {
+        for (int x = lane; x < NX; x += 32) row[x] = zero_c<T>();
+        __syncwarp();
+        for (int c = lane; c < nxc; c += 32) row[pm.xpos[c]] = A[c * LDY + y];
+        __syncwarp();
+        fft_warp<T, +1, NX>(row, lane, twx);
+        const R* vr = vz + y * NX;
+        for (int x = lane; x < NX; x += 32) row[x] = cscale(row[x], vr[x]);
+        __syncwarp();
+        fft_warp<T, -1, NX>(row, lane, twx);
+        for (int c = lane; c < nxc; c += 32) A[c * LDY + y] = row[pm.xpos[c]];
+        __syncwarp();
+    }
+    __syncthreads();
+    for (int c = warp; c < nxc; c += kPlaneWarps) fft_warp<T, -1, NY>(A + c * LDY, lane, twy);
+    __syncthreads();
+    for (int s = tid; s < pm.nst; s += NT) plane[s] = A[pm.xc[s] * LDY + pm.sy[s]];
+}
+
+template <typename T> const T* twp(const FftAxis& a);
+template <> const double2* twp<double2>(const FftAxis& a) { return a.tw64.ptr; }
+template <> const float2* twp<float2>(const FftAxis& a) { return a.tw32.ptr; }
+
+template <typename K> void smem_attr(K kernel, size_t bytes) {
+    if (bytes > 48 * 1024) B200_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
+}
+
+template <typename T, typename R, int NZ>
+void zpasses(bool inv, const PWGrid& g, int ik, int nb, int ld, const T* psi, T* hpsi, T* sb, double tpiba2,
+             int accumulate, cudaStream_t s) {
+    const dim3 grid(ceil_div(g.nst, kStickTile), nb);
+    if (inv) {
+        k_zinv_w<T, NZ><<<grid, kZWarps * 32, 0, s>>>(g.stick_view(ik), twp<T>(g.az), psi, ld, sb);
+        note_launch();
+    } else {
+        const KMap& km = g.kmaps[ik];
+        const R* gk2 = std::is_same<R, double>::value ? (const R*)km.gk2.ptr : (const R*)km.gk2f.ptr;
+        k_zfwd_w<T, R, NZ><<<grid, kZWarps * 32, 0, s>>>(g.stick_view(ik), twp<T>(g.az), sb, psi, hpsi, ld, km.npw,
+                                                        gk2, R(tpiba2), R(1.0 / double(g.nxyz())), accumulate);
+        note_launch();
+    }
+    B200_CUDA(cudaGetLastError());
+}
+
+template <typename T, typename R>
+bool zpass_dispatch(bool inv, const PWGrid& g, int ik, int nb, int ld, const T* psi, T* hpsi, T* sb, double tpiba2,
+                    int accumulate, cudaStream_t s) {
+    switch (g.nz) {
+        case 18: zpasses<T, R, 18>(inv, g, ik, nb, ld, psi, hpsi, sb, tpiba2, accumulate, s); return true;
+        case 36: zpasses<T, R, 36>(inv, g, ik, nb, ld, psi, hpsi, sb, tpiba2, accumulate, s); return true;
+        case 45: zpasses<T, R, 45>(inv, g, ik, nb, ld, psi, hpsi, sb, tpiba2, accumulate, s); return true;
+        case 90: zpasses<T, R, 90>(inv, g, ik, nb, ld, psi, hpsi, sb, tpiba2, accumulate, s); return true;
+        case 96: zpasses<T, R, 96>(inv, g, ik, nb, ld, psi, hpsi, sb, tpiba2, accumulate, s); return true;
+        case 125: zpasses<T, R, 125>(inv, g, ik, nb, ld, psi, hpsi, sb, tpiba2, accumulate, s); return true;
+        case 128: zpasses<T, R, 128>(inv, g, ik, nb, ld, psi, hpsi, sb, tpiba2, accumulate, s); return true;
+        default: return false;
+    }
+}
+
+template <typename T, typename R, int N>
+bool plane_launch(const PWGrid& g, int nb, const R* veff, T* sb, cudaStream_t s) {
+    const size_t smem = (size_t(kPlaneWarps) * N + size_t(g.nxc) * (N | 1)) * sizeof(T);
+    if (smem > 227 * 1024) return false;
+    smem_attr(k_plane_w<T, R, N, N>, smem);
+    k_plane_w<T, R, N, N><<<dim3(nb, g.nz), kPlaneWarps * 32, smem, s>>>(g.plane_view(), g.nz, twp<T>(g.ax),
+                                                                         twp<T>(g.ay), veff, sb);
+    note_launch();
+    B200_CUDA(cudaGetLastError());
+    return true;
+}
+
+template <typename T, typename R> bool plane_dispatch(const PWGrid& g, int nb, const R* veff, T* sb, cudaStream_t s) {
+    if (g.nx != g.ny) return false;
+    switch (g.nx) {
+        case 18: return plane_launch<T, R, 18>(g, nb, veff, sb, s);
+        case 36: return plane_launch<T, R, 36>(g, nb, veff, sb, s);
+        case 45: return plane_launch<T, R, 45>(g, nb, veff, sb, s);
+        case 96: return plane_launch<T, R, 96>(g, nb, veff, sb, s);
+        case 125: return plane_launch<T, R, 125>(g, nb, veff, sb, s);
+        case 128: return plane_launch<T, R, 128>(g, nb, veff, sb, s);
+        default: return false;
+    }
+}
+
+bool supported_z(int n) { return n == 18 || n == 36 || n == 45 || n == 90 || n == 96 || n == 125 || n == 128; }
+bool supported_xy(int nx, int ny) {
+    return nx == ny && (nx == 18 || nx == 36 || nx == 45 || nx == 96 || nx == 125 || nx == 128);
+}
+
+}  // namespace
+
+template <typename T, typename R>
+bool launch_hpsi_local_fast(const PWGrid& g, int ik, const R* veff_zyx, int nb, int ld, const T* psi, T* hpsi,
+                            T* stickbuf, double tpiba2, int accumulate, cudaStream_t s) {
+    if (!supported_z(g.nz) || !supported_xy(g.nx, g.ny)) return false;
+    const size_t smem = (size_t(kPlaneWarps) * g.nx + size_t(g.nxc) * (g.ny | 1)) * sizeof(T);
+    if (smem > 227 * 1024) return false;
+    zpass_dispatch<T, R>(true, g, ik, nb, ld, psi, hpsi, stickbuf, tpiba2, accumulate, s);
+    plane_dispatch<T, R>(g, nb, veff_zyx, stickbuf, s);
+    zpass_dispatch<T, R>(false, g, ik, nb, ld, psi, hpsi, stickbuf, tpiba2, accumulate, s);
+    return true;
+}
+
+template bool launch_hpsi_local_fast<double2, double>(const PWGrid&, int, const double*, int, int, const double2*,
+                                                      double2*, double2*, double, int, cudaStream_t);
+template bool launch_hpsi_local_fast<float2, float>(const PWGrid&, int, const float*, int, int, const float2*, float2*,
+                                                    float2*, double, int, cudaStream_t);
+
+}  // namespace b200

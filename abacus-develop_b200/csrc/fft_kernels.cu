@@ -416,6 +416,8 @@ void launch_hpsi_local(const PWGrid& g, int ik, const R* veff_zyx, int nb, int l
                        double tpiba2, int accumulate, cudaStream_t s) {
     if (nb <= 0) return;
     B200_CHECK(nb <= 65535, kInvalidArgument, "too many bands in one launch");
+    // compile-time warp transforms for the standard grid sizes; generic Stockham kernels otherwise
+    if (launch_hpsi_local_fast<T, R>(g, ik, veff_zyx, nb, ld, psi, hpsi, stickbuf, tpiba2, accumulate, s)) return;
     const size_t zs = zpass_smem(g, sizeof(T));
     const size_t ps = plane_smem(g, sizeof(T));
     B200_CHECK(ps <= 227 * 1024, kCapacityError, "plane pass does not fit in shared memory for this grid");

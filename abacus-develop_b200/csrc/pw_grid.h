@@ -92,6 +92,11 @@ size_t plane_smem(const PWGrid& g, size_t elem);
 template <typename T, typename R>
 void launch_hpsi_local(const PWGrid& g, int ik, const R* veff_zyx, int nb, int ld, const T* psi, T* hpsi, T* stickbuf,
                        double tpiba2, int accumulate, cudaStream_t s);
+// Same, with warp-synchronous compile-time transforms; returns false (launching nothing) for
+// grid sizes it does not cover.
+template <typename T, typename R>
+bool launch_hpsi_local_fast(const PWGrid& g, int ik, const R* veff_zyx, int nb, int ld, const T* psi, T* hpsi,
+                            T* stickbuf, double tpiba2, int accumulate, cudaStream_t s);
 // Drop-in transforms (PW_Basis_K::recip_to_real / real_to_recip on the GPU), one band.
 template <typename T>
 void launch_recip_to_real(const PWGrid& g, int ik, const T* in, T* out, T* aux, int add, double factor, cudaStream_t s);

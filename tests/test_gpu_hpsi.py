@@ -32,7 +32,7 @@ def _setup(pkg, spec, kpt=None, nb=None):
     return wl, ref, psi, nb, npwx
 
 
-@pytest.mark.parametrize("cfg", ["si2", "diamond8", "diamond8_k", "diamond16"])
+@pytest.mark.parametrize("cfg", ["si2", "diamond8", "diamond8_k", "diamond16", "diamond8_grid40"])
 def test_hpsi_fp64_matches_oracle(pkg, cfg):
     S = pkg.synth
     if cfg == "si2":
@@ -41,8 +41,11 @@ def test_hpsi_fp64_matches_oracle(pkg, cfg):
         spec, kpt, nb = S.config(0), None, 32
     elif cfg == "diamond8_k":
         spec, kpt, nb = S.config(0), np.array([0.125, -0.375, 0.375]), 12
-    else:
+    elif cfg == "diamond16":
         spec, kpt, nb = S.serving_cells()[2], None, 6
+    else:  # a grid outside the compiled warp-transform sizes exercises the generic kernels
+        import dataclasses
+        spec, kpt, nb = dataclasses.replace(S.config(0), grid=(40, 40, 40)), None, 10
     wl, ref, psi, nb, ld = _setup(pkg, spec, kpt, nb)
     href = ref.hpsi(psi, nb, ld)
     h = pkg.pwdft.device_hamilt(wl, pkg.pwdft.PREC_FP64)
