@@ -68,6 +68,8 @@ _SIGS = {
     "b200_david_diag": ([vp, HPSI_CB, vp, i32, vp, pf64, f64, i32, i32, i32, pi32], i32),
     "b200_david_diag_hamilt": ([vp, vp, i32, i32, i32, vp, pf64, f64, i32, i32, i32, pi32], i32),
     "b200_david_stats": ([vp, pi32, pi32, pi32], i32),
+    "b200_david_set_verbosity": ([vp, i32], i32),
+    "b200_david_set_mixed_threshold": ([vp, f64], i32),
 }
 
 _lib = None

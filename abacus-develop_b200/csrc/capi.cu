@@ -357,6 +357,18 @@ int b200_tc_cgemm_error(int* code) {
         *code = g_tc_ws.read_error();
     });
 }
+int b200_david_set_verbosity(b200_david* d, int level) {
+    return guarded([&] {
+        B200_CHECK(d != nullptr, b200::kInvalidArgument, "NULL argument");
+        d->d->set_verbosity(level);
+    });
+}
+int b200_david_set_mixed_threshold(b200_david* d, double thr) {
+    return guarded([&] {
+        B200_CHECK(d != nullptr && thr > 0.0, b200::kInvalidArgument, "bad argument");
+        d->d->set_mixed_thr(thr);
+    });
+}
 int b200_david_stats(const b200_david* d, int* iters_low, int* iters_fp64, int* hpsi_bands) {
     return guarded([&] {
         B200_CHECK(d != nullptr, b200::kInvalidArgument, "NULL argument");

@@ -22,12 +22,15 @@
 #include <cublas_v2.h>
 #include <cusolverDn.h>
 
+#include <chrono>
 #include <cmath>
+#include <cstdio>
 #include <vector>
 
 #include "common.h"
 #include "david.h"
 #include "fft_core.cuh"
+#include "gemm_tc.h"
 
 namespace b200 {
 
@@ -56,18 +59,22 @@ inline int grid_of(long n) {
 }
 
 template <typename T, typename R>
-__global__ void k_precond(long dim, int nc, T* __restrict__ v, const R* __restrict__ pc) {
+__global__ void k_precond(long dim, long ld, int nc, T* __restrict__ v, const R* __restrict__ pc) {
     const long n = dim * nc;
     for (long i = blockIdx.x * long(blockDim.x) + threadIdx.x; i < n; i += long(gridDim.x) * blockDim.x) {
-        const R p = pc[i % dim];
-        v[i] = cmake<T>(v[i].x / p, v[i].y / p);
+        const long m = i / dim;
+        const long g = i - m * dim;
+        const R p = pc[g];
+        T* x = v + m * ld + g;
+        *x = cmake<T>(x->x / p, x->y / p);
     }
 }
 
 // vc(:, m) = vcc(:nbase, unconv[m]); vcl(:, m) = -lambda_{unconv[m]} vc(:, m)
 template <typename T>
-__global__ void k_gather_cols(int nbase, int nbase_x, int nc, const int* __restrict__ unconv, const T* __restrict__ vcc,
-                              const double* __restrict__ w, T* __restrict__ vc, T* __restrict__ vcl) {
+__global__ void k_gather_cols(int nbase, int nbase_x, int nc, int ldv, const int* __restrict__ unconv,
+                              const T* __restrict__ vcc, const double* __restrict__ w, T* __restrict__ vc,
+                              T* __restrict__ vcl) {
     using R = typename RealOf<T>::type;
     const long n = long(nbase) * nc;
     for (long i = blockIdx.x * long(blockDim.x) + threadIdx.x; i < n; i += long(gridDim.x) * blockDim.x) {
@@ -75,8 +82,8 @@ __global__ void k_gather_cols(int nbase, int nbase_x, int nc, const int* __restr
         const int r = int(i - long(m) * nbase);
         const int col = unconv[m];
         const T v = vcc[long(col) * nbase_x + r];
-        vc[i] = v;
-        vcl[i] = cscale(v, R(-w[col]));
+        vc[long(m) * ldv + r] = v;
+        vcl[long(m) * ldv + r] = cscale(v, R(-w[col]));
     }
 }
 
@@ -134,40 +141,73 @@ template <> struct Lin<float2> {
     }
 };
 
+__global__ void k_identity(int n, int ld, double2* __restrict__ w) {
+    const long total = long(n) * ld;
+    for (long i = blockIdx.x * long(blockDim.x) + threadIdx.x; i < total; i += long(gridDim.x) * blockDim.x) {
+        const int c = int(i / ld), r = int(i - long(c) * ld);
+        w[i] = make_double2(r == c ? 1.0 : 0.0, 0.0);
+    }
+}
+
+inline int even(int n) { return n + (n & 1); }
+
+// Vectors of length dim are stored with stride ld (dim for FP64; dim rounded up to even for FP32 so
+// that every block is a valid TMA operand of the tensor-core GEMM).
 template <typename T> struct Engine {
     using R = typename RealOf<T>::type;
-    int nband, dim, nbase_x;
+    static constexpr bool kF32 = std::is_same<T, float2>::value;
+    int nband, dim, nbase_x, ld, L, ncp;
     cudaStream_t s = 0;
     cublasHandle_t cb = nullptr;
     cusolverDnHandle_t cs = nullptr;
     DeviceArray<T> basis, hp, newv, hcc, vcc, vc, vcl, lag, gram;
-    DeviceArray<double2> A64, gram64, work;
+    DeviceArray<double2> A64, gram64, winv, work;
     DeviceArray<double> w, ein;
     DeviceArray<R> pc;
     DeviceArray<int> unconv_d, info;
+    TcGemmWorkspace tcw;
     int lwork = 0;
     std::vector<double> eig_h;
     std::vector<int> unconv_h;
     bool ref_refresh = true;
     int hpsi_bands = 0;
+    int verbosity = 0;
+    // verbosity >= 2: synchronising phase timers (seconds) for H|psi>, subspace GEMMs / orthogonalisation, eigensolve
+    double t_hpsi = 0, t_lin = 0, t_eig = 0;
+    std::chrono::steady_clock::time_point tmark;
+    void tick() {
+        if (verbosity >= 2) {
+            B200_CUDA(cudaStreamSynchronize(s));
+            tmark = std::chrono::steady_clock::now();
+        }
+    }
+    void tock(double& acc) {
+        if (verbosity >= 2) {
+            B200_CUDA(cudaStreamSynchronize(s));
+            acc += std::chrono::duration<double>(std::chrono::steady_clock::now() - tmark).count();
+            tmark = std::chrono::steady_clock::now();
+        }
+    }
 
-    Engine(int nb, int d, int ndim, const double* precond_d) : nband(nb), dim(d), nbase_x(ndim * nb) {
+    Engine(int nb, int d, int ndim, const double* precond_d)
+        : nband(nb), dim(d), nbase_x(ndim * nb), ld(kF32 ? even(d) : d), L(even(ndim * nb)), ncp(even(nb)) {
         B200_CHECK(ndim > 1 && nb > 0 && ndim * nb < d, kInvalidArgument, "need david_ndim > 1 and david_ndim*nband < dim");
         B200_CUBLAS_D(cublasCreate(&cb));
         B200_CUSOLVER(cusolverDnCreate(&cs));
         B200_CUBLAS_D(cublasSetStream(cb, s));
         B200_CUSOLVER(cusolverDnSetStream(cs, s));
-        basis.resize(size_t(nbase_x) * dim);
-        hp.resize(size_t(nbase_x) * dim);
-        newv.resize(size_t(nband) * dim);
+        basis.resize(size_t(nbase_x) * ld);
+        hp.resize(size_t(nbase_x) * ld);
+        newv.resize(size_t(nband) * ld);
         hcc.resize(size_t(nbase_x) * nbase_x);
         vcc.resize(size_t(nbase_x) * nbase_x);
-        vc.resize(size_t(nbase_x) * nband);
-        vcl.resize(size_t(nbase_x) * nband);
-        lag.resize(size_t(nbase_x) * nband);
-        gram.resize(size_t(nband) * nband);
+        vc.resize(size_t(L) * nband);
+        vcl.resize(size_t(L) * nband);
+        lag.resize(size_t(L) * nband);
+        gram.resize(size_t(ncp) * ncp);
         A64.resize(size_t(nbase_x) * nbase_x);
-        gram64.resize(size_t(nband) * nband);
+        gram64.resize(size_t(ncp) * ncp);
+        winv.resize(size_t(ncp) * ncp);
         w.resize(nbase_x);
         ein.resize(nband);
         pc.resize(dim);
@@ -176,6 +216,8 @@ template <typename T> struct Engine {
         B200_CUDA(cudaMemsetAsync(hcc.ptr, 0, hcc.n * sizeof(T), s));
         B200_CUDA(cudaMemsetAsync(vcc.ptr, 0, vcc.n * sizeof(T), s));
         B200_CUDA(cudaMemsetAsync(basis.ptr, 0, basis.n * sizeof(T), s));
+        B200_CUDA(cudaMemsetAsync(hp.ptr, 0, hp.n * sizeof(T), s));
+        B200_CUDA(cudaMemsetAsync(newv.ptr, 0, newv.n * sizeof(T), s));
         B200_CUDA(cudaMemsetAsync(info.ptr, 0, 4 * sizeof(int), s));
         if constexpr (std::is_same<R, double>::value) {
             B200_CUDA(cudaMemcpyAsync(pc.ptr, precond_d, dim * sizeof(double), cudaMemcpyDeviceToDevice, s));
@@ -184,10 +226,14 @@ template <typename T> struct Engine {
             note_launch();
             B200_CUDA(cudaGetLastError());
         }
-        int l1 = 0, l2 = 0;
+        int l1 = 0, l2 = 0, l3 = 0, meig = 0;
         B200_CUSOLVER(cusolverDnZheevd_bufferSize(cs, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, nbase_x,
                                                   (cuDoubleComplex*)A64.ptr, nbase_x, w.ptr, &l1));
-        B200_CUSOLVER(cusolverDnZpotrf_bufferSize(cs, CUBLAS_FILL_MODE_UPPER, nband, (cuDoubleComplex*)gram64.ptr, nband, &l2));
+        B200_CUSOLVER(cusolverDnZheevdx_bufferSize(cs, CUSOLVER_EIG_MODE_VECTOR, CUSOLVER_EIG_RANGE_I,
+                                                   CUBLAS_FILL_MODE_LOWER, nbase_x, (cuDoubleComplex*)A64.ptr, nbase_x,
+                                                   0.0, 0.0, 1, nband, &meig, w.ptr, &l3));
+        l1 = l1 > l3 ? l1 : l3;
+        B200_CUSOLVER(cusolverDnZpotrf_bufferSize(cs, CUBLAS_FILL_MODE_UPPER, nband, (cuDoubleComplex*)gram64.ptr, ncp, &l2));
         lwork = l1 > l2 ? l1 : l2;
         work.resize(size_t(lwork > 0 ? lwork : 1));
         eig_h.assign(nbase_x, 0.0);
@@ -199,36 +245,54 @@ template <typename T> struct Engine {
         if (cs) cusolverDnDestroy(cs);
     }
 
+    // C = al op(A) B + be C; FP32 operands go to the tensor cores (3xTF32) whenever they are valid TMA operands
     void gemm(cublasOperation_t a, cublasOperation_t b, int m, int n, int k, T al, const T* A, int lda, const T* B,
               int ldb, T be, T* C, int ldc) {
         if (m <= 0 || n <= 0) return;
+        if constexpr (kF32) {
+            const bool aligned = ((reinterpret_cast<uintptr_t>(A) | reinterpret_cast<uintptr_t>(B)) & 15) == 0;
+            if (k > 0 && b == CUBLAS_OP_N && (a == CUBLAS_OP_N || a == CUBLAS_OP_C) && lda % 2 == 0 && ldb % 2 == 0 &&
+                aligned) {
+                tc_cgemm(a == CUBLAS_OP_N ? 'N' : 'C', m, n, k, al, A, lda, B, ldb, be, C, ldc, tcw, s);
+                return;
+            }
+        }
         Lin<T>::gemm(cb, a, b, m, n, k, al, A, lda, B, ldb, be, C, ldc);
     }
 
-    // X (dim x nc) <- X U^-1 with X^H X = U^H U, U from an FP64 Cholesky
+    // X (dim x nc, stride ld) <- X U^-1 with X^H X = U^H U, U from an FP64 Cholesky
     void cholqr(T* X, int nc) {
-        Lin<T>::herk(cb, nc, dim, X, dim, gram.ptr, nc);
-        const long n2 = long(nc) * nc;
+        const T one = cmake<T>(1, 0), zero = cmake<T>(0, 0);
+        const long n2 = long(ncp) * nc;
         double2* G = gram64.ptr;
-        if constexpr (std::is_same<T, double2>::value) {
+        if constexpr (!kF32) {
+            Lin<T>::herk(cb, nc, dim, X, ld, gram.ptr, ncp);
             B200_CUDA(cudaMemcpyAsync(G, gram.ptr, n2 * sizeof(double2), cudaMemcpyDeviceToDevice, s));
         } else {
+            gemm(CUBLAS_OP_C, CUBLAS_OP_N, nc, nc, dim, one, X, ld, X, ld, zero, gram.ptr, ncp);
             k_convert<T, double2><<<grid_of(n2), kT, 0, s>>>(n2, gram.ptr, G);
             note_launch();
             B200_CUDA(cudaGetLastError());
         }
-        B200_CUSOLVER(cusolverDnZpotrf(cs, CUBLAS_FILL_MODE_UPPER, nc, (cuDoubleComplex*)G, nc, (cuDoubleComplex*)work.ptr,
+        B200_CUSOLVER(cusolverDnZpotrf(cs, CUBLAS_FILL_MODE_UPPER, nc, (cuDoubleComplex*)G, ncp, (cuDoubleComplex*)work.ptr,
                                        lwork, info.ptr + 1));
-        const T* U;
-        if constexpr (std::is_same<T, double2>::value) {
-            U = G;
+        if constexpr (!kF32) {
+            Lin<T>::trsm(cb, dim, nc, G, ncp, X, ld);
         } else {
-            k_convert<double2, T><<<grid_of(n2), kT, 0, s>>>(n2, G, gram.ptr);
+            // U^-1 in FP64 (triangular solve against I), then X U^-1 as one tensor-core GEMM
+            k_identity<<<grid_of(n2), kT, 0, s>>>(nc, ncp, winv.ptr);
             note_launch();
             B200_CUDA(cudaGetLastError());
-            U = gram.ptr;
+            const double2 done = make_double2(1.0, 0.0);
+            B200_CUBLAS_D(cublasZtrsm(cb, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, nc, nc,
+                                      (const cuDoubleComplex*)&done, (const cuDoubleComplex*)G, ncp,
+                                      (cuDoubleComplex*)winv.ptr, ncp));
+            k_convert<double2, T><<<grid_of(n2), kT, 0, s>>>(n2, winv.ptr, gram.ptr);
+            note_launch();
+            B200_CUDA(cudaGetLastError());
+            gemm(CUBLAS_OP_N, CUBLAS_OP_N, dim, nc, nc, one, X, ld, gram.ptr, ncp, zero, newv.ptr, ld);
+            B200_CUDA(cudaMemcpyAsync(X, newv.ptr, size_t(nc) * ld * sizeof(T), cudaMemcpyDeviceToDevice, s));
         }
-        Lin<T>::trsm(cb, dim, nc, U, nc, X, dim);
     }
 
     // orthonormalise X (dim x nc) against basis[:, :nprev] and within itself
@@ -236,8 +300,8 @@ template <typename T> struct Engine {
         const T one = cmake<T>(1, 0), zero = cmake<T>(0, 0), mone = cmake<T>(-1, 0);
         for (int pass = 0; pass < 2; ++pass) {
             if (nprev > 0) {
-                gemm(CUBLAS_OP_C, CUBLAS_OP_N, nprev, nc, dim, one, basis.ptr, dim, X, dim, zero, lag.ptr, nprev);
-                gemm(CUBLAS_OP_N, CUBLAS_OP_N, dim, nc, nprev, mone, basis.ptr, dim, lag.ptr, nprev, one, X, dim);
+                gemm(CUBLAS_OP_C, CUBLAS_OP_N, nprev, nc, dim, one, basis.ptr, ld, X, ld, zero, lag.ptr, L);
+                gemm(CUBLAS_OP_N, CUBLAS_OP_N, dim, nc, nprev, mone, basis.ptr, ld, lag.ptr, L, one, X, ld);
             }
             cholqr(X, nc);
         }
@@ -245,11 +309,12 @@ template <typename T> struct Engine {
 
     void cal_elem(int nbase, int nc) {
         const T one = cmake<T>(1, 0), zero = cmake<T>(0, 0);
-        gemm(CUBLAS_OP_C, CUBLAS_OP_N, nc, nbase + nc, dim, one, basis.ptr + size_t(nbase) * dim, dim, hp.ptr, dim, zero,
+        gemm(CUBLAS_OP_C, CUBLAS_OP_N, nc, nbase + nc, dim, one, basis.ptr + size_t(nbase) * ld, ld, hp.ptr, ld, zero,
              hcc.ptr + nbase, nbase_x);
     }
 
     void eigsolve(int nbase) {
+        tick();
         const long n = long(nbase_x) * nbase;
         if constexpr (std::is_same<T, double2>::value) {
             B200_CUDA(cudaMemcpyAsync(A64.ptr, hcc.ptr, n * sizeof(double2), cudaMemcpyDeviceToDevice, s));
@@ -258,9 +323,18 @@ template <typename T> struct Engine {
             note_launch();
             B200_CUDA(cudaGetLastError());
         }
-        B200_CUSOLVER(cusolverDnZheevd(cs, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, nbase,
-                                       (cuDoubleComplex*)A64.ptr, nbase_x, w.ptr, (cuDoubleComplex*)work.ptr, lwork,
-                                       info.ptr));
+        // lowest nband eigenpairs only (the reference's zheevx range 'I', dngvd_op.cpp:142-235): divide and
+        // conquer on the tridiagonal form, back-transforming nband vectors instead of nbase
+        if (nbase > nband) {
+            int meig = 0;
+            B200_CUSOLVER(cusolverDnZheevdx(cs, CUSOLVER_EIG_MODE_VECTOR, CUSOLVER_EIG_RANGE_I, CUBLAS_FILL_MODE_LOWER,
+                                            nbase, (cuDoubleComplex*)A64.ptr, nbase_x, 0.0, 0.0, 1, nband, &meig, w.ptr,
+                                            (cuDoubleComplex*)work.ptr, lwork, info.ptr));
+        } else {
+            B200_CUSOLVER(cusolverDnZheevd(cs, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, nbase,
+                                           (cuDoubleComplex*)A64.ptr, nbase_x, w.ptr, (cuDoubleComplex*)work.ptr, lwork,
+                                           info.ptr));
+        }
         const long nv = long(nbase_x) * nband;
         if constexpr (std::is_same<T, double2>::value) {
             B200_CUDA(cudaMemcpyAsync(vcc.ptr, A64.ptr, nv * sizeof(double2), cudaMemcpyDeviceToDevice, s));
@@ -278,31 +352,39 @@ template <typename T> struct Engine {
         B200_CHECK(hinfo[0] == 0, kNumericalError, "subspace eigensolver failed, info " + std::to_string(hinfo[0]));
         for (int m = 0; m < nband; ++m)
             B200_CHECK(std::isfinite(eig_h[m]), kNumericalError, "non-finite eigenvalue (NaN/Inf in H|psi> or psi)");
+        tock(t_eig);
+        if constexpr (kF32) {
+            const int e = tcw.err.ptr ? tcw.read_error() : 0;
+            B200_CHECK(e == 0, kCudaError, "tensor-core GEMM wait ran out (error word " + std::to_string(e) + ")");
+        }
     }
 
     void cal_grad(const HPsiDevice& f, int nbase, int nc) {
         const T one = cmake<T>(1, 0), zero = cmake<T>(0, 0);
+        tick();
         B200_CUDA(cudaMemcpyAsync(unconv_d.ptr, unconv_h.data(), nc * sizeof(int), cudaMemcpyHostToDevice, s));
-        k_gather_cols<T><<<grid_of(long(nbase) * nc), kT, 0, s>>>(nbase, nbase_x, nc, unconv_d.ptr, vcc.ptr, w.ptr, vc.ptr,
-                                                                  vcl.ptr);
+        k_gather_cols<T><<<grid_of(long(nbase) * nc), kT, 0, s>>>(nbase, nbase_x, nc, L, unconv_d.ptr, vcc.ptr, w.ptr,
+                                                                  vc.ptr, vcl.ptr);
         note_launch();
         B200_CUDA(cudaGetLastError());
-        T* X = basis.ptr + size_t(nbase) * dim;
-        gemm(CUBLAS_OP_N, CUBLAS_OP_N, dim, nc, nbase, one, hp.ptr, dim, vc.ptr, nbase, zero, X, dim);
-        gemm(CUBLAS_OP_N, CUBLAS_OP_N, dim, nc, nbase, one, basis.ptr, dim, vcl.ptr, nbase, one, X, dim);
-        k_precond<T, R><<<grid_of(long(dim) * nc), kT, 0, s>>>(dim, nc, X, pc.ptr);
+        T* X = basis.ptr + size_t(nbase) * ld;
+        gemm(CUBLAS_OP_N, CUBLAS_OP_N, dim, nc, nbase, one, hp.ptr, ld, vc.ptr, L, zero, X, ld);
+        gemm(CUBLAS_OP_N, CUBLAS_OP_N, dim, nc, nbase, one, basis.ptr, ld, vcl.ptr, L, one, X, ld);
+        k_precond<T, R><<<grid_of(long(dim) * nc), kT, 0, s>>>(dim, ld, nc, X, pc.ptr);
         note_launch();
         B200_CUDA(cudaGetLastError());
         orth_block(X, nc, nbase);
-        f(basis.ptr, hp.ptr + size_t(nbase) * dim, nbase_x, dim, nbase, nbase + nc - 1, s);
+        tock(t_lin);
+        f(basis.ptr, hp.ptr + size_t(nbase) * ld, nbase_x, ld, nbase, nbase + nc - 1, s);
         hpsi_bands += nc;
+        tock(t_hpsi);
     }
 
     void refresh(int nbase, const double* eig_in, T* psi, int ldpsi) {
         const T one = cmake<T>(1, 0), zero = cmake<T>(0, 0);
-        gemm(CUBLAS_OP_N, CUBLAS_OP_N, dim, nband, nbase, one, hp.ptr, dim, vcc.ptr, nbase_x, zero, newv.ptr, dim);
-        B200_CUDA(cudaMemcpyAsync(hp.ptr, newv.ptr, size_t(nband) * dim * sizeof(T), cudaMemcpyDeviceToDevice, s));
-        B200_CUDA(cudaMemcpy2DAsync(basis.ptr, dim * sizeof(T), psi, size_t(ldpsi) * sizeof(T), dim * sizeof(T), nband,
+        gemm(CUBLAS_OP_N, CUBLAS_OP_N, dim, nband, nbase, one, hp.ptr, ld, vcc.ptr, nbase_x, zero, newv.ptr, ld);
+        B200_CUDA(cudaMemcpyAsync(hp.ptr, newv.ptr, size_t(nband) * ld * sizeof(T), cudaMemcpyDeviceToDevice, s));
+        B200_CUDA(cudaMemcpy2DAsync(basis.ptr, ld * sizeof(T), psi, size_t(ldpsi) * sizeof(T), dim * sizeof(T), nband,
                                     cudaMemcpyDeviceToDevice, s));
         B200_CUDA(cudaMemsetAsync(hcc.ptr, 0, hcc.n * sizeof(T), s));
         if (!ref_refresh) B200_CUDA(cudaMemsetAsync(vcc.ptr, 0, vcc.n * sizeof(T), s));
@@ -315,10 +397,10 @@ template <typename T> struct Engine {
     int diag_once(const HPsiDevice& f, int ldpsi, T* psi, double* eig_in, double thr, int maxiter, int& notconv) {
         const T one = cmake<T>(1, 0), zero = cmake<T>(0, 0);
         B200_CUDA(cudaMemsetAsync(info.ptr, 0, 4 * sizeof(int), s));
-        B200_CUDA(cudaMemcpy2DAsync(basis.ptr, dim * sizeof(T), psi, size_t(ldpsi) * sizeof(T), dim * sizeof(T), nband,
+        B200_CUDA(cudaMemcpy2DAsync(basis.ptr, ld * sizeof(T), psi, size_t(ldpsi) * sizeof(T), dim * sizeof(T), nband,
                                     cudaMemcpyDeviceToDevice, s));
         orth_block(basis.ptr, nband, 0);
-        f(basis.ptr, hp.ptr, nbase_x, dim, 0, nband - 1, s);
+        f(basis.ptr, hp.ptr, nbase_x, ld, 0, nband - 1, s);
         hpsi_bands += nband;
         cal_elem(0, nband);
         int nbase = nband;
@@ -330,17 +412,25 @@ template <typename T> struct Engine {
         while (true) {
             ++iter;
             cal_grad(f, nbase, notconv);
+            tick();
             cal_elem(nbase, notconv);
+            tock(t_lin);
             nbase += notconv;
             eigsolve(nbase);
             notconv = 0;
+            double dmax = 0.0;
             for (int m = 0; m < nband; ++m) {
-                if (!(std::fabs(eig_h[m] - eig_in[m]) < thr)) unconv_h[notconv++] = m;
+                const double de = std::fabs(eig_h[m] - eig_in[m]);
+                dmax = de > dmax ? de : dmax;
+                if (!(de < thr)) unconv_h[notconv++] = m;
                 eig_in[m] = eig_h[m];
             }
+            if (verbosity > 0)
+                std::fprintf(stderr, "[david %s] iter %3d nbase %4d notconv %4d max|dE| %.3e  t(hpsi/lin/eig) %.3f %.3f %.3f\n",
+                             kF32 ? "fp32" : "fp64", iter, nbase, notconv, dmax, t_hpsi, t_lin, t_eig);
             if (notconv == 0 || nbase + notconv > nbase_x || iter == maxiter) {
                 B200_CUDA(cudaMemsetAsync(psi, 0, size_t(nband) * ldpsi * sizeof(T), s));
-                gemm(CUBLAS_OP_N, CUBLAS_OP_N, dim, nband, nbase, one, basis.ptr, dim, vcc.ptr, nbase_x, zero, psi, ldpsi);
+                gemm(CUBLAS_OP_N, CUBLAS_OP_N, dim, nband, nbase, one, basis.ptr, ld, vcc.ptr, nbase_x, zero, psi, ldpsi);
                 if (notconv == 0 || iter == maxiter) break;
                 refresh(nbase, eig_in, psi, ldpsi);
                 nbase = nband;
@@ -390,6 +480,7 @@ class David : public DavidBase {
         if (precision == 1) {
             if (!e32_) e32_ = std::make_unique<Engine<float2>>(nband_, dim_, ndim_, pc_.ptr);
             e32_->ref_refresh = e64_->ref_refresh;
+            e32_->verbosity = verbosity_;
             e32_->hpsi_bands = 0;
             psi32_.resize(size_t(nband_) * ldpsi);
             const long n = long(nband_) * ldpsi;
@@ -415,6 +506,11 @@ class David : public DavidBase {
     const DavidStats& stats() const override { return stats_; }
     void set_mixed_thr(double thr) override { mixed_thr_ = thr; }
     int precision() const override { return precision_; }
+    void set_verbosity(int level) override {
+        verbosity_ = level;
+        e64_->verbosity = level;
+        if (e32_) e32_->verbosity = level;
+    }
     void set_reference_refresh(bool on) override {
         e64_->ref_refresh = on;
         if (e32_) e32_->ref_refresh = on;
@@ -423,7 +519,8 @@ class David : public DavidBase {
   private:
     int nband_, dim_, ndim_, precision_;
     int notconv_ = 0;
-    double mixed_thr_ = 1e-5;
+    int verbosity_ = 0;
+    double mixed_thr_ = 1e-6;
     DeviceArray<double> pc_;
     DeviceArray<float2> psi32_;
     std::unique_ptr<Engine<double2>> e64_;

@@ -29,6 +29,9 @@ struct DavidBase {
     virtual void set_mixed_thr(double thr) = 0;
     virtual void set_reference_refresh(bool on) = 0;
     virtual int precision() const = 0;
+    // 0 = quiet; 1 = one line per Davidson iteration on stderr (iteration, basis size, unconverged bands,
+    // largest eigenvalue change), the role of DiagoDavid's test_david levels (diago_david.cpp:53-58)
+    virtual void set_verbosity(int level) = 0;
 };
 
 std::unique_ptr<DavidBase> make_david(int nband, int dim, int david_ndim, int precision, const double* precond_d);

@@ -17,9 +17,9 @@
 // the row multiplied by i (pairs (a, b) -> (-b, a)).  The same pass writes the
 // hi/lo split, so nothing is pre-processed in HBM.
 //
-// CTA: 6 warps.  warp 0 issues TMA loads (cp.async.bulk.tensor, no multicast),
-// warp 1 allocates TMEM and one lane issues tcgen05.mma, warps 2-5 split/expand
-// the tiles and then run the epilogue (tcgen05.ld -> alpha/beta -> global).
+// CTA: 10 warps.  warp 0 issues TMA loads (cp.async.bulk.tensor, no multicast),
+// warp 1 allocates TMEM and one lane issues tcgen05.mma, warps 2-9 split/expand
+// the tiles, drain TMEM and run the epilogue (alpha/beta -> global).
 // 3-stage mbarrier pipeline, two TMEM accumulators.  Every wait is bounded in time; a wait that runs out
 // sets an error word, the CTA drains its own copies in flight, frees TMEM and
 // returns.  Long K is split across CTAs (grid.z) with a deterministic reduction.
@@ -37,7 +37,7 @@ namespace {
 constexpr int kBM = 128;     // real rows of C per tile
 constexpr int kBK = 32;      // real K per stage (one 128-byte swizzle row of fp32)
 constexpr int kStages = 3;
-constexpr int kThreads = 192;
+constexpr int kThreads = 320;   // warp 0 TMA, warp 1 MMA, warps 2-9 split / drain / store
 constexpr unsigned long long kWaitNs = 2000000000ull;  // 2 s bound on any single wait
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) {
@@ -180,12 +180,12 @@ __global__ void __launch_bounds__(kThreads, 1)
     if (threadIdx.x == 0) {
         for (int s = 0; s < kStages; ++s) {
             mbar_init(smem_u32(&full[s]), 1);
-            mbar_init(smem_u32(&ready[s]), 128);
+            mbar_init(smem_u32(&ready[s]), 256);
             mbar_init(smem_u32(&empty[s]), 1);
         }
         for (int b = 0; b < 2; ++b) {
             mbar_init(smem_u32(&acc_full[b]), 1);
-            mbar_init(smem_u32(&acc_empty[b]), 128);
+            mbar_init(smem_u32(&acc_empty[b]), 256);
         }
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -279,12 +279,15 @@ __global__ void __launch_bounds__(kThreads, 1)
             }
         }
     } else {
-        // warps 2..5: split / expand stage i, drain stage i-1, finally store
-        const int t = threadIdx.x - 64;  // 0..127
-        const int q = warp & 3;          // TMEM lane quarter of this warp
-        float acc[BN];
+        // warps 2..9: split / expand stage i, drain stage i-1, finally store.  TMEM lane quarter
+        // q = warp % 4 (the lanes this warp may access); warps 2-5 own columns [0, BN/2), warps 6-9 [BN/2, BN)
+        constexpr int HB = BN / 2;
+        const int t = threadIdx.x - 64;  // 0..255
+        const int q = warp & 3;
+        const int col0 = (warp >= 6) ? HB : 0;
+        float acc[HB];
 #pragma unroll
-        for (int j = 0; j < BN; ++j) acc[j] = 0.f;
+        for (int j = 0; j < HB; ++j) acc[j] = 0.f;
         bool ok = true;
         auto drain = [&](int i) {
             const int bf = i & 1;
@@ -294,9 +297,9 @@ __global__ void __launch_bounds__(kThreads, 1)
                 return;
             }
             tc_fence_after();
-            const unsigned ta = tmem + (unsigned(32 * q) << 16) + unsigned(bf * BN);
+            const unsigned ta = tmem + (unsigned(32 * q) << 16) + unsigned(bf * BN + col0);
 #pragma unroll
-            for (int c0 = 0; c0 < BN; c0 += 16) {
+            for (int c0 = 0; c0 < HB; c0 += 16) {
                 float v[16];
                 tmem_ld16(ta + unsigned(c0), v);
 #pragma unroll
@@ -318,7 +321,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             unsigned char* bhi = ahi + 2 * TB::a_exp;
             unsigned char* blo = bhi + TB::b;
             // A: 512 raw 16-byte chunks -> 2 expanded rows each (hi and lo)
-            for (int qq = t; qq < 512; qq += 128) {
+            for (int qq = t; qq < 512; qq += 256) {
                 unsigned src, d0, d1;
                 if (OPA == 1) {
                     const unsigned r = qq >> 3, c = qq & 7;  // raw row r (one complex row of A^H), chunk c
@@ -341,7 +344,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                 *reinterpret_cast<float4*>(alo + d1) = make_float4(-l.y, l.x, -l.w, l.z);
             }
             // B: in-place hi, lo beside it (same layout)
-            for (int qq = t; qq < BN * 8; qq += 128) {
+            for (int qq = t; qq < BN * 8; qq += 256) {
                 float4* p = reinterpret_cast<float4*>(bhi + qq * 16);
                 const float4 x = *p;
                 const float4 h = make_float4(tf32_trunc(x.x), tf32_trunc(x.y), tf32_trunc(x.z), tf32_trunc(x.w));
@@ -362,8 +365,8 @@ __global__ void __launch_bounds__(kThreads, 1)
             const bool im = row & 1;
             const bool use_beta = (beta.x != 0.f || beta.y != 0.f);
 #pragma unroll
-            for (int j = 0; j < BN; ++j) {
-                const int n = tile_n * BN + j;
+            for (int j = 0; j < HB; ++j) {
+                const int n = tile_n * BN + col0 + j;
                 const bool valid = row_ok && n < N;
                 const float v = acc[j];
                 const float partner = __shfl_xor_sync(0xffffffffu, v, 1);
@@ -459,9 +462,23 @@ void launch(int M, int N, int K, float2 alpha, const float2* A, int lda, const f
     CUtensorMap mB = make_map(B, 2L * K, N, 2L * ldb, 32, BN);
     const int tm = (M2 + kBM - 1) / kBM, tn = (N + BN - 1) / BN;
     const int nk = (K2 + kBK - 1) / kBK;
-    // split K until the grid covers the 148 SMs (at least 4 stages per split)
+    // split K so that whole waves of one CTA per SM (148 SMs) are filled: minimise
+    // waves * stages-per-CTA, with a small charge per split for the reduction traffic
     int splits = 1;
-    while (tm * tn * splits < 148 && nk / (splits * 2) >= 4) splits *= 2;
+    {
+        const long tiles = long(tm) * tn;
+        double best = 1e300;
+        const int smax = nk < 1024 ? nk : 1024;
+        for (int sp = 1; sp <= smax; ++sp) {
+            const long per_s = (nk + sp - 1) / sp;
+            const long waves = (tiles * sp + 147) / 148;
+            const double cost = double(waves) * double(per_s) + (sp > 1 ? 0.05 * sp + 2.0 : 0.0);
+            if (cost < best - 1e-9) {
+                best = cost;
+                splits = sp;
+            }
+        }
+    }
     const int per = (nk + splits - 1) / splits;
     splits = (nk + per - 1) / per;
     float* ws = nullptr;

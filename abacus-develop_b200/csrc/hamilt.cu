@@ -8,9 +8,33 @@ namespace b200 {
 __global__ void k_d2f(long n, const double* __restrict__ a, float* __restrict__ b) {
     for (long i = blockIdx.x * long(blockDim.x) + threadIdx.x; i < n; i += long(gridDim.x) * blockDim.x) b[i] = float(a[i]);
 }
-__global__ void k_z2c(long n, const double2* __restrict__ a, float2* __restrict__ b) {
-    for (long i = blockIdx.x * long(blockDim.x) + threadIdx.x; i < n; i += long(gridDim.x) * blockDim.x)
-        b[i] = make_float2(float(a[i].x), float(a[i].y));
+// rows x cols (row pitch lda) complex128 -> complex64 with row pitch ldb (the extra column zeroed)
+__global__ void k_z2c_pitch(int rows, int cols, int lda, int ldb, const double2* __restrict__ a, float2* __restrict__ b) {
+    const long n = long(rows) * ldb;
+    for (long i = blockIdx.x * long(blockDim.x) + threadIdx.x; i < n; i += long(gridDim.x) * blockDim.x) {
+        const int r = int(i / ldb);
+        const int c = int(i - long(r) * ldb);
+        b[i] = c < cols ? make_float2(float(a[long(r) * lda + c].x), float(a[long(r) * lda + c].y)) : make_float2(0.f, 0.f);
+    }
+}
+
+// ps in the K-major (becp) layout, ps[b*nkb + j] = sum_x D[x, k] becp[b*nkb + x] over the atom block of j:
+// the same contraction as nonlocal_pw_op (nonlocal_op.cpp:8-41) with the output transposed for the GEMM that follows
+template <typename T, typename R>
+__global__ void k_nonlocal_kmajor(int l1, int nb, int l3, int sum, int iat, int spin, int nkb, int dx, int dy, int dz,
+                                  const R* __restrict__ deeq, T* __restrict__ ps, const T* __restrict__ becp) {
+    const long total = long(l1) * l3 * nb;
+    for (long t = blockIdx.x * long(blockDim.x) + threadIdx.x; t < total; t += long(gridDim.x) * blockDim.x) {
+        const int kk = int(t % l3);
+        const long r = t / l3;
+        const int ii = int(r % l1);
+        const int b = int(r / l1);
+        const R* d = deeq + (long(spin * dx + iat + ii) * dy) * dz + kk;
+        const T* bp = becp + long(b) * nkb + sum + ii * l3;
+        T acc = cmake<T>(0, 0);
+        for (int xx = 0; xx < l3; ++xx) acc = cadd(acc, cscale(bp[xx], d[long(xx) * dz]));
+        ps[long(b) * nkb + sum + ii * l3 + kk] = acc;
+    }
 }
 
 Hamilt::Hamilt(PWGrid* g, int prec) : grid(g), precision(prec) {
@@ -42,8 +66,9 @@ void Hamilt::set_vkb(int ik, int nkb, int npwx, const double2* vkb_d) {
     const long n = long(nkb) * npwx;
     k.vkb.resize(n);
     B200_CUDA(cudaMemcpyAsync(k.vkb.ptr, vkb_d, n * sizeof(double2), cudaMemcpyDeviceToDevice, 0));
-    k.vkbf.resize(n);
-    k_z2c<<<592, 256>>>(n, vkb_d, k.vkbf.ptr);
+    k.ldf = npwx + (npwx & 1);
+    k.vkbf.resize(size_t(nkb) * k.ldf);
+    k_z2c_pitch<<<592, 256>>>(nkb, npwx, npwx, k.ldf, vkb_d, k.vkbf.ptr);
     note_launch();
     B200_CUDA(cudaGetLastError());
     B200_CUDA(cudaStreamSynchronize(0));
@@ -144,21 +169,61 @@ template <typename T> void Hamilt::hpsi(int ik, int spin, int nb, int ld, const 
         becp = becp32.ptr;
         ps = ps32.ptr;
     }
-    const T* vkb = f64 ? (const T*)k.vkb.ptr : (const T*)k.vkbf.ptr;
     const T one = cmake<T>(1, 0), zero = cmake<T>(0, 0);
-    B200_CUBLAS(cublasSetStream(cublas, s));
-    // becp = vkb^H psi (Nonlocal::act, nonlocal_pw.cpp:261-276)
-    B200_CUBLAS(Blas<T>::gemm(cublas, CUBLAS_OP_C, CUBLAS_OP_N, nkb, nb, npw, &one, vkb, k.npwx, psi, ld, &zero, becp, nkb));
-    // ps = D becp per atom type (add_nonlocal_pp, nonlocal_pw.cpp:64-110)
-    B200_CUDA(cudaMemsetAsync(ps, 0, size_t(nkb) * nb * sizeof(T), s));
-    int sum = 0, iat = 0;
     const R* d = f64 ? (const R*)deeq.ptr : (const R*)deeqf.ptr;
     B200_CHECK(d != nullptr, kInvalidArgument, "deeq not set");
     B200_CHECK(spin >= 0 && spin < nspin, kInvalidArgument, "spin out of range");
-    for (int it = 0; it < ntype; ++it) nonlocal_pw<T, R>(na[it], nb, nh[it], sum, iat, spin, nkb, dx, dy, dz, d, ps, becp, s);
-    B200_CHECK(sum == nkb, kInvalidArgument, "sum of na*nh over types differs from nkb");
-    // hpsi += vkb ps^T (nonlocal_pw.cpp:190-205)
-    B200_CUBLAS(Blas<T>::gemm(cublas, CUBLAS_OP_N, CUBLAS_OP_T, npw, nb, nkb, &one, vkb, k.npwx, ps, nb, &one, hpsi, ld));
+    if constexpr (f64) {
+        const T* vkb = (const T*)k.vkb.ptr;
+        B200_CUBLAS(cublasSetStream(cublas, s));
+        // becp = vkb^H psi (Nonlocal::act, nonlocal_pw.cpp:261-276)
+        B200_CUBLAS(Blas<T>::gemm(cublas, CUBLAS_OP_C, CUBLAS_OP_N, nkb, nb, npw, &one, vkb, k.npwx, psi, ld, &zero, becp,
+                                  nkb));
+        // ps = D becp per atom type (add_nonlocal_pp, nonlocal_pw.cpp:64-110)
+        B200_CUDA(cudaMemsetAsync(ps, 0, size_t(nkb) * nb * sizeof(T), s));
+        int sum = 0, iat = 0;
+        for (int it = 0; it < ntype; ++it)
+            nonlocal_pw<T, R>(na[it], nb, nh[it], sum, iat, spin, nkb, dx, dy, dz, d, ps, becp, s);
+        B200_CHECK(sum == nkb, kInvalidArgument, "sum of na*nh over types differs from nkb");
+        // hpsi += vkb ps^T (nonlocal_pw.cpp:190-205)
+        B200_CUBLAS(Blas<T>::gemm(cublas, CUBLAS_OP_N, CUBLAS_OP_T, npw, nb, nkb, &one, vkb, k.npwx, ps, nb, &one, hpsi,
+                                  ld));
+    } else {
+        // mixed precision: both projector products on the tensor cores (3xTF32), ps kept in becp's layout
+        const float2* psi_b = psi;
+        int ldb = ld;
+        if (ld & 1) {  // the TMA row pitch must be a multiple of 16 bytes: stage psi with an even pitch
+            ldb = ld + 1;
+            psi_pad32.resize(size_t(nb) * ldb);
+            B200_CUDA(cudaMemcpy2DAsync(psi_pad32.ptr, size_t(ldb) * sizeof(float2), psi, size_t(ld) * sizeof(float2),
+                                        size_t(npw) * sizeof(float2), nb, cudaMemcpyDeviceToDevice, s));
+            psi_b = psi_pad32.ptr;
+        }
+        const int ldps = nkb + (nkb & 1);
+        if (ldps != nkb) {
+            becp32.resize(size_t(ldps) * nb);
+            ps32.resize(size_t(ldps) * nb);
+            becp = becp32.ptr;
+            ps = ps32.ptr;
+        }
+        tc_cgemm('C', nkb, nb, npw, one, k.vkbf.ptr, k.ldf, psi_b, ldb, zero, becp, ldps, tcw, s);
+        int sum = 0, iat = 0;
+        for (int it = 0; it < ntype; ++it) {
+            const long total = long(na[it]) * nh[it] * nb;
+            if (total > 0) {
+                int blocks = int((total + 255) / 256);
+                if (blocks > 148 * 8) blocks = 148 * 8;
+                k_nonlocal_kmajor<T, R><<<blocks, 256, 0, s>>>(na[it], nb, nh[it], sum, iat, spin, ldps, dx, dy, dz, d, ps,
+                                                              becp);
+                note_launch();
+                B200_CUDA(cudaGetLastError());
+            }
+            sum += na[it] * nh[it];
+            iat += na[it];
+        }
+        B200_CHECK(sum == nkb, kInvalidArgument, "sum of na*nh over types differs from nkb");
+        tc_cgemm('N', npw, nb, nkb, one, k.vkbf.ptr, k.ldf, ps, ldps, one, hpsi, ld, tcw, s);
+    }
 }
 
 template void Hamilt::hpsi<double2>(int, int, int, int, const double2*, double2*, int, cudaStream_t);

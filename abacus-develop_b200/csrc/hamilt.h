@@ -5,6 +5,7 @@
 #include <vector>
 
 #include "common.h"
+#include "gemm_tc.h"
 #include "pw_grid.h"
 
 namespace b200 {
@@ -20,7 +21,8 @@ namespace b200 {
 struct NonlocalK {
     int nkb = 0, npwx = 0;
     DeviceArray<double2> vkb;   // nkb x npwx row-major (column-major npwx x nkb)
-    DeviceArray<float2> vkbf;
+    DeviceArray<float2> vkbf;   // FP32 copy, leading dimension ldf = npwx rounded up to even (TMA row pitch)
+    int ldf = 0;
 };
 
 struct Hamilt {
@@ -36,8 +38,9 @@ struct Hamilt {
     DeviceArray<float> deeqf;
     // workspaces
     DeviceArray<double2> sb64, becp64, ps64;
-    DeviceArray<float2> sb32, becp32, ps32;
+    DeviceArray<float2> sb32, becp32, ps32, psi_pad32;
     cublasHandle_t cublas = nullptr;
+    TcGemmWorkspace tcw;  // tensor-core GEMM workspace (mixed precision projectors)
 
     explicit Hamilt(PWGrid* g, int prec);
     ~Hamilt();

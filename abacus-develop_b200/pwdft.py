@@ -274,6 +274,12 @@ class DiagoDavid:
              eigenvalue.ctypes.data_as(_lib.pf64), thr, maxiter, ntry_max, notconv_max, C.byref(it))
         return it.value
 
+    def set_verbosity(self, level):
+        call("b200_david_set_verbosity", self._h, int(level))
+
+    def set_mixed_threshold(self, thr):
+        call("b200_david_set_mixed_threshold", self._h, float(thr))
+
     def stats(self):
         """(iterations in the FP32 stage, iterations in FP64, single-band H applications) of the last solve."""
         a, b, c = C.c_int(), C.c_int(), C.c_int()

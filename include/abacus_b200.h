@@ -202,6 +202,12 @@ int b200_david_diag(b200_david* d, b200_hpsi_cb hpsi, void* user, int ldpsi, voi
 int b200_david_diag_hamilt(b200_david* d, b200_hamilt* h, int ik, int spin, int ldpsi, void* psi_d,
                            double* eigenvalue, double thr, int maxiter, int ntry_max, int notconv_max, int* iters);
 
+/* Verbosity of the solver (the role of DiagoDavid's test_david, diago_david.cpp:53-58):
+ * 0 = quiet, 1 = one line per iteration on stderr. */
+int b200_david_set_verbosity(b200_david* d, int level);
+/* Mixed precision only: eigenvalue-change threshold at which the FP32 stage hands over to the
+ * FP64 refinement (default 1e-6 Ry; never below the requested thr). */
+int b200_david_set_mixed_threshold(b200_david* d, double thr);
 /* Statistics of the last solve: Davidson iterations in the FP32 stage (mixed only), in FP64,
  * and the number of single-band H applications (all stages). */
 int b200_david_stats(const b200_david* d, int* iters_low, int* iters_fp64, int* hpsi_bands);
