@@ -61,6 +61,14 @@ _SIGS = {
     "b200_hamilt_hpsi": ([vp, i32, i32, i32, i32, vp, vp, vp], i32),
     "b200_hamilt_hpsi_part": ([vp, i32, i32, i32, i32, vp, vp, i32, vp], i32),
     "b200_hamilt_hpsi_local_noalloc": ([vp, i32, i32, i32, vp, vp, vp], i32),
+    "b200_hamilt_hpsi_kbatch": ([vp, i32, pi32, i32, i32, i32, C.POINTER(vp), C.POINTER(vp), vp], i32),
+    "b200_graph_capture_hpsi_kbatch": ([vp, i32, pi32, i32, i32, i32, C.POINTER(vp), C.POINTER(vp), vp,
+                                        C.POINTER(vp)], i32),
+    "b200_graph_launch": ([vp, vp], i32),
+    "b200_graph_destroy": ([vp], i32),
+    "b200_hamilt_autotune": ([vp, i32, i32, i32, vp, vp, vp, pi32], i32),
+    "b200_solve_kpoints": ([vp, i32, pi32, i32, i32, i32, i32, C.POINTER(vp), C.POINTER(vp), i32, pf64, f64, i32,
+                            i32, i32, i32, pi32], i32),
     "b200_tc_cgemm": ([C.c_char, C.c_char, i32, i32, i32, f32, f32, vp, i32, vp, i32, f32, f32, vp, i32, vp], i32),
     "b200_tc_cgemm_error": ([pi32], i32),
     "b200_david_create": ([i32, i32, i32, i32, vp, C.POINTER(vp)], i32),
@@ -69,6 +77,7 @@ _SIGS = {
     "b200_david_diag_hamilt": ([vp, vp, i32, i32, i32, vp, pf64, f64, i32, i32, i32, pi32], i32),
     "b200_david_stats": ([vp, pi32, pi32, pi32], i32),
     "b200_david_set_verbosity": ([vp, i32], i32),
+    "b200_david_set_stream": ([vp, vp], i32),
     "b200_david_set_mixed_threshold": ([vp, f64], i32),
 }
 

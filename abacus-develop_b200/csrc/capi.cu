@@ -357,6 +357,12 @@ int b200_tc_cgemm_error(int* code) {
         *code = g_tc_ws.read_error();
     });
 }
+int b200_david_set_stream(b200_david* d, void* stream) {
+    return guarded([&] {
+        B200_CHECK(d != nullptr, b200::kInvalidArgument, "NULL argument");
+        d->d->set_stream(S(stream));
+    });
+}
 int b200_david_set_verbosity(b200_david* d, int level) {
     return guarded([&] {
         B200_CHECK(d != nullptr, b200::kInvalidArgument, "NULL argument");
@@ -383,13 +389,14 @@ int b200_david_diag_hamilt(b200_david* d, b200_hamilt* h, int ik, int spin, int 
     return guarded([&] {
         B200_CHECK(d && h && psi && eig, b200::kInvalidArgument, "NULL argument");
         b200::Hamilt* H = h->h.get();
-        b200::HPsiDevice f64 = [H, ik, spin](const void* x, void* hx, int, int dim, int i0, int i1, cudaStream_t s) {
+        b200::HpsiWork* W = &d->work;
+        b200::HPsiDevice f64 = [H, W, ik, spin](const void* x, void* hx, int, int dim, int i0, int i1, cudaStream_t s) {
             const double2* X = (const double2*)x + size_t(i0) * dim;
-            H->hpsi<double2>(ik, spin, i1 - i0 + 1, dim, X, (double2*)hx, 0, s);
+            H->hpsi<double2>(ik, spin, i1 - i0 + 1, dim, X, (double2*)hx, 0, s, W);
         };
-        b200::HPsiDevice f32 = [H, ik, spin](const void* x, void* hx, int, int dim, int i0, int i1, cudaStream_t s) {
+        b200::HPsiDevice f32 = [H, W, ik, spin](const void* x, void* hx, int, int dim, int i0, int i1, cudaStream_t s) {
             const float2* X = (const float2*)x + size_t(i0) * dim;
-            H->hpsi<float2>(ik, spin, i1 - i0 + 1, dim, X, (float2*)hx, 0, s);
+            H->hpsi<float2>(ik, spin, i1 - i0 + 1, dim, X, (float2*)hx, 0, s, W);
         };
         const int it = d->d->diag_hamilt(f64, f32, d->d->precision(), ldpsi, psi, eig, thr, maxiter, ntry_max, notconv_max);
         if (iters) *iters = it;

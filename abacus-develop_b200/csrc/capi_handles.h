@@ -16,4 +16,5 @@ struct b200_hamilt {
 };
 struct b200_david {
     std::unique_ptr<b200::DavidBase> d;
+    b200::HpsiWork work;  // H|psi> scratch used when the solver applies a Hamiltonian handle
 };

@@ -244,6 +244,12 @@ template <typename T> struct Engine {
         if (cb) cublasDestroy(cb);
         if (cs) cusolverDnDestroy(cs);
     }
+    void set_stream(cudaStream_t st) {
+        B200_CUDA(cudaStreamSynchronize(s));
+        s = st;
+        B200_CUBLAS_D(cublasSetStream(cb, s));
+        B200_CUSOLVER(cusolverDnSetStream(cs, s));
+    }
 
     // C = al op(A) B + be C; FP32 operands go to the tensor cores (3xTF32) whenever they are valid TMA operands
     void gemm(cublasOperation_t a, cublasOperation_t b, int m, int n, int k, T al, const T* A, int lda, const T* B,
@@ -478,18 +484,21 @@ class David : public DavidBase {
         stats_ = DavidStats{};
         int total = 0, nc = 0;
         if (precision == 1) {
-            if (!e32_) e32_ = std::make_unique<Engine<float2>>(nband_, dim_, ndim_, pc_.ptr);
+            if (!e32_) {
+                e32_ = std::make_unique<Engine<float2>>(nband_, dim_, ndim_, pc_.ptr);
+                e32_->set_stream(stream_);
+            }
             e32_->ref_refresh = e64_->ref_refresh;
             e32_->verbosity = verbosity_;
             e32_->hpsi_bands = 0;
             psi32_.resize(size_t(nband_) * ldpsi);
             const long n = long(nband_) * ldpsi;
-            k_convert<double2, float2><<<grid_of(n), kT>>>(n, (const double2*)psi, psi32_.ptr);
+            k_convert<double2, float2><<<grid_of(n), kT, 0, stream_>>>(n, (const double2*)psi, psi32_.ptr);
             note_launch();
             B200_CUDA(cudaGetLastError());
             const double t32 = thr > mixed_thr_ ? thr : mixed_thr_;
             const int it32 = e32_->diag(f32, ldpsi, psi32_.ptr, eig, t32, maxiter, 0, nband_, nc);
-            k_convert<float2, double2><<<grid_of(n), kT>>>(n, psi32_.ptr, (double2*)psi);
+            k_convert<float2, double2><<<grid_of(n), kT, 0, stream_>>>(n, psi32_.ptr, (double2*)psi);
             note_launch();
             B200_CUDA(cudaGetLastError());
             stats_.iters_low = it32;
@@ -506,6 +515,11 @@ class David : public DavidBase {
     const DavidStats& stats() const override { return stats_; }
     void set_mixed_thr(double thr) override { mixed_thr_ = thr; }
     int precision() const override { return precision_; }
+    void set_stream(cudaStream_t st) override {
+        stream_ = st;
+        e64_->set_stream(st);
+        if (e32_) e32_->set_stream(st);
+    }
     void set_verbosity(int level) override {
         verbosity_ = level;
         e64_->verbosity = level;
@@ -520,6 +534,7 @@ class David : public DavidBase {
     int nband_, dim_, ndim_, precision_;
     int notconv_ = 0;
     int verbosity_ = 0;
+    cudaStream_t stream_ = 0;
     double mixed_thr_ = 1e-6;
     DeviceArray<double> pc_;
     DeviceArray<float2> psi32_;

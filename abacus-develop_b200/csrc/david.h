@@ -32,6 +32,8 @@ struct DavidBase {
     // 0 = quiet; 1 = one line per Davidson iteration on stderr (iteration, basis size, unconverged bands,
     // largest eigenvalue change), the role of DiagoDavid's test_david levels (diago_david.cpp:53-58)
     virtual void set_verbosity(int level) = 0;
+    // stream for all of the solver's work (default: the legacy default stream, as the reference)
+    virtual void set_stream(cudaStream_t s) = 0;
 };
 
 std::unique_ptr<DavidBase> make_david(int nband, int dim, int david_ndim, int precision, const double* precond_d);

@@ -120,6 +120,74 @@ __global__ void __launch_bounds__(kPlaneWarps * 32) k_plane_w(PlaneMapView pm, i
     for (int s = tid; s < pm.nst; s += NT) plane[s] = A[pm.xc[s] * LDY + pm.sy[s]];
 }
 
+// ---- k-point batched z passes: one launch covers every k-point of a batch (blockIdx.z = k slot) ----
+template <typename T, int NZ>
+__global__ void __launch_bounds__(kZWarps * 32) k_zinv_wb(KBatchArgs args, int b0, int nbc, const T* __restrict__ twz,
+                                                         T* __restrict__ sb) {
+    constexpr int LDZ = NZ | 1;
+    __shared__ T A[kStickTile * LDZ];
+    const KBatchEntry& e = args.e[blockIdx.z];
+    const StickMapView sm = e.sm;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int s0 = blockIdx.x * kStickTile;
+    if (s0 >= sm.nst) return;
+    const int ns = min(kStickTile, sm.nst - s0);
+    const int band = blockIdx.y;
+    for (int i = tid; i < kStickTile * LDZ; i += kZWarps * 32) A[i] = zero_c<T>();
+    __syncthreads();
+    const T* p = reinterpret_cast<const T*>(e.psi) + size_t(b0 + band) * e.ld;
+    const int j0 = sm.gofs[s0], j1 = sm.gofs[s0 + ns];
+    for (int j = j0 + tid; j < j1; j += kZWarps * 32) {
+        const int pk = sm.gpk[j];
+        A[((pk >> 10) - s0) * LDZ + (pk & 1023)] = p[sm.glist[j]];
+    }
+    __syncthreads();
+    for (int sl = warp; sl < ns; sl += kZWarps) fft_warp<T, +1, NZ>(A + sl * LDZ, lane, twz);
+    __syncthreads();
+    T* out = sb + (size_t(blockIdx.z) * nbc + band) * NZ * sm.nst;
+    for (int i = tid; i < ns * NZ; i += kZWarps * 32) {
+        const int z = i / ns;
+        const int sl = i - z * ns;
+        out[size_t(z) * sm.nst + s0 + sl] = A[sl * LDZ + z];
+    }
+}
+
+template <typename T, typename R, int NZ>
+__global__ void __launch_bounds__(kZWarps * 32) k_zfwd_wb(KBatchArgs args, int b0, int nbc, const T* __restrict__ twz,
+                                                         const T* __restrict__ sb, R tpiba2, R invn) {
+    constexpr int LDZ = NZ | 1;
+    __shared__ T A[kStickTile * LDZ];
+    const KBatchEntry& e = args.e[blockIdx.z];
+    const StickMapView sm = e.sm;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int s0 = blockIdx.x * kStickTile;
+    if (s0 >= sm.nst) return;
+    const int ns = min(kStickTile, sm.nst - s0);
+    const int band = blockIdx.y;
+    const T* in = sb + (size_t(blockIdx.z) * nbc + band) * NZ * sm.nst;
+    for (int i = tid; i < ns * NZ; i += kZWarps * 32) {
+        const int z = i / ns;
+        const int sl = i - z * ns;
+        A[sl * LDZ + z] = in[size_t(z) * sm.nst + s0 + sl];
+    }
+    __syncthreads();
+    for (int sl = warp; sl < ns; sl += kZWarps) fft_warp<T, -1, NZ>(A + sl * LDZ, lane, twz);
+    __syncthreads();
+    const T* p = reinterpret_cast<const T*>(e.psi) + size_t(b0 + band) * e.ld;
+    T* h = reinterpret_cast<T*>(e.hpsi) + size_t(b0 + band) * e.ld;
+    const R* gk2 = reinterpret_cast<const R*>(e.gk2);
+    const int j0 = sm.gofs[s0], j1 = sm.gofs[s0 + ns];
+    for (int j = j0 + tid; j < j1; j += kZWarps * 32) {
+        const int pk = sm.gpk[j];
+        const int g = sm.glist[j];
+        T v = cscale(A[((pk >> 10) - s0) * LDZ + (pk & 1023)], invn);
+        v = cadd(v, cscale(p[g], gk2[g] * tpiba2));
+        h[g] = v;
+    }
+    if (blockIdx.x == 0)
+        for (int g = e.npw + tid; g < e.ld; g += kZWarps * 32) h[g] = zero_c<T>();
+}
+
 template <typename T> const T* twp(const FftAxis& a);
 template <> const double2* twp<double2>(const FftAxis& a) { return a.tw64.ptr; }
 template <> const float2* twp<float2>(const FftAxis& a) { return a.tw32.ptr; }
@@ -190,7 +258,58 @@ bool supported_xy(int nx, int ny) {
     return nx == ny && (nx == 18 || nx == 36 || nx == 45 || nx == 96 || nx == 125 || nx == 128);
 }
 
+template <typename T, typename R, int NZ>
+void zbatch(bool inv, const PWGrid& g, const KBatchArgs& args, int nk, int b0, int nbc, T* sb, double tpiba2, cudaStream_t s) {
+    const dim3 grid(ceil_div(g.nst, kStickTile), nbc, nk);
+    if (inv) {
+        k_zinv_wb<T, NZ><<<grid, kZWarps * 32, 0, s>>>(args, b0, nbc, twp<T>(g.az), sb);
+    } else {
+        k_zfwd_wb<T, R, NZ><<<grid, kZWarps * 32, 0, s>>>(args, b0, nbc, twp<T>(g.az), sb, R(tpiba2),
+                                                         R(1.0 / double(g.nxyz())));
+    }
+    note_launch();
+    B200_CUDA(cudaGetLastError());
+}
+
+template <typename T, typename R>
+bool zbatch_dispatch(bool inv, const PWGrid& g, const KBatchArgs& args, int nk, int b0, int nbc, T* sb, double tpiba2,
+                     cudaStream_t s) {
+    switch (g.nz) {
+        case 18: zbatch<T, R, 18>(inv, g, args, nk, b0, nbc, sb, tpiba2, s); return true;
+        case 36: zbatch<T, R, 36>(inv, g, args, nk, b0, nbc, sb, tpiba2, s); return true;
+        case 45: zbatch<T, R, 45>(inv, g, args, nk, b0, nbc, sb, tpiba2, s); return true;
+        case 90: zbatch<T, R, 90>(inv, g, args, nk, b0, nbc, sb, tpiba2, s); return true;
+        case 96: zbatch<T, R, 96>(inv, g, args, nk, b0, nbc, sb, tpiba2, s); return true;
+        case 125: zbatch<T, R, 125>(inv, g, args, nk, b0, nbc, sb, tpiba2, s); return true;
+        case 128: zbatch<T, R, 128>(inv, g, args, nk, b0, nbc, sb, tpiba2, s); return true;
+        default: return false;
+    }
+}
+
 }  // namespace
+
+template <typename T, typename R>
+bool launch_hpsi_local_kbatch(const PWGrid& g, const KBatchArgs& args, int nk, int nb, const R* veff_zyx, T* stickbuf,
+                              int chunk, double tpiba2, cudaStream_t s) {
+    if (!supported_z(g.nz) || !supported_xy(g.nx, g.ny)) return false;
+    const size_t smem = (size_t(kPlaneWarps) * g.nx + size_t(g.nxc) * (g.ny | 1)) * sizeof(T);
+    if (smem > 227 * 1024) return false;
+    for (int b0 = 0; b0 < nb; b0 += chunk) {
+        const int nbc = nb - b0 < chunk ? nb - b0 : chunk;
+        zbatch_dispatch<T, R>(true, g, args, nk, b0, nbc, stickbuf, tpiba2, s);
+        plane_dispatch<T, R>(g, nk * nbc, veff_zyx, stickbuf, s);
+        zbatch_dispatch<T, R>(false, g, args, nk, b0, nbc, stickbuf, tpiba2, s);
+    }
+    return true;
+}
+
+namespace {
+}  // namespace
+
+template bool launch_hpsi_local_kbatch<double2, double>(const PWGrid&, const KBatchArgs&, int, int, const double*,
+                                                        double2*, int, double, cudaStream_t);
+template bool launch_hpsi_local_kbatch<float2, float>(const PWGrid&, const KBatchArgs&, int, int, const float*, float2*,
+                                                      int, double, cudaStream_t);
 
 template <typename T, typename R>
 bool launch_hpsi_local_fast(const PWGrid& g, int ik, const R* veff_zyx, int nb, int ld, const T* psi, T* hpsi,

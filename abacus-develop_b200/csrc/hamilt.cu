@@ -37,14 +37,14 @@ __global__ void k_nonlocal_kmajor(int l1, int nb, int l3, int sum, int iat, int 
     }
 }
 
-Hamilt::Hamilt(PWGrid* g, int prec) : grid(g), precision(prec) {
-    B200_CUBLAS(cublasCreate(&cublas));
-    nl.resize(g->kmaps.size());
-}
-
-Hamilt::~Hamilt() {
+HpsiWork::HpsiWork() { B200_CUBLAS(cublasCreate(&cublas)); }
+HpsiWork::~HpsiWork() {
     if (cublas) cublasDestroy(cublas);
 }
+
+Hamilt::Hamilt(PWGrid* g, int prec) : grid(g), precision(prec) { nl.resize(g->kmaps.size()); }
+
+Hamilt::~Hamilt() = default;
 
 void Hamilt::set_veff(const double* veff_d) {
     const size_t N = size_t(grid->nxyz());
@@ -95,6 +95,7 @@ void Hamilt::set_deeq(int ntype_, const int* na_, const int* nh_, int nspin_, in
 }
 
 int Hamilt::band_chunk(size_t elem) const {
+    if (chunk_override > 0) return chunk_override;
     // keep one chunk's stick buffer (nst*nz per band) inside ~48 MB so the three passes hit L2
     const size_t per_band = size_t(grid->nst) * grid->nz * elem;
     size_t c = (size_t(48) << 20) / (per_band ? per_band : 1);
@@ -125,8 +126,19 @@ template <> struct Blas<float2> {
 };
 }  // namespace
 
-template <typename T> void Hamilt::hpsi(int ik, int spin, int nb, int ld, const T* psi, T* hpsi, int mode, cudaStream_t s) {
+template <typename T>
+void Hamilt::hpsi(int ik, int spin, int nb, int ld, const T* psi, T* hpsi, int mode, cudaStream_t s, HpsiWork* wk) {
     using R = typename RealOf<T>::type;
+    HpsiWork& W = wk ? *wk : work;
+    auto& sb64 = W.sb64;
+    auto& sb32 = W.sb32;
+    auto& becp64 = W.becp64;
+    auto& ps64 = W.ps64;
+    auto& becp32 = W.becp32;
+    auto& ps32 = W.ps32;
+    auto& psi_pad32 = W.psi_pad32;
+    auto& tcw = W.tcw;
+    cublasHandle_t cublas = W.cublas;
     constexpr bool f64 = std::is_same<T, double2>::value;
     B200_CHECK(ik >= 0 && ik < int(grid->kmaps.size()), kInvalidArgument, "k-point index out of range");
     const int npw = grid->kmaps[ik].npw;
@@ -226,7 +238,51 @@ template <typename T> void Hamilt::hpsi(int ik, int spin, int nb, int ld, const 
     }
 }
 
-template void Hamilt::hpsi<double2>(int, int, int, int, const double2*, double2*, int, cudaStream_t);
-template void Hamilt::hpsi<float2>(int, int, int, int, const float2*, float2*, int, cudaStream_t);
+template <typename T>
+void Hamilt::hpsi_kbatch(int nk, const int* iks, int spin, int nb, int ld, const T* const* psis, T* const* hpsis,
+                         cudaStream_t s, HpsiWork* wk) {
+    using R = typename RealOf<T>::type;
+    constexpr bool f64 = std::is_same<T, double2>::value;
+    B200_CHECK(nk >= 1 && nk <= kMaxKBatch, kInvalidArgument, "k-point batch must hold 1..128 k-points");
+    B200_CHECK(has_veff, kInvalidArgument, "V_eff not set");
+    HpsiWork& W = wk ? *wk : work;
+    KBatchArgs args;
+    for (int q = 0; q < nk; ++q) {
+        const int ik = iks[q];
+        B200_CHECK(ik >= 0 && ik < int(grid->kmaps.size()), kInvalidArgument, "k-point index out of range");
+        const KMap& km = grid->kmaps[ik];
+        B200_CHECK(ld >= km.npw, kInvalidArgument, "ld smaller than npwk");
+        args.e[q].sm = grid->stick_view(ik);
+        args.e[q].psi = psis[q];
+        args.e[q].hpsi = hpsis[q];
+        args.e[q].ld = ld;
+        args.e[q].npw = km.npw;
+        args.e[q].gk2 = f64 ? (const void*)km.gk2.ptr : (const void*)km.gk2f.ptr;
+    }
+    const size_t per_band = size_t(grid->nst) * grid->nz * sizeof(T);
+    int chunk = chunk_override > 0 ? chunk_override : int((size_t(48) << 20) / (per_band * nk));
+    if (chunk < 1) chunk = 1;
+    if (chunk > nb) chunk = nb;
+    const R* veff = f64 ? (const R*)veff_zyx.ptr : (const R*)veff_zyxf.ptr;
+    T* sb;
+    if constexpr (f64) {
+        W.sb64.resize(size_t(nk) * chunk * grid->nst * grid->nz);
+        sb = W.sb64.ptr;
+    } else {
+        W.sb32.resize(size_t(nk) * chunk * grid->nst * grid->nz);
+        sb = W.sb32.ptr;
+    }
+    if (!launch_hpsi_local_kbatch<T, R>(*grid, args, nk, nb, veff, sb, chunk, grid->basis.tpiba2, s)) {
+        for (int q = 0; q < nk; ++q) hpsi<T>(iks[q], spin, nb, ld, psis[q], hpsis[q], 1, s, &W);
+    }
+    for (int q = 0; q < nk; ++q) hpsi<T>(iks[q], spin, nb, ld, psis[q], hpsis[q], 2, s, &W);
+}
+
+template void Hamilt::hpsi_kbatch<double2>(int, const int*, int, int, int, const double2* const*, double2* const*,
+                                           cudaStream_t, HpsiWork*);
+template void Hamilt::hpsi_kbatch<float2>(int, const int*, int, int, int, const float2* const*, float2* const*,
+                                          cudaStream_t, HpsiWork*);
+template void Hamilt::hpsi<double2>(int, int, int, int, const double2*, double2*, int, cudaStream_t, HpsiWork*);
+template void Hamilt::hpsi<float2>(int, int, int, int, const float2*, float2*, int, cudaStream_t, HpsiWork*);
 
 }  // namespace b200

@@ -25,6 +25,20 @@ struct NonlocalK {
     int ldf = 0;
 };
 
+// Scratch of one H|psi> caller: stick buffer, becp / ps, the padded-psi stage, a cuBLAS handle and the
+// tensor-core GEMM workspace.  Callers that run H|psi> concurrently (different streams or threads) each
+// own one; the Hamiltonian itself is read-only after set-up.
+struct HpsiWork {
+    DeviceArray<double2> sb64, becp64, ps64;
+    DeviceArray<float2> sb32, becp32, ps32, psi_pad32;
+    cublasHandle_t cublas = nullptr;
+    TcGemmWorkspace tcw;
+    HpsiWork();
+    ~HpsiWork();
+    HpsiWork(const HpsiWork&) = delete;
+    HpsiWork& operator=(const HpsiWork&) = delete;
+};
+
 struct Hamilt {
     PWGrid* grid = nullptr;
     int precision = 0;  // 0 = FP64, 1 = mixed
@@ -36,11 +50,8 @@ struct Hamilt {
     std::vector<int> na, nh;
     DeviceArray<double> deeq;
     DeviceArray<float> deeqf;
-    // workspaces
-    DeviceArray<double2> sb64, becp64, ps64;
-    DeviceArray<float2> sb32, becp32, ps32, psi_pad32;
-    cublasHandle_t cublas = nullptr;
-    TcGemmWorkspace tcw;  // tensor-core GEMM workspace (mixed precision projectors)
+    HpsiWork work;  // default scratch for callers that do not bring their own
+    int chunk_override = 0;  // bands per stick-buffer chunk chosen by the autotuner (0 = 48 MB rule)
 
     explicit Hamilt(PWGrid* g, int prec);
     ~Hamilt();
@@ -49,7 +60,13 @@ struct Hamilt {
     void set_deeq(int ntype, const int* na, const int* nh, int nspin, int dx, int dy, int dz, const double* deeq_d);
     int band_chunk(size_t elem) const;
     // mode 0 = full H, 1 = kinetic + local only (overwrites hpsi), 2 = nonlocal only (accumulates)
-    template <typename T> void hpsi(int ik, int spin, int nb, int ld, const T* psi, T* hpsi, int mode, cudaStream_t s);
+    template <typename T>
+    void hpsi(int ik, int spin, int nb, int ld, const T* psi, T* hpsi, int mode, cudaStream_t s, HpsiWork* w = nullptr);
+    // H|psi> for nb bands of nk k-points: the local part in one launch per pass for all k (per band chunk),
+    // the projectors per k.  psis / hpsis are host arrays of device pointers (leading dimension ld).
+    template <typename T>
+    void hpsi_kbatch(int nk, const int* iks, int spin, int nb, int ld, const T* const* psis, T* const* hpsis,
+                     cudaStream_t s, HpsiWork* w = nullptr);
 };
 
 }  // namespace b200

@@ -1,0 +1,203 @@
+// k-point batches: batched H|psi>, its capture into a CUDA graph, the band-chunk autotuner, and concurrent
+// Davidson solves of many k-points (one stream and one H|psi> scratch per worker).
+//
+// ABACUS solves its k-points one after another inside a pool (HSolverPW::solve, hsolver_pw.cpp:240-270) and
+// parallelises over k only across processes.  On one B200 the k-points of a pool are independent work that
+// can share the device: their local H|psi> passes are launched together (one launch per pass for all k),
+// and their Davidson solves run concurrently on separate streams.
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <exception>
+#include <memory>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+#include "../../include/abacus_b200.h"
+#include "capi_handles.h"
+
+struct b200_graph {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    ~b200_graph() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+    }
+};
+
+namespace {
+
+template <typename F> int guarded_k(F&& f) {
+    try {
+        f();
+        b200::set_last_error("");
+        return B200_STATUS_OK;
+    } catch (const b200::Error& e) {
+        b200::set_last_error(e.what());
+        return e.code;
+    } catch (const std::exception& e) {
+        b200::set_last_error(e.what());
+        return B200_STATUS_INVALID_ARGUMENT;
+    }
+}
+
+void kbatch_call(b200_hamilt* h, int nk, const int* iks, int spin, int nb, int ld, void* const* psi, void* const* hpsi,
+                 cudaStream_t s) {
+    B200_CHECK(h && iks && psi && hpsi, b200::kInvalidArgument, "NULL argument");
+    if (h->h->precision == B200_PREC_FP64)
+        h->h->hpsi_kbatch<double2>(nk, iks, spin, nb, ld, reinterpret_cast<const double2* const*>(psi),
+                                   reinterpret_cast<double2* const*>(hpsi), s);
+    else
+        h->h->hpsi_kbatch<float2>(nk, iks, spin, nb, ld, reinterpret_cast<const float2* const*>(psi),
+                                  reinterpret_cast<float2* const*>(hpsi), s);
+}
+
+}  // namespace
+
+extern "C" {
+
+int b200_hamilt_hpsi_kbatch(b200_hamilt* h, int nk, const int* iks, int spin, int nbands, int ld, void* const* psi_d,
+                            void* const* hpsi_d, void* stream) {
+    return guarded_k([&] { kbatch_call(h, nk, iks, spin, nbands, ld, psi_d, hpsi_d, reinterpret_cast<cudaStream_t>(stream)); });
+}
+
+int b200_graph_capture_hpsi_kbatch(b200_hamilt* h, int nk, const int* iks, int spin, int nbands, int ld,
+                                   void* const* psi_d, void* const* hpsi_d, void* stream, b200_graph** out) {
+    return guarded_k([&] {
+        B200_CHECK(out != nullptr, b200::kInvalidArgument, "NULL argument");
+        cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+        B200_CHECK(s != nullptr, b200::kInvalidArgument, "capture needs a non-default stream");
+        // one eager call first: every workspace is allocated and every kernel attribute set before capture
+        kbatch_call(h, nk, iks, spin, nbands, ld, psi_d, hpsi_d, s);
+        B200_CUDA(cudaStreamSynchronize(s));
+        auto g = std::make_unique<b200_graph>();
+        B200_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        try {
+            kbatch_call(h, nk, iks, spin, nbands, ld, psi_d, hpsi_d, s);
+        } catch (...) {
+            cudaGraph_t dead = nullptr;
+            cudaStreamEndCapture(s, &dead);
+            if (dead) cudaGraphDestroy(dead);
+            throw;
+        }
+        B200_CUDA(cudaStreamEndCapture(s, &g->graph));
+        B200_CUDA(cudaGraphInstantiate(&g->exec, g->graph, 0));
+        *out = g.release();
+    });
+}
+
+int b200_graph_launch(b200_graph* g, void* stream) {
+    return guarded_k([&] {
+        B200_CHECK(g && g->exec, b200::kInvalidArgument, "NULL graph");
+        B200_CUDA(cudaGraphLaunch(g->exec, reinterpret_cast<cudaStream_t>(stream)));
+    });
+}
+
+int b200_graph_destroy(b200_graph* g) {
+    return guarded_k([&] { delete g; });
+}
+
+int b200_hamilt_autotune(b200_hamilt* h, int ik, int nbands, int ld, const void* psi_d, void* hpsi_d, void* stream,
+                         int* best_chunk) {
+    return guarded_k([&] {
+        B200_CHECK(h && psi_d && hpsi_d, b200::kInvalidArgument, "NULL argument");
+        cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+        b200::Hamilt& H = *h->h;
+        const bool f64 = H.precision == B200_PREC_FP64;
+        std::vector<int> cand = {1, 2, 4, 8, 16, 32, 64, 128};
+        cand.push_back(nbands);
+        std::sort(cand.begin(), cand.end());
+        cand.erase(std::unique(cand.begin(), cand.end()), cand.end());
+        cudaEvent_t e0, e1;
+        B200_CUDA(cudaEventCreate(&e0));
+        B200_CUDA(cudaEventCreate(&e1));
+        float best = 1e30f;
+        int best_c = 0;
+        const int saved = H.chunk_override;
+        for (int c : cand) {
+            if (c > nbands) continue;
+            H.chunk_override = c;
+            auto run = [&] {
+                if (f64)
+                    H.hpsi<double2>(ik, 0, nbands, ld, (const double2*)psi_d, (double2*)hpsi_d, 1, s);
+                else
+                    H.hpsi<float2>(ik, 0, nbands, ld, (const float2*)psi_d, (float2*)hpsi_d, 1, s);
+            };
+            run();  // warm-up (allocates the stick buffer for this chunk size)
+            B200_CUDA(cudaEventRecord(e0, s));
+            for (int r = 0; r < 3; ++r) run();
+            B200_CUDA(cudaEventRecord(e1, s));
+            B200_CUDA(cudaEventSynchronize(e1));
+            float ms = 0.f;
+            B200_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            if (ms < best) {
+                best = ms;
+                best_c = c;
+            }
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        H.chunk_override = best_c > 0 ? best_c : saved;
+        if (best_chunk) *best_chunk = H.chunk_override;
+    });
+}
+
+int b200_solve_kpoints(b200_hamilt* h, int nk, const int* iks, int spin, int nband, int david_ndim, int precision,
+                       const double* const* precond_d, void* const* psi_d, int ldpsi, double* eigenvalues,
+                       double thr, int maxiter, int ntry_max, int notconv_max, int nworkers, int* iters) {
+    return guarded_k([&] {
+        B200_CHECK(h && iks && precond_d && psi_d && eigenvalues, b200::kInvalidArgument, "NULL argument");
+        B200_CHECK(nk >= 1 && nworkers >= 1, b200::kInvalidArgument, "need nk >= 1 and nworkers >= 1");
+        b200::Hamilt* H = h->h.get();
+        int dev = 0;
+        B200_CUDA(cudaGetDevice(&dev));
+        std::atomic<int> next{0};
+        std::mutex err_mu;
+        std::exception_ptr first_err;
+        auto worker = [&]() {
+            try {
+                B200_CUDA(cudaSetDevice(dev));
+                cudaStream_t s = nullptr;
+                B200_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+                auto work = std::make_unique<b200::HpsiWork>();
+                for (int q = next.fetch_add(1); q < nk; q = next.fetch_add(1)) {
+                    {
+                        std::lock_guard<std::mutex> lk(err_mu);
+                        if (first_err) break;
+                    }
+                    const int ik = iks[q];
+                    const int dim = H->grid->kmaps.at(ik).npw;
+                    auto d = b200::make_david(nband, dim, david_ndim, precision, precond_d[q]);
+                    d->set_stream(s);
+                    b200::HpsiWork* W = work.get();
+                    b200::HPsiDevice f64 = [H, W, ik, spin](const void* x, void* hx, int, int ld, int i0, int i1,
+                                                            cudaStream_t st) {
+                        H->hpsi<double2>(ik, spin, i1 - i0 + 1, ld, (const double2*)x + size_t(i0) * ld, (double2*)hx, 0,
+                                         st, W);
+                    };
+                    b200::HPsiDevice f32 = [H, W, ik, spin](const void* x, void* hx, int, int ld, int i0, int i1,
+                                                            cudaStream_t st) {
+                        H->hpsi<float2>(ik, spin, i1 - i0 + 1, ld, (const float2*)x + size_t(i0) * ld, (float2*)hx, 0,
+                                        st, W);
+                    };
+                    const int it = d->diag_hamilt(f64, f32, precision, ldpsi, psi_d[q], eigenvalues + size_t(q) * nband,
+                                                  thr, maxiter, ntry_max, notconv_max);
+                    if (iters) iters[q] = it;
+                }
+                B200_CUDA(cudaStreamSynchronize(s));
+                cudaStreamDestroy(s);
+            } catch (...) {
+                std::lock_guard<std::mutex> lk(err_mu);
+                if (!first_err) first_err = std::current_exception();
+            }
+        };
+        const int nw = std::min(nworkers, nk);
+        std::vector<std::thread> pool;
+        for (int w = 0; w < nw; ++w) pool.emplace_back(worker);
+        for (auto& t : pool) t.join();
+        if (first_err) std::rethrow_exception(first_err);
+    });
+}
+
+}  // extern "C"

@@ -97,6 +97,24 @@ void launch_hpsi_local(const PWGrid& g, int ik, const R* veff_zyx, int nb, int l
 template <typename T, typename R>
 bool launch_hpsi_local_fast(const PWGrid& g, int ik, const R* veff_zyx, int nb, int ld, const T* psi, T* hpsi,
                             T* stickbuf, double tpiba2, int accumulate, cudaStream_t s);
+// k-point batch: one entry per k (its stick maps, psi / hpsi with leading dimension ld, npwk, gk2 in the
+// precision of the call); passed by value so a launch needs no device-side argument buffer.
+constexpr int kMaxKBatch = 128;
+struct KBatchEntry {
+    StickMapView sm;
+    const void* psi;
+    void* hpsi;
+    int ld, npw;
+    const void* gk2;
+};
+struct KBatchArgs {
+    KBatchEntry e[kMaxKBatch];
+};
+// Kinetic + local part of H|psi> for nb bands of nk k-points in one launch per pass (per band chunk);
+// returns false for grid sizes without compiled warp transforms.
+template <typename T, typename R>
+bool launch_hpsi_local_kbatch(const PWGrid& g, const KBatchArgs& args, int nk, int nb, const R* veff_zyx, T* stickbuf,
+                              int chunk, double tpiba2, cudaStream_t s);
 // Drop-in transforms (PW_Basis_K::recip_to_real / real_to_recip on the GPU), one band.
 template <typename T>
 void launch_recip_to_real(const PWGrid& g, int ik, const T* in, T* out, T* aux, int add, double factor, cudaStream_t s);

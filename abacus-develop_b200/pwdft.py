@@ -233,10 +233,74 @@ class HamiltPW:
         inside the library shared by all calls, so concurrent calls on one device must be serialised."""
         call("b200_hamilt_hpsi_local_noalloc", self._h, ik, nbands, ld, ptr(psi), ptr(hpsi), stream_ptr(stream))
 
+    @staticmethod
+    def _kbatch_args(iks, psis, hpsis):
+        nk = len(iks)
+        if len(psis) != nk or len(hpsis) != nk:
+            raise ValueError("iks, psis and hpsis must have the same length")
+        return (nk, (C.c_int * nk)(*[int(i) for i in iks]), (_lib.vp * nk)(*[ptr(p) for p in psis]),
+                (_lib.vp * nk)(*[ptr(p) for p in hpsis]))
+
+    def hpsi_kbatch(self, iks, psis, hpsis, nbands, ld, spin=0, stream=None):
+        """H|psi> of nbands bands for each k-point in iks (psis[q], hpsis[q]: that k-point's blocks); the
+        kinetic + local part of all k-points in one launch per FFT pass."""
+        nk, ik_a, p_a, h_a = self._kbatch_args(iks, psis, hpsis)
+        call("b200_hamilt_hpsi_kbatch", self._h, nk, ik_a, spin, nbands, ld, p_a, h_a, stream_ptr(stream))
+
+    def capture_hpsi_kbatch(self, iks, psis, hpsis, nbands, ld, stream, spin=0):
+        """hpsi_kbatch captured into a CUDA graph on a non-default stream; returns a HpsiGraph whose
+        launch() replays it on the captured buffers."""
+        nk, ik_a, p_a, h_a = self._kbatch_args(iks, psis, hpsis)
+        g = _lib.vp()
+        call("b200_graph_capture_hpsi_kbatch", self._h, nk, ik_a, spin, nbands, ld, p_a, h_a, stream_ptr(stream),
+             C.byref(g))
+        return HpsiGraph(g, keep=(self, list(psis), list(hpsis)))
+
+    def autotune(self, ik, psi, hpsi, nbands, ld, stream=None):
+        """Pick the band-chunk size of the local pass by timing candidates; returns the chosen size."""
+        best = C.c_int()
+        call("b200_hamilt_autotune", self._h, ik, nbands, ld, ptr(psi), ptr(hpsi), stream_ptr(stream), C.byref(best))
+        return best.value
+
+    def solve_kpoints(self, iks, precond_ds, psis, ld_psi, nband, thr, maxiter, david_ndim=4, precision=PREC_FP64,
+                      nworkers=4, ntry_max=5, notconv_max=0, spin=0):
+        """Davidson solves of the k-points iks, nworkers at a time on separate streams.  psis[q] (complex128,
+        nband x ld_psi) is overwritten with the eigenvectors.  Returns (eigenvalues nk x nband, iterations)."""
+        nk = len(iks)
+        ik_a = (C.c_int * nk)(*[int(i) for i in iks])
+        pc_a = (_lib.vp * nk)(*[ptr(p) for p in precond_ds])
+        ps_a = (_lib.vp * nk)(*[ptr(p) for p in psis])
+        eig = np.zeros((nk, nband))
+        its = np.zeros(nk, dtype=np.int32)
+        call("b200_solve_kpoints", self._h, nk, ik_a, spin, nband, david_ndim, precision,
+             C.cast(pc_a, C.POINTER(_lib.vp)), ps_a, ld_psi, eig.ctypes.data_as(_lib.pf64), thr, maxiter, ntry_max,
+             notconv_max, nworkers, its.ctypes.data_as(_lib.pi32))
+        return eig, its
+
     def __del__(self):
         try:
             if getattr(self, "_h", None):
                 self._lib.b200_hamilt_destroy(self._h)
+                self._h = None
+        except Exception:
+            pass
+
+
+class HpsiGraph:
+    """An instantiated CUDA graph of a captured H|psi> call (keeps its Hamiltonian and buffers alive)."""
+
+    def __init__(self, handle, keep):
+        self._h = handle
+        self._keep = keep
+        self._lib = _lib.load()
+
+    def launch(self, stream=None):
+        call("b200_graph_launch", self._h, stream_ptr(stream))
+
+    def __del__(self):
+        try:
+            if getattr(self, "_h", None):
+                self._lib.b200_graph_destroy(self._h)
                 self._h = None
         except Exception:
             pass
@@ -273,6 +337,11 @@ class DiagoDavid:
         call("b200_david_diag_hamilt", self._h, hamilt.handle, ik, spin, ld_psi, ptr(psi),
              eigenvalue.ctypes.data_as(_lib.pf64), thr, maxiter, ntry_max, notconv_max, C.byref(it))
         return it.value
+
+    def set_stream(self, stream):
+        """Run the solver's work on a torch.cuda.Stream (or raw stream pointer)."""
+        sp = stream.cuda_stream if hasattr(stream, "cuda_stream") else stream
+        call("b200_david_set_stream", self._h, sp)
 
     def set_verbosity(self, level):
         call("b200_david_set_verbosity", self._h, int(level))

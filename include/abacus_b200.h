@@ -38,6 +38,7 @@ extern "C" {
 typedef struct b200_pw_basis b200_pw_basis; /* host + device plane-wave basis of one pool */
 typedef struct b200_hamilt b200_hamilt;     /* V_eff, projectors, D and workspaces */
 typedef struct b200_david b200_david;       /* Davidson workspaces */
+typedef struct b200_graph b200_graph;       /* an instantiated CUDA graph of a captured call */
 
 /* Message of the last failed call on this thread ("" if none). */
 const char* b200_last_error(void);
@@ -172,6 +173,26 @@ int b200_hamilt_hpsi_part(b200_hamilt* h, int ik, int spin, int nbands, int ld, 
 int b200_hamilt_hpsi_local_noalloc(b200_hamilt* h, int ik, int nbands, int ld, const void* psi_d, void* hpsi_d,
                                    void* stream);
 
+/* H|psi> for nbands bands of each of nk k-points (1 <= nk <= 128) in one call: the same result as
+ * b200_hamilt_hpsi once per k-point (HamiltPW::updateHk + Operator::hPsi per k, hsolver_pw.cpp:240-270),
+ * with the kinetic + local part of all k-points done in one launch per FFT pass.
+ * iks: host array of nk k-point indices; psi_d / hpsi_d: host arrays of nk device pointers. */
+int b200_hamilt_hpsi_kbatch(b200_hamilt* h, int nk, const int* iks, int spin, int nbands, int ld, void* const* psi_d,
+                            void* const* hpsi_d, void* stream);
+/* Captures b200_hamilt_hpsi_kbatch with these arguments into a CUDA graph (after one eager call that
+ * allocates every workspace; the eager call's output is the same as a replay's).  stream must not be
+ * the legacy default stream.  Replays read psi_d and write hpsi_d at the captured addresses.
+ * No counterpart in the reference. */
+int b200_graph_capture_hpsi_kbatch(b200_hamilt* h, int nk, const int* iks, int spin, int nbands, int ld,
+                                   void* const* psi_d, void* const* hpsi_d, void* stream, b200_graph** out);
+int b200_graph_launch(b200_graph* g, void* stream);
+int b200_graph_destroy(b200_graph* g);
+/* Times the kinetic + local pass of k-point ik over candidate band-chunk sizes (1, 2, 4 ... 128 and
+ * nbands; three timed repetitions each after one warm-up) and keeps the fastest for this handle.
+ * Overwrites hpsi_d.  No counterpart in the reference. */
+int b200_hamilt_autotune(b200_hamilt* h, int ik, int nbands, int ld, const void* psi_d, void* hpsi_d, void* stream,
+                         int* best_chunk);
+
 /* gemm_op<std::complex<float>, DEVICE_GPU> (module_hsolver/kernels/math_kernel_op.h:240-265) on the
  * tensor cores: C = alpha * op(A) * B + beta * C, complex64 column-major, transa 'N' or 'C', transb 'N'.
  * Split precision (3xTF32: hi*hi + hi*lo + lo*hi, FP32 accumulate), about FP32 accuracy.
@@ -202,6 +223,10 @@ int b200_david_diag(b200_david* d, b200_hpsi_cb hpsi, void* user, int ldpsi, voi
 int b200_david_diag_hamilt(b200_david* d, b200_hamilt* h, int ik, int spin, int ldpsi, void* psi_d,
                            double* eigenvalue, double thr, int maxiter, int ntry_max, int notconv_max, int* iters);
 
+/* Stream on which the solver runs all its work (default NULL = legacy default stream, as the
+ * reference).  Solvers on different streams run concurrently; each solver handle owns its own
+ * H|psi> scratch, so several solvers may share one Hamiltonian handle. */
+int b200_david_set_stream(b200_david* d, void* stream);
 /* Verbosity of the solver (the role of DiagoDavid's test_david, diago_david.cpp:53-58):
  * 0 = quiet, 1 = one line per iteration on stderr. */
 int b200_david_set_verbosity(b200_david* d, int level);
@@ -211,6 +236,15 @@ int b200_david_set_mixed_threshold(b200_david* d, double thr);
 /* Statistics of the last solve: Davidson iterations in the FP32 stage (mixed only), in FP64,
  * and the number of single-band H applications (all stages). */
 int b200_david_stats(const b200_david* d, int* iters_low, int* iters_fp64, int* hpsi_bands);
+
+/* Davidson solves of nk k-points of one Hamiltonian handle, nworkers at a time on separate streams
+ * (the k loop of HSolverPW::solve, hsolver_pw.cpp:240-270, with the k-points running concurrently).
+ * precision: B200_PREC_FP64 or B200_PREC_MIXED; precond_d / psi_d: host arrays of nk device pointers
+ * (psi_d[q]: complex128, nband vectors at ldpsi); eigenvalues: host, nk x nband; iters: host, nk
+ * (or NULL).  Each k-point's result is the same as a b200_david_diag_hamilt solve of it alone. */
+int b200_solve_kpoints(b200_hamilt* h, int nk, const int* iks, int spin, int nband, int david_ndim, int precision,
+                       const double* const* precond_d, void* const* psi_d, int ldpsi, double* eigenvalues, double thr,
+                       int maxiter, int ntry_max, int notconv_max, int nworkers, int* iters);
 
 #ifdef __cplusplus
 }
