@@ -67,6 +67,16 @@ _SIGS = {
     "b200_graph_launch": ([vp, vp], i32),
     "b200_graph_destroy": ([vp], i32),
     "b200_hamilt_autotune": ([vp, i32, i32, i32, vp, vp, vp, pi32], i32),
+    "b200_cal_ylm_real_op_f64": ([i32, i32, vp, vp, vp], i32),
+    "b200_cal_ylm_real_op_f32": ([i32, i32, vp, vp, vp], i32),
+    "b200_cal_sk_op_f64": ([i32] * 14 + [pi32, vp, vp, f64, vp, vp, vp, vp, vp, vp, vp], i32),
+    "b200_cal_sk_op_f32": ([i32] * 14 + [pi32, vp, vp, f32, vp, vp, vp, vp, vp, vp, vp], i32),
+    "b200_cal_vnl_op_f64": ([i32] * 6 + [pi32, pi32, pi32, f64, f64] + [vp] * 10, i32),
+    "b200_cal_vnl_op_f32": ([i32] * 6 + [pi32, pi32, pi32, f32, f32] + [vp] * 10, i32),
+    "b200_hamilt_set_projectors": ([vp, i32, pi32, pi32, pi32, i32, i32, pi32, pi32, pi32, i32, i32, f64, pf64, pf64],
+                                   i32),
+    "b200_hamilt_build_vkb": ([vp, i32, vp], i32),
+    "b200_hamilt_copy_vkb": ([vp, i32, vp, vp], i32),
     "b200_solve_kpoints": ([vp, i32, pi32, i32, i32, i32, i32, C.POINTER(vp), C.POINTER(vp), i32, pf64, f64, i32,
                             i32, i32, i32, pi32], i32),
     "b200_tc_cgemm": ([C.c_char, C.c_char, i32, i32, i32, f32, f32, vp, i32, vp, i32, f32, f32, vp, i32, vp], i32),

@@ -143,6 +143,10 @@ void PWGrid::ensure_device() {
         for (int g = 0; g < npw; ++g) gf[g] = float(basis.gk2[ik * L + g]);
         km.gk2f.upload(gf.data(), npw);
         km.precond.upload(km.h_precond.data(), npw);
+        std::vector<double> gk(size_t(npw) * 3);
+        for (int g = 0; g < npw; ++g)
+            for (int j = 0; j < 3; ++j) gk[size_t(g) * 3 + j] = basis.gcar[(ik * L + g) * 3 + j] + basis.kvec_c[ik * 3 + j];
+        km.gkcar.upload(gk.data(), size_t(npw) * 3);
     }
     B200_CUDA(cudaDeviceSynchronize());
     on_device = true;

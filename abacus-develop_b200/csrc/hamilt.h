@@ -39,6 +39,25 @@ struct HpsiWork {
     HpsiWork& operator=(const HpsiWork&) = delete;
 };
 
+// Projector tables of one cell, the inputs of pseudopot_cell_vnl::getvnl (VNL_in_pw.cpp:412-540):
+// radial tables tab(it, ib, iq) on a q grid of step dq, per-type (ih -> beta, l, lm) maps and atom positions.
+constexpr int kVnlMaxTypes = 8;
+constexpr int kVnlMaxNh = 32;
+constexpr int kVnlMaxL = 4;
+struct VnlParams {  // handed to the kernel by value
+    int ntype, nhm, lmax, tab_2, tab_3, nkb;
+    double dq, tpiba;
+    int na[kVnlMaxTypes], nbeta[kVnlMaxTypes], nh[kVnlMaxTypes];
+    unsigned char indv[kVnlMaxTypes][kVnlMaxNh], nhtol[kVnlMaxTypes][kVnlMaxNh], nhtolm[kVnlMaxTypes][kVnlMaxNh];
+};
+struct VnlTables {
+    bool set = false;
+    VnlParams p{};
+    int nat = 0;
+    DeviceArray<double> tab;  // ntype * tab_2 * tab_3
+    DeviceArray<double> tau;  // nat * 3, units of lat0, atoms grouped by type
+};
+
 struct Hamilt {
     PWGrid* grid = nullptr;
     int precision = 0;  // 0 = FP64, 1 = mixed
@@ -52,6 +71,13 @@ struct Hamilt {
     DeviceArray<float> deeqf;
     HpsiWork work;  // default scratch for callers that do not bring their own
     int chunk_override = 0;  // bands per stick-buffer chunk chosen by the autotuner (0 = 48 MB rule)
+    VnlTables vnl;           // projector tables for on-device getvnl
+
+    void set_projectors(int ntype, const int* na, const int* nbeta, const int* nh, int nhm, int lmax, const int* indv,
+                        const int* nhtol, const int* nhtolm, int tab_2, int tab_3, double dq, const double* tab_h,
+                        const double* tau_h);
+    // getvnl for k-point ik: the FP64 projectors and their FP32 copy, built on the device (stream s)
+    void build_vkb(int ik, cudaStream_t s);
 
     explicit Hamilt(PWGrid* g, int prec);
     ~Hamilt();

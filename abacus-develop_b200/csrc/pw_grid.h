@@ -43,6 +43,7 @@ struct KMap {
     DeviceArray<double> gk2;
     DeviceArray<float> gk2f;
     DeviceArray<double> precond;  // Davidson preconditioner 1 + g2 + sqrt(1 + (g2-1)^2)
+    DeviceArray<double> gkcar;    // k+G cartesian (npw x 3, units of tpiba): PW_Basis_K::getgpluskcar
 };
 
 // Index maps handed to kernels by value.

@@ -103,6 +103,67 @@ def tc_cgemm_error():
     return code.value
 
 
+def _ints(v):
+    v = [int(x) for x in v]
+    return (C.c_int * max(1, len(v)))(*v)
+
+
+def cal_ylm_real_op(ng, lmax, g, ylm, stream=None):
+    """ModuleBase::cal_ylm_real_op<FP, DEVICE_GPU>: g (ng x 3) -> ylm ((lmax+1)^2 x ng)."""
+    torch = _torch()
+    f = "b200_cal_ylm_real_op_f64" if ylm.dtype == torch.float64 else "b200_cal_ylm_real_op_f32"
+    call(f, ng, lmax, ptr(g), ptr(ylm), stream_ptr(stream))
+
+
+def cal_sk_op(ik, ntype, nx, ny, nz, rho_nx, rho_ny, rho_nz, npw, npwx, fftny, eigts1_nc, eigts2_nc, eigts3_nc,
+              atom_na, igl2isz, is2fftixy, two_pi, kvec_c, atom_tau, eigts1, eigts2, eigts3, sk, stream=None):
+    """hamilt::cal_sk_op<FP, DEVICE_GPU> (wf_op.h); atom_na is a host sequence, the rest device tensors."""
+    torch = _torch()
+    f = "b200_cal_sk_op_f64" if sk.dtype == torch.complex128 else "b200_cal_sk_op_f32"
+    call(f, ik, ntype, nx, ny, nz, rho_nx, rho_ny, rho_nz, npw, npwx, fftny, eigts1_nc, eigts2_nc, eigts3_nc,
+         _ints(atom_na), ptr(igl2isz), ptr(is2fftixy), two_pi, ptr(kvec_c), ptr(atom_tau), ptr(eigts1), ptr(eigts2),
+         ptr(eigts3), ptr(sk), stream_ptr(stream))
+
+
+def cal_vnl_op(ntype, npw, npwx, nhm, tab_2, tab_3, atom_na, atom_nb, atom_nh, dq, tpiba, gk, ylm, indv, nhtol,
+               nhtolm, tab, vkb1, sk, vkb, stream=None):
+    """hamilt::cal_vnl_op<FP, DEVICE_GPU> (vnl_op.h:58-100); per-type counts are host sequences."""
+    torch = _torch()
+    f = "b200_cal_vnl_op_f64" if vkb.dtype == torch.complex128 else "b200_cal_vnl_op_f32"
+    call(f, ntype, npw, npwx, nhm, tab_2, tab_3, _ints(atom_na), _ints(atom_nb), _ints(atom_nh), dq, tpiba, ptr(gk),
+         ptr(ylm), ptr(indv), ptr(nhtol), ptr(nhtolm), ptr(tab), ptr(vkb1), ptr(sk), ptr(vkb), stream_ptr(stream))
+
+
+@dataclass
+class ProjectorSet:
+    """The projector tables getvnl reads (pseudopot_cell_vnl after init_vnl): per type na / nbeta / nh, the
+    (ih -> beta, l, lm) maps indv / nhtol / nhtolm (ntype x nhm), the radial table tab (ntype x tab_2 x tab_3,
+    step dq in bohr^-1) and lmax."""
+    ntype: int
+    na: list
+    nbeta: list
+    nh: list
+    nhm: int
+    lmax: int
+    indv: np.ndarray
+    nhtol: np.ndarray
+    nhtolm: np.ndarray
+    tab: np.ndarray
+    dq: float
+
+    @property
+    def tab_2(self):
+        return int(self.tab.shape[1])
+
+    @property
+    def tab_3(self):
+        return int(self.tab.shape[2])
+
+    @property
+    def nkb(self):
+        return int(sum(a * h for a, h in zip(self.na, self.nh)))
+
+
 # ------------------------------------------------------------------ basis
 class PWBasisK:
     """ModulePW::PW_Basis_K for one pool: grid, G sphere, index maps, device transforms."""
@@ -232,6 +293,22 @@ class HamiltPW:
         cannot allocate (graph capture, externally owned memory pools); scratch is a fixed 32 MiB array
         inside the library shared by all calls, so concurrent calls on one device must be serialised."""
         call("b200_hamilt_hpsi_local_noalloc", self._h, ik, nbands, ld, ptr(psi), ptr(hpsi), stream_ptr(stream))
+
+    def set_projectors(self, proj: ProjectorSet, tau_lat0):
+        """Projector tables for on-device getvnl; tau_lat0: (nat, 3) positions in units of lat0, by type."""
+        tab = np.ascontiguousarray(proj.tab, dtype=np.float64).reshape(-1)
+        tau = np.ascontiguousarray(tau_lat0, dtype=np.float64).reshape(-1)
+        call("b200_hamilt_set_projectors", self._h, proj.ntype, _ints(proj.na), _ints(proj.nbeta), _ints(proj.nh),
+             proj.nhm, proj.lmax, _ints(np.asarray(proj.indv).reshape(-1)), _ints(np.asarray(proj.nhtol).reshape(-1)),
+             _ints(np.asarray(proj.nhtolm).reshape(-1)), proj.tab_2, proj.tab_3, float(proj.dq),
+             tab.ctypes.data_as(_lib.pf64), tau.ctypes.data_as(_lib.pf64))
+
+    def build_vkb(self, ik, stream=None):
+        """getvnl on the device for k-point ik (replaces any set_vkb of that k-point)."""
+        call("b200_hamilt_build_vkb", self._h, ik, stream_ptr(stream))
+
+    def copy_vkb(self, ik, out, stream=None):
+        call("b200_hamilt_copy_vkb", self._h, ik, ptr(out), stream_ptr(stream))
 
     @staticmethod
     def _kbatch_args(iks, psis, hpsis):

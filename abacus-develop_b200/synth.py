@@ -170,6 +170,26 @@ class SynthCell:
                 out[ia * NH + j, :npw] = ((-1j) ** l) * radial[(rc, l)] * _ylm_real(l, m, q) * sk
         return out
 
+    def projector_tables(self, omega: float, ecut: float, dq: float = 0.01):
+        """The same projectors as ``vkb`` as getvnl tables: one atom type, 4 radial functions (r_c, l) on a q
+        grid of step dq reaching past sqrt(ecut), 8 (beta, l, lm) channels per atom in the order of ``vkb``.
+        getvnl's real Y_lm differ from ``vkb``'s by a sign for (l, m) = (1, +-1); D is diagonal, so the
+        Hamiltonian is the same."""
+        from .pwdft import ProjectorSet
+        nq = int(math.sqrt(ecut) / dq + 4) + 1
+        q = np.arange(nq) * dq
+        betas = [(0.8, 0), (0.8, 1), (1.2, 0), (1.2, 1)]
+        tab = np.zeros((1, len(betas), nq))
+        for ib, (rc, l) in enumerate(betas):
+            integ = math.gamma(l + 1.5) / (2.0 * rc ** (2 * l + 3))
+            c = math.sqrt((2 * math.pi) ** 3 / omega / integ)
+            tab[0, ib] = c * q ** l * np.exp(-0.5 * q * q * rc * rc)
+        indv = np.array([[0, 1, 1, 1, 2, 3, 3, 3]])
+        nhtol = np.array([[0, 1, 1, 1, 0, 1, 1, 1]])
+        nhtolm = np.array([[0, 1, 2, 3, 0, 1, 2, 3]])
+        return ProjectorSet(ntype=1, na=[self.nat], nbeta=[len(betas)], nh=[NH], nhm=NH, lmax=1, indv=indv,
+                            nhtol=nhtol, nhtolm=nhtolm, tab=tab, dq=dq)
+
     def psi0(self, q: np.ndarray, nbands: int, npwx: int, seed_offset: int = 0) -> np.ndarray:
         """Start vectors, (nbands, npwx) row-major complex128 (band b at b*npwx)."""
         rng = np.random.Generator(np.random.PCG64(self.spec.seed * 7919 + 17 + seed_offset))

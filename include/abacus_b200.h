@@ -193,6 +193,48 @@ int b200_graph_destroy(b200_graph* g);
 int b200_hamilt_autotune(b200_hamilt* h, int ik, int nbands, int ld, const void* psi_d, void* hpsi_d, void* stream,
                          int* best_chunk);
 
+/* ---- projector generation (pseudopot_cell_vnl::getvnl, VNL_in_pw.cpp:412-540) ---- */
+/* ModuleBase::cal_ylm_real_op<FP, DEVICE_GPU> (module_base/kernels/math_op.h): real Y_lm of ng vectors
+ * g (ng x 3) into ylm ((lmax+1)^2 x ng), lmax <= 4.  The reference's scratch p is internal here. */
+int b200_cal_ylm_real_op_f64(int ng, int lmax, const double* g_d, double* ylm_d, void* stream);
+int b200_cal_ylm_real_op_f32(int ng, int lmax, const float* g_d, float* ylm_d, void* stream);
+/* hamilt::cal_sk_op<FP, DEVICE_GPU> (kernels/wf_op.h): structure factor sk (nat x npw complex).
+ * atom_na is a host array of ntype counts; every other pointer is device memory, as the reference's. */
+int b200_cal_sk_op_f64(int ik, int ntype, int nx, int ny, int nz, int rho_nx, int rho_ny, int rho_nz, int npw, int npwx,
+                       int fftny, int eigts1_nc, int eigts2_nc, int eigts3_nc, const int* atom_na,
+                       const int* igl2isz_d, const int* is2fftixy_d, double two_pi, const double* kvec_c_d,
+                       const double* atom_tau_d, const void* eigts1_d, const void* eigts2_d, const void* eigts3_d,
+                       void* sk_d, void* stream);
+int b200_cal_sk_op_f32(int ik, int ntype, int nx, int ny, int nz, int rho_nx, int rho_ny, int rho_nz, int npw, int npwx,
+                       int fftny, int eigts1_nc, int eigts2_nc, int eigts3_nc, const int* atom_na,
+                       const int* igl2isz_d, const int* is2fftixy_d, float two_pi, const float* kvec_c_d,
+                       const float* atom_tau_d, const void* eigts1_d, const void* eigts2_d, const void* eigts3_d,
+                       void* sk_d, void* stream);
+/* hamilt::cal_vnl_op<FP, DEVICE_GPU> (kernels/vnl_op.h:58-100): vkb (nkb x npwx complex, entries < npw
+ * written) from gk, ylm, the radial table and sk.  atom_na / atom_nb / atom_nh are host arrays (ntype <= 8;
+ * the reference copies them to the device first, VNL_in_pw.cpp:467-473); vkb1_d is accepted and unused
+ * (the product kernel keeps that intermediate in registers). */
+int b200_cal_vnl_op_f64(int ntype, int npw, int npwx, int nhm, int tab_2, int tab_3, const int* atom_na,
+                        const int* atom_nb, const int* atom_nh, double dq, double tpiba, const double* gk_d,
+                        const double* ylm_d, const double* indv_d, const double* nhtol_d, const double* nhtolm_d,
+                        const double* tab_d, double* vkb1_d, const void* sk_d, void* vkb_d, void* stream);
+int b200_cal_vnl_op_f32(int ntype, int npw, int npwx, int nhm, int tab_2, int tab_3, const int* atom_na,
+                        const int* atom_nb, const int* atom_nh, float dq, float tpiba, const float* gk_d,
+                        const float* ylm_d, const float* indv_d, const float* nhtol_d, const float* nhtolm_d,
+                        const float* tab_d, float* vkb1_d, const void* sk_d, void* vkb_d, void* stream);
+/* Projector tables of the handle's cell (the state pseudopot_cell_vnl::init_vnl prepares): per type na,
+ * nbeta, nh; per (type, ih) indv / nhtol / nhtolm (host, ntype x nhm); the radial table tab
+ * (host, ntype x tab_2 x tab_3, step dq in bohr^-1, the 4-pi/sqrt(omega) factor included); atom positions
+ * tau (host, nat x 3, units of lat0, grouped by type).  The table must reach past the cut-off. */
+int b200_hamilt_set_projectors(b200_hamilt* h, int ntype, const int* na, const int* nbeta, const int* nh, int nhm,
+                               int lmax, const int* indv, const int* nhtol, const int* nhtolm, int tab_2, int tab_3,
+                               double dq, const double* tab, const double* tau);
+/* getvnl for k-point ik into the handle's projectors (FP64 and the FP32 copy), one fused launch;
+ * replaces any b200_hamilt_set_vkb of that k-point. */
+int b200_hamilt_build_vkb(b200_hamilt* h, int ik, void* stream);
+/* Copies the handle's FP64 projectors of k-point ik (nkb x npwk_max complex128) to vkb_d. */
+int b200_hamilt_copy_vkb(const b200_hamilt* h, int ik, void* vkb_d, void* stream);
+
 /* gemm_op<std::complex<float>, DEVICE_GPU> (module_hsolver/kernels/math_kernel_op.h:240-265) on the
  * tensor cores: C = alpha * op(A) * B + beta * C, complex64 column-major, transa 'N' or 'C', transb 'N'.
  * Split precision (3xTF32: hi*hi + hi*lo + lo*hi, FP32 accumulate), about FP32 accuracy.

@@ -8,6 +8,9 @@ reference's unit tests as text and writes ``tests/golden/*.npz``:
   nonlocal_op.npz  <- .../kernels/test/nonlocal_op_test.cpp
   veff_op.npz      <- .../kernels/test/veff_op_test.cpp
   pw_op.npz        <- source/module_basis/module_pw/kernels/test/pw_op_test.cpp
+  vnl_op.npz       <- .../kernels/test/vnl_op_test.cpp
+  wf_op.npz        <- .../kernels/test/wf_op_test.cpp
+  ylm_op.npz       <- source/module_base/kernels/test/math_op_test.cpp
   pyabacus_si2.npz <- python/pyabacus/tests/test_diag/Si2.mat (sparse H, CSC arrays)
 
 The fixtures are committed; tests never read the reference tree.
@@ -38,7 +41,7 @@ def _parse_block(text: str):
 def _vectors(path: Path) -> dict:
     src = path.read_text()
     out = {}
-    for m in re.finditer(r"std::vector<[^=;{]*?>\s+(\w+)\s*=\s*\{", src):
+    for m in re.finditer(r"std::vector<[^=;{]*?>\s+(\w+)\s*=?\s*\{", src):
         name = m.group(1)
         i = m.end()
         depth = 1
@@ -85,6 +88,32 @@ def main():
     np.savez(OUT / "pw_op.npz", box_index=v["box_index"].astype(np.int64), in_1=v["in_1"], out_1=v["out_1"],
              in_2=v["in_2"], out_2=v["out_2"], in_3=v["in_3"], out_3=v["out_3"], out_3_init=v["out_3_init"],
              npwk=int(s["npwk"]), nxyz=int(s["nxyz"]), factor=s["factor"])
+
+    # projector generation: cal_vnl_op, cal_sk_op and cal_ylm_real_op literals
+    v = _vectors(kt / "vnl_op_test.cpp")
+    s = _scalars(kt / "vnl_op_test.cpp", ["ntype", "npw", "npwx", "nhm", "tab_2", "tab_3", "DQ", "tpiba"])
+    src = (kt / "vnl_op_test.cpp").read_text()
+    brace = {n: int(re.search(r"std::vector<int>\s+" + n + r"\{(\d+)\}", src).group(1))
+             for n in ("atom_na", "atom_nb", "atom_nh")}
+    np.savez(OUT / "vnl_op.npz", gk=v["gk"], ylm=v["ylm"], indv=v["indv"], nhtol=v["nhtol"], nhtolm=v["nhtolm"],
+             tab=v["tab"], sk=v["sk"], expected_vkb=v["expected_vkb"],
+             **{k: (x if k in ("DQ", "tpiba") else int(x)) for k, x in s.items()}, **brace)
+
+    wt = kt / "wf_op_test.cpp"
+    v = _vectors(wt)
+    s = _scalars(wt, ["ik", "ntype", "nx", "ny", "nz", "rho_nx", "rho_ny", "rho_nz", "npw", "npwx", "fftny",
+                      "eigts1_nc", "eigts2_nc", "eigts3_nc", "TWO_PI"])
+    src = wt.read_text()
+    na = int(re.search(r"std::vector<int>\s+atom_na\{(\d+)\}", src).group(1))
+    np.savez(OUT / "wf_op.npz", igl2isz=v["igl2isz"].astype(np.int64), is2fftixy=v["is2fftixy"].astype(np.int64),
+             kvec_c=v["kvec_c"], atom_tau=v["atom_tau"], eigts1=v["eigts1"], eigts2=v["eigts2"],
+             eigts3=v["eigts3"], expected_sk=v["expected_sk"], atom_na=na,
+             **{k: (x if k == "TWO_PI" else int(x)) for k, x in s.items()})
+
+    mt = REF / "source/module_base/kernels/test/math_op_test.cpp"
+    v = _vectors(mt)
+    s = _scalars(mt, ["ng", "lmax"])
+    np.savez(OUT / "ylm_op.npz", g=v["g"], expected_ylm=v["expected_ylm"], ng=int(s["ng"]), lmax=int(s["lmax"]))
 
     try:
         import scipy.io
