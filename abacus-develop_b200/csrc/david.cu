@@ -157,6 +157,7 @@ template <typename T> struct Engine {
     using R = typename RealOf<T>::type;
     static constexpr bool kF32 = std::is_same<T, float2>::value;
     int nband, dim, nbase_x, ld, L, ncp;
+    int dim_cap;  // capacity: every buffer holds vectors of up to dim_cap entries
     cudaStream_t s = 0;
     cublasHandle_t cb = nullptr;
     cusolverDnHandle_t cs = nullptr;
@@ -190,7 +191,7 @@ template <typename T> struct Engine {
     }
 
     Engine(int nb, int d, int ndim, const double* precond_d)
-        : nband(nb), dim(d), nbase_x(ndim * nb), ld(kF32 ? even(d) : d), L(even(ndim * nb)), ncp(even(nb)) {
+        : nband(nb), dim(d), nbase_x(ndim * nb), ld(kF32 ? even(d) : d), L(even(ndim * nb)), ncp(even(nb)), dim_cap(d) {
         B200_CHECK(ndim > 1 && nb > 0 && ndim * nb < d, kInvalidArgument, "need david_ndim > 1 and david_ndim*nband < dim");
         B200_CUBLAS_D(cublasCreate(&cb));
         B200_CUSOLVER(cusolverDnCreate(&cs));
@@ -239,6 +240,25 @@ template <typename T> struct Engine {
         eig_h.assign(nbase_x, 0.0);
         unconv_h.assign(nband, 0);
         B200_CUDA(cudaStreamSynchronize(s));
+    }
+    // Re-use the buffers for vectors of length d <= dim_cap (another k-point of the same cell) with its
+    // preconditioner; nothing is allocated.
+    void retarget(int d, const double* precond_d) {
+        B200_CHECK(d <= dim_cap && nbase_x < d, kInvalidArgument, "retarget: need david_ndim*nband < dim <= capacity");
+        dim = d;
+        ld = kF32 ? even(d) : d;
+        if constexpr (std::is_same<R, double>::value) {
+            B200_CUDA(cudaMemcpyAsync(pc.ptr, precond_d, dim * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        } else {
+            k_convert_real<R><<<grid_of(dim), kT, 0, s>>>(dim, precond_d, pc.ptr);
+            note_launch();
+            B200_CUDA(cudaGetLastError());
+        }
+    }
+    size_t device_bytes() const {
+        return (basis.n + hp.n + newv.n + hcc.n + vcc.n + vc.n + vcl.n + lag.n + gram.n) * sizeof(T) +
+               (A64.n + gram64.n + winv.n + work.n) * sizeof(double2) + (w.n + ein.n) * sizeof(double) +
+               pc.n * sizeof(R) + tcw.device_bytes();
     }
     ~Engine() {
         if (cb) cublasDestroy(cb);
@@ -360,7 +380,7 @@ template <typename T> struct Engine {
             B200_CHECK(std::isfinite(eig_h[m]), kNumericalError, "non-finite eigenvalue (NaN/Inf in H|psi> or psi)");
         tock(t_eig);
         if constexpr (kF32) {
-            const int e = tcw.err.ptr ? tcw.read_error() : 0;
+            const int e = tcw.err.ptr ? tcw.read_error(s) : 0;
             B200_CHECK(e == 0, kCudaError, "tensor-core GEMM wait ran out (error word " + std::to_string(e) + ")");
         }
     }
@@ -450,6 +470,10 @@ template <typename T> struct Engine {
              int& notconv) {
         int ntry = 0, total = 0;
         notconv = 0;
+        // a fresh subspace, as a newly constructed DiagoDavid has (diago_david.cpp:34-148): the refresh reads
+        // columns of vcc that this solve may not have written, so a reused solver must start from zeros
+        B200_CUDA(cudaMemsetAsync(hcc.ptr, 0, hcc.n * sizeof(T), s));
+        B200_CUDA(cudaMemsetAsync(vcc.ptr, 0, vcc.n * sizeof(T), s));
         do {
             total += diag_once(f, ldpsi, psi, eig, thr, maxiter, notconv);
             ++ntry;
@@ -461,7 +485,7 @@ template <typename T> struct Engine {
 class David : public DavidBase {
   public:
     David(int nband, int dim, int ndim, int precision, const double* precond_d)
-        : nband_(nband), dim_(dim), ndim_(ndim), precision_(precision) {
+        : nband_(nband), dim_(dim), cap_(dim), ndim_(ndim), precision_(precision) {
         B200_CHECK(precision == 0 || precision == 1, kInvalidArgument, "bad precision");
         pc_.resize(dim);
         B200_CUDA(cudaMemcpy(pc_.ptr, precond_d, dim * sizeof(double), cudaMemcpyDeviceToDevice));
@@ -485,8 +509,9 @@ class David : public DavidBase {
         int total = 0, nc = 0;
         if (precision == 1) {
             if (!e32_) {
-                e32_ = std::make_unique<Engine<float2>>(nband_, dim_, ndim_, pc_.ptr);
+                e32_ = std::make_unique<Engine<float2>>(nband_, cap_, ndim_, pc_.ptr);
                 e32_->set_stream(stream_);
+                if (dim_ != cap_) e32_->retarget(dim_, pc_.ptr);
             }
             e32_->ref_refresh = e64_->ref_refresh;
             e32_->verbosity = verbosity_;
@@ -525,13 +550,25 @@ class David : public DavidBase {
         e64_->verbosity = level;
         if (e32_) e32_->verbosity = level;
     }
+    void retarget(int dim, const double* precond_d) override {
+        B200_CHECK(dim <= cap_, kInvalidArgument, "retarget beyond the solver's capacity");
+        B200_CUDA(cudaMemcpyAsync(pc_.ptr, precond_d, dim * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
+        dim_ = dim;
+        e64_->retarget(dim, pc_.ptr);
+        if (e32_) e32_->retarget(dim, pc_.ptr);
+    }
+    size_t device_bytes() const override {
+        size_t b = pc_.n * sizeof(double) + psi32_.n * sizeof(float2) + e64_->device_bytes();
+        if (e32_) b += e32_->device_bytes();
+        return b;
+    }
     void set_reference_refresh(bool on) override {
         e64_->ref_refresh = on;
         if (e32_) e32_->ref_refresh = on;
     }
 
   private:
-    int nband_, dim_, ndim_, precision_;
+    int nband_, dim_, cap_, ndim_, precision_;
     int notconv_ = 0;
     int verbosity_ = 0;
     cudaStream_t stream_ = 0;

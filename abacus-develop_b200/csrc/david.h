@@ -34,6 +34,11 @@ struct DavidBase {
     virtual void set_verbosity(int level) = 0;
     // stream for all of the solver's work (default: the legacy default stream, as the reference)
     virtual void set_stream(cudaStream_t s) = 0;
+    // solve vectors of length dim <= the construction dim next (another k-point of the same cell), with
+    // that k-point's preconditioner; reuses every buffer
+    virtual void retarget(int dim, const double* precond_d) = 0;
+    // device memory held by the solver (bytes)
+    virtual size_t device_bytes() const = 0;
 };
 
 std::unique_ptr<DavidBase> make_david(int nband, int dim, int david_ndim, int precision, const double* precond_d);

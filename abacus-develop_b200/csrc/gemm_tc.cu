@@ -510,9 +510,12 @@ void TcGemmWorkspace::ensure() {
     }
 }
 
-int TcGemmWorkspace::read_error() {
+int TcGemmWorkspace::read_error(cudaStream_t s) {
     int h = 0;
-    if (err.ptr) B200_CUDA(cudaMemcpy(&h, err.ptr, sizeof(int), cudaMemcpyDeviceToHost));
+    if (err.ptr) {
+        B200_CUDA(cudaMemcpyAsync(&h, err.ptr, sizeof(int), cudaMemcpyDeviceToHost, s));
+        B200_CUDA(cudaStreamSynchronize(s));
+    }
     return h;
 }
 

@@ -10,7 +10,8 @@ struct TcGemmWorkspace {
     DeviceArray<float> ws;  // split-K partial tiles
     DeviceArray<int> err;   // nonzero after a bounded wait ran out inside the kernel
     void ensure();
-    int read_error();       // synchronous read of the error word
+    int read_error(cudaStream_t s = 0);  // read of the error word after the work queued on s
+    size_t device_bytes() const { return ws.n * sizeof(float) + err.n * sizeof(int); }
 };
 
 // C (M x N) = alpha * op(A) * B + beta * C, complex64, column-major, op(A) in {'N', 'C'}.

@@ -288,6 +288,32 @@ int b200_solve_kpoints(b200_hamilt* h, int nk, const int* iks, int spin, int nba
                        const double* const* precond_d, void* const* psi_d, int ldpsi, double* eigenvalues, double thr,
                        int maxiter, int ntry_max, int notconv_max, int nworkers, int* iters);
 
+/* ---- serving: non-self-consistent band solves with continuous admission (no counterpart in the
+ * reference, whose NSCF driver solves its k-points one after another, hsolver_pw.cpp:212-299) ----
+ * A server owns nworkers threads, each with its own non-blocking stream.  Cells are Hamiltonian handles
+ * with V_eff, D and the projectors of all their k-points set; they stay resident.  A request (cell,
+ * k-point, nbands, precision, thr, seed) is queued; the queue head is admitted when a worker is idle and
+ * a solver slot for its shape is pooled or fits in the HBM budget (idle slots of other shapes are
+ * released to make room).  Start vectors are generated on the device from the seed, so a result does
+ * not depend on the other requests in flight.  Times are seconds since the server was created. */
+typedef struct b200_server b200_server;
+int b200_server_create(unsigned long long hbm_budget_bytes, int nworkers, int david_ndim, b200_server** out);
+int b200_server_destroy(b200_server* s);
+int b200_server_add_cell(b200_server* s, b200_hamilt* h, int* cell_id);
+/* eig_out (host, nbands doubles) must stay valid until the request is reported by b200_server_poll. */
+int b200_server_submit(b200_server* s, int cell, int ik, int nbands, int precision, double thr, int maxiter,
+                       unsigned long long seed, double* eig_out, long long* req_id);
+/* Reports up to max_out completed requests (wait != 0: blocks until one is done or none is outstanding):
+ * id, status (B200_STATUS_*), submit / admit / completion times, Davidson iterations (all stages and
+ * the low-precision stage).  The message of the last failed request reported is b200_last_error(). */
+int b200_server_poll(b200_server* s, int max_out, int wait, long long* ids, int* status, double* t_submit,
+                     double* t_admit, double* t_done, int* iters, int* iters_low, int* n_out);
+/* Blocks until every submitted request has completed. */
+int b200_server_drain(b200_server* s);
+/* out6: pooled slot bytes, peak pooled bytes, peak requests in flight, slots created, slots evicted,
+ * seconds since creation. */
+int b200_server_stats(b200_server* s, double* out6);
+
 #ifdef __cplusplus
 }
 #endif
