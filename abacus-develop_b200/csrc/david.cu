@@ -509,9 +509,13 @@ class David : public DavidBase {
         int total = 0, nc = 0;
         if (precision == 1) {
             if (!e32_) {
+                // the engine's constructor works on the legacy stream: let the writes of pc_ queued on the
+                // solver's stream finish first, then re-target on that stream (the current k-point's
+                // preconditioner, in stream order)
+                B200_CUDA(cudaStreamSynchronize(stream_));
                 e32_ = std::make_unique<Engine<float2>>(nband_, cap_, ndim_, pc_.ptr);
                 e32_->set_stream(stream_);
-                if (dim_ != cap_) e32_->retarget(dim_, pc_.ptr);
+                e32_->retarget(dim_, pc_.ptr);
             }
             e32_->ref_refresh = e64_->ref_refresh;
             e32_->verbosity = verbosity_;
