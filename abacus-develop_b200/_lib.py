@@ -93,6 +93,8 @@ _SIGS = {
     "b200_david_diag": ([vp, HPSI_CB, vp, i32, vp, pf64, f64, i32, i32, i32, pi32], i32),
     "b200_david_diag_hamilt": ([vp, vp, i32, i32, i32, vp, pf64, f64, i32, i32, i32, pi32], i32),
     "b200_david_stats": ([vp, pi32, pi32, pi32], i32),
+    "b200_david_set_trace": ([vp, i32], i32),
+    "b200_david_trace": ([vp, i32, i32, pf64, pi32, pf64, pi32], i32),
     "b200_david_set_verbosity": ([vp, i32], i32),
     "b200_david_set_stream": ([vp, vp], i32),
     "b200_david_set_mixed_threshold": ([vp, f64], i32),

@@ -1,3 +1,4 @@
+#include <algorithm>
 // C-ABI entry points (include/abacus_b200.h).  Every call catches library
 // errors and returns a status; the message is kept per thread.
 #include <cstring>
@@ -373,6 +374,27 @@ int b200_david_set_mixed_threshold(b200_david* d, double thr) {
     return guarded([&] {
         B200_CHECK(d != nullptr && thr > 0.0, b200::kInvalidArgument, "bad argument");
         d->d->set_mixed_thr(thr);
+    });
+}
+int b200_david_set_trace(b200_david* d, int on) {
+    return guarded([&] {
+        B200_CHECK(d != nullptr, b200::kInvalidArgument, "NULL argument");
+        d->d->trace().on = on != 0;
+    });
+}
+int b200_david_trace(b200_david* d, int max_iters, int nband, double* t, int* stage, double* eig, int* n_out) {
+    return guarded([&] {
+        B200_CHECK(d && n_out, b200::kInvalidArgument, "NULL argument");
+        const b200::DavidTrace& tr = d->d->trace();
+        const int n = int(tr.t.size());
+        B200_CHECK(n == 0 || int(tr.eig.size()) == n * nband, b200::kInvalidArgument, "nband differs from the solver's");
+        const int m = n < max_iters ? n : max_iters;
+        for (int i = 0; i < m; ++i) {
+            if (t) t[i] = tr.t[i];
+            if (stage) stage[i] = tr.stage[i];
+            if (eig) std::copy(tr.eig.begin() + size_t(i) * nband, tr.eig.begin() + size_t(i + 1) * nband, eig + size_t(i) * nband);
+        }
+        *n_out = n;
     });
 }
 int b200_david_stats(const b200_david* d, int* iters_low, int* iters_fp64, int* hpsi_bands) {

@@ -173,6 +173,10 @@ template <typename T> struct Engine {
     bool ref_refresh = true;
     int hpsi_bands = 0;
     int verbosity = 0;
+    DavidTrace* trace = nullptr;
+    void record() {
+        if (trace) trace->record(kF32 ? 1 : 0, eig_h.data(), nband);
+    }
     // verbosity >= 2: synchronising phase timers (seconds) for H|psi>, subspace GEMMs / orthogonalisation, eigensolve
     double t_hpsi = 0, t_lin = 0, t_eig = 0;
     std::chrono::steady_clock::time_point tmark;
@@ -431,6 +435,7 @@ template <typename T> struct Engine {
         cal_elem(0, nband);
         int nbase = nband;
         eigsolve(nbase);
+        record();
         for (int m = 0; m < nband; ++m) eig_in[m] = eig_h[m];
         notconv = nband;
         for (int m = 0; m < nband; ++m) unconv_h[m] = m;
@@ -443,6 +448,7 @@ template <typename T> struct Engine {
             tock(t_lin);
             nbase += notconv;
             eigsolve(nbase);
+            record();
             notconv = 0;
             double dmax = 0.0;
             for (int m = 0; m < nband; ++m) {
@@ -495,6 +501,8 @@ class David : public DavidBase {
              int notconv_max) override {
         B200_CHECK(precision_ == 0, kInvalidArgument, "a mixed-precision solve needs a Hamiltonian handle");
         stats_ = DavidStats{};
+        trace_.reset();
+        e64_->trace = &trace_;
         e64_->hpsi_bands = 0;
         int nc = 0;
         const int it = e64_->diag(f64, ldpsi, (double2*)psi, eig, thr, maxiter, ntry_max, notconv_max, nc);
@@ -506,6 +514,8 @@ class David : public DavidBase {
     int diag_hamilt(const HPsiDevice& f64, const HPsiDevice& f32, int precision, int ldpsi, void* psi, double* eig,
                     double thr, int maxiter, int ntry_max, int notconv_max) override {
         stats_ = DavidStats{};
+        trace_.reset();
+        e64_->trace = &trace_;
         int total = 0, nc = 0;
         if (precision == 1) {
             if (!e32_) {
@@ -518,6 +528,7 @@ class David : public DavidBase {
                 e32_->retarget(dim_, pc_.ptr);
             }
             e32_->ref_refresh = e64_->ref_refresh;
+            e32_->trace = &trace_;
             e32_->verbosity = verbosity_;
             e32_->hpsi_bands = 0;
             psi32_.resize(size_t(nband_) * ldpsi);
@@ -542,6 +553,7 @@ class David : public DavidBase {
         return total + it64;
     }
     const DavidStats& stats() const override { return stats_; }
+    DavidTrace& trace() override { return trace_; }
     void set_mixed_thr(double thr) override { mixed_thr_ = thr; }
     int precision() const override { return precision_; }
     void set_stream(cudaStream_t st) override {
@@ -582,6 +594,7 @@ class David : public DavidBase {
     std::unique_ptr<Engine<double2>> e64_;
     std::unique_ptr<Engine<float2>> e32_;
     DavidStats stats_;
+    DavidTrace trace_;
 };
 
 }  // namespace

@@ -2,8 +2,10 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <chrono>
 #include <functional>
 #include <memory>
+#include <vector>
 
 namespace b200 {
 
@@ -15,6 +17,28 @@ struct DavidStats {
     int iters_low = 0;     // Davidson iterations in the low-precision stage (mixed only)
     int iters_fp64 = 0;    // Davidson iterations in FP64
     int hpsi_bands = 0;    // band applications of H (all stages)
+};
+
+// Per-iteration record of a solve: seconds since the solve began (taken when the iteration's eigenvalues
+// reach the host, which every iteration does for its convergence test), the stage (0 = FP64, 1 = FP32)
+// and the nband Ritz values.
+struct DavidTrace {
+    bool on = false;
+    std::chrono::steady_clock::time_point t0;
+    std::vector<double> t, eig;
+    std::vector<int> stage;
+    void reset() {
+        t0 = std::chrono::steady_clock::now();
+        t.clear();
+        eig.clear();
+        stage.clear();
+    }
+    void record(int st, const double* e, int n) {
+        if (!on) return;
+        t.push_back(std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count());
+        stage.push_back(st);
+        eig.insert(eig.end(), e, e + n);
+    }
 };
 
 struct DavidBase {
@@ -39,6 +63,8 @@ struct DavidBase {
     virtual void retarget(int dim, const double* precond_d) = 0;
     // device memory held by the solver (bytes)
     virtual size_t device_bytes() const = 0;
+    // per-iteration eigenvalue trace of the next solves (off by default)
+    virtual DavidTrace& trace() = 0;
 };
 
 std::unique_ptr<DavidBase> make_david(int nband, int dim, int david_ndim, int precision, const double* precond_d);

@@ -426,6 +426,23 @@ class DiagoDavid:
     def set_mixed_threshold(self, thr):
         call("b200_david_set_mixed_threshold", self._h, float(thr))
 
+    def set_trace(self, on=True):
+        """Record per-iteration eigenvalues and times of the next solves (see trace())."""
+        call("b200_david_set_trace", self._h, int(bool(on)))
+
+    def trace(self):
+        """(t seconds since the solve began, stage 0 = FP64 / 1 = FP32, eigenvalues iters x nband) of the last
+        solve, one row per Davidson iteration (the initial Rayleigh-Ritz included)."""
+        n = C.c_int()
+        call("b200_david_trace", self._h, 0, self.nband, None, None, None, C.byref(n))
+        m = n.value
+        t = np.zeros(max(m, 1))
+        st = np.zeros(max(m, 1), dtype=np.int32)
+        e = np.zeros((max(m, 1), self.nband))
+        call("b200_david_trace", self._h, m, self.nband, t.ctypes.data_as(_lib.pf64), st.ctypes.data_as(_lib.pi32),
+             e.ctypes.data_as(_lib.pf64), C.byref(n))
+        return t[:m], st[:m], e[:m]
+
     def stats(self):
         """(iterations in the FP32 stage, iterations in FP64, single-band H applications) of the last solve."""
         a, b, c = C.c_int(), C.c_int(), C.c_int()

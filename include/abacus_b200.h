@@ -278,6 +278,13 @@ int b200_david_set_mixed_threshold(b200_david* d, double thr);
 /* Statistics of the last solve: Davidson iterations in the FP32 stage (mixed only), in FP64,
  * and the number of single-band H applications (all stages). */
 int b200_david_stats(const b200_david* d, int* iters_low, int* iters_fp64, int* hpsi_bands);
+/* Eigenvalue trace (no counterpart in the reference): with on != 0 the next solves record, per
+ * iteration, the seconds since the solve began (taken when that iteration's eigenvalues reach the host
+ * for the convergence test), the stage (0 = FP64, 1 = FP32) and the nband Ritz values.
+ * b200_david_trace copies up to max_iters records (t, stage: max_iters entries; eig: max_iters x nband,
+ * any may be NULL) of the last solve and sets *n_out to the number recorded. */
+int b200_david_set_trace(b200_david* d, int on);
+int b200_david_trace(b200_david* d, int max_iters, int nband, double* t, int* stage, double* eig, int* n_out);
 
 /* Davidson solves of nk k-points of one Hamiltonian handle, nworkers at a time on separate streams
  * (the k loop of HSolverPW::solve, hsolver_pw.cpp:240-270, with the k-points running concurrently).

@@ -80,10 +80,18 @@ def test_david_diamond8(pkg, diamond8, prec):
     nband = wl.spec.nbands
     pc = P.precondition_d(wl.basis, 0)
     dav = P.DiagoDavid(pc, nband, ld, 4, p)
+    dav.set_trace(True)
     psi = torch.from_numpy(psi0.copy()).cuda()
     e = np.zeros(nband)
     it = dav.diag_hamilt(h, 0, ld, psi, e, 1e-10, 100)
     assert np.max(np.abs(e - e_ref)) < 1e-8, (e - e_ref)
+    # trace: one record per iteration plus the initial Rayleigh-Ritz of each stage, times increasing,
+    # FP32 records before FP64 ones, the last record the returned eigenvalues
+    tt, st, te = dav.trace()
+    nstage = 2 if prec == "mixed" else 1
+    assert len(tt) == it + nstage and np.all(np.diff(tt) >= 0)
+    assert np.all(np.diff(st) <= 0) and st[-1] == 0
+    assert np.array_equal(te[-1], e)
     it_low, it64, nh = dav.stats()
     assert it == it_low + it64 and nh > 0
     if prec == "mixed":
