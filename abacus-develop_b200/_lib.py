@@ -78,7 +78,7 @@ _SIGS = {
     "b200_hamilt_build_vkb": ([vp, i32, vp], i32),
     "b200_server_create": ([C.c_ulonglong, i32, i32, C.POINTER(vp)], i32),
     "b200_server_destroy": ([vp], i32),
-    "b200_server_add_cell": ([vp, vp, pi32], i32),
+    "b200_server_add_cell": ([vp, vp, i32, pi32], i32),
     "b200_server_submit": ([vp, i32, i32, i32, i32, f64, i32, C.c_ulonglong, pf64, C.POINTER(C.c_longlong)], i32),
     "b200_server_poll": ([vp, i32, i32, C.POINTER(C.c_longlong), pi32, pf64, pf64, pf64, pi32, pi32, pi32], i32),
     "b200_server_drain": ([vp], i32),

@@ -10,8 +10,10 @@
 //    k-point and the request's band count, the start / result vectors and an H|psi> scratch.  Slots are
 //    pooled and re-targeted to the request's k-point, so the steady state allocates nothing (cudaFree
 //    would synchronise the device and stall every other request in flight);
-//  * admission is first come, first served: the queue head is admitted as soon as a worker is idle and a
-//    slot for it exists or fits in the HBM budget (idle slots of other shapes are released to make room);
+//  * admission is first come, first served within a cell: a worker that falls idle takes the oldest queued
+//    request whose cell is below its in-flight cap and whose slot is pooled or fits in the HBM budget (idle
+//    slots of other shapes are released to make room).  The per-cell caps keep small requests from waiting
+//    behind large ones and bound how many large solves share the device at once;
 //  * every worker owns a non-blocking stream, so admitted requests overlap on the device.
 // A request's result depends only on (cell, k-point, nbands, thr, precision, seed): the start vectors come
 // from a counter-based generator keyed by the seed, each solve starts from a zeroed subspace, and no
@@ -69,6 +71,7 @@ double now_s(std::chrono::steady_clock::time_point t0) {
 struct ServeCell {
     b200_hamilt* h;
     int dim_max, npwx, nks, nkb, kmax;
+    int max_inflight, inflight;
 };
 
 struct Slot {
@@ -114,11 +117,12 @@ class Server {
         free_.clear();
     }
 
-    int add_cell(b200_hamilt* h) {
+    int add_cell(b200_hamilt* h, int max_inflight) {
         B200_CHECK(h != nullptr, kInvalidArgument, "NULL Hamiltonian");
         const PWGrid& g = *h->h->grid;
         B200_CHECK(h->h->has_veff, kInvalidArgument, "cell without V_eff");
-        ServeCell c{h, 0, g.basis.npwk_max, g.basis.nks, 0, 0};
+        B200_CHECK(max_inflight >= 1, kInvalidArgument, "max_inflight must be at least 1");
+        ServeCell c{h, 0, g.basis.npwk_max, g.basis.nks, 0, 0, max_inflight, 0};
         for (int ik = 0; ik < c.nks; ++ik) {
             if (g.kmaps[ik].npw > c.dim_max) {
                 c.dim_max = g.kmaps[ik].npw;
@@ -229,6 +233,19 @@ class Server {
         return b;
     }
 
+    // the oldest queued request whose cell is below its cap and whose slot can be had; for each cell only
+    // its oldest request is considered (first come, first served within a cell)
+    std::deque<Request*>::iterator next_admissible_locked() {
+        std::vector<char> seen(cells_.size(), 0);
+        for (auto it = queue_.begin(); it != queue_.end(); ++it) {
+            const int c = (*it)->cell;
+            if (seen[c]) continue;
+            seen[c] = 1;
+            if (cells_[c].inflight < cells_[c].max_inflight && can_admit_locked(**it)) return it;
+        }
+        return queue_.end();
+    }
+
     bool can_admit_locked(const Request& r) const {
         const SlotKey key{r.cell, r.nbands, r.precision};
         if (free_.count(key)) return true;
@@ -315,10 +332,17 @@ class Server {
         if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) s = nullptr;
         std::unique_lock<std::mutex> lk(mu_);
         for (;;) {
-            cv_work_.wait(lk, [&] { return stop_ || (s && !queue_.empty() && can_admit_locked(*queue_.front())); });
+            std::deque<Request*>::iterator pick;
+            cv_work_.wait(lk, [&] {
+                if (stop_) return true;
+                if (!s) return false;
+                pick = next_admissible_locked();
+                return pick != queue_.end();
+            });
             if (stop_) break;
-            Request* r = queue_.front();
-            queue_.pop_front();
+            Request* r = *pick;
+            queue_.erase(pick);
+            ++cells_[r->cell].inflight;
             size_t reserve = 0;
             std::vector<std::unique_ptr<Slot>> victims;
             std::unique_ptr<Slot> slot = take_slot_locked(*r, reserve, victims);
@@ -353,6 +377,7 @@ class Server {
                 pool_bytes_ -= reserve;  // the slot could not be made
             }
             --inflight_;
+            --cells_[r->cell].inflight;
             done_.push_back(r);
             cv_done_.notify_all();
             cv_work_.notify_all();
@@ -417,10 +442,10 @@ int b200_server_destroy(b200_server* s) {
     return guarded_s([&] { delete s; });
 }
 
-int b200_server_add_cell(b200_server* s, b200_hamilt* h, int* cell_id) {
+int b200_server_add_cell(b200_server* s, b200_hamilt* h, int max_inflight, int* cell_id) {
     return guarded_s([&] {
         B200_CHECK(s && h && cell_id, b200::kInvalidArgument, "NULL argument");
-        *cell_id = s->s->add_cell(h);
+        *cell_id = s->s->add_cell(h, max_inflight);
     });
 }
 

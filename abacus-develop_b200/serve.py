@@ -1,8 +1,9 @@
 """Serving loop for non-self-consistent band solves: resident cells, requests admitted as they arrive.
 
 ``Server`` wraps the native server (include/abacus_b200.h, ``b200_server_*``): worker threads with one
-non-blocking stream each, first-come-first-served admission of the queue head when a worker is idle and
-a solver slot fits in the HBM budget, pooled solver slots re-targeted to each request's k-point.
+non-blocking stream each; an idle worker takes the oldest queued request whose cell is under its in-flight
+cap and whose solver slot fits in the HBM budget (first come, first served within a cell); pooled solver
+slots are re-targeted to each request's k-point.
 
 ``build_serving_cells`` makes the resident cells of the serving workload (the 2-, 8-, 16- and 64-atom
 diamond-lattice cells, each with a high-symmetry k-path whose projectors are built on the device by
@@ -52,9 +53,10 @@ class Server:
         self._pending = {}
         self._mu = threading.Lock()
 
-    def add_cell(self, hamilt: HamiltPW) -> int:
+    def add_cell(self, hamilt: HamiltPW, max_inflight: int = 2) -> int:
+        """Register a resident cell; at most max_inflight of its requests run at once."""
         cid = C.c_int()
-        call("b200_server_add_cell", self._h, hamilt.handle, C.byref(cid))
+        call("b200_server_add_cell", self._h, hamilt.handle, int(max_inflight), C.byref(cid))
         self._cells.append(hamilt)
         return cid.value
 

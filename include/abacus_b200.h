@@ -299,14 +299,15 @@ int b200_solve_kpoints(b200_hamilt* h, int nk, const int* iks, int spin, int nba
  * reference, whose NSCF driver solves its k-points one after another, hsolver_pw.cpp:212-299) ----
  * A server owns nworkers threads, each with its own non-blocking stream.  Cells are Hamiltonian handles
  * with V_eff, D and the projectors of all their k-points set; they stay resident.  A request (cell,
- * k-point, nbands, precision, thr, seed) is queued; the queue head is admitted when a worker is idle and
- * a solver slot for its shape is pooled or fits in the HBM budget (idle slots of other shapes are
- * released to make room).  Start vectors are generated on the device from the seed, so a result does
+ * k-point, nbands, precision, thr, seed) is queued; a worker that falls idle takes the oldest queued
+ * request whose cell has fewer than max_inflight requests running and whose solver slot is pooled or fits
+ * in the HBM budget (idle slots of other shapes are released to make room); requests of one cell are
+ * served first come, first served.  Start vectors are generated on the device from the seed, so a result does
  * not depend on the other requests in flight.  Times are seconds since the server was created. */
 typedef struct b200_server b200_server;
 int b200_server_create(unsigned long long hbm_budget_bytes, int nworkers, int david_ndim, b200_server** out);
 int b200_server_destroy(b200_server* s);
-int b200_server_add_cell(b200_server* s, b200_hamilt* h, int* cell_id);
+int b200_server_add_cell(b200_server* s, b200_hamilt* h, int max_inflight, int* cell_id);
 /* eig_out (host, nbands doubles) must stay valid until the request is reported by b200_server_poll. */
 int b200_server_submit(b200_server* s, int cell, int ik, int nbands, int precision, double thr, int maxiter,
                        unsigned long long seed, double* eig_out, long long* req_id);
