@@ -276,9 +276,33 @@ template <typename T> struct Engine {
     }
 
     // C = al op(A) B + be C; FP32 operands go to the tensor cores (3xTF32) whenever they are valid TMA operands
+    // verbosity >= 3: every GEMM and H|psi> call timed on its own (synchronising); calls over 20 ms reported
+    struct SlowCall {
+        Engine* e;
+        const char* what;
+        int m, n, k;
+        std::chrono::steady_clock::time_point t0;
+        SlowCall(Engine* en, const char* w, int m_, int n_, int k_) : e(en), what(w), m(m_), n(n_), k(k_) {
+            if (e->verbosity >= 3) {
+                cudaStreamSynchronize(e->s);
+                t0 = std::chrono::steady_clock::now();
+            }
+        }
+        ~SlowCall() {
+            if (e->verbosity >= 3) {
+                cudaStreamSynchronize(e->s);
+                const double dt = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+                if (dt > 0.02)
+                    std::fprintf(stderr, "[david %s] slow %s m %d n %d k %d: %.3f s\n", kF32 ? "fp32" : "fp64", what, m, n,
+                                 k, dt);
+            }
+        }
+    };
+
     void gemm(cublasOperation_t a, cublasOperation_t b, int m, int n, int k, T al, const T* A, int lda, const T* B,
               int ldb, T be, T* C, int ldc) {
         if (m <= 0 || n <= 0) return;
+        SlowCall sc(this, a == CUBLAS_OP_N ? "gemm N" : "gemm C", m, n, k);
         if constexpr (kF32) {
             const bool aligned = ((reinterpret_cast<uintptr_t>(A) | reinterpret_cast<uintptr_t>(B)) & 15) == 0;
             if (k > 0 && b == CUBLAS_OP_N && (a == CUBLAS_OP_N || a == CUBLAS_OP_C) && lda % 2 == 0 && ldb % 2 == 0 &&
@@ -405,7 +429,10 @@ template <typename T> struct Engine {
         B200_CUDA(cudaGetLastError());
         orth_block(X, nc, nbase);
         tock(t_lin);
-        f(basis.ptr, hp.ptr + size_t(nbase) * ld, nbase_x, ld, nbase, nbase + nc - 1, s);
+        {
+            SlowCall sc(this, "hpsi", dim, nc, 0);
+            f(basis.ptr, hp.ptr + size_t(nbase) * ld, nbase_x, ld, nbase, nbase + nc - 1, s);
+        }
         hpsi_bands += nc;
         tock(t_hpsi);
     }

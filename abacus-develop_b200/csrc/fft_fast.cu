@@ -120,6 +120,148 @@ __global__ void __launch_bounds__(kPlaneWarps * 32) k_plane_w(PlaneMapView pm, i
     for (int s = tid; s < pm.nst; s += NT) plane[s] = A[pm.xc[s] * LDY + pm.sy[s]];
 }
 
+// ---- register / shuffle transforms for square planes of N = 32*M (M = 2, 3, 4) ----
+// One warp holds one length-N vector, M values per lane.  The inverse transform (exp(+i)) is decimation in
+// frequency: x[32*n1 + lane] -> a radix-M DFT in registers, twiddles W_N^{-lane*k1}, then a 32-point
+// transform across the lanes (five radix-2 stages, partner values by warp shuffles); lane L then holds
+// the outputs k1 + M*bitrev5(L).  The forward transform (exp(-i)) is the transposed algorithm
+// (decimation in time): it takes the values in that permuted order and returns x[32*n1 + lane] in natural
+// order.  The r-space product with V_eff happens in between, on the permuted order, with V_eff stored
+// permuted once (launch_permute_veff); no transform touches shared memory, which the plane pass then uses
+// only to hold the plane and to move a row or column into registers.
+template <typename T> __device__ __forceinline__ T shfl_x(T v, int m) {
+    return cmake<T>(__shfl_xor_sync(0xffffffffu, v.x, m), __shfl_xor_sync(0xffffffffu, v.y, m));
+}
+
+// this lane's forward-sign twiddles: lk[k1] = W_N^{lane*k1}, st[j] = W_{2h}^{lane mod h} with h = 16 >> j
+template <typename T, int N>
+__device__ __forceinline__ void lane_twiddles(const T* __restrict__ roots, int lane, T* lk, T* st) {
+    constexpr int M = N / 32;
+#pragma unroll
+    for (int k1 = 0; k1 < M; ++k1) lk[k1] = roots[(lane * k1) % N];
+#pragma unroll
+    for (int j = 0; j < 5; ++j) {
+        const int h = 16 >> j;
+        st[j] = roots[M * (lane % h) * (16 / h)];
+    }
+}
+
+template <typename T, int M>
+__device__ __forceinline__ void regfft_inv_dif(T* u, const T* lk, const T* st, int lane) {
+    dftR<T, +1, M>(u);
+#pragma unroll
+    for (int k1 = 1; k1 < M; ++k1) u[k1] = cmulc(u[k1], lk[k1]);
+#pragma unroll
+    for (int j = 0; j < 5; ++j) {
+        const int h = 16 >> j;
+        const bool bottom = lane & h;
+#pragma unroll
+        for (int k1 = 0; k1 < M; ++k1) {
+            const T p = shfl_x(u[k1], h);
+            u[k1] = bottom ? cmulc(csub(p, u[k1]), st[j]) : cadd(u[k1], p);
+        }
+    }
+}
+
+template <typename T, int M>
+__device__ __forceinline__ void regfft_fwd_dit(T* u, const T* lk, const T* st, int lane) {
+#pragma unroll
+    for (int j = 4; j >= 0; --j) {
+        const int h = 16 >> j;
+        const bool bottom = lane & h;
+#pragma unroll
+        for (int k1 = 0; k1 < M; ++k1) {
+            const T p = shfl_x(u[k1], h);
+            u[k1] = bottom ? csub(p, cmul(st[j], u[k1])) : cadd(u[k1], cmul(st[j], p));
+        }
+    }
+#pragma unroll
+    for (int k1 = 1; k1 < M; ++k1) u[k1] = cmul(u[k1], lk[k1]);
+    dftR<T, -1, M>(u);
+}
+
+// Plane pass with register transforms; V_eff in the permuted order of launch_permute_veff.
+// Shared memory: the plane (nxc occupied x-columns of N | 1) and the x -> column map.
+template <typename T, typename R, int N>
+__global__ void __launch_bounds__(kPlaneWarps * 32) k_plane_r(PlaneMapView pm, int nz, const T* __restrict__ roots,
+                                                             const R* __restrict__ vperm, T* __restrict__ sb) {
+    constexpr int M = N / 32;
+    constexpr int LD = N | 1;
+    constexpr int NT = kPlaneWarps * 32;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* A = reinterpret_cast<T*>(smem_raw);
+    const int nxc = pm.nxc;
+    int* cmap = reinterpret_cast<int*>(A + nxc * LD);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int band = blockIdx.x;
+    const int z = blockIdx.y;
+    for (int i = tid; i < nxc * LD; i += NT) A[i] = zero_c<T>();
+    for (int i = tid; i < N; i += NT) cmap[i] = -1;
+    __syncthreads();
+    for (int c = tid; c < nxc; c += NT) cmap[pm.xpos[c]] = c;
+    T* plane = sb + (size_t(band) * nz + z) * pm.nst;
+    for (int s = tid; s < pm.nst; s += NT) A[pm.xc[s] * LD + pm.sy[s]] = plane[s];
+    T lk[M], st[5];
+    lane_twiddles<T, N>(roots, lane, lk, st);
+    __syncthreads();
+    int cm[M];
+#pragma unroll
+    for (int n1 = 0; n1 < M; ++n1) cm[n1] = cmap[32 * n1 + lane];
+    // inverse y transform of every occupied column; the result stays in the permuted slot order
+    for (int c = warp; c < nxc; c += kPlaneWarps) {
+        T u[M];
+        T* col = A + c * LD;
+#pragma unroll
+        for (int n1 = 0; n1 < M; ++n1) u[n1] = col[32 * n1 + lane];
+        regfft_inv_dif<T, M>(u, lk, st, lane);
+#pragma unroll
+        for (int k1 = 0; k1 < M; ++k1) col[32 * k1 + lane] = u[k1];
+    }
+    __syncthreads();
+    // each row slot: inverse x transform, times V_eff(r), forward x transform
+    const R* vz = vperm + size_t(z) * N * N;
+    for (int sy = warp; sy < N; sy += kPlaneWarps) {
+        T u[M];
+#pragma unroll
+        for (int n1 = 0; n1 < M; ++n1) u[n1] = cm[n1] >= 0 ? A[cm[n1] * LD + sy] : zero_c<T>();
+        regfft_inv_dif<T, M>(u, lk, st, lane);
+        const R* vr = vz + sy * N;
+#pragma unroll
+        for (int k1 = 0; k1 < M; ++k1) u[k1] = cscale(u[k1], vr[32 * k1 + lane]);
+        regfft_fwd_dit<T, M>(u, lk, st, lane);
+#pragma unroll
+        for (int n1 = 0; n1 < M; ++n1)
+            if (cm[n1] >= 0) A[cm[n1] * LD + sy] = u[n1];
+    }
+    __syncthreads();
+    // forward y transform back to natural order
+    for (int c = warp; c < nxc; c += kPlaneWarps) {
+        T u[M];
+        T* col = A + c * LD;
+#pragma unroll
+        for (int k1 = 0; k1 < M; ++k1) u[k1] = col[32 * k1 + lane];
+        regfft_fwd_dit<T, M>(u, lk, st, lane);
+#pragma unroll
+        for (int n1 = 0; n1 < M; ++n1) col[32 * n1 + lane] = u[n1];
+    }
+    __syncthreads();
+    for (int s = tid; s < pm.nst; s += NT) plane[s] = A[pm.xc[s] * LD + pm.sy[s]];
+}
+
+template <typename R>
+__global__ void k_permute_veff(int nz, int n, int m, const R* __restrict__ in, R* __restrict__ out) {
+    const long total = long(nz) * n * n;
+    for (long i = blockIdx.x * long(blockDim.x) + threadIdx.x; i < total; i += long(gridDim.x) * blockDim.x) {
+        const int sx = int(i % n);
+        const long r = i / n;
+        const int sy = int(r % n);
+        const int z = int(r / n);
+        const int px = (sx >> 5) + m * int(__brev(unsigned(sx & 31)) >> 27);
+        const int py = (sy >> 5) + m * int(__brev(unsigned(sy & 31)) >> 27);
+        out[i] = in[(long(z) * n + py) * n + px];
+    }
+}
+
 // ---- k-point batched z passes: one launch covers every k-point of a batch (blockIdx.z = k slot) ----
 template <typename T, int NZ>
 __global__ void __launch_bounds__(kZWarps * 32) k_zinv_wb(KBatchArgs args, int b0, int nbc, const T* __restrict__ twz,
@@ -191,6 +333,9 @@ __global__ void __launch_bounds__(kZWarps * 32) k_zfwd_wb(KBatchArgs args, int b
 template <typename T> const T* twp(const FftAxis& a);
 template <> const double2* twp<double2>(const FftAxis& a) { return a.tw64.ptr; }
 template <> const float2* twp<float2>(const FftAxis& a) { return a.tw32.ptr; }
+template <typename T> const T* rtp(const FftAxis& a);
+template <> const double2* rtp<double2>(const FftAxis& a) { return a.rt64.ptr; }
+template <> const float2* rtp<float2>(const FftAxis& a) { return a.rt32.ptr; }
 
 template <typename K> void smem_attr(K kernel, size_t bytes) {
     if (bytes > 48 * 1024) B200_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
@@ -240,8 +385,28 @@ bool plane_launch(const PWGrid& g, int nb, const R* veff, T* sb, cudaStream_t s)
     return true;
 }
 
-template <typename T, typename R> bool plane_dispatch(const PWGrid& g, int nb, const R* veff, T* sb, cudaStream_t s) {
+template <typename T, typename R, int N>
+bool plane_launch_r(const PWGrid& g, int nb, const R* vperm, T* sb, cudaStream_t s) {
+    const size_t smem = size_t(g.nxc) * (N | 1) * sizeof(T) + size_t(N) * sizeof(int);
+    if (smem > 227 * 1024) return false;
+    smem_attr(k_plane_r<T, R, N>, smem);
+    k_plane_r<T, R, N><<<dim3(nb, g.nz), kPlaneWarps * 32, smem, s>>>(g.plane_view(), g.nz, rtp<T>(g.ax), vperm, sb);
+    note_launch();
+    B200_CUDA(cudaGetLastError());
+    return true;
+}
+
+template <typename T, typename R>
+bool plane_dispatch(const PWGrid& g, int nb, const R* veff, const R* vperm, T* sb, cudaStream_t s) {
     if (g.nx != g.ny) return false;
+    if (vperm) {
+        switch (g.nx) {
+            case 64: if (plane_launch_r<T, R, 64>(g, nb, vperm, sb, s)) return true; break;
+            case 96: if (plane_launch_r<T, R, 96>(g, nb, vperm, sb, s)) return true; break;
+            case 128: if (plane_launch_r<T, R, 128>(g, nb, vperm, sb, s)) return true; break;
+            default: break;
+        }
+    }
     switch (g.nx) {
         case 18: return plane_launch<T, R, 18>(g, nb, veff, sb, s);
         case 36: return plane_launch<T, R, 36>(g, nb, veff, sb, s);
@@ -289,15 +454,15 @@ bool zbatch_dispatch(bool inv, const PWGrid& g, const KBatchArgs& args, int nk, 
 }  // namespace
 
 template <typename T, typename R>
-bool launch_hpsi_local_kbatch(const PWGrid& g, const KBatchArgs& args, int nk, int nb, const R* veff_zyx, T* stickbuf,
-                              int chunk, double tpiba2, cudaStream_t s) {
+bool launch_hpsi_local_kbatch(const PWGrid& g, const KBatchArgs& args, int nk, int nb, const R* veff_zyx,
+                              const R* veff_perm, T* stickbuf, int chunk, double tpiba2, cudaStream_t s) {
     if (!supported_z(g.nz) || !supported_xy(g.nx, g.ny)) return false;
     const size_t smem = (size_t(kPlaneWarps) * g.nx + size_t(g.nxc) * (g.ny | 1)) * sizeof(T);
     if (smem > 227 * 1024) return false;
     for (int b0 = 0; b0 < nb; b0 += chunk) {
         const int nbc = nb - b0 < chunk ? nb - b0 : chunk;
         zbatch_dispatch<T, R>(true, g, args, nk, b0, nbc, stickbuf, tpiba2, s);
-        plane_dispatch<T, R>(g, nk * nbc, veff_zyx, stickbuf, s);
+        plane_dispatch<T, R>(g, nk * nbc, veff_zyx, veff_perm, stickbuf, s);
         zbatch_dispatch<T, R>(false, g, args, nk, b0, nbc, stickbuf, tpiba2, s);
     }
     return true;
@@ -307,25 +472,40 @@ namespace {
 }  // namespace
 
 template bool launch_hpsi_local_kbatch<double2, double>(const PWGrid&, const KBatchArgs&, int, int, const double*,
-                                                        double2*, int, double, cudaStream_t);
-template bool launch_hpsi_local_kbatch<float2, float>(const PWGrid&, const KBatchArgs&, int, int, const float*, float2*,
-                                                      int, double, cudaStream_t);
+                                                        const double*, double2*, int, double, cudaStream_t);
+template bool launch_hpsi_local_kbatch<float2, float>(const PWGrid&, const KBatchArgs&, int, int, const float*,
+                                                      const float*, float2*, int, double, cudaStream_t);
 
 template <typename T, typename R>
-bool launch_hpsi_local_fast(const PWGrid& g, int ik, const R* veff_zyx, int nb, int ld, const T* psi, T* hpsi,
-                            T* stickbuf, double tpiba2, int accumulate, cudaStream_t s) {
+bool launch_hpsi_local_fast(const PWGrid& g, int ik, const R* veff_zyx, const R* veff_perm, int nb, int ld,
+                            const T* psi, T* hpsi, T* stickbuf, double tpiba2, int accumulate, cudaStream_t s) {
     if (!supported_z(g.nz) || !supported_xy(g.nx, g.ny)) return false;
     const size_t smem = (size_t(kPlaneWarps) * g.nx + size_t(g.nxc) * (g.ny | 1)) * sizeof(T);
     if (smem > 227 * 1024) return false;
     zpass_dispatch<T, R>(true, g, ik, nb, ld, psi, hpsi, stickbuf, tpiba2, accumulate, s);
-    plane_dispatch<T, R>(g, nb, veff_zyx, stickbuf, s);
+    plane_dispatch<T, R>(g, nb, veff_zyx, veff_perm, stickbuf, s);
     zpass_dispatch<T, R>(false, g, ik, nb, ld, psi, hpsi, stickbuf, tpiba2, accumulate, s);
     return true;
 }
 
-template bool launch_hpsi_local_fast<double2, double>(const PWGrid&, int, const double*, int, int, const double2*,
-                                                      double2*, double2*, double, int, cudaStream_t);
-template bool launch_hpsi_local_fast<float2, float>(const PWGrid&, int, const float*, int, int, const float2*, float2*,
-                                                    float2*, double, int, cudaStream_t);
+template bool launch_hpsi_local_fast<double2, double>(const PWGrid&, int, const double*, const double*, int, int,
+                                                      const double2*, double2*, double2*, double, int, cudaStream_t);
+template bool launch_hpsi_local_fast<float2, float>(const PWGrid&, int, const float*, const float*, int, int,
+                                                    const float2*, float2*, float2*, double, int, cudaStream_t);
+
+bool plane_perm_supported(const PWGrid& g) {
+    return g.nx == g.ny && (g.nx == 64 || g.nx == 96 || g.nx == 128) && supported_z(g.nz);
+}
+
+template <typename R>
+bool launch_permute_veff(const PWGrid& g, const R* veff_zyx, R* out, cudaStream_t s) {
+    if (!plane_perm_supported(g)) return false;
+    k_permute_veff<R><<<1184, 256, 0, s>>>(g.nz, g.nx, g.nx / 32, veff_zyx, out);
+    note_launch();
+    B200_CUDA(cudaGetLastError());
+    return true;
+}
+template bool launch_permute_veff<double>(const PWGrid&, const double*, double*, cudaStream_t);
+template bool launch_permute_veff<float>(const PWGrid&, const float*, float*, cudaStream_t);
 
 }  // namespace b200

@@ -60,6 +60,16 @@ void FftAxis::upload() {
     for (size_t i = 0; i < h_tw64.size(); ++i) t32[i] = make_float2(float(h_tw64[i].x), float(h_tw64[i].y));
     tw64.upload(h_tw64.data(), h_tw64.size());
     tw32.upload(t32.data(), t32.size());
+    const int n = plan.n;
+    std::vector<double2> r64(n);
+    std::vector<float2> r32(n);
+    for (int j = 0; j < n; ++j) {
+        const long double ang = -2.0L * 3.141592653589793238462643383279502884L * (long double)j / (long double)n;
+        r64[j] = make_double2(double(std::cos(ang)), double(std::sin(ang)));
+        r32[j] = make_float2(float(std::cos(ang)), float(std::sin(ang)));
+    }
+    rt64.upload(r64.data(), n);
+    rt32.upload(r32.data(), n);
 }
 
 void PWGrid::build(const PWBasisK& b) {
@@ -416,12 +426,13 @@ template <typename K> static void set_smem(K kernel, size_t bytes) {
 }
 
 template <typename T, typename R>
-void launch_hpsi_local(const PWGrid& g, int ik, const R* veff_zyx, int nb, int ld, const T* psi, T* hpsi, T* stickbuf,
-                       double tpiba2, int accumulate, cudaStream_t s) {
+void launch_hpsi_local(const PWGrid& g, int ik, const R* veff_zyx, const R* veff_perm, int nb, int ld, const T* psi,
+                       T* hpsi, T* stickbuf, double tpiba2, int accumulate, cudaStream_t s) {
     if (nb <= 0) return;
     B200_CHECK(nb <= 65535, kInvalidArgument, "too many bands in one launch");
     // compile-time warp transforms for the standard grid sizes; generic Stockham kernels otherwise
-    if (launch_hpsi_local_fast<T, R>(g, ik, veff_zyx, nb, ld, psi, hpsi, stickbuf, tpiba2, accumulate, s)) return;
+    if (launch_hpsi_local_fast<T, R>(g, ik, veff_zyx, veff_perm, nb, ld, psi, hpsi, stickbuf, tpiba2, accumulate, s))
+        return;
     const size_t zs = zpass_smem(g, sizeof(T));
     const size_t ps = plane_smem(g, sizeof(T));
     B200_CHECK(ps <= 227 * 1024, kCapacityError, "plane pass does not fit in shared memory for this grid");
@@ -502,9 +513,11 @@ void launch_transpose_veff(const PWGrid& g, const double* veff, R* out, cudaStre
     B200_CUDA(cudaGetLastError());
 }
 
-template void launch_hpsi_local<double2, double>(const PWGrid&, int, const double*, int, int, const double2*, double2*,
+template void launch_hpsi_local<double2, double>(const PWGrid&, int, const double*, const double*, int, int,
+                                                 const double2*, double2*,
                                                  double2*, double, int, cudaStream_t);
-template void launch_hpsi_local<float2, float>(const PWGrid&, int, const float*, int, int, const float2*, float2*, float2*,
+template void launch_hpsi_local<float2, float>(const PWGrid&, int, const float*, const float*, int, int, const float2*,
+                                               float2*, float2*,
                                                double, int, cudaStream_t);
 template void launch_recip_to_real<double2>(const PWGrid&, int, const double2*, double2*, double2*, int, double, cudaStream_t);
 template void launch_recip_to_real<float2>(const PWGrid&, int, const float2*, float2*, float2*, int, double, cudaStream_t);

@@ -52,9 +52,21 @@ void Hamilt::set_veff(const double* veff_d) {
     launch_transpose_veff<double>(*grid, veff_d, veff_zyx.ptr, 0);
     veff_zyxf.resize(N);
     launch_transpose_veff<float>(*grid, veff_d, veff_zyxf.ptr, 0);
+    has_perm = plane_perm_supported(*grid);
+    if (has_perm) {
+        veff_perm.resize(N);
+        veff_permf.resize(N);
+        launch_permute_veff<double>(*grid, veff_zyx.ptr, veff_perm.ptr, 0);
+        launch_permute_veff<float>(*grid, veff_zyxf.ptr, veff_permf.ptr, 0);
+    }
     B200_CUDA(cudaStreamSynchronize(0));
     has_veff = true;
 }
+
+template <> const double* Hamilt::veff_of<double>() const { return veff_zyx.ptr; }
+template <> const float* Hamilt::veff_of<float>() const { return veff_zyxf.ptr; }
+template <> const double* Hamilt::veff_perm_of<double>() const { return has_perm ? veff_perm.ptr : nullptr; }
+template <> const float* Hamilt::veff_perm_of<float>() const { return has_perm ? veff_permf.ptr : nullptr; }
 
 void Hamilt::set_vkb(int ik, int nkb, int npwx, const double2* vkb_d) {
     B200_CHECK(ik >= 0 && ik < int(nl.size()), kInvalidArgument, "k-point index out of range");
@@ -160,7 +172,8 @@ void Hamilt::hpsi(int ik, int spin, int nb, int ld, const T* psi, T* hpsi, int m
         }
         for (int b0 = 0; b0 < nb; b0 += chunk) {
             const int nbc = nb - b0 < chunk ? nb - b0 : chunk;
-            launch_hpsi_local<T, R>(*grid, ik, veff, nbc, ld, psi + size_t(b0) * ld, hpsi + size_t(b0) * ld, sb,
+            launch_hpsi_local<T, R>(*grid, ik, veff, veff_perm_of<R>(), nbc, ld, psi + size_t(b0) * ld,
+                                    hpsi + size_t(b0) * ld, sb,
                                     grid->basis.tpiba2, 0, s);
         }
     }
@@ -272,7 +285,8 @@ void Hamilt::hpsi_kbatch(int nk, const int* iks, int spin, int nb, int ld, const
         W.sb32.resize(size_t(nk) * chunk * grid->nst * grid->nz);
         sb = W.sb32.ptr;
     }
-    if (!launch_hpsi_local_kbatch<T, R>(*grid, args, nk, nb, veff, sb, chunk, grid->basis.tpiba2, s)) {
+    if (!launch_hpsi_local_kbatch<T, R>(*grid, args, nk, nb, veff, veff_perm_of<R>(), sb, chunk, grid->basis.tpiba2,
+                                        s)) {
         for (int q = 0; q < nk; ++q) hpsi<T>(iks[q], spin, nb, ld, psis[q], hpsis[q], 1, s, &W);
     }
     for (int q = 0; q < nk; ++q) hpsi<T>(iks[q], spin, nb, ld, psis[q], hpsis[q], 2, s, &W);

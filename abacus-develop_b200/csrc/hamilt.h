@@ -63,6 +63,11 @@ struct Hamilt {
     int precision = 0;  // 0 = FP64, 1 = mixed
     DeviceArray<double> veff_zyx;
     DeviceArray<float> veff_zyxf;
+    DeviceArray<double> veff_perm;  // (z, y, x) in the register-transform order (grids with 32*m square planes)
+    DeviceArray<float> veff_permf;
+    bool has_perm = false;
+    template <typename R> const R* veff_of() const;
+    template <typename R> const R* veff_perm_of() const;
     bool has_veff = false;
     std::vector<NonlocalK> nl;
     int ntype = 0, nspin = 1, dx = 0, dy = 0, dz = 0;

@@ -74,10 +74,11 @@ void hpsi_local_noalloc(b200::Hamilt& H, int ik, int nb, int ld, const T* psi, T
     if (nb == 0) return;
     T* sb = static_cast<T*>(noalloc_scratch_on_current_device());
     const int chunk = int(kNoAllocScratchBytes / per_band);
-    const R* veff = std::is_same<T, double2>::value ? (const R*)H.veff_zyx.ptr : (const R*)H.veff_zyxf.ptr;
+    const R* veff = H.veff_of<R>();
+    const R* veffp = H.veff_perm_of<R>();
     for (int b0 = 0; b0 < nb; b0 += chunk) {
         const int nbc = nb - b0 < chunk ? nb - b0 : chunk;
-        b200::launch_hpsi_local<T, R>(g, ik, veff, nbc, ld, psi + size_t(b0) * ld, hpsi + size_t(b0) * ld, sb,
+        b200::launch_hpsi_local<T, R>(g, ik, veff, veffp, nbc, ld, psi + size_t(b0) * ld, hpsi + size_t(b0) * ld, sb,
                                       g.basis.tpiba2, 0, s);
     }
 }

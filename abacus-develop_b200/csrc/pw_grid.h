@@ -27,6 +27,8 @@ struct FftAxis {
     std::vector<double2> h_tw64;
     DeviceArray<double2> tw64;
     DeviceArray<float2> tw32;
+    DeviceArray<double2> rt64;  // the n roots W_n^j = exp(-2 pi i j / n), j < n (register/shuffle transforms)
+    DeviceArray<float2> rt32;
     void build(int n);  // host plan + twiddles
     void upload();
 };
@@ -91,13 +93,13 @@ size_t plane_smem(const PWGrid& g, size_t elem);
 // ---- launchers (fft_kernels.cu); all asynchronous on `s` ----
 // Fused local part of H|psi> for nb bands (one chunk): hpsi = Ekin psi + V_loc psi (accumulate==0 zeroes padding).
 template <typename T, typename R>
-void launch_hpsi_local(const PWGrid& g, int ik, const R* veff_zyx, int nb, int ld, const T* psi, T* hpsi, T* stickbuf,
-                       double tpiba2, int accumulate, cudaStream_t s);
+void launch_hpsi_local(const PWGrid& g, int ik, const R* veff_zyx, const R* veff_perm, int nb, int ld, const T* psi,
+                       T* hpsi, T* stickbuf, double tpiba2, int accumulate, cudaStream_t s);
 // Same, with warp-synchronous compile-time transforms; returns false (launching nothing) for
 // grid sizes it does not cover.
 template <typename T, typename R>
-bool launch_hpsi_local_fast(const PWGrid& g, int ik, const R* veff_zyx, int nb, int ld, const T* psi, T* hpsi,
-                            T* stickbuf, double tpiba2, int accumulate, cudaStream_t s);
+bool launch_hpsi_local_fast(const PWGrid& g, int ik, const R* veff_zyx, const R* veff_perm, int nb, int ld,
+                            const T* psi, T* hpsi, T* stickbuf, double tpiba2, int accumulate, cudaStream_t s);
 // k-point batch: one entry per k (its stick maps, psi / hpsi with leading dimension ld, npwk, gk2 in the
 // precision of the call); passed by value so a launch needs no device-side argument buffer.
 constexpr int kMaxKBatch = 128;
@@ -114,8 +116,8 @@ struct KBatchArgs {
 // Kinetic + local part of H|psi> for nb bands of nk k-points in one launch per pass (per band chunk);
 // returns false for grid sizes without compiled warp transforms.
 template <typename T, typename R>
-bool launch_hpsi_local_kbatch(const PWGrid& g, const KBatchArgs& args, int nk, int nb, const R* veff_zyx, T* stickbuf,
-                              int chunk, double tpiba2, cudaStream_t s);
+bool launch_hpsi_local_kbatch(const PWGrid& g, const KBatchArgs& args, int nk, int nb, const R* veff_zyx,
+                              const R* veff_perm, T* stickbuf, int chunk, double tpiba2, cudaStream_t s);
 // Drop-in transforms (PW_Basis_K::recip_to_real / real_to_recip on the GPU), one band.
 template <typename T>
 void launch_recip_to_real(const PWGrid& g, int ik, const T* in, T* out, T* aux, int add, double factor, cudaStream_t s);
@@ -124,5 +126,11 @@ void launch_real_to_recip(const PWGrid& g, int ik, const T* in, T* out, T* aux, 
 // V_eff (ABACUS r order) -> (z, y, x) transposed copy, in precision R.
 template <typename R>
 void launch_transpose_veff(const PWGrid& g, const double* veff, R* out, cudaStream_t s);
+// Square xy planes of n = 32*m (m = 2, 3, 4) use register/shuffle transforms whose r-space values come out
+// in a permuted order; V_eff is stored once in that order: out[z][sy][sx] = veff_zyx[z][p(sy)][p(sx)],
+// p(s) = s/32 + m*bitrev5(s mod 32).  Returns false (nothing done) for other grids.
+bool plane_perm_supported(const PWGrid& g);
+template <typename R>
+bool launch_permute_veff(const PWGrid& g, const R* veff_zyx, R* out, cudaStream_t s);
 
 }  // namespace b200

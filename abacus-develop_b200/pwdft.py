@@ -108,6 +108,19 @@ def _ints(v):
     return (C.c_int * max(1, len(v)))(*v)
 
 
+def _check_block(t, complex128: bool, nbands: int, ld: int, what: str):
+    """The C-ABI takes device pointers without types or sizes: refuse a tensor whose element type is not the
+    one the call will read or that holds fewer than nbands*ld elements (an out-of-bounds device access)."""
+    torch = _torch()
+    want = torch.complex128 if complex128 else torch.complex64
+    if t.dtype != want:
+        raise TypeError(f"{what}: expected {want}, got {t.dtype}")
+    if not t.is_cuda or not t.is_contiguous():
+        raise ValueError(f"{what}: expected a contiguous CUDA tensor")
+    if t.numel() < int(nbands) * int(ld):
+        raise ValueError(f"{what}: {t.numel()} elements, the call reads or writes {int(nbands) * int(ld)}")
+
+
 def cal_ylm_real_op(ng, lmax, g, ylm, stream=None):
     """ModuleBase::cal_ylm_real_op<FP, DEVICE_GPU>: g (ng x 3) -> ylm ((lmax+1)^2 x ng)."""
     torch = _torch()
@@ -281,17 +294,25 @@ class HamiltPW:
         ns, dx, dy, dz = (int(v) for v in deeq_d.shape)
         call("b200_hamilt_set_deeq", self._h, len(na), na_a, nh_a, ns, dx, dy, dz, ptr(deeq_d))
 
+    def _chk(self, psi, hpsi, nbands, ld):
+        f64 = self.precision == PREC_FP64
+        _check_block(psi, f64, nbands, ld, "psi")
+        _check_block(hpsi, f64, nbands, ld, "hpsi")
+
     def hpsi(self, ik, psi, hpsi, nbands, ld, spin=0, stream=None):
         """Operator::hPsi: hpsi = H psi for bands [0, nbands)."""
+        self._chk(psi, hpsi, nbands, ld)
         call("b200_hamilt_hpsi", self._h, ik, spin, nbands, ld, ptr(psi), ptr(hpsi), stream_ptr(stream))
 
     def hpsi_part(self, ik, psi, hpsi, nbands, ld, mode, spin=0, stream=None):
+        self._chk(psi, hpsi, nbands, ld)
         call("b200_hamilt_hpsi_part", self._h, ik, spin, nbands, ld, ptr(psi), ptr(hpsi), mode, stream_ptr(stream))
 
     def hpsi_local_noalloc(self, ik, psi, hpsi, nbands, ld, stream=None):
         """Kinetic + local part of H|psi> without any device allocation during the call, for callers that
         cannot allocate (graph capture, externally owned memory pools); scratch is a fixed 32 MiB array
         inside the library shared by all calls, so concurrent calls on one device must be serialised."""
+        self._chk(psi, hpsi, nbands, ld)
         call("b200_hamilt_hpsi_local_noalloc", self._h, ik, nbands, ld, ptr(psi), ptr(hpsi), stream_ptr(stream))
 
     def set_projectors(self, proj: ProjectorSet, tau_lat0):
@@ -310,24 +331,25 @@ class HamiltPW:
     def copy_vkb(self, ik, out, stream=None):
         call("b200_hamilt_copy_vkb", self._h, ik, ptr(out), stream_ptr(stream))
 
-    @staticmethod
-    def _kbatch_args(iks, psis, hpsis):
+    def _kbatch_args(self, iks, psis, hpsis, nbands, ld):
         nk = len(iks)
         if len(psis) != nk or len(hpsis) != nk:
             raise ValueError("iks, psis and hpsis must have the same length")
+        for p, hp in zip(psis, hpsis):
+            self._chk(p, hp, nbands, ld)
         return (nk, (C.c_int * nk)(*[int(i) for i in iks]), (_lib.vp * nk)(*[ptr(p) for p in psis]),
                 (_lib.vp * nk)(*[ptr(p) for p in hpsis]))
 
     def hpsi_kbatch(self, iks, psis, hpsis, nbands, ld, spin=0, stream=None):
         """H|psi> of nbands bands for each k-point in iks (psis[q], hpsis[q]: that k-point's blocks); the
         kinetic + local part of all k-points in one launch per FFT pass."""
-        nk, ik_a, p_a, h_a = self._kbatch_args(iks, psis, hpsis)
+        nk, ik_a, p_a, h_a = self._kbatch_args(iks, psis, hpsis, nbands, ld)
         call("b200_hamilt_hpsi_kbatch", self._h, nk, ik_a, spin, nbands, ld, p_a, h_a, stream_ptr(stream))
 
     def capture_hpsi_kbatch(self, iks, psis, hpsis, nbands, ld, stream, spin=0):
         """hpsi_kbatch captured into a CUDA graph on a non-default stream; returns a HpsiGraph whose
         launch() replays it on the captured buffers."""
-        nk, ik_a, p_a, h_a = self._kbatch_args(iks, psis, hpsis)
+        nk, ik_a, p_a, h_a = self._kbatch_args(iks, psis, hpsis, nbands, ld)
         g = _lib.vp()
         call("b200_graph_capture_hpsi_kbatch", self._h, nk, ik_a, spin, nbands, ld, p_a, h_a, stream_ptr(stream),
              C.byref(g))
@@ -335,6 +357,7 @@ class HamiltPW:
 
     def autotune(self, ik, psi, hpsi, nbands, ld, stream=None):
         """Pick the band-chunk size of the local pass by timing candidates; returns the chosen size."""
+        self._chk(psi, hpsi, nbands, ld)
         best = C.c_int()
         call("b200_hamilt_autotune", self._h, ik, nbands, ld, ptr(psi), ptr(hpsi), stream_ptr(stream), C.byref(best))
         return best.value
@@ -344,6 +367,8 @@ class HamiltPW:
         """Davidson solves of the k-points iks, nworkers at a time on separate streams.  psis[q] (complex128,
         nband x ld_psi) is overwritten with the eigenvectors.  Returns (eigenvalues nk x nband, iterations)."""
         nk = len(iks)
+        for p in psis:
+            _check_block(p, True, nband, ld_psi, "psi")
         ik_a = (C.c_int * nk)(*[int(i) for i in iks])
         pc_a = (_lib.vp * nk)(*[ptr(p) for p in precond_ds])
         ps_a = (_lib.vp * nk)(*[ptr(p) for p in psis])
@@ -402,6 +427,9 @@ class DiagoDavid:
         def cb(user, x, hx, nvec, dim, i0, i1):
             hpsi_func(x, hx, nvec, dim, i0, i1)
 
+        _check_block(psi, True, self.nband, ld_psi, "psi")
+        if len(eigenvalue) < self.nband or eigenvalue.dtype != np.float64:
+            raise ValueError("eigenvalue: need a float64 array of nband entries")
         cfn = _lib.HPSI_CB(cb)
         it = C.c_int()
         call("b200_david_diag", self._h, cfn, None, ld_psi, ptr(psi), eigenvalue.ctypes.data_as(_lib.pf64), thr, maxiter,
@@ -410,6 +438,9 @@ class DiagoDavid:
 
     def diag_hamilt(self, hamilt: HamiltPW, ik, ld_psi, psi, eigenvalue, thr, maxiter, ntry_max=5, notconv_max=0,
                     spin=0):
+        _check_block(psi, True, self.nband, ld_psi, "psi")
+        if len(eigenvalue) < self.nband or eigenvalue.dtype != np.float64:
+            raise ValueError("eigenvalue: need a float64 array of nband entries")
         it = C.c_int()
         call("b200_david_diag_hamilt", self._h, hamilt.handle, ik, spin, ld_psi, ptr(psi),
              eigenvalue.ctypes.data_as(_lib.pf64), thr, maxiter, ntry_max, notconv_max, C.byref(it))

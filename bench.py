@@ -379,7 +379,7 @@ def settle_time(trace, ref, tol=1e-8):
     return float(t[i])
 
 
-def solve_pair(P, h, pc, nb, ld, psi0_h, thr_ref=1e-11, thr=1e-9):
+def solve_pair(P, h, pc, nb, ld, psi0_h, thr_ref=1e-11, thr=1e-9, repeats=2):
     """FP64 reference solve to thr_ref, then FP64 and mixed solves to thr with eigenvalue traces: wall time
     of each solve and time until every eigenvalue is within 1e-8 Ry of the reference."""
     import torch
@@ -399,11 +399,17 @@ def solve_pair(P, h, pc, nb, ld, psi0_h, thr_ref=1e-11, thr=1e-9):
         torch.cuda.empty_cache()
         return out
 
+    solve(P.PREC_MIXED, 1e-6)  # warm-up: first use of every kernel, handle and workspace shape
     _, e_ref, st_ref, _ = solve(P.PREC_FP64, thr_ref)
-    w64, e64, st64, tr64 = solve(P.PREC_FP64, thr)
-    wmx, emx, stmx, trmx = solve(P.PREC_MIXED, thr)
+    runs64, runsmx = [], []
+    for _ in range(repeats):  # alternating, the faster of each arm is reported
+        runs64.append(solve(P.PREC_FP64, thr))
+        runsmx.append(solve(P.PREC_MIXED, thr))
+    w64, e64, st64, tr64 = min(runs64, key=lambda r: r[0])
+    wmx, emx, stmx, trmx = min(runsmx, key=lambda r: r[0])
     s64, smx = settle_time(tr64, e_ref), settle_time(trmx, e_ref)
     return {"fp64_s": w64, "mixed_s": wmx, "speedup": w64 / wmx,
+            "fp64_runs_s": [r[0] for r in runs64], "mixed_runs_s": [r[0] for r in runsmx],
             "fp64_to_1e-8_s": s64, "mixed_to_1e-8_s": smx,
             "speedup_to_1e-8": (s64 / smx) if (s64 and smx) else None,
             "fp64_iters": st64[1], "mixed_iters_fp32": stmx[0], "mixed_iters_fp64": stmx[1],

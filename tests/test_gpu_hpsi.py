@@ -32,7 +32,8 @@ def _setup(pkg, spec, kpt=None, nb=None):
     return wl, ref, psi, nb, npwx
 
 
-@pytest.mark.parametrize("cfg", ["si2", "diamond8", "diamond8_k", "diamond16", "diamond8_grid40"])
+@pytest.mark.parametrize("cfg", ["si2", "diamond8", "diamond8_k", "diamond16", "diamond8_grid40", "diamond8_grid96_k",
+                                 "diamond8_grid128"])
 def test_hpsi_fp64_matches_oracle(pkg, cfg):
     S = pkg.synth
     if cfg == "si2":
@@ -43,9 +44,14 @@ def test_hpsi_fp64_matches_oracle(pkg, cfg):
         spec, kpt, nb = S.config(0), np.array([0.125, -0.375, 0.375]), 12
     elif cfg == "diamond16":
         spec, kpt, nb = S.serving_cells()[2], None, 6
-    else:  # a grid outside the compiled warp-transform sizes exercises the generic kernels
+    elif cfg == "diamond8_grid40":  # a grid outside the compiled warp-transform sizes: the generic kernels
         import dataclasses
         spec, kpt, nb = dataclasses.replace(S.config(0), grid=(40, 40, 40)), None, 10
+    else:  # square planes of 32*m points: the register/shuffle plane transforms
+        import dataclasses
+        n = 96 if "96" in cfg else 128
+        kpt = np.array([0.25, -0.125, 0.375]) if cfg.endswith("_k") else None
+        spec, nb = dataclasses.replace(S.config(0), grid=(n, n, n)), 6
     wl, ref, psi, nb, ld = _setup(pkg, spec, kpt, nb)
     href = ref.hpsi(psi, nb, ld)
     h = pkg.pwdft.device_hamilt(wl, pkg.pwdft.PREC_FP64)
@@ -62,9 +68,11 @@ def test_hpsi_fp64_matches_oracle(pkg, cfg):
     assert rel(hl.cpu().numpy(), ref.hpsi_local(psi, nb, ld)) < 1e-12
 
 
-def test_hpsi_mixed_matches_oracle(pkg):
-    spec = pkg.synth.config(0)
-    wl, ref, psi, nb, ld = _setup(pkg, spec, None, 32)
+@pytest.mark.parametrize("grid", [None, (96, 96, 96)])
+def test_hpsi_mixed_matches_oracle(pkg, grid):
+    import dataclasses
+    spec = pkg.synth.config(0) if grid is None else dataclasses.replace(pkg.synth.config(0), grid=grid)
+    wl, ref, psi, nb, ld = _setup(pkg, spec, None, 32 if grid is None else 6)
     href = ref.hpsi(psi, nb, ld)
     h = pkg.pwdft.device_hamilt(wl, pkg.pwdft.PREC_MIXED)
     pd = torch.from_numpy(psi.astype(np.complex64)).cuda()
