@@ -248,17 +248,120 @@ __global__ void __launch_bounds__(kPlaneWarps * 32) k_plane_r(PlaneMapView pm, i
     for (int s = tid; s < pm.nst; s += NT) plane[s] = A[pm.xc[s] * LD + pm.sy[s]];
 }
 
+// ---- register z passes for nz = 32*M: the inverse transform leaves every stick in the permuted order, so
+// the planes of the stick buffer are stored by slot (plane slot sz holds z = sz/32 + M*bitrev5(sz mod 32));
+// V_eff is permuted along z as well, and the forward z transform takes the slots back to natural z.
+// Src gives the k-point entry of a block: one k-point (OneK) or a batch indexed by blockIdx.z (ManyK).
+struct OneK {
+    KBatchEntry e;
+    __device__ __forceinline__ const KBatchEntry& get(int) const { return e; }
+};
+struct ManyK {
+    KBatchArgs a;
+    __device__ __forceinline__ const KBatchEntry& get(int q) const { return a.e[q]; }
+};
+
+template <typename T, int NZ, typename Src>
+__global__ void __launch_bounds__(kZWarps * 32) k_zinv_r(Src src, int b0, int nbc, const T* __restrict__ roots,
+                                                        T* __restrict__ sb) {
+    constexpr int M = NZ / 32;
+    constexpr int LDZ = NZ | 1;
+    __shared__ T A[kStickTile * LDZ];
+    const KBatchEntry& e = src.get(blockIdx.z);
+    const StickMapView sm = e.sm;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int s0 = blockIdx.x * kStickTile;
+    if (s0 >= sm.nst) return;
+    const int ns = min(kStickTile, sm.nst - s0);
+    const int band = blockIdx.y;
+    for (int i = tid; i < kStickTile * LDZ; i += kZWarps * 32) A[i] = zero_c<T>();
+    T lk[M], st[5];
+    lane_twiddles<T, NZ>(roots, lane, lk, st);
+    __syncthreads();
+    const T* p = reinterpret_cast<const T*>(e.psi) + size_t(b0 + band) * e.ld;
+    const int j0 = sm.gofs[s0], j1 = sm.gofs[s0 + ns];
+    for (int j = j0 + tid; j < j1; j += kZWarps * 32) {
+        const int pk = sm.gpk[j];
+        A[((pk >> 10) - s0) * LDZ + (pk & 1023)] = p[sm.glist[j]];
+    }
+    __syncthreads();
+    for (int sl = warp; sl < ns; sl += kZWarps) {
+        T u[M];
+        T* stick = A + sl * LDZ;
+#pragma unroll
+        for (int n1 = 0; n1 < M; ++n1) u[n1] = stick[32 * n1 + lane];
+        regfft_inv_dif<T, M>(u, lk, st, lane);
+#pragma unroll
+        for (int k1 = 0; k1 < M; ++k1) stick[32 * k1 + lane] = u[k1];
+    }
+    __syncthreads();
+    T* out = sb + (size_t(blockIdx.z) * nbc + band) * NZ * sm.nst;
+    for (int i = tid; i < ns * NZ; i += kZWarps * 32) {
+        const int sz = i / ns;
+        const int sl = i - sz * ns;
+        out[size_t(sz) * sm.nst + s0 + sl] = A[sl * LDZ + sz];
+    }
+}
+
+template <typename T, typename R, int NZ, typename Src>
+__global__ void __launch_bounds__(kZWarps * 32) k_zfwd_r(Src src, int b0, int nbc, const T* __restrict__ roots,
+                                                        const T* __restrict__ sb, R tpiba2, R invn, int accumulate) {
+    constexpr int M = NZ / 32;
+    constexpr int LDZ = NZ | 1;
+    __shared__ T A[kStickTile * LDZ];
+    const KBatchEntry& e = src.get(blockIdx.z);
+    const StickMapView sm = e.sm;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int s0 = blockIdx.x * kStickTile;
+    if (s0 >= sm.nst) return;
+    const int ns = min(kStickTile, sm.nst - s0);
+    const int band = blockIdx.y;
+    const T* in = sb + (size_t(blockIdx.z) * nbc + band) * NZ * sm.nst;
+    for (int i = tid; i < ns * NZ; i += kZWarps * 32) {
+        const int sz = i / ns;
+        const int sl = i - sz * ns;
+        A[sl * LDZ + sz] = in[size_t(sz) * sm.nst + s0 + sl];
+    }
+    T lk[M], st[5];
+    lane_twiddles<T, NZ>(roots, lane, lk, st);
+    __syncthreads();
+    for (int sl = warp; sl < ns; sl += kZWarps) {
+        T u[M];
+        T* stick = A + sl * LDZ;
+#pragma unroll
+        for (int k1 = 0; k1 < M; ++k1) u[k1] = stick[32 * k1 + lane];
+        regfft_fwd_dit<T, M>(u, lk, st, lane);
+#pragma unroll
+        for (int n1 = 0; n1 < M; ++n1) stick[32 * n1 + lane] = u[n1];
+    }
+    __syncthreads();
+    const T* p = reinterpret_cast<const T*>(e.psi) + size_t(b0 + band) * e.ld;
+    T* h = reinterpret_cast<T*>(e.hpsi) + size_t(b0 + band) * e.ld;
+    const R* gk2 = reinterpret_cast<const R*>(e.gk2);
+    const int j0 = sm.gofs[s0], j1 = sm.gofs[s0 + ns];
+    for (int j = j0 + tid; j < j1; j += kZWarps * 32) {
+        const int pk = sm.gpk[j];
+        const int g = sm.glist[j];
+        T v = cscale(A[((pk >> 10) - s0) * LDZ + (pk & 1023)], invn);
+        v = cadd(v, cscale(p[g], gk2[g] * tpiba2));
+        if (accumulate) v = cadd(v, h[g]);
+        h[g] = v;
+    }
+    if (!accumulate && blockIdx.x == 0)
+        for (int g = e.npw + tid; g < e.ld; g += kZWarps * 32) h[g] = zero_c<T>();
+}
+
+__device__ __forceinline__ int perm_slot(int s, int m) { return (s >> 5) + m * int(__brev(unsigned(s & 31)) >> 27); }
+
 template <typename R>
-__global__ void k_permute_veff(int nz, int n, int m, const R* __restrict__ in, R* __restrict__ out) {
+__global__ void k_permute_veff(int nz, int n, int m, int mz, const R* __restrict__ in, R* __restrict__ out) {
     const long total = long(nz) * n * n;
     for (long i = blockIdx.x * long(blockDim.x) + threadIdx.x; i < total; i += long(gridDim.x) * blockDim.x) {
         const int sx = int(i % n);
         const long r = i / n;
         const int sy = int(r % n);
-        const int z = int(r / n);
-        const int px = (sx >> 5) + m * int(__brev(unsigned(sx & 31)) >> 27);
-        const int py = (sy >> 5) + m * int(__brev(unsigned(sy & 31)) >> 27);
-        out[i] = in[(long(z) * n + py) * n + px];
+        const int sz = int(r / n);
+        out[i] = in[(long(perm_slot(sz, mz)) * n + perm_slot(sy, m)) * n + perm_slot(sx, m)];
     }
 }
 
@@ -399,14 +502,7 @@ bool plane_launch_r(const PWGrid& g, int nb, const R* vperm, T* sb, cudaStream_t
 template <typename T, typename R>
 bool plane_dispatch(const PWGrid& g, int nb, const R* veff, const R* vperm, T* sb, cudaStream_t s) {
     if (g.nx != g.ny) return false;
-    if (vperm) {
-        switch (g.nx) {
-            case 64: if (plane_launch_r<T, R, 64>(g, nb, vperm, sb, s)) return true; break;
-            case 96: if (plane_launch_r<T, R, 96>(g, nb, vperm, sb, s)) return true; break;
-            case 128: if (plane_launch_r<T, R, 128>(g, nb, vperm, sb, s)) return true; break;
-            default: break;
-        }
-    }
+    (void)vperm;
     switch (g.nx) {
         case 18: return plane_launch<T, R, 18>(g, nb, veff, sb, s);
         case 36: return plane_launch<T, R, 36>(g, nb, veff, sb, s);
@@ -453,9 +549,65 @@ bool zbatch_dispatch(bool inv, const PWGrid& g, const KBatchArgs& args, int nk, 
 
 }  // namespace
 
+template <typename T, typename R, int NZ, typename Src>
+void zpass_r(bool inv, const PWGrid& g, const Src& src, int nk, int b0, int nbc, T* sb, double tpiba2, int accumulate,
+             cudaStream_t s) {
+    const dim3 grid(ceil_div(g.nst, kStickTile), nbc, nk);
+    if (inv)
+        k_zinv_r<T, NZ, Src><<<grid, kZWarps * 32, 0, s>>>(src, b0, nbc, rtp<T>(g.az), sb);
+    else
+        k_zfwd_r<T, R, NZ, Src><<<grid, kZWarps * 32, 0, s>>>(src, b0, nbc, rtp<T>(g.az), sb, R(tpiba2),
+                                                             R(1.0 / double(g.nxyz())), accumulate);
+    note_launch();
+    B200_CUDA(cudaGetLastError());
+}
+
+template <typename T, typename R, typename Src>
+bool zpass_r_dispatch(bool inv, const PWGrid& g, const Src& src, int nk, int b0, int nbc, T* sb, double tpiba2,
+                      int accumulate, cudaStream_t s) {
+    switch (g.nz) {
+        case 64: zpass_r<T, R, 64>(inv, g, src, nk, b0, nbc, sb, tpiba2, accumulate, s); return true;
+        case 96: zpass_r<T, R, 96>(inv, g, src, nk, b0, nbc, sb, tpiba2, accumulate, s); return true;
+        case 128: zpass_r<T, R, 128>(inv, g, src, nk, b0, nbc, sb, tpiba2, accumulate, s); return true;
+        default: return false;
+    }
+}
+
+template <typename T, typename R>
+bool plane_r_dispatch(const PWGrid& g, int nb, const R* vperm, T* sb, cudaStream_t s) {
+    switch (g.nx) {
+        case 64: return plane_launch_r<T, R, 64>(g, nb, vperm, sb, s);
+        case 96: return plane_launch_r<T, R, 96>(g, nb, vperm, sb, s);
+        case 128: return plane_launch_r<T, R, 128>(g, nb, vperm, sb, s);
+        default: return false;
+    }
+}
+
+// all three passes with register transforms (grids with plane_perm_supported); false if the plane does not fit
+template <typename T, typename R, typename Src>
+bool local_r(const PWGrid& g, const Src& src, int nk, int b0, int nbc, const R* vperm, T* sb, double tpiba2,
+             int accumulate, cudaStream_t s) {
+    const size_t smem = size_t(g.nxc) * (g.nx | 1) * sizeof(T) + size_t(g.nx) * sizeof(int);
+    if (smem > 227 * 1024) return false;
+    zpass_r_dispatch<T, R>(true, g, src, nk, b0, nbc, sb, tpiba2, accumulate, s);
+    plane_r_dispatch<T, R>(g, nk * nbc, vperm, sb, s);
+    zpass_r_dispatch<T, R>(false, g, src, nk, b0, nbc, sb, tpiba2, accumulate, s);
+    return true;
+}
+
 template <typename T, typename R>
 bool launch_hpsi_local_kbatch(const PWGrid& g, const KBatchArgs& args, int nk, int nb, const R* veff_zyx,
                               const R* veff_perm, T* stickbuf, int chunk, double tpiba2, cudaStream_t s) {
+    if (veff_perm && plane_perm_supported(g)) {
+        ManyK src;
+        src.a = args;
+        bool ok = true;
+        for (int b0 = 0; b0 < nb && ok; b0 += chunk) {
+            const int nbc = nb - b0 < chunk ? nb - b0 : chunk;
+            ok = local_r<T, R>(g, src, nk, b0, nbc, veff_perm, stickbuf, tpiba2, 0, s);
+        }
+        if (ok) return true;
+    }
     if (!supported_z(g.nz) || !supported_xy(g.nx, g.ny)) return false;
     const size_t smem = (size_t(kPlaneWarps) * g.nx + size_t(g.nxc) * (g.ny | 1)) * sizeof(T);
     if (smem > 227 * 1024) return false;
@@ -479,6 +631,17 @@ template bool launch_hpsi_local_kbatch<float2, float>(const PWGrid&, const KBatc
 template <typename T, typename R>
 bool launch_hpsi_local_fast(const PWGrid& g, int ik, const R* veff_zyx, const R* veff_perm, int nb, int ld,
                             const T* psi, T* hpsi, T* stickbuf, double tpiba2, int accumulate, cudaStream_t s) {
+    if (veff_perm && plane_perm_supported(g)) {
+        const KMap& km = g.kmaps[ik];
+        OneK src;
+        src.e.sm = g.stick_view(ik);
+        src.e.psi = psi;
+        src.e.hpsi = hpsi;
+        src.e.ld = ld;
+        src.e.npw = km.npw;
+        src.e.gk2 = std::is_same<T, double2>::value ? (const void*)km.gk2.ptr : (const void*)km.gk2f.ptr;
+        if (local_r<T, R>(g, src, 1, 0, nb, veff_perm, stickbuf, tpiba2, accumulate, s)) return true;
+    }
     if (!supported_z(g.nz) || !supported_xy(g.nx, g.ny)) return false;
     const size_t smem = (size_t(kPlaneWarps) * g.nx + size_t(g.nxc) * (g.ny | 1)) * sizeof(T);
     if (smem > 227 * 1024) return false;
@@ -494,13 +657,14 @@ template bool launch_hpsi_local_fast<float2, float>(const PWGrid&, int, const fl
                                                     const float2*, float2*, float2*, double, int, cudaStream_t);
 
 bool plane_perm_supported(const PWGrid& g) {
-    return g.nx == g.ny && (g.nx == 64 || g.nx == 96 || g.nx == 128) && supported_z(g.nz);
+    auto ok = [](int n) { return n == 64 || n == 96 || n == 128; };
+    return g.nx == g.ny && ok(g.nx) && ok(g.nz) && g.nz < 1024;
 }
 
 template <typename R>
 bool launch_permute_veff(const PWGrid& g, const R* veff_zyx, R* out, cudaStream_t s) {
     if (!plane_perm_supported(g)) return false;
-    k_permute_veff<R><<<1184, 256, 0, s>>>(g.nz, g.nx, g.nx / 32, veff_zyx, out);
+    k_permute_veff<R><<<1184, 256, 0, s>>>(g.nz, g.nx, g.nx / 32, g.nz / 32, veff_zyx, out);
     note_launch();
     B200_CUDA(cudaGetLastError());
     return true;

@@ -65,6 +65,34 @@ def test_hpsi_kbatch_equals_per_k(pkg, mp444, prec):
         assert rel(got, href) < (1e-12 if prec == "fp64" else 2e-5), ik
 
 
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_hpsi_kbatch_register_transforms(pkg, prec):
+    """A 96^3 grid takes the register/shuffle transforms in both the batched and the per-k-point calls;
+    they give the same H|psi>, and one k-point agrees with the oracle."""
+    spec = dataclasses.replace(pkg.synth.config(0), grid=(96, 96, 96))
+    kpts = pkg.synth.mp_grid(2, True)[:3]
+    P = pkg.pwdft
+    wl = P.build_workload(spec, kpts=kpts)
+    p = P.PREC_FP64 if prec == "fp64" else P.PREC_MIXED
+    dt = np.complex128 if prec == "fp64" else np.complex64
+    h = P.device_hamilt(wl, p)
+    nb, ld = 5, wl.basis.npwk_max
+    psis = _psis(wl, nb, dt)
+    outs = [torch.zeros_like(x) for x in psis]
+    h.hpsi_kbatch([0, 1, 2], psis, outs, nb, ld)
+    for ik in range(3):
+        one = torch.zeros_like(psis[ik])
+        h.hpsi(ik, psis[ik], one, nb, ld)
+        torch.cuda.synchronize()
+        assert rel(outs[ik].cpu().numpy(), one.cpu().numpy()) < (1e-14 if prec == "fp64" else 1e-6)
+    ref_b = PWBasisKRef(spec.a, wl.cell.latvec, spec.ecut, kpts[1:2], grid=spec.grid)
+    ref = H.HamiltPWRef(ref_b, 0, wl.veff_h, wl.vkb_h[1][:, :ref_b.npwk_max], wl.deeq_h, [8], [wl.cell.nat])
+    npw = ref_b.npwk[0]
+    href = ref.hpsi(wl.psi0_h[1][:nb, :npw].reshape(-1), nb, npw).reshape(nb, npw)
+    got = outs[1].cpu().numpy().reshape(nb, ld)[:, :npw].astype(np.complex128)
+    assert rel(got, href) < (1e-12 if prec == "fp64" else 2e-5)
+
+
 def test_hpsi_kbatch_generic_grid_falls_back(pkg):
     """A grid outside the compiled warp-transform sizes takes the per-k path inside the batch call."""
     spec = dataclasses.replace(pkg.synth.config(0), grid=(40, 40, 40))
