@@ -133,38 +133,54 @@ template <typename T> __device__ __forceinline__ T shfl_x(T v, int m) {
     return cmake<T>(__shfl_xor_sync(0xffffffffu, v.x, m), __shfl_xor_sync(0xffffffffu, v.y, m));
 }
 
-// this lane's forward-sign twiddles: lk[k1] = W_N^{lane*k1}, st[j] = W_{2h}^{lane mod h} with h = 16 >> j
+// Per-lane twiddles.  lk[k1] = W_N^{lane*k1}.  For the five lane stages (h = 16 >> j) the butterflies are
+// written without branches, with this lane's role folded into its twiddles:
+//   inverse (DIF):  u' = (p + sg*u) * wi[j]     sg = -1 on the bottom lane of a pair, +1 on the top;
+//                                               wi = conj(W_{2h}^{lane mod h}) on the bottom, 1 on the top;
+//   forward (DIT):  u' = a + wf[j] * b          (a, b) = (u, p) on the top, (p, u) on the bottom;
+//                                               wf = W_{2h}^{lane mod h} on the top, its negative on the bottom.
+template <typename T> struct LaneTw {
+    using R = typename RealOf<T>::type;
+    R sg[5];
+    T wi[5], wf[5];
+};
+
 template <typename T, int N>
-__device__ __forceinline__ void lane_twiddles(const T* __restrict__ roots, int lane, T* lk, T* st) {
+__device__ __forceinline__ void lane_twiddles(const T* __restrict__ roots, int lane, T* lk, LaneTw<T>& tw) {
+    using R = typename RealOf<T>::type;
     constexpr int M = N / 32;
 #pragma unroll
     for (int k1 = 0; k1 < M; ++k1) lk[k1] = roots[(lane * k1) % N];
 #pragma unroll
     for (int j = 0; j < 5; ++j) {
         const int h = 16 >> j;
-        st[j] = roots[M * (lane % h) * (16 / h)];
+        const bool bottom = lane & h;
+        const T w = roots[M * (lane % h) * (16 / h)];
+        tw.sg[j] = bottom ? R(-1) : R(1);
+        tw.wi[j] = bottom ? cmake<T>(w.x, -w.y) : cmake<T>(R(1), R(0));
+        tw.wf[j] = bottom ? cmake<T>(-w.x, -w.y) : w;
     }
 }
 
 template <typename T, int M>
-__device__ __forceinline__ void regfft_inv_dif(T* u, const T* lk, const T* st, int lane) {
+__device__ __forceinline__ void regfft_inv_dif(T* u, const T* lk, const LaneTw<T>& tw, int lane) {
     dftR<T, +1, M>(u);
 #pragma unroll
     for (int k1 = 1; k1 < M; ++k1) u[k1] = cmulc(u[k1], lk[k1]);
 #pragma unroll
     for (int j = 0; j < 5; ++j) {
         const int h = 16 >> j;
-        const bool bottom = lane & h;
 #pragma unroll
         for (int k1 = 0; k1 < M; ++k1) {
             const T p = shfl_x(u[k1], h);
-            u[k1] = bottom ? cmulc(csub(p, u[k1]), st[j]) : cadd(u[k1], p);
+            const T t = cmake<T>(fma(tw.sg[j], u[k1].x, p.x), fma(tw.sg[j], u[k1].y, p.y));
+            u[k1] = (j == 4) ? t : cmul(t, tw.wi[j]);  // the last stage's twiddle is 1
         }
     }
 }
 
 template <typename T, int M>
-__device__ __forceinline__ void regfft_fwd_dit(T* u, const T* lk, const T* st, int lane) {
+__device__ __forceinline__ void regfft_fwd_dit(T* u, const T* lk, const LaneTw<T>& tw, int lane) {
 #pragma unroll
     for (int j = 4; j >= 0; --j) {
         const int h = 16 >> j;
@@ -172,7 +188,10 @@ __device__ __forceinline__ void regfft_fwd_dit(T* u, const T* lk, const T* st, i
 #pragma unroll
         for (int k1 = 0; k1 < M; ++k1) {
             const T p = shfl_x(u[k1], h);
-            u[k1] = bottom ? csub(p, cmul(st[j], u[k1])) : cadd(u[k1], cmul(st[j], p));
+            const T a = bottom ? p : u[k1];
+            const T b = bottom ? u[k1] : p;
+            const T w = tw.wf[j];
+            u[k1] = cmake<T>(fma(-w.y, b.y, fma(w.x, b.x, a.x)), fma(w.y, b.x, fma(w.x, b.y, a.y)));
         }
     }
 #pragma unroll
@@ -201,8 +220,9 @@ __global__ void __launch_bounds__(kPlaneWarps * 32) k_plane_r(PlaneMapView pm, i
     for (int c = tid; c < nxc; c += NT) cmap[pm.xpos[c]] = c;
     T* plane = sb + (size_t(band) * nz + z) * pm.nst;
     for (int s = tid; s < pm.nst; s += NT) A[pm.xc[s] * LD + pm.sy[s]] = plane[s];
-    T lk[M], st[5];
-    lane_twiddles<T, N>(roots, lane, lk, st);
+    T lk[M];
+    LaneTw<T> tw;
+    lane_twiddles<T, N>(roots, lane, lk, tw);
     __syncthreads();
     int cm[M];
 #pragma unroll
@@ -213,7 +233,7 @@ __global__ void __launch_bounds__(kPlaneWarps * 32) k_plane_r(PlaneMapView pm, i
         T* col = A + c * LD;
 #pragma unroll
         for (int n1 = 0; n1 < M; ++n1) u[n1] = col[32 * n1 + lane];
-        regfft_inv_dif<T, M>(u, lk, st, lane);
+        regfft_inv_dif<T, M>(u, lk, tw, lane);
 #pragma unroll
         for (int k1 = 0; k1 < M; ++k1) col[32 * k1 + lane] = u[k1];
     }
@@ -224,11 +244,11 @@ __global__ void __launch_bounds__(kPlaneWarps * 32) k_plane_r(PlaneMapView pm, i
         T u[M];
 #pragma unroll
         for (int n1 = 0; n1 < M; ++n1) u[n1] = cm[n1] >= 0 ? A[cm[n1] * LD + sy] : zero_c<T>();
-        regfft_inv_dif<T, M>(u, lk, st, lane);
+        regfft_inv_dif<T, M>(u, lk, tw, lane);
         const R* vr = vz + sy * N;
 #pragma unroll
         for (int k1 = 0; k1 < M; ++k1) u[k1] = cscale(u[k1], vr[32 * k1 + lane]);
-        regfft_fwd_dit<T, M>(u, lk, st, lane);
+        regfft_fwd_dit<T, M>(u, lk, tw, lane);
 #pragma unroll
         for (int n1 = 0; n1 < M; ++n1)
             if (cm[n1] >= 0) A[cm[n1] * LD + sy] = u[n1];
@@ -240,7 +260,7 @@ __global__ void __launch_bounds__(kPlaneWarps * 32) k_plane_r(PlaneMapView pm, i
         T* col = A + c * LD;
 #pragma unroll
         for (int k1 = 0; k1 < M; ++k1) u[k1] = col[32 * k1 + lane];
-        regfft_fwd_dit<T, M>(u, lk, st, lane);
+        regfft_fwd_dit<T, M>(u, lk, tw, lane);
 #pragma unroll
         for (int n1 = 0; n1 < M; ++n1) col[32 * n1 + lane] = u[n1];
     }
@@ -275,8 +295,9 @@ __global__ void __launch_bounds__(kZWarps * 32) k_zinv_r(Src src, int b0, int nb
     const int ns = min(kStickTile, sm.nst - s0);
     const int band = blockIdx.y;
     for (int i = tid; i < kStickTile * LDZ; i += kZWarps * 32) A[i] = zero_c<T>();
-    T lk[M], st[5];
-    lane_twiddles<T, NZ>(roots, lane, lk, st);
+    T lk[M];
+    LaneTw<T> tw;
+    lane_twiddles<T, NZ>(roots, lane, lk, tw);
     __syncthreads();
     const T* p = reinterpret_cast<const T*>(e.psi) + size_t(b0 + band) * e.ld;
     const int j0 = sm.gofs[s0], j1 = sm.gofs[s0 + ns];
@@ -290,7 +311,7 @@ __global__ void __launch_bounds__(kZWarps * 32) k_zinv_r(Src src, int b0, int nb
         T* stick = A + sl * LDZ;
 #pragma unroll
         for (int n1 = 0; n1 < M; ++n1) u[n1] = stick[32 * n1 + lane];
-        regfft_inv_dif<T, M>(u, lk, st, lane);
+        regfft_inv_dif<T, M>(u, lk, tw, lane);
 #pragma unroll
         for (int k1 = 0; k1 < M; ++k1) stick[32 * k1 + lane] = u[k1];
     }
@@ -322,15 +343,16 @@ __global__ void __launch_bounds__(kZWarps * 32) k_zfwd_r(Src src, int b0, int nb
         const int sl = i - sz * ns;
         A[sl * LDZ + sz] = in[size_t(sz) * sm.nst + s0 + sl];
     }
-    T lk[M], st[5];
-    lane_twiddles<T, NZ>(roots, lane, lk, st);
+    T lk[M];
+    LaneTw<T> tw;
+    lane_twiddles<T, NZ>(roots, lane, lk, tw);
     __syncthreads();
     for (int sl = warp; sl < ns; sl += kZWarps) {
         T u[M];
         T* stick = A + sl * LDZ;
 #pragma unroll
         for (int k1 = 0; k1 < M; ++k1) u[k1] = stick[32 * k1 + lane];
-        regfft_fwd_dit<T, M>(u, lk, st, lane);
+        regfft_fwd_dit<T, M>(u, lk, tw, lane);
 #pragma unroll
         for (int n1 = 0; n1 < M; ++n1) stick[32 * n1 + lane] = u[n1];
     }
