@@ -43,9 +43,10 @@ ROOT = Path(__file__).resolve().parent
 WORKLOAD_NAME = ("64-atom diamond supercell a=20.52 bohr, ecut 50 Ry, 96^3 grid, npw 51627, "
                  "160 bands, 512 projectors, Gamma")
 METRIC = "H|psi> bands/s (FP64) + Davidson time-to-1e-8 Ry, mixed vs FP64"
-# dram__bytes_read.sum + dram__bytes_write.sum of the fused local H|psi> kernels for one 160-band
-# application, from the ncu capture summarised in profiles/hpsi_local_diamond64.md (None until captured)
-NCU_TRAFFIC_LOCAL_FP64 = None
+# dram__bytes_read.sum + dram__bytes_write.sum of the fused local H|psi> kernels (27 launches: 9 band
+# chunks x 3 passes) for one 160-band FP64 application, from the ncu capture without cache flush summarised
+# in profiles/hpsi_local_diamond64_traffic.md
+NCU_TRAFFIC_LOCAL_FP64 = 648301312
 
 
 def load_package():
@@ -327,10 +328,12 @@ def run_ours(args, ws, rank, local):
                    "l2": "inputs larger than L2 (psi+hpsi+projectors ~690 MB), no flush"},
         "mixed": {"value": ws * nb / (ms32 * 1e-3), "unit": "bands/s", "ms_per_step": ms32,
                   "dtype": "f32 FFT + f32 projector GEMM"},
-        "roofline": {"kernel": "fused local H|psi> FP64 (k_zpass_inv + k_plane + k_zpass_fwd)",
+        "roofline": {"kernel": "fused local H|psi> FP64 (k_zinv_r + k_plane_r + k_zfwd_r, 9 band chunks)",
                      "bound": "hbm", "achieved": ach64, "peak": hbm_peak, "unit": "GB/s",
                      "frac": ach64 / hbm_peak, "peak_kind": peak_kind,
                      "traffic": NCU_TRAFFIC_LOCAL_FP64,
+                     "traffic_note": "DRAM bytes of one 160-band local pass (27 launches), ncu without cache flush; "
+                                     "achieved and algorithmic_bytes are per the same pass",
                      "algorithmic_bytes": b_local64, "ms": ms_loc64,
                      "mixed": {"achieved": ach32, "frac": ach32 / hbm_peak, "ms": ms_loc32,
                                "algorithmic_bytes": b_local32}},
