@@ -364,23 +364,35 @@ __global__ void __launch_bounds__(kThreads, 1)
             const bool row_ok = row < M2;
             const bool im = row & 1;
             const bool use_beta = (beta.x != 0.f || beta.y != 0.f);
+            if (ws) {
 #pragma unroll
-            for (int j = 0; j < HB; ++j) {
-                const int n = tile_n * BN + col0 + j;
-                const bool valid = row_ok && n < N;
-                const float v = acc[j];
-                const float partner = __shfl_xor_sync(0xffffffffu, v, 1);
-                if (ws) {
-                    if (valid) ws[(size_t(split) * N + n) * size_t(M2) + row] = v;
-                    continue;
+                for (int j = 0; j < HB; ++j) {
+                    const int n = tile_n * BN + col0 + j;
+                    if (row_ok && n < N) ws[(size_t(split) * N + n) * size_t(M2) + row] = acc[j];
                 }
-                // (alpha * acc): re = ar*vr - ai*vi, im = ar*vi + ai*vr
-                float out = im ? alpha.x * v + alpha.y * partner : alpha.x * v - alpha.y * partner;
-                float* cp = C + size_t(n) * ldc2 + row;
-                const float cs = (use_beta && valid) ? *cp : 0.f;
-                const float cpart = __shfl_xor_sync(0xffffffffu, cs, 1);
-                if (use_beta) out += im ? beta.x * cs + beta.y * cpart : beta.x * cs - beta.y * cpart;
-                if (valid) *cp = out;
+            } else {
+                // groups of 16 columns: all loads of C in a group are issued before any is used
+                constexpr int G = 16;
+#pragma unroll
+                for (int j0 = 0; j0 < HB; j0 += G) {
+                    float cs[G];
+#pragma unroll
+                    for (int j = 0; j < G; ++j) {
+                        const int n = tile_n * BN + col0 + j0 + j;
+                        cs[j] = (use_beta && row_ok && n < N) ? C[size_t(n) * ldc2 + row] : 0.f;
+                    }
+#pragma unroll
+                    for (int j = 0; j < G; ++j) {
+                        const int n = tile_n * BN + col0 + j0 + j;
+                        const float v = acc[j0 + j];
+                        const float partner = __shfl_xor_sync(0xffffffffu, v, 1);
+                        // (alpha * acc): re = ar*vr - ai*vi, im = ar*vi + ai*vr
+                        float out = im ? alpha.x * v + alpha.y * partner : alpha.x * v - alpha.y * partner;
+                        const float cpart = __shfl_xor_sync(0xffffffffu, cs[j], 1);
+                        if (use_beta) out += im ? beta.x * cs[j] + beta.y * cpart : beta.x * cs[j] - beta.y * cpart;
+                        if (row_ok && n < N) C[size_t(n) * ldc2 + row] = out;
+                    }
+                }
             }
         }
     }
