@@ -67,6 +67,12 @@ _SIGS = {
     "b200_graph_launch": ([vp, vp], i32),
     "b200_graph_destroy": ([vp], i32),
     "b200_hamilt_autotune": ([vp, i32, i32, i32, vp, vp, vp, pi32], i32),
+    "b200_elecstate_pw_op_f64": ([i32, i32, f64, C.POINTER(vp), vp, vp], i32),
+    "b200_elecstate_pw_op_f32": ([i32, i32, f32, C.POINTER(vp), vp, vp], i32),
+    "b200_elecstate_pw_op_nc_f64": ([i32, i32, i32, f64, C.POINTER(vp), vp, vp, vp], i32),
+    "b200_elecstate_pw_op_nc_f32": ([i32, i32, i32, f32, C.POINTER(vp), vp, vp, vp], i32),
+    "b200_pw_basis_psi_to_rho_f64": ([vp, i32, i32, i32, vp, pf64, vp, vp], i32),
+    "b200_pw_basis_psi_to_rho_f32": ([vp, i32, i32, i32, vp, pf64, vp, vp], i32),
     "b200_cal_ylm_real_op_f64": ([i32, i32, vp, vp, vp], i32),
     "b200_cal_ylm_real_op_f32": ([i32, i32, vp, vp, vp], i32),
     "b200_cal_sk_op_f64": ([i32] * 14 + [pi32, vp, vp, f64, vp, vp, vp, vp, vp, vp, vp], i32),
@@ -94,6 +100,7 @@ _SIGS = {
     "b200_david_diag_hamilt": ([vp, vp, i32, i32, i32, vp, pf64, f64, i32, i32, i32, pi32], i32),
     "b200_david_stats": ([vp, pi32, pi32, pi32], i32),
     "b200_david_set_trace": ([vp, i32], i32),
+    "b200_david_set_low_ndim": ([vp, i32], i32),
     "b200_david_trace": ([vp, i32, i32, pf64, pi32, pf64, pi32], i32),
     "b200_david_set_verbosity": ([vp, i32], i32),
     "b200_david_set_stream": ([vp, vp], i32),

@@ -376,6 +376,12 @@ int b200_david_set_mixed_threshold(b200_david* d, double thr) {
         d->d->set_mixed_thr(thr);
     });
 }
+int b200_david_set_low_ndim(b200_david* d, int ndim) {
+    return guarded([&] {
+        B200_CHECK(d != nullptr, b200::kInvalidArgument, "NULL argument");
+        d->d->set_low_ndim(ndim);
+    });
+}
 int b200_david_set_trace(b200_david* d, int on) {
     return guarded([&] {
         B200_CHECK(d != nullptr, b200::kInvalidArgument, "NULL argument");

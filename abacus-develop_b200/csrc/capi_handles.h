@@ -10,6 +10,8 @@ struct b200_pw_basis {
     b200::PWGrid grid;
     b200::DeviceArray<double2> aux64;
     b200::DeviceArray<float2> aux32;
+    b200::DeviceArray<double2> rho_box64;  // psi(r) of one band (psi -> rho)
+    b200::DeviceArray<float2> rho_box32;
 };
 struct b200_hamilt {
     std::unique_ptr<b200::Hamilt> h;

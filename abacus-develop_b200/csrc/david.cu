@@ -550,7 +550,7 @@ class David : public DavidBase {
                 // solver's stream finish first, then re-target on that stream (the current k-point's
                 // preconditioner, in stream order)
                 B200_CUDA(cudaStreamSynchronize(stream_));
-                e32_ = std::make_unique<Engine<float2>>(nband_, cap_, ndim_, pc_.ptr);
+                e32_ = std::make_unique<Engine<float2>>(nband_, cap_, low_ndim_ > 0 ? low_ndim_ : ndim_, pc_.ptr);
                 e32_->set_stream(stream_);
                 e32_->retarget(dim_, pc_.ptr);
             }
@@ -582,6 +582,11 @@ class David : public DavidBase {
     const DavidStats& stats() const override { return stats_; }
     DavidTrace& trace() override { return trace_; }
     void set_mixed_thr(double thr) override { mixed_thr_ = thr; }
+    void set_low_ndim(int ndim) override {
+        B200_CHECK(ndim >= 2, kInvalidArgument, "david_ndim of the FP32 stage must be at least 2");
+        if (ndim != (low_ndim_ > 0 ? low_ndim_ : ndim_)) e32_.reset();  // rebuilt at the next mixed solve
+        low_ndim_ = ndim;
+    }
     int precision() const override { return precision_; }
     void set_stream(cudaStream_t st) override {
         stream_ = st;
@@ -616,6 +621,7 @@ class David : public DavidBase {
     int verbosity_ = 0;
     cudaStream_t stream_ = 0;
     double mixed_thr_ = 1e-6;
+    int low_ndim_ = 0;
     DeviceArray<double> pc_;
     DeviceArray<float2> psi32_;
     std::unique_ptr<Engine<double2>> e64_;

@@ -51,6 +51,9 @@ struct DavidBase {
                             double* eig, double thr, int maxiter, int ntry_max, int notconv_max) = 0;
     virtual const DavidStats& stats() const = 0;
     virtual void set_mixed_thr(double thr) = 0;
+    // mixed precision only: subspace size factor (nbase_x = ndim * nband) of the FP32 stage (default: the
+    // solver's own david_ndim); a smaller FP32 subspace means smaller FP64 subspace eigensolves there
+    virtual void set_low_ndim(int ndim) = 0;
     virtual void set_reference_refresh(bool on) = 0;
     virtual int precision() const = 0;
     // 0 = quiet; 1 = one line per Davidson iteration on stderr (iteration, basis size, unconverged bands,

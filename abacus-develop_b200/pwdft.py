@@ -121,6 +121,22 @@ def _check_block(t, complex128: bool, nbands: int, ld: int, what: str):
         raise ValueError(f"{what}: {t.numel()} elements, the call reads or writes {int(nbands) * int(ld)}")
 
 
+def elecstate_pw_op(spin, nrxx, w1, rho, wfcr, stream=None):
+    """elecstate_pw_op<FP, DEVICE_GPU>: rho[spin] += w1*|wfcr|^2; rho is a sequence of nspin device tensors."""
+    torch = _torch()
+    f = "b200_elecstate_pw_op_f64" if wfcr.dtype == torch.complex128 else "b200_elecstate_pw_op_f32"
+    arr = (_lib.vp * len(rho))(*[ptr(r) for r in rho])
+    call(f, spin, nrxx, w1, arr, ptr(wfcr), stream_ptr(stream))
+
+
+def elecstate_pw_op_nc(domag, domag_z, nrxx, w1, rho, wfcr, wfcr_another_spin, stream=None):
+    """The nspin = 4 overload of elecstate_pw_op; rho is a sequence of 4 device tensors."""
+    torch = _torch()
+    f = "b200_elecstate_pw_op_nc_f64" if wfcr.dtype == torch.complex128 else "b200_elecstate_pw_op_nc_f32"
+    arr = (_lib.vp * 4)(*[ptr(r) for r in rho])
+    call(f, int(domag), int(domag_z), nrxx, w1, arr, ptr(wfcr), ptr(wfcr_another_spin), stream_ptr(stream))
+
+
 def cal_ylm_real_op(ng, lmax, g, ylm, stream=None):
     """ModuleBase::cal_ylm_real_op<FP, DEVICE_GPU>: g (ng x 3) -> ylm ((lmax+1)^2 x ng)."""
     torch = _torch()
@@ -254,6 +270,19 @@ class PWBasisK:
         torch = _torch()
         f = "b200_real_to_recip_f64" if out.dtype == torch.complex128 else "b200_real_to_recip_f32"
         call(f, self._h, ptr(inp), ptr(out), ik, int(add), factor, stream_ptr(stream))
+
+    def psi_to_rho(self, ik, psi, nbands, ld, w1, rho, stream=None):
+        """psiToRho's band loop for k-point ik: rho[r] += w1[ib]*|psi_ib(r)|^2 (rho in ABACUS's r order)."""
+        torch = _torch()
+        f64 = psi.dtype == torch.complex128
+        _check_block(psi, f64, nbands, ld, "psi")
+        if rho.dtype != (torch.float64 if f64 else torch.float32) or rho.numel() < self.nx * self.ny * self.nz:
+            raise ValueError("rho: need a real tensor of the psi precision with nx*ny*nz entries")
+        w = np.ascontiguousarray(np.asarray(w1, dtype=np.float64))
+        if len(w) < nbands:
+            raise ValueError("w1: need nbands weights")
+        call("b200_pw_basis_psi_to_rho_f64" if f64 else "b200_pw_basis_psi_to_rho_f32", self._h, ik, nbands, ld,
+             ptr(psi), w.ctypes.data_as(_lib.pf64), ptr(rho), stream_ptr(stream))
 
     def __del__(self):
         try:
@@ -456,6 +485,10 @@ class DiagoDavid:
 
     def set_mixed_threshold(self, thr):
         call("b200_david_set_mixed_threshold", self._h, float(thr))
+
+    def set_low_ndim(self, ndim):
+        """Mixed precision: david_ndim of the FP32 stage (smaller subspace, smaller FP64 eigensolves)."""
+        call("b200_david_set_low_ndim", self._h, int(ndim))
 
     def set_trace(self, on=True):
         """Record per-iteration eigenvalues and times of the next solves (see trace())."""

@@ -193,6 +193,25 @@ int b200_graph_destroy(b200_graph* g);
 int b200_hamilt_autotune(b200_hamilt* h, int ik, int nbands, int ld, const void* psi_d, void* hpsi_d, void* stream,
                          int* best_chunk);
 
+/* ---- psi -> rho (ElecStatePW::psiToRho, module_elecstate/elecstate_pw.cpp:78-216) ---- */
+/* elecstate::elecstate_pw_op<FP, DEVICE_GPU> (module_elecstate/kernels/elecstate_op.h):
+ * rho[spin][ir] += w1 * |wfcr[ir]|^2.  rho is a host array of device pointers, as the reference's FPTYPE**. */
+int b200_elecstate_pw_op_f64(int spin, int nrxx, double w1, double* const* rho, const void* wfcr_d, void* stream);
+int b200_elecstate_pw_op_f32(int spin, int nrxx, float w1, float* const* rho, const void* wfcr_d, void* stream);
+/* the nspin = 4 overload (DOMAG, DOMAG_Z, four rho components) */
+int b200_elecstate_pw_op_nc_f64(int domag, int domag_z, int nrxx, double w1, double* const* rho, const void* wfcr_d,
+                                const void* wfcr_another_spin_d, void* stream);
+int b200_elecstate_pw_op_nc_f32(int domag, int domag_z, int nrxx, float w1, float* const* rho, const void* wfcr_d,
+                                const void* wfcr_another_spin_d, void* stream);
+/* The band loop of psiToRho for k-point ik (collinear): for every band with w1[ib] != 0,
+ * rho_d[r] += w1[ib] * |psi_ib(r)|^2, psi(r) = recip_to_real of band ib (psi_d + ib*ld).
+ * w1: host array of nbands weights (wg(ik, ib) / omega in the reference); rho_d: nx*ny*nz in ABACUS's
+ * r order, accumulated into. */
+int b200_pw_basis_psi_to_rho_f64(b200_pw_basis* b, int ik, int nbands, int ld, const void* psi_d, const double* w1,
+                                 double* rho_d, void* stream);
+int b200_pw_basis_psi_to_rho_f32(b200_pw_basis* b, int ik, int nbands, int ld, const void* psi_d, const double* w1,
+                                 float* rho_d, void* stream);
+
 /* ---- projector generation (pseudopot_cell_vnl::getvnl, VNL_in_pw.cpp:412-540) ---- */
 /* ModuleBase::cal_ylm_real_op<FP, DEVICE_GPU> (module_base/kernels/math_op.h): real Y_lm of ng vectors
  * g (ng x 3) into ylm ((lmax+1)^2 x ng), lmax <= 4.  The reference's scratch p is internal here. */
@@ -278,6 +297,9 @@ int b200_david_set_mixed_threshold(b200_david* d, double thr);
 /* Statistics of the last solve: Davidson iterations in the FP32 stage (mixed only), in FP64,
  * and the number of single-band H applications (all stages). */
 int b200_david_stats(const b200_david* d, int* iters_low, int* iters_fp64, int* hpsi_bands);
+/* Mixed precision only: subspace size factor of the FP32 stage (nbase_x = ndim * nband, ndim >= 2;
+ * default: the solver's david_ndim).  No counterpart in the reference. */
+int b200_david_set_low_ndim(b200_david* d, int ndim);
 /* Eigenvalue trace (no counterpart in the reference): with on != 0 the next solves record, per
  * iteration, the seconds since the solve began (taken when that iteration's eigenvalues reach the host
  * for the convergence test), the stage (0 = FP64, 1 = FP32) and the nband Ritz values.

@@ -11,6 +11,7 @@ reference's unit tests as text and writes ``tests/golden/*.npz``:
   vnl_op.npz       <- .../kernels/test/vnl_op_test.cpp
   wf_op.npz        <- .../kernels/test/wf_op_test.cpp
   ylm_op.npz       <- source/module_base/kernels/test/math_op_test.cpp
+  elecstate_op.npz <- source/module_elecstate/kernels/test/elecstate_op_test.cpp
   pyabacus_si2.npz <- python/pyabacus/tests/test_diag/Si2.mat (sparse H, CSC arrays)
 
 The fixtures are committed; tests never read the reference tree.
@@ -114,6 +115,15 @@ def main():
     v = _vectors(mt)
     s = _scalars(mt, ["ng", "lmax"])
     np.savez(OUT / "ylm_op.npz", g=v["g"], expected_ylm=v["expected_ylm"], ng=int(s["ng"]), lmax=int(s["lmax"]))
+
+    et = REF / "source/module_elecstate/kernels/test/elecstate_op_test.cpp"
+    v = _vectors(et)
+    s = _scalars(et, ["spin", "nrxx", "w1", "w2"])
+    src = et.read_text()
+    flags = {n: int(re.search(r"\b" + n + r"\s*=\s*(true|false)", src).group(1) == "true") for n in ("DOMAG", "DOMAG_Z")}
+    np.savez(OUT / "elecstate_op.npz", wfcr=v["wfcr"], expected_rho=v["expected_rho"], wfcr_2=v["wfcr_2"],
+             wfcr_another_spin_2=v["wfcr_another_spin_2"], expected_rho_2=v["expected_rho_2"],
+             spin=int(s["spin"]), nrxx=int(s["nrxx"]), w1=s["w1"], w2=s["w2"], **flags)
 
     try:
         import scipy.io
