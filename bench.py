@@ -239,6 +239,10 @@ def run_reference(args, ws, rank):
                                    f"reference CPU functors and PW_Basis_K transforms, {cores} FFT/BLAS threads"},
         "e2e": {"value": val, "unit": "bands/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    ref = cpu_reference_davidson_8atom(load_package())
+    if ref is not None:
+        ref.pop("eig")
+        line["davidson_8atom"] = ref
     print(json.dumps(line), flush=True)
 
 
@@ -344,6 +348,7 @@ def run_ours(args, ws, rank, local):
         "clocks": clk.summary(),
     }
 
+    line["psi_to_rho"] = rho_bench(P, wl, psi, args.steps, stream)
     if not args.skip_david:
         line["davidson"] = davidson_bench(P, wl, h64)
     del h32, psi32, hpsi32
@@ -360,12 +365,98 @@ def run_ours(args, ws, rank, local):
         torch.cuda.empty_cache()
 
     if rank == 0 and ws == 1 and not args.skip_cpu:
+        line["davidson_8atom"] = davidson_8atom(pkg)
         bps, done, el = cpu_port_bands_per_s(wl, budget_s=args.cpu_budget)
         line["cpu_baseline"] = {"value": bps, "unit": "bands/s", "cores": 1, "kind": "port",
                                 "sample": f"{done} bands of the 160-band block in {el:.1f} s, numpy restatement "
                                           f"of the reference CPU functors + PW_Basis_K transforms, 1 thread"}
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def rho_bench(P, wl, psi, steps, stream):
+    """psiToRho's band loop on the 64-atom cell (160 bands, FP64): bands/s and bytes moved per band by the
+    drop-in transform path (sphere read, three full-box sweeps of the transform, rho read + write)."""
+    import torch
+    b = wl.basis
+    nb, ld = wl.spec.nbands, b.npwk_max
+    N = b.nx * b.ny * b.nz
+    rho = torch.zeros(N, dtype=torch.float64, device="cuda")
+    w1 = np.full(nb, 2.0 / b.omega)
+    step = lambda: b.psi_to_rho(0, psi, nb, ld, w1, rho)  # noqa: E731
+    for _ in range(2):
+        step()
+    ms = time_steps(step, max(3, steps // 4), stream)
+    return {"bands_per_s": nb / (ms * 1e-3), "ms_per_160_bands": ms,
+            "path": "recip_to_real into a full box per band + elecstate_pw_op (the reference's loop)"}
+
+
+def cpu_reference_davidson_8atom(pkg):
+    """The reference's own CPU DiagoDavid (compiled from its sources, oracle/_ref) on the 8-atom cell
+    (32 bands, npw 2945, thr 1e-9), H|psi> by the oracle port on all host cores.  None if not built."""
+    sys.path.insert(0, str(ROOT))
+    from oracle import hamilt_ref as H
+    from oracle import ref_david
+    from oracle.pw_basis_ref import PWBasisKRef
+    if not ref_david.available():
+        return None
+    cores = os.cpu_count() or 1
+    H.FFT_WORKERS = cores
+    spec = pkg.synth.config(0)
+    cell = pkg.synth.make_cell(spec)
+    b = PWBasisKRef(spec.a, cell.latvec, spec.ecut, np.zeros((1, 3)))
+    ld = int(b.npwk_max)
+    ham = H.HamiltPWRef(b, 0, cell.veff(b.nx, b.ny, b.nz), cell.vkb(b.gplusk_cart(0), ld, b.omega), cell.deeq(), [8],
+                        [cell.nat])
+    psi = cell.psi0(b.gplusk_cart(0), spec.nbands, ld).reshape(-1).copy()
+    e = np.zeros(spec.nbands)
+    t0 = time.perf_counter()
+    it = ref_david.diag(lambda x, nv, dim, i0, i1: ham.hpsi(x[i0:i1 + 1].reshape(-1), i1 - i0 + 1, dim)
+                        .reshape(i1 - i0 + 1, dim), H.precondition(b, 0), spec.nbands, ld, 4, ld, psi, e, 1e-9, 200)
+    return {"seconds": time.perf_counter() - t0, "iters": it, "eig": e, "cores": cores,
+            "kind": "reference", "what": "DiagoDavid<complex<double>, CPU> compiled from the reference sources "
+                                        "(diago_david.cpp, math_kernel_op.cpp, dngvd_op.cpp; scipy OpenBLAS), "
+                                        "H|psi> by the numpy port of the reference functors"}
+
+
+def davidson_8atom(pkg):
+    """8-atom cell (a = 10.26 bohr, ecut 30 Ry, 36^3, npw 2945, 32 bands, thr 1e-9): GPU FP64 and mixed solves
+    next to the reference's CPU DiagoDavid on the same inputs."""
+    import torch
+    P = pkg.pwdft
+    spec = pkg.synth.config(0)
+    wl = P.build_workload(spec)
+    h = P.device_hamilt(wl, P.PREC_FP64)
+    ld, nb = wl.basis.npwk_max, spec.nbands
+    pc = P.precondition_d(wl.basis, 0)
+    out = {"workload": "8-atom diamond a=10.26 bohr, ecut 30 Ry, 36^3 grid, npw 2945, 32 bands, Gamma, thr 1e-9"}
+    for name, prec in (("gpu_fp64", P.PREC_FP64), ("gpu_mixed", P.PREC_MIXED)):
+        best = None
+        for _ in range(3):
+            dav = P.DiagoDavid(pc, nb, ld, 4, prec)
+            x = torch.from_numpy(wl.psi0_h[0].reshape(-1).copy()).cuda()
+            e = np.zeros(nb)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            it = dav.diag_hamilt(h, 0, ld, x, e, 1e-9, 200)
+            torch.cuda.synchronize()
+            dt = time.perf_counter() - t0
+            best = dt if best is None else min(best, dt)
+        out[name + "_s"] = best
+        out[name + "_iters"] = it
+        out[name + "_eig"] = e
+    ref = cpu_reference_davidson_8atom(pkg)
+    if ref is not None:
+        out["cpu_reference_s"] = ref["seconds"]
+        out["cpu_reference_iters"] = ref["iters"]
+        out["cpu_reference_cores"] = ref["cores"]
+        out["cpu_reference"] = ref["what"]
+        out["max_abs_diff_fp64_vs_reference_ry"] = float(np.max(np.abs(out["gpu_fp64_eig"] - ref["eig"])))
+        out["max_abs_diff_mixed_vs_reference_ry"] = float(np.max(np.abs(out["gpu_mixed_eig"] - ref["eig"])))
+        out["gpu_fp64_speedup_vs_cpu_reference"] = ref["seconds"] / out["gpu_fp64_s"]
+    out.pop("gpu_fp64_eig")
+    out.pop("gpu_mixed_eig")
+    return out
 
 
 def settle_time(trace, ref, tol=1e-8):

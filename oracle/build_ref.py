@@ -1,0 +1,86 @@
+"""Build oracle/_ref/libref_david.so: the reference's own CPU DiagoDavid, compiled from its sources.
+
+Test infrastructure: only the tests and bench.py's CPU reference arm load the library.  Run in a container
+where the reference tree is mounted (default /root/reference, override with ABACUS_REF); the result is a
+shared library under oracle/_ref/ (git-ignored) that needs only scipy's bundled OpenBLAS at run time.
+
+Compiled from the reference (unchanged, from where they lie):
+  source/module_hsolver/diago_david.cpp            the Davidson iteration
+  source/module_hsolver/kernels/math_kernel_op.cpp the CPU BLAS functors it calls (gemm_op, gemv_op, ...)
+  source/module_hsolver/kernels/dngvd_op.cpp       dnevx_op / dngvd_op (LAPACK zheevx, zhegvd, ...)
+  source/module_base/module_device/memory_op.cpp   resize / set / sync / delete memory ops
+  source/module_base/timer.cpp                     ModuleBase::timer::tick
+plus this directory's ref/shim.cpp (process-level services: WARNING_QUIT throws, TITLE is silent, the CPU
+device tag, a one-process reduce_pool) and ref/david_capi.cpp (a C entry point with a callback H|psi>).
+
+The reference calls Fortran BLAS/LAPACK (zgemm_, zheevx_, ...); scipy's OpenBLAS exports the same routines
+under a scipy_ prefix, so the object files' references are renamed with objcopy before linking.
+No cmake, no reference build system, no network.
+"""
+from __future__ import annotations
+
+import glob
+import os
+import shutil
+import subprocess
+import sys
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+OUT = HERE / "_ref"
+REF = Path(os.environ.get("ABACUS_REF", "/root/reference")) / "source"
+SOURCES = [
+    "module_hsolver/diago_david.cpp",
+    "module_hsolver/kernels/math_kernel_op.cpp",
+    "module_hsolver/kernels/dngvd_op.cpp",
+    "module_base/module_device/memory_op.cpp",
+    "module_base/timer.cpp",
+]
+OWN = [HERE / "ref" / "shim.cpp", HERE / "ref" / "david_capi.cpp"]
+
+
+def openblas() -> Path:
+    import scipy
+    libs = sorted(glob.glob(str(Path(scipy.__file__).resolve().parent.parent / "scipy.libs" / "libscipy_openblas*.so")))
+    if not libs:
+        raise RuntimeError("scipy's bundled OpenBLAS not found")
+    return Path(libs[0])
+
+
+def run(cmd):
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(" ".join(map(str, cmd)) + "\n" + r.stdout + r.stderr)
+    return r.stdout
+
+
+def build(quiet: bool = False) -> Path | None:
+    if not REF.exists():
+        if not quiet:
+            print("reference tree not present: oracle/_ref not rebuilt", file=sys.stderr)
+        return None
+    OUT.mkdir(exist_ok=True)
+    tmp = OUT / "obj"
+    tmp.mkdir(exist_ok=True)
+    flags = ["-std=c++14", "-O2", "-fPIC", "-fopenmp", f"-I{REF}", f"-I{REF / 'module_base/module_container'}"]
+    objs = []
+    for src in [REF / s for s in SOURCES] + OWN:
+        obj = tmp / (src.stem + ".o")
+        run(["g++", *flags, "-c", str(src), "-o", str(obj)])
+        objs.append(obj)
+    # Fortran BLAS / LAPACK references -> scipy_ names
+    lib = openblas()
+    exported = set(ln.split()[-1] for ln in run(["nm", "-D", "--defined-only", str(lib)]).splitlines() if ln.strip())
+    for obj in objs:
+        undef = [ln.split()[-1] for ln in run(["nm", "-u", str(obj)]).splitlines() if ln.strip()]
+        ren = [f"--redefine-sym={s}=scipy_{s}" for s in undef if s.endswith("_") and ("scipy_" + s) in exported]
+        if ren:
+            run(["objcopy", *ren, str(obj)])
+    so = OUT / "libref_david.so"
+    run(["g++", "-shared", "-fopenmp", "-o", str(so), *map(str, objs), str(lib), f"-Wl,-rpath,{lib.parent}"])
+    shutil.rmtree(tmp)
+    return so
+
+
+if __name__ == "__main__":
+    print(build())

@@ -1,0 +1,54 @@
+"""Oracle (test infrastructure only): ctypes access to the reference's own CPU DiagoDavid, compiled from
+the reference sources into oracle/_ref/libref_david.so by oracle/build_ref.py.  Only the tests and the
+benchmark's CPU reference arm use it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+LIB = Path(__file__).resolve().parent / "_ref" / "libref_david.so"
+_CB = C.CFUNCTYPE(None, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int)
+_lib = None
+
+
+def available() -> bool:
+    return LIB.exists()
+
+
+def _load():
+    global _lib
+    if _lib is None:
+        lib = C.CDLL(str(LIB))
+        lib.ref_david.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_double), _CB, C.c_void_p,
+                                  C.c_void_p, C.POINTER(C.c_double), C.c_double, C.c_int, C.c_int, C.c_int,
+                                  C.POINTER(C.c_int)]
+        lib.ref_david.restype = C.c_int
+        lib.ref_last_error.restype = C.c_char_p
+        _lib = lib
+    return _lib
+
+
+def diag(hpsi, precond, nband, dim, david_ndim, ldpsi, psi, eig, thr, maxiter, ntry_max=5, notconv_max=0):
+    """DiagoDavid<complex<double>, CPU>::diag.  hpsi(x, nvec, dim, i0, i1) -> H applied to vectors i0..i1 of
+    the block x (nvec x dim complex128), returned as ((i1-i0+1) x dim).  psi (complex128, nband vectors at
+    m*ldpsi) and eig (float64, nband) are updated in place; returns the iteration count."""
+    lib = _load()
+    assert psi.dtype == np.complex128 and psi.flags.c_contiguous and eig.dtype == np.float64
+
+    def cb(user, x, hx, nvec, d, i0, i1):
+        m = i1 - i0 + 1
+        X = np.ctypeslib.as_array(C.cast(x, C.POINTER(C.c_double)), shape=(nvec * d * 2,)).view(np.complex128)
+        HX = np.ctypeslib.as_array(C.cast(hx, C.POINTER(C.c_double)), shape=(m * d * 2,)).view(np.complex128)
+        HX[:] = hpsi(X.reshape(nvec, d), nvec, d, i0, i1).reshape(-1)
+
+    fn = _CB(cb)
+    pc = np.ascontiguousarray(precond, dtype=np.float64)
+    it = C.c_int()
+    rc = lib.ref_david(nband, dim, david_ndim, ldpsi, pc.ctypes.data_as(C.POINTER(C.c_double)), fn, None, psi.ctypes.data,
+                       eig.ctypes.data_as(C.POINTER(C.c_double)), thr, maxiter, ntry_max, notconv_max, C.byref(it))
+    if rc != 0:
+        raise RuntimeError("reference DiagoDavid failed: " + lib.ref_last_error().decode())
+    return it.value
