@@ -523,6 +523,9 @@ class David : public DavidBase {
         pc_.resize(dim);
         B200_CUDA(cudaMemcpy(pc_.ptr, precond_d, dim * sizeof(double), cudaMemcpyDeviceToDevice));
         e64_ = std::make_unique<Engine<double2>>(nband, dim, ndim, pc_.ptr);
+        // a mixed solver holds its FP32 engine from the start: every allocation happens here, as the
+        // reference's constructor does (diago_david.cpp:34-148), not inside a solve
+        if (precision == 1) e32_ = std::make_unique<Engine<float2>>(nband, dim, ndim, pc_.ptr);
     }
     int diag(const HPsiDevice& f64, int ldpsi, void* psi, double* eig, double thr, int maxiter, int ntry_max,
              int notconv_max) override {
