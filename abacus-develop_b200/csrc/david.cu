@@ -525,7 +525,10 @@ class David : public DavidBase {
         e64_ = std::make_unique<Engine<double2>>(nband, dim, ndim, pc_.ptr);
         // a mixed solver holds its FP32 engine from the start: every allocation happens here, as the
         // reference's constructor does (diago_david.cpp:34-148), not inside a solve
-        if (precision == 1) e32_ = std::make_unique<Engine<float2>>(nband, dim, ndim, pc_.ptr);
+        if (precision == 1) {
+            e32_ = std::make_unique<Engine<float2>>(nband, dim, ndim, pc_.ptr);
+            psi32_.resize(size_t(nband) * dim);  // FP32 copy of psi for ldpsi == dim (grown only for a wider ldpsi)
+        }
     }
     int diag(const HPsiDevice& f64, int ldpsi, void* psi, double* eig, double thr, int maxiter, int ntry_max,
              int notconv_max) override {

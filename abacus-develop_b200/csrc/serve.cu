@@ -14,7 +14,9 @@
 //    request whose cell is below its in-flight cap and whose slot is pooled or fits in the HBM budget (idle
 //    slots of other shapes are released to make room).  The per-cell caps keep small requests from waiting
 //    behind large ones and bound how many large solves share the device at once;
-//  * every worker owns a non-blocking stream, so admitted requests overlap on the device.
+//  * every slot owns a non-blocking stream, so admitted requests overlap on the device; its priority
+//    follows the cell's size (smallest cell highest), so short solves are not queued behind the blocks of a
+//    large cell's kernels.  A slot keeps its stream for life, whichever worker runs it.
 // A request's result depends only on (cell, k-point, nbands, thr, precision, seed): the start vectors come
 // from a counter-based generator keyed by the seed, each solve starts from a zeroed subspace, and no
 // kernel's result depends on what else runs.
@@ -74,8 +76,20 @@ struct ServeCell {
     int max_inflight, inflight;
 };
 
+// a solver slot's own stream, destroyed after everything else in the slot (declared first)
+struct SlotStream {
+    cudaStream_t s = nullptr;
+    ~SlotStream() {
+        if (s) {
+            cudaStreamSynchronize(s);
+            cudaStreamDestroy(s);
+        }
+    }
+};
+
 struct Slot {
-    int cell = 0, nbands = 0, precision = 0;
+    SlotStream stream;  // every request on this slot runs on it: start vectors, solve, H|psi>
+    int cell = 0, nbands = 0, precision = 0, priority = 0;
     std::unique_ptr<DavidBase> dav;
     DeviceArray<double2> psi;
     std::unique_ptr<HpsiWork> work;
@@ -284,22 +298,40 @@ class Server {
         return nullptr;
     }
 
-    std::unique_ptr<Slot> make_slot(const Request& r, cudaStream_t s) {
-        const ServeCell& c = cells_[r.cell];
+    // stream priority of a cell: smaller cells (fewer plane waves) run at higher priority, so the block
+    // scheduler dispatches their short kernels as soon as blocks of a larger cell's kernels retire instead of
+    // after them; levels spread over the device's range by the cell's rank among the resident cells
+    int priority_locked(int cell) const {
+        int least = 0, greatest = 0;
+        if (cudaDeviceGetStreamPriorityRange(&least, &greatest) != cudaSuccess) return 0;
+        int rank = 0, n = 0;
+        std::vector<int> sizes;
+        for (const ServeCell& c : cells_) sizes.push_back(c.dim_max);
+        std::sort(sizes.begin(), sizes.end());
+        sizes.erase(std::unique(sizes.begin(), sizes.end()), sizes.end());
+        n = int(sizes.size());
+        rank = int(std::lower_bound(sizes.begin(), sizes.end(), cells_[cell].dim_max) - sizes.begin());
+        if (n <= 1) return least;
+        return greatest + (least - greatest) * rank / (n - 1);
+    }
+
+    std::unique_ptr<Slot> make_slot(const Request& r, const ServeCell& c, int priority) {
         auto slot = std::make_unique<Slot>();
+        B200_CUDA(cudaStreamCreateWithPriority(&slot->stream.s, cudaStreamNonBlocking, priority));
+        slot->priority = priority;
         slot->cell = r.cell;
         slot->nbands = r.nbands;
         slot->precision = r.precision;
         slot->dav = make_david(r.nbands, c.dim_max, ndim_, r.precision, c.h->h->grid->kmaps[c.kmax].precond.ptr);
-        slot->dav->set_stream(s);
+        slot->dav->set_stream(slot->stream.s);
         slot->psi.resize(size_t(r.nbands) * c.npwx);
         slot->work = std::make_unique<HpsiWork>();
         slot->bytes = slot_bytes(r.cell, r.nbands, r.precision);
         return slot;
     }
 
-    void run(Request& r, Slot& slot, cudaStream_t s) {
-        const ServeCell& c = cells_[r.cell];
+    void run(Request& r, const ServeCell& c, Slot& slot) {
+        cudaStream_t s = slot.stream.s;
         Hamilt* H = c.h->h.get();
         const KMap& km = H->grid->kmaps[r.ik];
         slot.dav->retarget(km.npw, km.precond.ptr);
@@ -328,14 +360,11 @@ class Server {
 
     void worker() {
         cudaSetDevice(dev_);
-        cudaStream_t s = nullptr;
-        if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) s = nullptr;
         std::unique_lock<std::mutex> lk(mu_);
         for (;;) {
             std::deque<Request*>::iterator pick;
             cv_work_.wait(lk, [&] {
                 if (stop_) return true;
-                if (!s) return false;
                 pick = next_admissible_locked();
                 return pick != queue_.end();
             });
@@ -346,6 +375,8 @@ class Server {
             size_t reserve = 0;
             std::vector<std::unique_ptr<Slot>> victims;
             std::unique_ptr<Slot> slot = take_slot_locked(*r, reserve, victims);
+            const ServeCell cell = cells_[r->cell];  // a copy: add_cell may grow cells_ while this request runs
+            const int priority = slot ? slot->priority : priority_locked(r->cell);
             ++inflight_;
             peak_inflight_ = std::max(peak_inflight_, inflight_);
             r->t_admit = now_s(t0_);
@@ -353,20 +384,20 @@ class Server {
             victims.clear();  // frees idle slots of other shapes (outside the lock)
             try {
                 if (!slot) {
-                    slot = make_slot(*r, s);
+                    slot = make_slot(*r, cell, priority);
                     std::lock_guard<std::mutex> g(mu_);
                     ++slots_created_;
                 }
-                run(*r, *slot, s);
+                run(*r, cell, *slot);
                 r->status = 0;
             } catch (const Error& e) {
                 r->status = e.code;
                 r->err = e.what();
-                cudaStreamSynchronize(s);
+                if (slot && slot->stream.s) cudaStreamSynchronize(slot->stream.s);
             } catch (const std::exception& e) {
                 r->status = kInvalidArgument;
                 r->err = e.what();
-                cudaStreamSynchronize(s);
+                if (slot && slot->stream.s) cudaStreamSynchronize(slot->stream.s);
             }
             r->t_done = now_s(t0_);
             lk.lock();
@@ -383,7 +414,6 @@ class Server {
             cv_work_.notify_all();
         }
         lk.unlock();
-        if (s) cudaStreamDestroy(s);
     }
 
     size_t budget_;
