@@ -474,17 +474,20 @@ void launch(int M, int N, int K, float2 alpha, const float2* A, int lda, const f
     CUtensorMap mB = make_map(B, 2L * K, N, 2L * ldb, 32, BN);
     const int tm = (M2 + kBM - 1) / kBM, tn = (N + BN - 1) / BN;
     const int nk = (K2 + kBK - 1) / kBK;
-    // split K so that whole waves of one CTA per SM (148 SMs) are filled: minimise
-    // waves * stages-per-CTA, with a small charge per split for the reduction traffic
+    // split K so that whole waves of one CTA per SM (148 SMs) are filled.  Cost in microseconds:
+    // waves * stages-per-CTA at about 1 us per CTA stage, plus for sp > 1 the reduction's traffic
+    // (the partial sums written by the GEMM and read back, C read and written: (2 sp + 2) * M * N * 8
+    // bytes at about 6 TB/s) and its launch
     int splits = 1;
     {
         const long tiles = long(tm) * tn;
+        const double mn_us = double(M) * double(N) * 8.0 / 6.0e6;
         double best = 1e300;
         const int smax = nk < 1024 ? nk : 1024;
         for (int sp = 1; sp <= smax; ++sp) {
             const long per_s = (nk + sp - 1) / sp;
             const long waves = (tiles * sp + 147) / 148;
-            const double cost = double(waves) * double(per_s) + (sp > 1 ? 0.05 * sp + 2.0 : 0.0);
+            const double cost = double(waves) * double(per_s) + (sp > 1 ? (2.0 * sp + 2.0) * mn_us + 4.0 : 0.0);
             if (cost < best - 1e-9) {
                 best = cost;
                 splits = sp;
