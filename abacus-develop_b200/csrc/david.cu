@@ -243,6 +243,12 @@ template <typename T> struct Engine {
         work.resize(size_t(lwork > 0 ? lwork : 1));
         eig_h.assign(nbase_x, 0.0);
         unconv_h.assign(nband, 0);
+        if constexpr (kF32) {
+            // tensor-core GEMM workspaces for every subspace product of this engine, so that a solve allocates
+            // nothing: split-K partial tiles of up to 16 splits of the largest C (nband x nbase_x), and B split
+            // once per call for the tall products (K <= nbase_x, N <= nband)
+            tcw.reserve(size_t(16) * 2 * size_t(nband) * nbase_x, size_t(2) * size_t(nbase_x + 1) * nband);
+        }
         B200_CUDA(cudaStreamSynchronize(s));
     }
     // Re-use the buffers for vectors of length d <= dim_cap (another k-point of the same cell) with its
@@ -626,7 +632,7 @@ class David : public DavidBase {
     int notconv_ = 0;
     int verbosity_ = 0;
     cudaStream_t stream_ = 0;
-    double mixed_thr_ = 1e-6;
+    double mixed_thr_ = 1e-7;
     int low_ndim_ = 0;
     DeviceArray<double> pc_;
     DeviceArray<float2> psi32_;

@@ -11,16 +11,19 @@
 // The complex product is done as one real GEMM of size 2M x N x 2K: with
 // interleaved (re, im) storage B is already the real 2K x N matrix, and op(A)
 // becomes the real 2M x 2K matrix whose 2x2 blocks are [[ar, -ai], [ai, ar]]
-// (for A^H: [[ar, ai], [-ai, ar]]).  Those blocks are built in shared memory from
-// the TMA-loaded tile: each 128-byte row of the raw tile (a column of A for "N",
-// MN-major; a row of A^H for "C", K-major) becomes two rows, the row itself and
-// the row multiplied by i (pairs (a, b) -> (-b, a)).  The same pass writes the
-// hi/lo split, so nothing is pre-processed in HBM.
+// (for A^H: [[ar, ai], [-ai, ar]]).  That expanded operand lives in tensor memory:
+// the TMA-loaded raw tile of A (a column of A per 128-byte row for "N", MN-major; a
+// row of A^H for "C", K-major) is read from shared memory by the epilogue warps, one
+// real row of op(A) per thread, split into hi/lo and written to TMEM with tcgen05.st,
+// and tcgen05.mma reads A from TMEM and only B from shared memory.  B is split in
+// shared memory (hi in place, lo beside it), or, when many M tiles read it, once per
+// call in HBM (k_split_b) so that the CTAs only copy it.
 //
 // CTA: 10 warps.  warp 0 issues TMA loads (cp.async.bulk.tensor, no multicast),
-// warp 1 allocates TMEM and one lane issues tcgen05.mma, warps 2-9 split/expand
-// the tiles, drain TMEM and run the epilogue (alpha/beta -> global).
-// 3-stage mbarrier pipeline, two TMEM accumulators.  Every wait is bounded in time; a wait that runs out
+// warp 1 allocates TMEM (512 columns: two accumulators + one expanded A tile per
+// stage) and one lane issues tcgen05.mma, warps 2-9 split/expand the tiles, drain
+// TMEM and run the epilogue (alpha/beta -> global).
+// 4-stage mbarrier pipeline, two TMEM accumulators.  Every wait is bounded in time; a wait that runs out
 // sets an error word, the CTA drains its own copies in flight, frees TMEM and
 // returns.  Long K is split across CTAs (grid.z) with a deterministic reduction.
 #include <cuda.h>
@@ -36,7 +39,7 @@ namespace {
 
 constexpr int kBM = 128;     // real rows of C per tile
 constexpr int kBK = 32;      // real K per stage (one 128-byte swizzle row of fp32)
-constexpr int kStages = 3;
+constexpr int kStages = 4;
 constexpr int kThreads = 320;   // warp 0 TMA, warp 1 MMA, warps 2-9 split / drain / store
 constexpr unsigned long long kWaitNs = 2000000000ull;  // 2 s bound on any single wait
 
@@ -87,9 +90,8 @@ __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.a
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
-// Shared-memory matrix descriptor (Blackwell version 1).  layout: 2 = SWIZZLE_128B (16-byte chunks XOR the
-// row within 8-row / 1024-byte atoms), 1 = SWIZZLE_128B_BASE32B (32-byte chunks XOR the row within 4-row /
-// 512-byte atoms, the only layout for MN-major TF32 operands).
+// Shared-memory matrix descriptor (Blackwell version 1).  layout 2 = SWIZZLE_128B (16-byte chunks XOR the
+// row within 8-row / 1024-byte atoms).
 __device__ __forceinline__ unsigned long long sdesc(unsigned addr, unsigned lbo, unsigned sbo, unsigned layout) {
     unsigned long long d = 0;
     d |= (unsigned long long)((addr >> 4) & 0x3FFF);
@@ -99,13 +101,14 @@ __device__ __forceinline__ unsigned long long sdesc(unsigned addr, unsigned lbo,
     d |= (unsigned long long)(layout & 7) << 61;
     return d;
 }
-__device__ __forceinline__ void mma_tf32(unsigned tmem_d, unsigned long long a, unsigned long long b, unsigned idesc,
-                                         unsigned accumulate) {
+// D (TMEM) (+)= A (TMEM: M = 128 rows in lanes 0..127, one column per K element) * B (shared-memory descriptor)
+__device__ __forceinline__ void mma_tf32_ta(unsigned tmem_d, unsigned tmem_a, unsigned long long b, unsigned idesc,
+                                            unsigned accumulate) {
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
         "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(tmem_d),
-        "l"(a), "l"(b), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(tmem_d),
+        "r"(tmem_a), "l"(b), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
 }
 __device__ __forceinline__ void mma_commit(unsigned bar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
@@ -124,39 +127,55 @@ __device__ __forceinline__ void tmem_ld16(unsigned taddr, float* v) {
     for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+// 16 consecutive TMEM columns of this thread's lane (warp w may access lanes 32 (w % 4) .. +31)
+__device__ __forceinline__ void tmem_st16(unsigned taddr, const float* v) {
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16};" ::
+            "r"(taddr),
+        "r"(__float_as_uint(v[0])), "r"(__float_as_uint(v[1])), "r"(__float_as_uint(v[2])), "r"(__float_as_uint(v[3])),
+        "r"(__float_as_uint(v[4])), "r"(__float_as_uint(v[5])), "r"(__float_as_uint(v[6])), "r"(__float_as_uint(v[7])),
+        "r"(__float_as_uint(v[8])), "r"(__float_as_uint(v[9])), "r"(__float_as_uint(v[10])), "r"(__float_as_uint(v[11])),
+        "r"(__float_as_uint(v[12])), "r"(__float_as_uint(v[13])), "r"(__float_as_uint(v[14])), "r"(__float_as_uint(v[15]))
+        : "memory");
+}
+__device__ __forceinline__ void tmem_st_wait() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
+
 // hi part of the split: x rounded to the nearest TF32 value (10 explicit mantissa bits); lo = x - hi is exact
-__device__ __forceinline__ float tf32_trunc(float x) {
+__device__ __forceinline__ float tf32_round(float x) {
     return __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xFFFFE000u);
 }
 // physical byte offset of (row, 16-byte chunk) in a 1024-byte-aligned SW128 tile with 128-byte rows
 __device__ __forceinline__ unsigned sw128(unsigned row, unsigned chunk) {
     return row * 128u + ((chunk ^ (row & 7u)) << 4);
 }
-// the same for the SW128_BASE32B pattern: 32-byte chunks XOR (row mod 4)
-__device__ __forceinline__ unsigned sw128_32b(unsigned row, unsigned chunk) {
-    return row * 128u + ((((chunk >> 1) ^ (row & 3u)) << 5) | ((chunk & 1u) << 4));
-}
-
+// per stage in shared memory: the raw A tile, then B (rounded hi in place, or the pre-split hi), then B lo
 template <int BN> struct TileBytes {
-    static constexpr int a_raw = 8192;             // 64 rows x 128 B ("C")  or 4 x 16 x 128 B ("N")
-    static constexpr int a_exp = kBM * 128;        // 16 KB
+    static constexpr int a_raw = 8192;   // 64 rows x 128 B ("C")  or 4 x 16 x 128 B ("N")
     static constexpr int b = BN * 128;
-    static constexpr int stage = a_raw + 2 * a_exp + 2 * b;
-    static constexpr int total = kStages * stage + 2048;  // + barriers / flags + 1024-byte alignment slack
+    static constexpr int stage = a_raw + 2 * b;
+    static constexpr int need = kStages * stage + 2048;  // + barriers / flags + 1024-byte alignment slack
+    // at least 120 KB, so that one CTA holds an SM and its 512 TMEM columns
+    static constexpr int total = need > 120 * 1024 ? need : 120 * 1024;
 };
 
+// TMEM columns: two accumulators [0, 2 BN), then per stage s the expanded A tile at 2 BN + 64 s: hi in
+// columns [0, 32), lo in [32, 64) (one column per real K, one lane per real row of C)
+template <int BN> constexpr unsigned a_col(int s) { return unsigned(2 * BN + 64 * s); }
+static_assert(2 * 128 + 64 * kStages <= 512, "TMEM columns");
+
 // OPA: 0 = "N" (A column-major M x K, MN-major tiles), 1 = "C" (A^H of a column-major K x M, K-major tiles)
+// PRE: B arrives already split (hi and lo tiles from HBM, written once per call by k_split_b)
 //
 // Accumulation: the tensor-core accumulator truncates on every accumulate, so a long
 // chain of MMAs into one TMEM accumulator drifts (about 2e-8 relative per MMA).  Each
 // K stage therefore starts a fresh accumulator in one of two TMEM buffers; the
 // epilogue warps drain the finished buffer into FP32 registers (IEEE round-to-nearest
 // adds) while the next stage runs in the other buffer.
-template <int BN, int OPA>
+template <int BN, int OPA, int PRE>
 __global__ void __launch_bounds__(kThreads, 1)
-    k_tc_cgemm(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB, int M2, int N, int K2,
-               int kstages_per_split, float2 alpha, float2 beta, float* __restrict__ C, long ldc2,
-               float* __restrict__ ws, int* __restrict__ err) {
+    k_tc_cgemm(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
+               const __grid_constant__ CUtensorMap mapBl, int M2, int N, int K2, int kstages_per_split, float2 alpha,
+               float2 beta, float* __restrict__ C, long ldc2, float* __restrict__ ws, int* __restrict__ err) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     using TB = TileBytes<BN>;
     // 1024-byte alignment of the tile area (the swizzle pattern depends on address bits 7..9)
@@ -192,7 +211,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
     if (warp == 1) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
-                     "r"(unsigned(2 * BN)));
+                     "r"(512u));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     tc_fence_before();
@@ -217,7 +236,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                 }
                 unsigned char* st = base + s * TB::stage;
                 const unsigned fb = smem_u32(&full[s]);
-                mbar_expect_tx(fb, unsigned(TB::a_raw + TB::b));
+                mbar_expect_tx(fb, unsigned(TB::a_raw + (PRE ? 2 : 1) * TB::b));
                 const int kr = (k_begin + i) * kBK;  // real K offset
                 if (OPA == 1) {
                     tma_load_2d(smem_u32(st), &mapA, kr, tile_m * (kBM / 2), fb);
@@ -225,7 +244,8 @@ __global__ void __launch_bounds__(kThreads, 1)
                     for (int b = 0; b < 4; ++b)
                         tma_load_2d(smem_u32(st + b * 2048), &mapA, tile_m * kBM + 32 * b, kr / 2, fb);
                 }
-                tma_load_2d(smem_u32(st + TB::a_raw + 2 * TB::a_exp), &mapB, kr, tile_n * BN, fb);
+                tma_load_2d(smem_u32(st + TB::a_raw), &mapB, kr, tile_n * BN, fb);
+                if (PRE) tma_load_2d(smem_u32(st + TB::a_raw + TB::b), &mapBl, kr, tile_n * BN, fb);
                 ++issued;
             }
             // drain: every load this thread issued must land before the CTA exits
@@ -236,9 +256,9 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
     } else if (warp == 1) {
         if (lane == 0) {
-            // MMA issuer: stage i accumulates (fresh) into TMEM buffer i & 1
-            const unsigned idesc = (1u << 4) | (2u << 7) | (2u << 10) | (unsigned(OPA == 0) << 15) |
-                                   (unsigned(BN >> 3) << 17) | (unsigned(kBM >> 4) << 24);
+            // MMA issuer: stage i accumulates (fresh) into TMEM buffer i & 1; A from TMEM, B from shared memory
+            const unsigned idesc =
+                (1u << 4) | (2u << 7) | (2u << 10) | (unsigned(BN >> 3) << 17) | (unsigned(kBM >> 4) << 24);
             for (int i = 0; i < nk && !*abort_flag; ++i) {
                 const int s = i % kStages;
                 const int bf = i & 1;
@@ -252,39 +272,37 @@ __global__ void __launch_bounds__(kThreads, 1)
                 }
                 tc_fence_after();
                 unsigned char* st = base + s * TB::stage;
-                const unsigned a_hi = smem_u32(st + TB::a_raw);
-                const unsigned a_lo = a_hi + TB::a_exp;
-                const unsigned b_hi = smem_u32(st + TB::a_raw + 2 * TB::a_exp);
+                const unsigned a_hi = tmem + a_col<BN>(s);
+                const unsigned a_lo = a_hi + 32u;
+                const unsigned b_hi = smem_u32(st + TB::a_raw);
                 const unsigned b_lo = b_hi + TB::b;
                 const unsigned d = tmem + unsigned(bf * BN);
 #pragma unroll
                 for (int kk = 0; kk < kBK / 8; ++kk) {
-                    unsigned long long dah, dal;
-                    if (OPA == 1) {  // K-major SW128: 8-row groups 1024 B apart, K step of 8 = 32 B
-                        dah = sdesc(a_hi + kk * 32, 16, 1024, 2);
-                        dal = sdesc(a_lo + kk * 32, 16, 1024, 2);
-                    } else {  // MN-major SW128_BASE32B: 32-float MN blocks 4 KB apart, 4-row K groups 512 B apart
-                        dah = sdesc(a_hi + kk * 1024, 4096, 512, 1);
-                        dal = sdesc(a_lo + kk * 1024, 4096, 512, 1);
-                    }
                     const unsigned long long dbh = sdesc(b_hi + kk * 32, 16, 1024, 2);
                     const unsigned long long dbl = sdesc(b_lo + kk * 32, 16, 1024, 2);
                     // small terms first, then the leading product
-                    mma_tf32(d, dah, dbl, idesc, kk > 0 ? 1u : 0u);
-                    mma_tf32(d, dal, dbh, idesc, 1u);
-                    mma_tf32(d, dah, dbh, idesc, 1u);
+                    mma_tf32_ta(d, a_hi + kk * 8, dbl, idesc, kk > 0 ? 1u : 0u);
+                    mma_tf32_ta(d, a_lo + kk * 8, dbh, idesc, 1u);
+                    mma_tf32_ta(d, a_hi + kk * 8, dbh, idesc, 1u);
                 }
                 mma_commit(smem_u32(&empty[s]));
                 mma_commit(smem_u32(&acc_full[bf]));
             }
         }
     } else {
-        // warps 2..9: split / expand stage i, drain stage i-1, finally store.  TMEM lane quarter
-        // q = warp % 4 (the lanes this warp may access); warps 2-5 own columns [0, BN/2), warps 6-9 [BN/2, BN)
+        // warps 2..9: expand + split stage i's A into TMEM (and split B in shared memory unless PRE), drain
+        // stage i-1, finally store.  TMEM lane quarter q = warp % 4 (the lanes this warp may access); warps
+        // 2-5 handle real K [0, 16) of a stage's A and columns [0, BN/2) of C, warps 6-9 K [16, 32) and
+        // columns [BN/2, BN)
         constexpr int HB = BN / 2;
         const int t = threadIdx.x - 64;  // 0..255
         const int q = warp & 3;
-        const int col0 = (warp >= 6) ? HB : 0;
+        const int g = (warp >= 6) ? 1 : 0;
+        const int col0 = g * HB;
+        const int rr = 32 * q + lane;        // real row of the tile = TMEM lane
+        const int m = rr >> 1;               // complex row of op(A) within the tile
+        const bool odd = (rr & 1) != 0;
         float acc[HB];
 #pragma unroll
         for (int j = 0; j < HB; ++j) acc[j] = 0.f;
@@ -314,44 +332,59 @@ __global__ void __launch_bounds__(kThreads, 1)
                 fail(4);
                 break;
             }
+            // the MMAs that last read this stage's TMEM columns have completed (they released the stage
+            // before its refill landed)
+            tc_fence_after();
             unsigned char* st = base + s * TB::stage;
-            unsigned char* araw = st;
-            unsigned char* ahi = st + TB::a_raw;
-            unsigned char* alo = ahi + TB::a_exp;
-            unsigned char* bhi = ahi + 2 * TB::a_exp;
-            unsigned char* blo = bhi + TB::b;
-            // A: 512 raw 16-byte chunks -> 2 expanded rows each (hi and lo)
-            for (int qq = t; qq < 512; qq += 256) {
-                unsigned src, d0, d1;
-                if (OPA == 1) {
-                    const unsigned r = qq >> 3, c = qq & 7;  // raw row r (one complex row of A^H), chunk c
-                    src = sw128(r, c);
-                    d0 = sw128(2 * r, c);
-                    d1 = sw128(2 * r + 1, c);
-                } else {
-                    const unsigned b = qq >> 7, k = (qq >> 3) & 15, c = qq & 7;  // MN block b, raw K-row k
-                    src = b * 2048 + sw128(k, c);
-                    d0 = b * 4096 + sw128_32b(2 * k, c);
-                    d1 = b * 4096 + sw128_32b(2 * k + 1, c);
+            const unsigned char* araw = st;
+            // A: this thread's real row of op(A) over its 16 real K of the stage.  Blocks of the real
+            // form: "N" [[ar, -ai], [ai, ar]], "C" [[ar, ai], [-ai, ar]]; an even real row takes the first
+            // row of each block, an odd one the second
+            float v[16];
+            if (OPA == 1) {
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {  // raw row m, 16-byte chunks 4g..4g+3 (two complex each)
+                    const float4 x = *reinterpret_cast<const float4*>(araw + sw128(unsigned(m), unsigned(4 * g + j)));
+                    v[4 * j + 0] = odd ? -x.y : x.x;
+                    v[4 * j + 1] = odd ? x.x : x.y;
+                    v[4 * j + 2] = odd ? -x.w : x.z;
+                    v[4 * j + 3] = odd ? x.z : x.w;
                 }
-                const float4 x = *reinterpret_cast<const float4*>(araw + src);
-                const float4 h = make_float4(tf32_trunc(x.x), tf32_trunc(x.y), tf32_trunc(x.z), tf32_trunc(x.w));
-                const float4 l = make_float4(x.x - h.x, x.y - h.y, x.z - h.z, x.w - h.w);
-                *reinterpret_cast<float4*>(ahi + d0) = h;
-                *reinterpret_cast<float4*>(alo + d0) = l;
-                // times i: (a, b) -> (-b, a)
-                *reinterpret_cast<float4*>(ahi + d1) = make_float4(-h.y, h.x, -h.w, h.z);
-                *reinterpret_cast<float4*>(alo + d1) = make_float4(-l.y, l.x, -l.w, l.z);
+            } else {
+                const int ml = m & 15;  // within MN block q (16 complex rows)
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {  // raw K-rows 8g..8g+7
+                    const float2 x = *reinterpret_cast<const float2*>(
+                        araw + q * 2048 + sw128(unsigned(8 * g + j), unsigned(ml >> 1)) + (ml & 1) * 8);
+                    v[2 * j + 0] = odd ? x.y : x.x;
+                    v[2 * j + 1] = odd ? x.x : -x.y;
+                }
             }
-            // B: in-place hi, lo beside it (same layout)
-            for (int qq = t; qq < BN * 8; qq += 256) {
-                float4* p = reinterpret_cast<float4*>(bhi + qq * 16);
-                const float4 x = *p;
-                const float4 h = make_float4(tf32_trunc(x.x), tf32_trunc(x.y), tf32_trunc(x.z), tf32_trunc(x.w));
-                *p = h;
-                *reinterpret_cast<float4*>(blo + qq * 16) = make_float4(x.x - h.x, x.y - h.y, x.z - h.z, x.w - h.w);
+            float lo[16];
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+                const float h = tf32_round(v[j]);
+                lo[j] = v[j] - h;
+                v[j] = h;
             }
-            fence_async_smem();
+            const unsigned tal = tmem + (unsigned(32 * q) << 16) + a_col<BN>(s) + unsigned(16 * g);
+            tmem_st16(tal, v);
+            tmem_st16(tal + 32u, lo);
+            if (!PRE) {
+                // B: in-place hi, lo beside it (same layout)
+                unsigned char* bhi = st + TB::a_raw;
+                unsigned char* blo = bhi + TB::b;
+                for (int qq = t; qq < BN * 8; qq += 256) {
+                    float4* p = reinterpret_cast<float4*>(bhi + qq * 16);
+                    const float4 x = *p;
+                    const float4 h = make_float4(tf32_round(x.x), tf32_round(x.y), tf32_round(x.z), tf32_round(x.w));
+                    *p = h;
+                    *reinterpret_cast<float4*>(blo + qq * 16) = make_float4(x.x - h.x, x.y - h.y, x.z - h.z, x.w - h.w);
+                }
+                fence_async_smem();
+            }
+            tmem_st_wait();
+            tc_fence_before();
             mbar_arrive(smem_u32(&ready[s]));
             if (i > 0) drain(i - 1);
             if (!ok) break;
@@ -360,9 +393,9 @@ __global__ void __launch_bounds__(kThreads, 1)
         // store (warp-uniform: the shuffles are collective)
         const bool go = __all_sync(0xffffffffu, ok && !*abort_flag && nk > 0);
         if (go) {
-            const int row = tile_m * kBM + 32 * q + lane;  // real row of C
+            const int row = tile_m * kBM + rr;  // real row of C
             const bool row_ok = row < M2;
-            const bool im = row & 1;
+            const bool im = odd;
             const bool use_beta = (beta.x != 0.f || beta.y != 0.f);
             if (ws) {
 #pragma unroll
@@ -400,7 +433,20 @@ __global__ void __launch_bounds__(kThreads, 1)
     __syncthreads();
     if (warp == 1) {
         tc_fence_after();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(unsigned(2 * BN)));
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512u));
+    }
+}
+
+// B (K x N complex, pitch ldb) -> hi = tf32 rounding, lo = B - hi, both with pitch ldh (even)
+__global__ void k_split_b(int K, int N, const float2* __restrict__ B, long ldb, float2* __restrict__ hi,
+                          float2* __restrict__ lo, long ldh) {
+    const long total = long(K) * N;
+    for (long t = blockIdx.x * long(blockDim.x) + threadIdx.x; t < total; t += long(gridDim.x) * blockDim.x) {
+        const long n = t / K, k = t - n * K;
+        const float2 x = B[n * ldb + k];
+        const float2 h = make_float2(tf32_round(x.x), tf32_round(x.y));
+        hi[n * ldh + k] = h;
+        lo[n * ldh + k] = make_float2(x.x - h.x, x.y - h.y);
     }
 }
 
@@ -457,10 +503,10 @@ CUtensorMap make_map(const void* base, long inner, long outer, long pitch_floats
     return m;
 }
 
-template <int BN, int OPA> void set_attr_once() {
+template <int BN, int OPA, int PRE> void set_attr_once() {
     static std::once_flag once;
     std::call_once(once, [] {
-        B200_CUDA(cudaFuncSetAttribute(k_tc_cgemm<BN, OPA>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        B200_CUDA(cudaFuncSetAttribute(k_tc_cgemm<BN, OPA, PRE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        TileBytes<BN>::total));
     });
 }
@@ -471,8 +517,28 @@ void launch(int M, int N, int K, float2 alpha, const float2* A, int lda, const f
     const int M2 = 2 * M, K2 = 2 * K;
     CUtensorMap mA = (OPA == 1) ? make_map(A, 2L * K, M, 2L * lda, 32, 64)   // rows of A^H = columns of A
                                 : make_map(A, 2L * M, K, 2L * lda, 32, 16);  // columns of A, MN-major
-    CUtensorMap mB = make_map(B, 2L * K, N, 2L * ldb, 32, BN);
     const int tm = (M2 + kBM - 1) / kBM, tn = (N + BN - 1) / BN;
+    // when many M tiles read B (tall op(A): the H|psi> and subspace updates), B is split into hi / lo once
+    // here and the CTAs only copy it; otherwise every CTA splits its B tiles in shared memory
+    const bool pre = tm >= 16;
+    CUtensorMap mB, mBl;
+    if (pre) {
+        const long ldh = long(K) + (K & 1);  // even: 16-byte row pitch
+        w.bsplit.resize(size_t(2) * size_t(ldh) * N);
+        float2* hi = w.bsplit.ptr;
+        float2* lo = hi + size_t(ldh) * N;
+        const long total = long(K) * N;
+        int blocks = int((total + 255) / 256);
+        if (blocks > 148 * 8) blocks = 148 * 8;
+        k_split_b<<<blocks, 256, 0, s>>>(K, N, B, ldb, hi, lo, ldh);
+        note_launch();
+        B200_CUDA(cudaGetLastError());
+        mB = make_map(hi, 2L * K, N, 2L * ldh, 32, BN);
+        mBl = make_map(lo, 2L * K, N, 2L * ldh, 32, BN);
+    } else {
+        mB = make_map(B, 2L * K, N, 2L * ldb, 32, BN);
+        mBl = mB;
+    }
     const int nk = (K2 + kBK - 1) / kBK;
     // split K so that whole waves of one CTA per SM (148 SMs) are filled.  Cost in microseconds:
     // waves * stages-per-CTA at about 1 us per CTA stage, plus for sp > 1 the reduction's traffic
@@ -485,6 +551,7 @@ void launch(int M, int N, int K, float2 alpha, const float2* A, int lda, const f
         double best = 1e300;
         const int smax = nk < 1024 ? nk : 1024;
         for (int sp = 1; sp <= smax; ++sp) {
+            if (sp > 1 && w.ws_cap && size_t(sp) * size_t(N) * size_t(M2) > w.ws_cap) break;
             const long per_s = (nk + sp - 1) / sp;
             const long waves = (tiles * sp + 147) / 148;
             const double cost = double(waves) * double(per_s) + (sp > 1 ? (2.0 * sp + 2.0) * mn_us + 4.0 : 0.0);
@@ -501,9 +568,15 @@ void launch(int M, int N, int K, float2 alpha, const float2* A, int lda, const f
         w.ws.resize(size_t(splits) * N * M2);
         ws = w.ws.ptr;
     }
-    set_attr_once<BN, OPA>();
-    k_tc_cgemm<BN, OPA><<<dim3(tm, tn, splits), kThreads, TileBytes<BN>::total, s>>>(
-        mA, mB, M2, N, K2, per, alpha, beta, reinterpret_cast<float*>(C), 2L * ldc, ws, w.err.ptr);
+    if (pre) {
+        set_attr_once<BN, OPA, 1>();
+        k_tc_cgemm<BN, OPA, 1><<<dim3(tm, tn, splits), kThreads, TileBytes<BN>::total, s>>>(
+            mA, mB, mBl, M2, N, K2, per, alpha, beta, reinterpret_cast<float*>(C), 2L * ldc, ws, w.err.ptr);
+    } else {
+        set_attr_once<BN, OPA, 0>();
+        k_tc_cgemm<BN, OPA, 0><<<dim3(tm, tn, splits), kThreads, TileBytes<BN>::total, s>>>(
+            mA, mB, mBl, M2, N, K2, per, alpha, beta, reinterpret_cast<float*>(C), 2L * ldc, ws, w.err.ptr);
+    }
     note_launch();
     B200_CUDA(cudaGetLastError());
     if (splits > 1) {
@@ -523,6 +596,13 @@ void TcGemmWorkspace::ensure() {
         err.resize(1);
         B200_CUDA(cudaMemset(err.ptr, 0, sizeof(int)));
     }
+}
+
+void TcGemmWorkspace::reserve(size_t ws_floats, size_t bsplit_elems) {
+    ensure();
+    ws_cap = ws_floats;
+    ws.resize(ws_floats);
+    bsplit.resize(bsplit_elems);
 }
 
 int TcGemmWorkspace::read_error(cudaStream_t s) {

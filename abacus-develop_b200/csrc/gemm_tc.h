@@ -8,10 +8,15 @@ namespace b200 {
 
 struct TcGemmWorkspace {
     DeviceArray<float> ws;  // split-K partial tiles
+    DeviceArray<float2> bsplit;  // hi / lo halves of a B split once per call
     DeviceArray<int> err;   // nonzero after a bounded wait ran out inside the kernel
+    size_t ws_cap = 0;      // floats; nonzero: split-K counts whose partial tiles exceed it are not used
     void ensure();
+    // allocate up front (no allocation inside later calls whose workspace fits): split-K partial tiles of
+    // at most ws_floats (also the cap), and a pre-split B of up to bsplit_elems complex values
+    void reserve(size_t ws_floats, size_t bsplit_elems);
     int read_error(cudaStream_t s = 0);  // read of the error word after the work queued on s
-    size_t device_bytes() const { return ws.n * sizeof(float) + err.n * sizeof(int); }
+    size_t device_bytes() const { return ws.n * sizeof(float) + bsplit.n * sizeof(float2) + err.n * sizeof(int); }
 };
 
 // C (M x N) = alpha * op(A) * B + beta * C, complex64, column-major, op(A) in {'N', 'C'}.

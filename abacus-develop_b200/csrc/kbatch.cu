@@ -152,6 +152,16 @@ int b200_solve_kpoints(b200_hamilt* h, int nk, const int* iks, int spin, int nba
         b200::Hamilt* H = h->h.get();
         int dev = 0;
         B200_CUDA(cudaGetDevice(&dev));
+        // one solver per worker, sized for the largest k-point and re-targeted to each k-point in turn: a solver
+        // made and destroyed per k-point would allocate inside the loop, and its cudaFree would synchronise the
+        // device under the other workers' solves
+        int q_max = 0;
+        for (int q = 0; q < nk; ++q) {
+            B200_CHECK(iks[q] >= 0 && iks[q] < int(H->grid->kmaps.size()), b200::kInvalidArgument,
+                       "k-point index out of range");
+            if (H->grid->kmaps[iks[q]].npw > H->grid->kmaps[iks[q_max]].npw) q_max = q;
+        }
+        const int dim_max = H->grid->kmaps[iks[q_max]].npw;
         std::atomic<int> next{0};
         std::mutex err_mu;
         std::exception_ptr first_err;
@@ -161,15 +171,16 @@ int b200_solve_kpoints(b200_hamilt* h, int nk, const int* iks, int spin, int nba
                 cudaStream_t s = nullptr;
                 B200_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
                 auto work = std::make_unique<b200::HpsiWork>();
+                auto d = b200::make_david(nband, dim_max, david_ndim, precision, precond_d[q_max]);
+                d->set_stream(s);
                 for (int q = next.fetch_add(1); q < nk; q = next.fetch_add(1)) {
                     {
                         std::lock_guard<std::mutex> lk(err_mu);
                         if (first_err) break;
                     }
                     const int ik = iks[q];
-                    const int dim = H->grid->kmaps.at(ik).npw;
-                    auto d = b200::make_david(nband, dim, david_ndim, precision, precond_d[q]);
-                    d->set_stream(s);
+                    const int dim = H->grid->kmaps[ik].npw;
+                    d->retarget(dim, precond_d[q]);
                     b200::HpsiWork* W = work.get();
                     b200::HPsiDevice f64 = [H, W, ik, spin](const void* x, void* hx, int, int ld, int i0, int i1,
                                                             cudaStream_t st) {
@@ -186,6 +197,8 @@ int b200_solve_kpoints(b200_hamilt* h, int nk, const int* iks, int spin, int nba
                     if (iters) iters[q] = it;
                 }
                 B200_CUDA(cudaStreamSynchronize(s));
+                d.reset();
+                work.reset();
                 cudaStreamDestroy(s);
             } catch (...) {
                 std::lock_guard<std::mutex> lk(err_mu);

@@ -239,7 +239,9 @@ class Server {
                    (2 * nbx * nbx + 3 * size_t(nb + 1) * (nb + 1)) * 16 + (size_t(8) << 20);
         };
         size_t b = engine(16, d) + size_t(nb) * c.npwx * 16;
-        if (precision == B200_PREC_MIXED) b += engine(8, d32) + size_t(nb) * c.npwx * 8;
+        // the FP32 engine also reserves its tensor-core GEMM workspaces (split-K tiles, pre-split B)
+        if (precision == B200_PREC_MIXED)
+            b += engine(8, d32) + size_t(nb) * c.npwx * 8 + size_t(16) * 2 * nb * nbx * 4 + 2 * (nbx + 1) * nb * 8;
         const PWGrid& g = *c.h->h->grid;
         const size_t per_band = size_t(g.nst) * g.nz * 16;
         b += std::max(per_band, std::min(per_band * nb, size_t(48) << 20)) + per_band;

@@ -292,7 +292,7 @@ int b200_david_set_stream(b200_david* d, void* stream);
  * 0 = quiet, 1 = one line per iteration on stderr. */
 int b200_david_set_verbosity(b200_david* d, int level);
 /* Mixed precision only: eigenvalue-change threshold at which the FP32 stage hands over to the
- * FP64 refinement (default 1e-6 Ry; never below the requested thr). */
+ * FP64 refinement (default 1e-7 Ry; never below the requested thr). */
 int b200_david_set_mixed_threshold(b200_david* d, double thr);
 /* Statistics of the last solve: Davidson iterations in the FP32 stage (mixed only), in FP64,
  * and the number of single-band H applications (all stages). */

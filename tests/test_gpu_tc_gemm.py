@@ -21,6 +21,9 @@ CASES = [
     ("C", 512, 160, 51626, 2, 1.0, 0.0),
     ("C", 33, 17, 129, 1, 1.0j, -1.0),
     ("N", 1, 1, 1, 1, 1.0, 0.0),
+    # many M tiles: B split once in HBM ("C" and "N", odd K, ragged N)
+    ("C", 1100, 90, 3001, 2, 1.0 - 1.0j, 0.5j),
+    ("N", 2100, 33, 77, 1, -0.5, 1.0 + 1.0j),
 ]
 
 
