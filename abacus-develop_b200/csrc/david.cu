@@ -566,7 +566,10 @@ class David : public DavidBase {
                 e32_->set_stream(stream_);
                 e32_->retarget(dim_, pc_.ptr);
             }
-            e32_->ref_refresh = e64_->ref_refresh;
+            // the FP32 stage is not the reference's iteration, so its restarts start from the exact Ritz
+            // basis (vcc = I); keeping the reference's stale off-diagonal vcc entries there makes the first
+            // residuals after each restart those of mixed vectors and costs iterations
+            e32_->ref_refresh = false;
             e32_->trace = &trace_;
             e32_->verbosity = verbosity_;
             e32_->hpsi_bands = 0;
@@ -622,10 +625,9 @@ class David : public DavidBase {
         if (e32_) b += e32_->device_bytes();
         return b;
     }
-    void set_reference_refresh(bool on) override {
-        e64_->ref_refresh = on;
-        if (e32_) e32_->ref_refresh = on;
-    }
+    // the reference's refresh (stale off-diagonal vcc entries) for the FP64 iteration; the FP32 stage of a
+    // mixed solve always restarts cleanly
+    void set_reference_refresh(bool on) override { e64_->ref_refresh = on; }
 
   private:
     int nband_, dim_, cap_, ndim_, precision_;
