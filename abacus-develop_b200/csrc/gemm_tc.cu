@@ -190,7 +190,10 @@ __global__ void __launch_bounds__(kThreads, 1)
     volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int tile_m = blockIdx.x, tile_n = blockIdx.y, split = blockIdx.z;
+    // "N": the N tile is the fastest grid index, so the few CTAs that read one A tile run together and
+    // A crosses HBM once; "C": the M tile is, for the same reason with B
+    const int tile_m = OPA == 0 ? blockIdx.y : blockIdx.x, tile_n = OPA == 0 ? blockIdx.x : blockIdx.y;
+    const int split = blockIdx.z;
     const int nk_total = (K2 + kBK - 1) / kBK;
     const int k_begin = split * kstages_per_split;
     const int k_end = min(nk_total, k_begin + kstages_per_split);
@@ -568,13 +571,15 @@ void launch(int M, int N, int K, float2 alpha, const float2* A, int lda, const f
         w.ws.resize(size_t(splits) * N * M2);
         ws = w.ws.ptr;
     }
+    B200_CHECK((OPA == 0 ? tm : tn) <= 65535, kInvalidArgument, "tc_cgemm: too many tiles for the grid");
+    const dim3 grid = OPA == 0 ? dim3(tn, tm, splits) : dim3(tm, tn, splits);
     if (pre) {
         set_attr_once<BN, OPA, 1>();
-        k_tc_cgemm<BN, OPA, 1><<<dim3(tm, tn, splits), kThreads, TileBytes<BN>::total, s>>>(
+        k_tc_cgemm<BN, OPA, 1><<<grid, kThreads, TileBytes<BN>::total, s>>>(
             mA, mB, mBl, M2, N, K2, per, alpha, beta, reinterpret_cast<float*>(C), 2L * ldc, ws, w.err.ptr);
     } else {
         set_attr_once<BN, OPA, 0>();
-        k_tc_cgemm<BN, OPA, 0><<<dim3(tm, tn, splits), kThreads, TileBytes<BN>::total, s>>>(
+        k_tc_cgemm<BN, OPA, 0><<<grid, kThreads, TileBytes<BN>::total, s>>>(
             mA, mB, mBl, M2, N, K2, per, alpha, beta, reinterpret_cast<float*>(C), 2L * ldc, ws, w.err.ptr);
     }
     note_launch();

@@ -349,6 +349,7 @@ def run_ours(args, ws, rank, local):
     }
 
     line["psi_to_rho"] = rho_bench(P, wl, psi, args.steps, stream)
+    line["tc_gemm"] = gemm_bench(P)
     if not args.skip_david:
         line["davidson"] = davidson_bench(P, wl, h64)
     del h32, psi32, hpsi32
@@ -564,6 +565,42 @@ def davidson_216(pkg):
     return out
 
 
+# complex64 3xTF32 tensor-core GEMM shapes: the subspace products of the 216-atom Davidson (dim 124289,
+# nband 480, subspace up to 1920) and the projector products of the 64-atom H|psi> (512 projectors, npw
+# 51627, 160 bands)
+GEMM_SHAPES = [("N", 124289, 480, 1300), ("N", 124289, 480, 480), ("C", 480, 1920, 124289),
+               ("C", 1920, 480, 124289), ("C", 480, 480, 124289), ("N", 51627, 160, 512), ("C", 512, 160, 51627)]
+
+
+def gemm_bench(P, reps=5):
+    """tc_cgemm (gemm_op<complex<float>, GPU> on tcgen05) on the shapes above: CUDA-event time per call and
+    complex-equivalent TFLOP/s (8 M N K flop per call)."""
+    import torch
+    out = []
+    for ta, M, N, K in GEMM_SHAPES:
+        rows_a, cols_a = (M, K) if ta == "N" else (K, M)
+        lda, ldb = rows_a + rows_a % 2, K + K % 2
+        g = torch.Generator(device="cuda").manual_seed(7)
+        a = torch.randn(cols_a, lda, dtype=torch.complex64, device="cuda", generator=g)
+        b = torch.randn(N, ldb, dtype=torch.complex64, device="cuda", generator=g)
+        c = torch.zeros(N, M, dtype=torch.complex64, device="cuda")
+        for _ in range(3):
+            P.tc_cgemm(ta, M, N, K, 1.0, a, lda, b, ldb, 0.0, c, M)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            P.tc_cgemm(ta, M, N, K, 1.0, a, lda, b, ldb, 0.0, c, M)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        out.append({"op": ta, "M": M, "N": N, "K": K, "ms": ms, "tflops": 8.0 * M * N * K / (ms * 1e-3) / 1e12})
+        del a, b, c
+        torch.cuda.empty_cache()
+    assert P.tc_cgemm_error() == 0
+    return out
+
+
 def kbatch_bench(pkg, steps):
     """8-atom cell, shifted 4x4x4 Monkhorst-Pack grid (64 k-points, uneven npw), 32 bands: H|psi> of all
     k-points per call (one launch per FFT pass), per-k-point calls, CUDA-graph replay; concurrent Davidson
@@ -660,7 +697,12 @@ def main():
     ap.add_argument("--skip-serve", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=10.0)
+    ap.add_argument("--gemm-only", action="store_true", help="only the tensor-core GEMM shapes (for profiling)")
     args = ap.parse_args()
+    if args.gemm_only:
+        pkg = load_package()
+        print(json.dumps({"tc_gemm": gemm_bench(pkg.pwdft, reps=1)}), flush=True)
+        return
     if args.impl == "reference":
         rank = int(os.environ.get("RANK", "0"))
         run_reference(args, int(os.environ.get("WORLD_SIZE", "1")), rank)
