@@ -60,6 +60,7 @@ _SIGS = {
     "b200_hamilt_set_deeq": ([vp, i32, pi32, pi32, i32, i32, i32, i32, vp], i32),
     "b200_hamilt_hpsi": ([vp, i32, i32, i32, i32, vp, vp, vp], i32),
     "b200_hamilt_hpsi_part": ([vp, i32, i32, i32, i32, vp, vp, i32, vp], i32),
+    "b200_hamilt_hpsi_host": ([vp, i32, i32, i32, i32, vp, vp, vp, vp, i32, vp], i32),
     "b200_hamilt_hpsi_local_noalloc": ([vp, i32, i32, i32, vp, vp, vp], i32),
     "b200_hamilt_hpsi_kbatch": ([vp, i32, pi32, i32, i32, i32, C.POINTER(vp), C.POINTER(vp), vp], i32),
     "b200_graph_capture_hpsi_kbatch": ([vp, i32, pi32, i32, i32, i32, C.POINTER(vp), C.POINTER(vp), vp,

@@ -1,6 +1,7 @@
 // Definitions of the opaque C-ABI handles (shared by the C-ABI translation units).
 #pragma once
 #include <memory>
+#include <vector>
 
 #include "david.h"
 #include "hamilt.h"
@@ -13,8 +14,19 @@ struct b200_pw_basis {
     b200::DeviceArray<double2> rho_box64;  // psi(r) of one band (psi -> rho)
     b200::DeviceArray<float2> rho_box32;
 };
+// copy streams and events of b200_hamilt_hpsi_host, made at its first use and kept with the handle
+struct HostPipe {
+    cudaStream_t up = nullptr, down = nullptr;
+    std::vector<cudaEvent_t> ev;
+    ~HostPipe() {
+        for (cudaEvent_t e : ev) cudaEventDestroy(e);
+        if (up) cudaStreamDestroy(up);
+        if (down) cudaStreamDestroy(down);
+    }
+};
 struct b200_hamilt {
     std::unique_ptr<b200::Hamilt> h;
+    std::unique_ptr<HostPipe> pipe;
 };
 struct b200_david {
     std::unique_ptr<b200::DavidBase> d;

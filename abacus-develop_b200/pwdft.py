@@ -333,6 +333,19 @@ class HamiltPW:
         self._chk(psi, hpsi, nbands, ld)
         call("b200_hamilt_hpsi", self._h, ik, spin, nbands, ld, ptr(psi), ptr(hpsi), stream_ptr(stream))
 
+    def hpsi_host(self, ik, psi_h, hpsi_h, psi_d, hpsi_d, nbands, ld, pieces=4, spin=0, stream=None):
+        """H|psi> from a host psi_h into a host hpsi_h through the device buffers psi_d / hpsi_d, with the
+        uploads, the H|psi> pieces and the downloads overlapped on three streams (pinned host tensors give
+        the overlap).  Asynchronous: hpsi_h is complete when the stream is."""
+        torch = _torch()
+        self._chk(psi_d, hpsi_d, nbands, ld)
+        want = torch.complex128 if self.precision == PREC_FP64 else torch.complex64
+        for t, what in ((psi_h, "psi_h"), (hpsi_h, "hpsi_h")):
+            if t.dtype != want or t.is_cuda or not t.is_contiguous() or t.numel() < int(nbands) * int(ld):
+                raise ValueError(f"{what}: expected a contiguous host {want} tensor of at least nbands*ld elements")
+        call("b200_hamilt_hpsi_host", self._h, ik, spin, nbands, ld, ptr(psi_h), ptr(hpsi_h), ptr(psi_d),
+             ptr(hpsi_d), int(pieces), stream_ptr(stream))
+
     def hpsi_part(self, ik, psi, hpsi, nbands, ld, mode, spin=0, stream=None):
         self._chk(psi, hpsi, nbands, ld)
         call("b200_hamilt_hpsi_part", self._h, ik, spin, nbands, ld, ptr(psi), ptr(hpsi), mode, stream_ptr(stream))

@@ -43,6 +43,9 @@ ROOT = Path(__file__).resolve().parent
 WORKLOAD_NAME = ("64-atom diamond supercell a=20.52 bohr, ecut 50 Ry, 96^3 grid, npw 51627, "
                  "160 bands, 512 projectors, Gamma")
 METRIC = "H|psi> bands/s (FP64) + Davidson time-to-1e-8 Ry, mixed vs FP64"
+# band pieces of the end-to-end H|psi> pipeline: 5 pieces of 32 bands (about two 48 MB band chunks of the
+# local pass each; 4, 8 or 10 pieces measured 13-19 % slower on B200)
+E2E_PIECES = 5
 # dram__bytes_read.sum + dram__bytes_write.sum of the fused local H|psi> kernels (27 launches: 9 band
 # chunks x 3 passes) for one 160-band FP64 application, from the ncu capture without cache flush summarised
 # in profiles/hpsi_local_diamond64_traffic.md
@@ -293,14 +296,13 @@ def run_ours(args, ws, rank, local):
     ms_loc64 = time_steps(local64, args.steps, stream)
     ms_loc32 = time_steps(local32, args.steps, stream)
 
-    # end to end through the public API: pinned host psi -> device, H|psi>, hpsi -> pinned host
+    # end to end through the public API: pinned host psi -> H|psi> -> pinned host hpsi, every step; the
+    # uploads, H|psi> pieces and downloads overlap on three streams (b200_hamilt_hpsi_host)
     psi_pin = torch.from_numpy(psi_h).pin_memory()
     out_pin = torch.empty_like(psi_pin).pin_memory()
 
     def e2e_step():
-        psi.copy_(psi_pin, non_blocking=True)
-        step64()
-        out_pin.copy_(hpsi, non_blocking=True)
+        h64.hpsi_host(0, psi_pin, out_pin, psi, hpsi, nb, ld, pieces=E2E_PIECES)
 
     for _ in range(2):
         e2e_step()

@@ -154,6 +154,15 @@ int b200_hamilt_set_deeq(b200_hamilt* h, int ntype, const int* na, const int* nh
  * spin selects the deeq spin channel (isk[ik]). */
 int b200_hamilt_hpsi(b200_hamilt* h, int ik, int spin, int nbands, int ld, const void* psi_d, void* hpsi_d,
                      void* stream);
+/* H|psi> between host buffers (psi_h in, hpsi_h out, band b at b*ld, the handle's element type), through
+ * the caller's device buffers psi_d / hpsi_d (nbands*ld each): the bands go in npieces pieces through
+ * three streams so that the upload of piece p+1, H|psi> of piece p and the download of piece p-1 overlap.
+ * Asynchronous: hpsi_h is complete when `stream` is.  Pinned (page-locked) host buffers give the overlap;
+ * pageable ones work with synchronous copies.  The handle's copy streams are shared: one call at a time
+ * per handle.  No counterpart in the reference (its Operator::hPsi works on device memory,
+ * module_hamilt_general/operator.cpp:39-88; the host <-> device copies are the caller's). */
+int b200_hamilt_hpsi_host(b200_hamilt* h, int ik, int spin, int nbands, int ld, const void* psi_h, void* hpsi_h,
+                          void* psi_d, void* hpsi_d, int npieces, void* stream);
 /* Parts of H|psi>, for checking and for callers that compose their own chain:
  * mode 1 = kinetic + local only, mode 2 = nonlocal only (accumulated into hpsi_d). */
 int b200_hamilt_hpsi_part(b200_hamilt* h, int ik, int spin, int nbands, int ld, const void* psi_d, void* hpsi_d,

@@ -102,3 +102,38 @@ def test_hpsi_is_hermitian_and_linear(pkg):
     ha, hb, hab = hx.cpu().numpy().reshape(3, ld)
     assert abs(np.vdot(a, hb) - np.vdot(ha, b)) < 1e-11 * abs(np.vdot(a, hb)) + 1e-9
     assert rel(hab, ha + 2 * hb) < 1e-13
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+@pytest.mark.parametrize("pieces,pinned", [(1, True), (3, True), (5, False)])
+def test_hpsi_host_pipeline_equals_device_hpsi(pkg, prec, pieces, pinned):
+    """b200_hamilt_hpsi_host (host buffers, uploads / H|psi> pieces / downloads overlapped on three streams)
+    gives the device H|psi> of the same pieces bit for bit (the projector GEMM of a smaller piece may round
+    differently from the whole block's: within 1e-13 of it), for uneven pieces and for pinned and pageable
+    host buffers."""
+    P = pkg.pwdft
+    wl, _, psi, nb, ld = _setup(pkg, pkg.synth.config(0), None, 13)
+    p = P.PREC_FP64 if prec == "fp64" else P.PREC_MIXED
+    ct = torch.complex128 if prec == "fp64" else torch.complex64
+    h = P.device_hamilt(wl, p)
+    ph = torch.from_numpy(psi.copy()).to(ct)
+    ref_d = torch.zeros(nb * ld, dtype=ct, device="cuda")
+    whole = torch.zeros(nb * ld, dtype=ct, device="cuda")
+    pdev = ph.cuda()
+    h.hpsi(0, pdev, whole, nb, ld)
+    P_ = min(pieces, nb)
+    for q in range(P_):
+        b0, b1 = q * nb // P_, (q + 1) * nb // P_
+        h.hpsi(0, pdev[b0 * ld:], ref_d[b0 * ld:], b1 - b0, ld)
+    if pinned:
+        ph = ph.pin_memory()
+    out_h = torch.full((nb * ld,), 7.0, dtype=ct)
+    if pinned:
+        out_h = out_h.pin_memory()
+    pd = torch.zeros(nb * ld, dtype=ct, device="cuda")
+    hd = torch.zeros(nb * ld, dtype=ct, device="cuda")
+    h.hpsi_host(0, ph, out_h, pd, hd, nb, ld, pieces=pieces)
+    torch.cuda.synchronize()
+    assert torch.equal(out_h, ref_d.cpu())
+    tol = 1e-13 if prec == "fp64" else 1e-6
+    assert rel(out_h.numpy(), whole.cpu().numpy()) < tol
