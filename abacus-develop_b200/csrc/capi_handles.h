@@ -11,8 +11,12 @@ struct b200_pw_basis {
     b200::PWGrid grid;
     b200::DeviceArray<double2> aux64;
     b200::DeviceArray<float2> aux32;
-    b200::DeviceArray<double2> rho_box64;  // psi(r) of one band (psi -> rho)
+    b200::DeviceArray<double2> rho_box64;  // psi(r) of one band (psi -> rho, generic grids)
     b200::DeviceArray<float2> rho_box32;
+    b200::DeviceArray<double2> rho_sb64;   // psi -> rho on the register transforms: stick buffer of a chunk,
+    b200::DeviceArray<float2> rho_sb32;    // partial rho planes, band weights
+    b200::DeviceArray<double> rho_ws64, rho_w;
+    b200::DeviceArray<float> rho_ws32;
 };
 // copy streams and events of b200_hamilt_hpsi_host, made at its first use and kept with the handle
 struct HostPipe {

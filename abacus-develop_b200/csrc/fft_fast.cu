@@ -268,6 +268,84 @@ __global__ void __launch_bounds__(kPlaneWarps * 32) k_plane_r(PlaneMapView pm, i
     for (int s = tid; s < pm.nst; s += NT) plane[s] = A[pm.xc[s] * LD + pm.sy[s]];
 }
 
+// psi -> rho on the register transforms (elecstate_pw.cpp:160-216: rho(r) += w_b |psi_b(r)|^2 with the
+// backward transform of each occupied band).  CTA (z slot, g): bands g, g + nsplit, ... of the chunk in the
+// stick buffer; per band the plane's inverse y transform on the occupied columns and the inverse x
+// transform of every row, and this warp's rows of w_b |psi|^2 summed in registers over the bands.  The
+// partial plane (slot order) goes to ws[g], overwritten on the first chunk and added to afterwards: each
+// (z slot, g) owns its plane, so the sums are deterministic.
+template <typename T, typename R, int N>
+__global__ void __launch_bounds__(kPlaneWarps * 32) k_rho_plane_r(PlaneMapView pm, int nz, const T* __restrict__ roots,
+                                                                 const T* __restrict__ sb, int nbc,
+                                                                 const double* __restrict__ w, int nsplit,
+                                                                 R* __restrict__ ws, int first) {
+    constexpr int M = N / 32;
+    constexpr int LD = N | 1;
+    constexpr int NT = kPlaneWarps * 32;
+    constexpr int RW = N / kPlaneWarps;  // rows per warp
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* A = reinterpret_cast<T*>(smem_raw);
+    const int nxc = pm.nxc;
+    int* cmap = reinterpret_cast<int*>(A + nxc * LD);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int sz = blockIdx.x, g = blockIdx.y;
+    for (int i = tid; i < N; i += NT) cmap[i] = -1;
+    __syncthreads();
+    for (int c = tid; c < nxc; c += NT) cmap[pm.xpos[c]] = c;
+    T lk[M];
+    LaneTw<T> tw;
+    lane_twiddles<T, N>(roots, lane, lk, tw);
+    __syncthreads();
+    int cm[M];
+#pragma unroll
+    for (int n1 = 0; n1 < M; ++n1) cm[n1] = cmap[32 * n1 + lane];
+    R acc[RW][M];
+#pragma unroll
+    for (int r = 0; r < RW; ++r)
+#pragma unroll
+        for (int k1 = 0; k1 < M; ++k1) acc[r][k1] = R(0);
+    for (int b = g; b < nbc; b += nsplit) {
+        const R wb = R(w[b]);
+        __syncthreads();  // the previous band's rows are read
+        for (int i = tid; i < nxc * LD; i += NT) A[i] = zero_c<T>();
+        __syncthreads();
+        const T* plane = sb + (size_t(b) * nz + sz) * pm.nst;
+        for (int s = tid; s < pm.nst; s += NT) A[pm.xc[s] * LD + pm.sy[s]] = plane[s];
+        __syncthreads();
+        for (int c = warp; c < nxc; c += kPlaneWarps) {
+            T u[M];
+            T* col = A + c * LD;
+#pragma unroll
+            for (int n1 = 0; n1 < M; ++n1) u[n1] = col[32 * n1 + lane];
+            regfft_inv_dif<T, M>(u, lk, tw, lane);
+#pragma unroll
+            for (int k1 = 0; k1 < M; ++k1) col[32 * k1 + lane] = u[k1];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int r = 0; r < RW; ++r) {
+            const int sy = warp + r * kPlaneWarps;
+            T u[M];
+#pragma unroll
+            for (int n1 = 0; n1 < M; ++n1) u[n1] = cm[n1] >= 0 ? A[cm[n1] * LD + sy] : zero_c<T>();
+            regfft_inv_dif<T, M>(u, lk, tw, lane);
+#pragma unroll
+            for (int k1 = 0; k1 < M; ++k1) acc[r][k1] = fma(wb, fma(u[k1].x, u[k1].x, u[k1].y * u[k1].y), acc[r][k1]);
+        }
+    }
+    if (!first && g >= nbc) return;  // nothing added to this partial plane
+    R* out = ws + (size_t(g) * nz + sz) * N * N;
+#pragma unroll
+    for (int r = 0; r < RW; ++r) {
+        const int sy = warp + r * kPlaneWarps;
+#pragma unroll
+        for (int k1 = 0; k1 < M; ++k1) {
+            R* o = out + sy * N + 32 * k1 + lane;
+            *o = first ? acc[r][k1] : *o + acc[r][k1];
+        }
+    }
+}
+
 // ---- register z passes for nz = 32*M: the inverse transform leaves every stick in the permuted order, so
 // the planes of the stick buffer are stored by slot (plane slot sz holds z = sz/32 + M*bitrev5(sz mod 32));
 // V_eff is permuted along z as well, and the forward z transform takes the slots back to natural z.
@@ -386,6 +464,22 @@ __global__ void k_permute_veff(int nz, int n, int m, int mz, const R* __restrict
         out[i] = in[(long(perm_slot(sz, mz)) * n + perm_slot(sy, m)) * n + perm_slot(sx, m)];
     }
 }
+
+// rho (x, y, z natural, z fastest) += sum over g of the partial planes (slot order), in a fixed order
+template <typename R>
+__global__ void k_rho_reduce(int nz, int n, int m, int mz, int nsplit, const R* __restrict__ ws, R* __restrict__ rho) {
+    const long total = long(nz) * n * n;
+    for (long i = blockIdx.x * long(blockDim.x) + threadIdx.x; i < total; i += long(gridDim.x) * blockDim.x) {
+        const int sx = int(i % n);
+        const int sy = int((i / n) % n);
+        const int sz = int(i / (long(n) * n));
+        R sum = ws[i];
+        for (int g = 1; g < nsplit; ++g) sum += ws[size_t(g) * total + i];
+        const int x = perm_slot(sx, m), y = perm_slot(sy, m), z = perm_slot(sz, mz);
+        rho[(size_t(x) * n + y) * nz + z] += sum;
+    }
+}
+
 
 // ---- k-point batched z passes: one launch covers every k-point of a batch (blockIdx.z = k slot) ----
 template <typename T, int NZ>
@@ -693,5 +787,55 @@ bool launch_permute_veff(const PWGrid& g, const R* veff_zyx, R* out, cudaStream_
 }
 template bool launch_permute_veff<double>(const PWGrid&, const double*, double*, cudaStream_t);
 template bool launch_permute_veff<float>(const PWGrid&, const float*, float*, cudaStream_t);
+
+bool rho_r_supported(const PWGrid& g) {
+    const size_t smem = size_t(g.nxc) * (g.nx | 1) * sizeof(double2) + size_t(g.nx) * sizeof(int);
+    return plane_perm_supported(g) && smem <= 227 * 1024;
+}
+
+template <typename T, typename R, int N>
+void rho_plane_launch(const PWGrid& g, const T* sb, int nbc, const double* w, int nsplit, R* ws, int first,
+                      cudaStream_t s) {
+    const size_t smem = size_t(g.nxc) * (N | 1) * sizeof(T) + size_t(N) * sizeof(int);
+    smem_attr(k_rho_plane_r<T, R, N>, smem);
+    k_rho_plane_r<T, R, N><<<dim3(g.nz, nsplit), kPlaneWarps * 32, smem, s>>>(g.plane_view(), g.nz, rtp<T>(g.ax), sb,
+                                                                               nbc, w, nsplit, ws, first);
+    note_launch();
+    B200_CUDA(cudaGetLastError());
+}
+
+template <typename T, typename R>
+void launch_rho_chunk_r(const PWGrid& g, int ik, int b0, int nbc, int ld, const T* psi, const double* w_chunk,
+                        T* sb, int nsplit, R* ws, int first, cudaStream_t s) {
+    OneK src;
+    src.e.sm = g.stick_view(ik);
+    src.e.psi = psi;
+    src.e.hpsi = nullptr;
+    src.e.ld = ld;
+    src.e.npw = g.kmaps[ik].npw;
+    src.e.gk2 = nullptr;
+    const bool zok = zpass_r_dispatch<T, R>(true, g, src, 1, b0, nbc, sb, 0.0, 0, s);
+    B200_CHECK(zok, kInvalidArgument, "psi -> rho: nz has no register transform");
+    switch (g.nx) {
+        case 64: rho_plane_launch<T, R, 64>(g, sb, nbc, w_chunk, nsplit, ws, first, s); break;
+        case 96: rho_plane_launch<T, R, 96>(g, sb, nbc, w_chunk, nsplit, ws, first, s); break;
+        case 128: rho_plane_launch<T, R, 128>(g, sb, nbc, w_chunk, nsplit, ws, first, s); break;
+        default: B200_CHECK(false, kInvalidArgument, "psi -> rho: nx has no register transform");
+    }
+}
+
+template <typename R>
+void launch_rho_reduce_r(const PWGrid& g, int nsplit, const R* ws, R* rho, cudaStream_t s) {
+    k_rho_reduce<R><<<1184, 256, 0, s>>>(g.nz, g.nx, g.nx / 32, g.nz / 32, nsplit, ws, rho);
+    note_launch();
+    B200_CUDA(cudaGetLastError());
+}
+
+template void launch_rho_chunk_r<double2, double>(const PWGrid&, int, int, int, int, const double2*, const double*,
+                                                  double2*, int, double*, int, cudaStream_t);
+template void launch_rho_chunk_r<float2, float>(const PWGrid&, int, int, int, int, const float2*, const double*,
+                                                float2*, int, float*, int, cudaStream_t);
+template void launch_rho_reduce_r<double>(const PWGrid&, int, const double*, double*, cudaStream_t);
+template void launch_rho_reduce_r<float>(const PWGrid&, int, const float*, float*, cudaStream_t);
 
 }  // namespace b200

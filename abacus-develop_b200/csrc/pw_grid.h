@@ -130,6 +130,15 @@ void launch_transpose_veff(const PWGrid& g, const double* veff, R* out, cudaStre
 // in a permuted order; V_eff is stored once in that order: out[z][sy][sx] = veff_zyx[z][p(sy)][p(sx)],
 // p(s) = s/32 + m*bitrev5(s mod 32).  Returns false (nothing done) for other grids.
 bool plane_perm_supported(const PWGrid& g);
+// psi -> rho on the register transforms (grids with plane_perm_supported whose plane fits shared memory):
+// bands [b0, b0 + nbc) of psi through the inverse z pass into sb, then w_chunk[b] |psi_b(r)|^2 summed into
+// nsplit partial planes ws (slot order; first = 1 overwrites them); launch_rho_reduce_r adds them to rho
+bool rho_r_supported(const PWGrid& g);
+template <typename T, typename R>
+void launch_rho_chunk_r(const PWGrid& g, int ik, int b0, int nbc, int ld, const T* psi, const double* w_chunk,
+                        T* sb, int nsplit, R* ws, int first, cudaStream_t s);
+template <typename R>
+void launch_rho_reduce_r(const PWGrid& g, int nsplit, const R* ws, R* rho, cudaStream_t s);
 template <typename R>
 bool launch_permute_veff(const PWGrid& g, const R* veff_zyx, R* out, cudaStream_t s);
 

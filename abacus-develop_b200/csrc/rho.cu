@@ -2,9 +2,13 @@
 // functor elecstate_pw_op (module_elecstate/kernels/elecstate_op.cpp:6-83).
 //
 // The functor entry points mirror the reference (rho is an array of nspin device pointers, host side).  The
-// product path b200_pw_basis_psi_to_rho runs the reference's loop on the device: for every band with a
-// non-zero weight, the drop-in transform recip_to_real into a full box, then rho[spin](r) += w1*|psi(r)|^2;
-// nothing goes back to the host between bands.
+// product path b200_pw_basis_psi_to_rho computes the reference's sum rho(r) += w1_b |psi_b(r)|^2 over the
+// bands with a non-zero weight: on grids with register transforms (nx = ny and nx, nz in {64, 96, 128})
+// fused into two passes per band chunk (inverse z transform of the sticks; per z plane the inverse y and x
+// transforms with |psi|^2 summed in registers) and one final reduction; elsewhere by the reference's loop,
+// the drop-in transform recip_to_real into a full box and elecstate_pw_op per band.  Nothing goes back to
+// the host between bands.  One call at a time per basis handle (its scratch is shared).
+#include <algorithm>
 #include <vector>
 
 #include "../../include/abacus_b200.h"
@@ -93,13 +97,40 @@ template <typename F> int guarded_r(F&& f) {
 }
 
 template <typename T, typename R>
-void psi_to_rho(b200_pw_basis* b, b200::DeviceArray<T>& box, b200::DeviceArray<T>& aux, int ik, int nbands, int ld,
-                const T* psi, const double* w1, R* rho, cudaStream_t s) {
+void psi_to_rho(b200_pw_basis* b, b200::DeviceArray<T>& box, b200::DeviceArray<T>& aux, b200::DeviceArray<T>& sbuf,
+                b200::DeviceArray<R>& ws, int ik, int nbands, int ld, const T* psi, const double* w1, R* rho,
+                cudaStream_t s) {
     b200::PWGrid& g = b->grid;
     B200_CHECK(ik >= 0 && ik < int(g.kmaps.size()), b200::kInvalidArgument, "k-point index out of range");
     B200_CHECK(nbands >= 0 && ld >= g.kmaps[ik].npw, b200::kInvalidArgument, "ld smaller than npwk");
     B200_CHECK(psi && w1 && rho, b200::kInvalidArgument, "NULL argument");
     g.ensure_device();
+    if (nbands > 0 && b200::rho_r_supported(g)) {
+        // the same sum on the register transforms: runs of consecutive bands with a non-zero weight (the
+        // reference skips the others, elecstate_pw.cpp:211), in chunks whose stick buffer is about 48 MB
+        b->rho_w.resize(size_t(nbands));
+        B200_CUDA(cudaMemcpyAsync(b->rho_w.ptr, w1, size_t(nbands) * sizeof(double), cudaMemcpyHostToDevice, s));
+        const size_t per_band = size_t(g.nz) * g.nst;
+        const int chunk = int(std::max<size_t>(1, (size_t(48) << 20) / (per_band * sizeof(T))));
+        sbuf.resize(size_t(std::min(chunk, nbands)) * per_band);
+        const int nsplit = std::max(1, std::min(8, (2 * 148 + g.nz - 1) / g.nz));  // about two CTAs per SM
+        ws.resize(size_t(nsplit) * size_t(g.nxyz()));
+        int first = 1;
+        for (int b0 = 0; b0 < nbands;) {
+            if (w1[b0] == 0.0) {
+                ++b0;
+                continue;
+            }
+            int b1 = b0;
+            while (b1 < nbands && w1[b1] != 0.0 && b1 - b0 < chunk) ++b1;
+            b200::launch_rho_chunk_r<T, R>(g, ik, b0, b1 - b0, ld, psi, b->rho_w.ptr + b0, sbuf.ptr, nsplit, ws.ptr,
+                                           first, s);
+            first = 0;
+            b0 = b1;
+        }
+        if (!first) b200::launch_rho_reduce_r<R>(g, nsplit, ws.ptr, rho, s);
+        return;
+    }
     const long N = g.nxyz();
     box.resize(size_t(N));
     aux.resize(size_t(N));
@@ -144,16 +175,16 @@ int b200_pw_basis_psi_to_rho_f64(b200_pw_basis* b, int ik, int nbands, int ld, c
                                  double* rho_d, void* stream) {
     return guarded_r([&] {
         B200_CHECK(b != nullptr, b200::kInvalidArgument, "NULL basis");
-        psi_to_rho<double2, double>(b, b->rho_box64, b->aux64, ik, nbands, ld, (const double2*)psi_d, w1, rho_d,
-                                    (cudaStream_t)stream);
+        psi_to_rho<double2, double>(b, b->rho_box64, b->aux64, b->rho_sb64, b->rho_ws64, ik, nbands, ld,
+                                    (const double2*)psi_d, w1, rho_d, (cudaStream_t)stream);
     });
 }
 int b200_pw_basis_psi_to_rho_f32(b200_pw_basis* b, int ik, int nbands, int ld, const void* psi_d, const double* w1,
                                  float* rho_d, void* stream) {
     return guarded_r([&] {
         B200_CHECK(b != nullptr, b200::kInvalidArgument, "NULL basis");
-        psi_to_rho<float2, float>(b, b->rho_box32, b->aux32, ik, nbands, ld, (const float2*)psi_d, w1, rho_d,
-                                  (cudaStream_t)stream);
+        psi_to_rho<float2, float>(b, b->rho_box32, b->aux32, b->rho_sb32, b->rho_ws32, ik, nbands, ld,
+                                  (const float2*)psi_d, w1, rho_d, (cudaStream_t)stream);
     });
 }
 

@@ -391,7 +391,7 @@ def rho_bench(P, wl, psi, steps, stream):
         step()
     ms = time_steps(step, max(3, steps // 4), stream)
     return {"bands_per_s": nb / (ms * 1e-3), "ms_per_160_bands": ms,
-            "path": "recip_to_real into a full box per band + elecstate_pw_op (the reference's loop)"}
+            "path": "register transforms: inverse z pass per band chunk, then per z plane inverse y and x transforms with w|psi|^2 summed in registers, partial planes reduced once (96^3 grid; other grids: recip_to_real per band + elecstate_pw_op, the reference's loop)"}
 
 
 def cpu_reference_davidson_8atom(pkg):
