@@ -134,11 +134,11 @@ template <typename T> __device__ __forceinline__ T shfl_x(T v, int m) {
 }
 
 // Per-lane twiddles.  lk[k1] = W_N^{lane*k1}.  For the five lane stages (h = 16 >> j) the butterflies are
-// written without branches, with this lane's role folded into its twiddles:
-//   inverse (DIF):  u' = (p + sg*u) * wi[j]     sg = -1 on the bottom lane of a pair, +1 on the top;
-//                                               wi = conj(W_{2h}^{lane mod h}) on the bottom, 1 on the top;
-//   forward (DIT):  u' = a + wf[j] * b          (a, b) = (u, p) on the top, (p, u) on the bottom;
-//                                               wf = W_{2h}^{lane mod h} on the top, its negative on the bottom.
+// written without branches or selects, with this lane's role folded into its twiddles:
+//   inverse (DIF):  u' = (p + sg*u) * wi[j]     p = partner's u; sg = -1 on the bottom lane of a pair, +1 on
+//                                               the top; wi = conj(W_{2h}^{lane mod h}) on the bottom, 1 on the top;
+//   forward (DIT):  s = wf[j] * u, u' = p + sg*s   p = partner's s; wf = W_{2h}^{lane mod h} on the bottom, 1
+//                                               on the top (top: u + w u_bottom, bottom: u_top - w u).
 template <typename T> struct LaneTw {
     using R = typename RealOf<T>::type;
     R sg[5];
@@ -158,7 +158,7 @@ __device__ __forceinline__ void lane_twiddles(const T* __restrict__ roots, int l
         const T w = roots[M * (lane % h) * (16 / h)];
         tw.sg[j] = bottom ? R(-1) : R(1);
         tw.wi[j] = bottom ? cmake<T>(w.x, -w.y) : cmake<T>(R(1), R(0));
-        tw.wf[j] = bottom ? cmake<T>(-w.x, -w.y) : w;
+        tw.wf[j] = bottom ? w : cmake<T>(R(1), R(0));
     }
 }
 
@@ -184,14 +184,11 @@ __device__ __forceinline__ void regfft_fwd_dit(T* u, const T* lk, const LaneTw<T
 #pragma unroll
     for (int j = 4; j >= 0; --j) {
         const int h = 16 >> j;
-        const bool bottom = lane & h;
 #pragma unroll
         for (int k1 = 0; k1 < M; ++k1) {
-            const T p = shfl_x(u[k1], h);
-            const T a = bottom ? p : u[k1];
-            const T b = bottom ? u[k1] : p;
-            const T w = tw.wf[j];
-            u[k1] = cmake<T>(fma(-w.y, b.y, fma(w.x, b.x, a.x)), fma(w.y, b.x, fma(w.x, b.y, a.y)));
+            const T sv = (j == 4) ? u[k1] : cmul(u[k1], tw.wf[j]);  // the first stage's twiddle is 1
+            const T p = shfl_x(sv, h);
+            u[k1] = cmake<T>(fma(tw.sg[j], sv.x, p.x), fma(tw.sg[j], sv.y, p.y));
         }
     }
 #pragma unroll
