@@ -49,7 +49,7 @@ E2E_PIECES = 5
 # dram__bytes_read.sum + dram__bytes_write.sum of the fused local H|psi> kernels (27 launches: 9 band
 # chunks x 3 passes) for one 160-band FP64 application, from the ncu capture without cache flush summarised
 # in profiles/hpsi_local_diamond64_traffic.md
-NCU_TRAFFIC_LOCAL_FP64 = 648301312
+NCU_TRAFFIC_LOCAL_FP64 = 643307264
 
 
 def load_package():
