@@ -47,8 +47,8 @@ METRIC = "H|psi> bands/s (FP64) + Davidson time-to-1e-8 Ry, mixed vs FP64"
 # local pass each; 4, 8 or 10 pieces measured 13-19 % slower on B200)
 E2E_PIECES = 5
 # dram__bytes_read.sum + dram__bytes_write.sum of the fused local H|psi> kernels (27 launches: 9 band
-# chunks x 3 passes) for one 160-band FP64 application, from the ncu capture without cache flush summarised
-# in profiles/hpsi_local_diamond64_traffic.md
+# chunks x 3 passes) for one 160-band FP64 application, from an ncu capture without cache flush (the
+# local-pass traffic summary under profiles/)
 NCU_TRAFFIC_LOCAL_FP64 = 643307264
 
 
