@@ -196,20 +196,131 @@ __device__ __forceinline__ void regfft_fwd_dit(T* u, const T* lk, const LaneTw<T
     dftR<T, -1, M>(u);
 }
 
-// Plane pass with register transforms; V_eff in the permuted order of launch_permute_veff.
-// Shared memory: the plane (nxc occupied x-columns of N | 1) and the x -> column map.  W warps per CTA,
-// at least MINB CTAs per SM.
-template <typename T, typename R, int N, int W, int MINB>
-__global__ void __launch_bounds__(W * 32, MINB) k_plane_r(PlaneMapView pm, int nz, const T* __restrict__ roots,
-                                                             const R* __restrict__ vperm, T* __restrict__ sb) {
-    constexpr int M = N / 32;
+// ---- register transforms with P lanes per line (N = P*Q; P = 8, 16 or 32) ----
+// The generalisation of the above: lane L of a group of P lanes holds x[P*n1 + L] (n1 < Q); the inverse
+// takes a Q-point DFT in registers, twiddles W_N^{-L*k1} and log2(P) radix-2 lane stages (xor h = P/2 .. 1,
+// inside the group) and leaves lane L with the outputs k1 + Q*bitrev(L); the forward is the transposed
+// algorithm.  Fewer lanes per line mean fewer lane stages: every lane stage moves each value through warp
+// shuffles (two 32-bit shuffles per double), so P = 8 moves each value 3 times instead of 5, and a warp
+// carries 32/P independent lines.  Lane twiddles come from the roots table (L1-resident) when used.
+
+// Q-point DFT in registers, natural order in and out (DIR +1: exp(+i), -1: exp(-i)); Q = A*B with A, B in
+// {2, 3, 4}: A-point DFTs of the stride-B subsets, twiddles W_Q^(n2 k1), B-point DFTs; roots[j] = W_N^j
+template <typename T, int DIR, int Q>
+__device__ __forceinline__ void dft_reg(T* u, const T* __restrict__ roots, int N) {
+    if constexpr (Q <= 4) {
+        dftR<T, DIR, Q>(u);
+    } else {
+        constexpr int A = (Q % 4 == 0) ? 4 : 3;
+        constexpr int B = Q / A;
+        static_assert(A * B == Q && B >= 2 && B <= 4, "Q = A*B with A, B in {2, 3, 4}");
+        T y[B][A];
+#pragma unroll
+        for (int n2 = 0; n2 < B; ++n2) {
+#pragma unroll
+            for (int n1 = 0; n1 < A; ++n1) y[n2][n1] = u[B * n1 + n2];
+            dftR<T, DIR, A>(y[n2]);
+#pragma unroll
+            for (int k1 = 1; k1 < A; ++k1)
+                if (n2 > 0) {
+                    const T w = __ldg(roots + n2 * k1 * (N / Q));
+                    y[n2][k1] = DIR < 0 ? cmul(y[n2][k1], w) : cmulc(y[n2][k1], w);
+                }
+        }
+#pragma unroll
+        for (int k1 = 0; k1 < A; ++k1) {
+            T z[B];
+#pragma unroll
+            for (int n2 = 0; n2 < B; ++n2) z[n2] = y[n2][k1];
+            dftR<T, DIR, B>(z);
+#pragma unroll
+            for (int k2 = 0; k2 < B; ++k2) u[k1 + A * k2] = z[k2];
+        }
+    }
+}
+
+template <int P> constexpr int log2i() { return P == 8 ? 3 : P == 16 ? 4 : 5; }
+
+// per-lane twiddle of each lane stage: w[j] = W_{2h}^{L mod h} (h = P >> (j + 1)); the butterflies derive
+// their signs and the top lane's unit twiddle from L & h
+template <typename T, int P> struct LaneTwP {
+    T w[log2i<P>()];
+};
+template <typename T, int N, int P>
+__device__ __forceinline__ void lane_twiddles_p(const T* __restrict__ roots, int L, LaneTwP<T, P>& tw) {
+#pragma unroll
+    for (int j = 0; j < log2i<P>(); ++j) {
+        const int h = P >> (j + 1);
+        tw.w[j] = roots[(N / (2 * h)) * (L % h)];
+    }
+}
+
+template <typename T, int P, int Q>
+__device__ __forceinline__ void regfftP_inv_dif(T* u, const T* __restrict__ roots, const LaneTwP<T, P>& tw, int L) {
+    using R = typename RealOf<T>::type;
+    constexpr int N = P * Q;
+    dft_reg<T, +1, Q>(u, roots, N);
+#pragma unroll
+    for (int k1 = 1; k1 < Q; ++k1) u[k1] = cmulc(u[k1], __ldg(roots + (L * k1) % N));
+#pragma unroll
+    for (int j = 0; j < log2i<P>(); ++j) {
+        const int h = P >> (j + 1);
+        const bool bottom = L & h;
+        const R sg = bottom ? R(-1) : R(1);
+        const T wi = bottom ? cmake<T>(tw.w[j].x, -tw.w[j].y) : cmake<T>(R(1), R(0));
+#pragma unroll
+        for (int k1 = 0; k1 < Q; ++k1) {
+            const T p = shfl_x(u[k1], h);
+            const T t = cmake<T>(fma(sg, u[k1].x, p.x), fma(sg, u[k1].y, p.y));
+            u[k1] = (j == log2i<P>() - 1) ? t : cmul(t, wi);  // the last stage's twiddle is 1
+        }
+    }
+}
+
+template <typename T, int P, int Q>
+__device__ __forceinline__ void regfftP_fwd_dit(T* u, const T* __restrict__ roots, const LaneTwP<T, P>& tw, int L) {
+    using R = typename RealOf<T>::type;
+    constexpr int N = P * Q;
+#pragma unroll
+    for (int j = log2i<P>() - 1; j >= 0; --j) {
+        const int h = P >> (j + 1);
+        const bool bottom = L & h;
+        const R sg = bottom ? R(-1) : R(1);
+        const T wf = bottom ? tw.w[j] : cmake<T>(R(1), R(0));
+#pragma unroll
+        for (int k1 = 0; k1 < Q; ++k1) {
+            const T sv = (j == log2i<P>() - 1) ? u[k1] : cmul(u[k1], wf);  // the first stage's twiddle is 1
+            const T p = shfl_x(sv, h);
+            u[k1] = cmake<T>(fma(sg, sv.x, p.x), fma(sg, sv.y, p.y));
+        }
+    }
+#pragma unroll
+    for (int k1 = 1; k1 < Q; ++k1) u[k1] = cmul(u[k1], __ldg(roots + (L * k1) % N));
+    dft_reg<T, -1, Q>(u, roots, N);
+}
+
+// lanes per line of the plane pass: 32 (measured on the 96^3 plane pass of B200: P = 16 was 3 % / 5 %
+// slower in FP64 / FP32 and P = 8 spills at two (FP64) or four (FP32) CTAs per SM; the values a lane holds
+// and the larger in-register DFTs cost more than the lane stages they save)
+template <typename T, int N> constexpr int plane_lanes() { return 32; }
+
+// Plane pass on P-lane transforms; V_eff permuted along x and y by the P-lane slot map (launch_permute_veff).
+// Shared memory: the plane (nxc occupied x-columns of N | 1) and the x -> column map.  W warps per CTA, at
+// least MINB CTAs per SM; each warp transforms 32/P lines at a time.
+template <typename T, typename R, int N, int P, int W, int MINB>
+__global__ void __launch_bounds__(W * 32, MINB) k_plane_p(PlaneMapView pm, int nz, const T* __restrict__ roots,
+                                                         const R* __restrict__ vperm, T* __restrict__ sb) {
+    constexpr int Q = N / P;
+    constexpr int G = 32 / P;
     constexpr int LD = N | 1;
     constexpr int NT = W * 32;
+    static_assert(N % (W * G) == 0, "rows per round");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* A = reinterpret_cast<T*>(smem_raw);
     const int nxc = pm.nxc;
     int* cmap = reinterpret_cast<int*>(A + nxc * LD);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int L = lane % P, grp = lane / P;
     const int band = blockIdx.x;
     const int z = blockIdx.y;
     for (int i = tid; i < nxc * LD; i += NT) A[i] = zero_c<T>();
@@ -218,49 +329,58 @@ __global__ void __launch_bounds__(W * 32, MINB) k_plane_r(PlaneMapView pm, int n
     for (int c = tid; c < nxc; c += NT) cmap[pm.xpos[c]] = c;
     T* plane = sb + (size_t(band) * nz + z) * pm.nst;
     for (int s = tid; s < pm.nst; s += NT) A[pm.xc[s] * LD + pm.sy[s]] = plane[s];
-    T lk[M];
-    LaneTw<T> tw;
-    lane_twiddles<T, N>(roots, lane, lk, tw);
+    LaneTwP<T, P> tw;
+    lane_twiddles_p<T, N, P>(roots, L, tw);
     __syncthreads();
-    int cm[M];
+    int cm[Q];
 #pragma unroll
-    for (int n1 = 0; n1 < M; ++n1) cm[n1] = cmap[32 * n1 + lane];
-    // inverse y transform of every occupied column; the result stays in the permuted slot order
-    for (int c = warp; c < nxc; c += W) {
-        T u[M];
-        T* col = A + c * LD;
+    for (int n1 = 0; n1 < Q; ++n1) cm[n1] = cmap[P * n1 + L];
+    // inverse y transform of every occupied column (a group past the last column transforms a valid one
+    // and stores nothing: the shuffles need the whole warp)
+    for (int c0 = warp * G; c0 < nxc; c0 += W * G) {
+        const int c = c0 + grp;
+        const T* colr = A + (c < nxc ? c : c0) * LD;
+        T u[Q];
 #pragma unroll
-        for (int n1 = 0; n1 < M; ++n1) u[n1] = col[32 * n1 + lane];
-        regfft_inv_dif<T, M>(u, lk, tw, lane);
+        for (int n1 = 0; n1 < Q; ++n1) u[n1] = colr[P * n1 + L];
+        regfftP_inv_dif<T, P, Q>(u, roots, tw, L);
+        if (c < nxc) {
+            T* col = A + c * LD;
 #pragma unroll
-        for (int k1 = 0; k1 < M; ++k1) col[32 * k1 + lane] = u[k1];
+            for (int k1 = 0; k1 < Q; ++k1) col[P * k1 + L] = u[k1];
+        }
     }
     __syncthreads();
     // each row slot: inverse x transform, times V_eff(r), forward x transform
     const R* vz = vperm + size_t(z) * N * N;
-    for (int sy = warp; sy < N; sy += W) {
-        T u[M];
+    for (int sy0 = warp * G; sy0 < N; sy0 += W * G) {
+        const int sy = sy0 + grp;
+        T u[Q];
 #pragma unroll
-        for (int n1 = 0; n1 < M; ++n1) u[n1] = cm[n1] >= 0 ? A[cm[n1] * LD + sy] : zero_c<T>();
-        regfft_inv_dif<T, M>(u, lk, tw, lane);
+        for (int n1 = 0; n1 < Q; ++n1) u[n1] = cm[n1] >= 0 ? A[cm[n1] * LD + sy] : zero_c<T>();
+        regfftP_inv_dif<T, P, Q>(u, roots, tw, L);
         const R* vr = vz + sy * N;
 #pragma unroll
-        for (int k1 = 0; k1 < M; ++k1) u[k1] = cscale(u[k1], vr[32 * k1 + lane]);
-        regfft_fwd_dit<T, M>(u, lk, tw, lane);
+        for (int k1 = 0; k1 < Q; ++k1) u[k1] = cscale(u[k1], vr[P * k1 + L]);
+        regfftP_fwd_dit<T, P, Q>(u, roots, tw, L);
 #pragma unroll
-        for (int n1 = 0; n1 < M; ++n1)
+        for (int n1 = 0; n1 < Q; ++n1)
             if (cm[n1] >= 0) A[cm[n1] * LD + sy] = u[n1];
     }
     __syncthreads();
     // forward y transform back to natural order
-    for (int c = warp; c < nxc; c += W) {
-        T u[M];
-        T* col = A + c * LD;
+    for (int c0 = warp * G; c0 < nxc; c0 += W * G) {
+        const int c = c0 + grp;
+        const T* colr = A + (c < nxc ? c : c0) * LD;
+        T u[Q];
 #pragma unroll
-        for (int k1 = 0; k1 < M; ++k1) u[k1] = col[32 * k1 + lane];
-        regfft_fwd_dit<T, M>(u, lk, tw, lane);
+        for (int k1 = 0; k1 < Q; ++k1) u[k1] = colr[P * k1 + L];
+        regfftP_fwd_dit<T, P, Q>(u, roots, tw, L);
+        if (c < nxc) {
+            T* col = A + c * LD;
 #pragma unroll
-        for (int n1 = 0; n1 < M; ++n1) col[32 * n1 + lane] = u[n1];
+            for (int n1 = 0; n1 < Q; ++n1) col[P * n1 + L] = u[n1];
+        }
     }
     __syncthreads();
     for (int s = tid; s < pm.nst; s += NT) plane[s] = A[pm.xc[s] * LD + pm.sy[s]];
@@ -450,16 +570,21 @@ __global__ void __launch_bounds__(kZWarps * 32) k_zfwd_r(Src src, int b0, int nb
 }
 
 __device__ __forceinline__ int perm_slot(int s, int m) { return (s >> 5) + m * int(__brev(unsigned(s & 31)) >> 27); }
+// the same for lines of P = 2^lp lanes and q values per lane: slot s holds index s/P + q * bitrev_lp(s mod P)
+__device__ __forceinline__ int perm_slot_p(int s, int lp, int q) {
+    return (s >> lp) + q * int(__brev(unsigned(s & ((1 << lp) - 1))) >> (32 - lp));
+}
 
 template <typename R>
-__global__ void k_permute_veff(int nz, int n, int m, int mz, const R* __restrict__ in, R* __restrict__ out) {
+__global__ void k_permute_veff(int nz, int n, int lp, int mz, const R* __restrict__ in, R* __restrict__ out) {
     const long total = long(nz) * n * n;
     for (long i = blockIdx.x * long(blockDim.x) + threadIdx.x; i < total; i += long(gridDim.x) * blockDim.x) {
         const int sx = int(i % n);
         const long r = i / n;
         const int sy = int(r % n);
         const int sz = int(r / n);
-        out[i] = in[(long(perm_slot(sz, mz)) * n + perm_slot(sy, m)) * n + perm_slot(sx, m)];
+        const int q = n >> lp;
+        out[i] = in[(long(perm_slot(sz, mz)) * n + perm_slot_p(sy, lp, q)) * n + perm_slot_p(sx, lp, q)];
     }
 }
 
@@ -608,13 +733,14 @@ bool plane_launch_r(const PWGrid& g, int nb, const R* vperm, T* sb, cudaStream_t
     if (smem > 227 * 1024) return false;
     // FP64: two CTAs of 8 warps per SM (up to 128 registers a thread, 2 x 73 KB of shared memory on the
     // 96^3 grid); FP32: four of 8 warps (64 registers).  Independent CTAs overlap one CTA's loads and
-    // barriers with another's transforms (one 16-warp CTA per SM was 15 % / 7 % slower).
+    // barriers with another's transforms.
+    constexpr int P = plane_lanes<T, N>();
     if constexpr (std::is_same<T, double2>::value) {
-        smem_attr(k_plane_r<T, R, N, 8, 2>, smem);
-        k_plane_r<T, R, N, 8, 2><<<dim3(nb, g.nz), 8 * 32, smem, s>>>(g.plane_view(), g.nz, rtp<T>(g.ax), vperm, sb);
+        smem_attr(k_plane_p<T, R, N, P, 8, 2>, smem);
+        k_plane_p<T, R, N, P, 8, 2><<<dim3(nb, g.nz), 8 * 32, smem, s>>>(g.plane_view(), g.nz, rtp<T>(g.ax), vperm, sb);
     } else {
-        smem_attr(k_plane_r<T, R, N, 8, 4>, smem);
-        k_plane_r<T, R, N, 8, 4><<<dim3(nb, g.nz), 8 * 32, smem, s>>>(g.plane_view(), g.nz, rtp<T>(g.ax), vperm, sb);
+        smem_attr(k_plane_p<T, R, N, P, 8, 4>, smem);
+        k_plane_p<T, R, N, P, 8, 4><<<dim3(nb, g.nz), 8 * 32, smem, s>>>(g.plane_view(), g.nz, rtp<T>(g.ax), vperm, sb);
     }
     note_launch();
     B200_CUDA(cudaGetLastError());
@@ -786,7 +912,16 @@ bool plane_perm_supported(const PWGrid& g) {
 template <typename R>
 bool launch_permute_veff(const PWGrid& g, const R* veff_zyx, R* out, cudaStream_t s) {
     if (!plane_perm_supported(g)) return false;
-    k_permute_veff<R><<<1184, 256, 0, s>>>(g.nz, g.nx, g.nx / 32, g.nz / 32, veff_zyx, out);
+    // x and y in the slot order of the plane pass's P-lane transforms, z in that of the 32-lane z passes
+    using T = typename std::conditional<std::is_same<R, double>::value, double2, float2>::type;
+    int P = 8;
+    switch (g.nx) {
+        case 64: P = plane_lanes<T, 64>(); break;
+        case 96: P = plane_lanes<T, 96>(); break;
+        default: P = plane_lanes<T, 128>(); break;
+    }
+    const int lp = P == 8 ? 3 : P == 16 ? 4 : 5;
+    k_permute_veff<R><<<1184, 256, 0, s>>>(g.nz, g.nx, lp, g.nz / 32, veff_zyx, out);
     note_launch();
     B200_CUDA(cudaGetLastError());
     return true;
