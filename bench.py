@@ -10,9 +10,14 @@ psi + hpsi + projectors (about 690 MB) exceed the 126 MB L2, so no flush is
 needed between steps.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--skip-david] [--skip-216] [--skip-kbatch] [--skip-serve] [--skip-cpu]
+                  [--skip-david] [--skip-216] [--skip-kbatch] [--skip-serve] [--skip-cpu] [--gemm-only]
 
 Besides the headline line, the same JSON line carries:
+  e2e           the same H|psi> from pinned host psi to pinned host hpsi through b200_hamilt_hpsi_host
+                (uploads, H|psi> pieces and downloads overlapped);
+  psi_to_rho    rho(r) += w|psi(r)|^2 over the 160 bands (ElecStatePW::psiToRho);
+  tc_gemm       the 3xTF32 tensor-core complex GEMM on the 216-atom subspace shapes and the projector
+                shapes (--gemm-only runs only this, for profiling);
   davidson      FP64 vs mixed Davidson on the 64-atom cell: wall time to thr 1e-9 and the time after which
                 every eigenvalue stays within 1e-8 Ry of an FP64 solve to 1e-11 (per-iteration traces);
   davidson_216  the same on the 216-atom cell (128^3 grid, 480 bands, 1728 projectors);
@@ -334,7 +339,7 @@ def run_ours(args, ws, rank, local):
                    "l2": "inputs larger than L2 (psi+hpsi+projectors ~690 MB), no flush"},
         "mixed": {"value": ws * nb / (ms32 * 1e-3), "unit": "bands/s", "ms_per_step": ms32,
                   "dtype": "f32 FFT + f32 projector GEMM"},
-        "roofline": {"kernel": "fused local H|psi> FP64 (k_zinv_r + k_plane_r + k_zfwd_r, 9 band chunks)",
+        "roofline": {"kernel": "fused local H|psi> FP64 (k_zinv_r + k_plane_p + k_zfwd_r, 9 band chunks)",
                      "bound": "hbm", "achieved": ach64, "peak": hbm_peak, "unit": "GB/s",
                      "frac": ach64 / hbm_peak, "peak_kind": peak_kind,
                      "traffic": NCU_TRAFFIC_LOCAL_FP64,
