@@ -39,7 +39,16 @@ __global__ void k_nonlocal_kmajor(int l1, int nb, int l3, int sum, int iat, int 
 
 HpsiWork::HpsiWork() { B200_CUBLAS(cublasCreate(&cublas)); }
 HpsiWork::~HpsiWork() {
+    if (side) cudaStreamSynchronize(side);
     if (cublas) cublasDestroy(cublas);
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    if (ev_join) cudaEventDestroy(ev_join);
+    if (side) cudaStreamDestroy(side);
+}
+void HpsiWork::ensure_side() {
+    if (!side) B200_CUDA(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
+    if (!ev_fork) B200_CUDA(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+    if (!ev_join) B200_CUDA(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
 }
 
 Hamilt::Hamilt(PWGrid* g, int prec) : grid(g), precision(prec) { nl.resize(g->kmaps.size()); }
@@ -156,7 +165,7 @@ void Hamilt::hpsi(int ik, int spin, int nb, int ld, const T* psi, T* hpsi, int m
     const int npw = grid->kmaps[ik].npw;
     B200_CHECK(nb >= 0 && ld >= npw, kInvalidArgument, "ld smaller than npwk or negative band count");
     if (nb == 0) return;
-    if (mode != 2) {
+    auto local_pass = [&](cudaStream_t st) {
         B200_CHECK(has_veff, kInvalidArgument, "V_eff not set");
         const R* veff = f64 ? (const R*)veff_zyx.ptr : (const R*)veff_zyxf.ptr;
         const int chunk = band_chunk(sizeof(T));
@@ -173,13 +182,15 @@ void Hamilt::hpsi(int ik, int spin, int nb, int ld, const T* psi, T* hpsi, int m
         for (int b0 = 0; b0 < nb; b0 += chunk) {
             const int nbc = nb - b0 < chunk ? nb - b0 : chunk;
             launch_hpsi_local<T, R>(*grid, ik, veff, veff_perm_of<R>(), nbc, ld, psi + size_t(b0) * ld,
-                                    hpsi + size_t(b0) * ld, sb,
-                                    grid->basis.tpiba2, 0, s);
+                                    hpsi + size_t(b0) * ld, sb, grid->basis.tpiba2, 0, st);
         }
-    }
-    if (mode == 1) return;
+    };
     const NonlocalK& k = nl[ik];
-    if (k.nkb <= 0) return;
+    const bool with_nl = mode != 1 && k.nkb > 0;
+    if (!with_nl) {
+        if (mode != 2) local_pass(s);
+        return;
+    }
     const int nkb = k.nkb;
     T* becp;
     T* ps;
@@ -198,55 +209,76 @@ void Hamilt::hpsi(int ik, int spin, int nb, int ld, const T* psi, T* hpsi, int m
     const R* d = f64 ? (const R*)deeq.ptr : (const R*)deeqf.ptr;
     B200_CHECK(d != nullptr, kInvalidArgument, "deeq not set");
     B200_CHECK(spin >= 0 && spin < nspin, kInvalidArgument, "spin out of range");
-    if constexpr (f64) {
-        const T* vkb = (const T*)k.vkb.ptr;
-        B200_CUBLAS(cublasSetStream(cublas, s));
-        // becp = vkb^H psi (Nonlocal::act, nonlocal_pw.cpp:261-276)
-        B200_CUBLAS(Blas<T>::gemm(cublas, CUBLAS_OP_C, CUBLAS_OP_N, nkb, nb, npw, &one, vkb, k.npwx, psi, ld, &zero, becp,
-                                  nkb));
-        // ps = D becp per atom type (add_nonlocal_pp, nonlocal_pw.cpp:64-110)
-        B200_CUDA(cudaMemsetAsync(ps, 0, size_t(nkb) * nb * sizeof(T), s));
-        int sum = 0, iat = 0;
-        for (int it = 0; it < ntype; ++it)
-            nonlocal_pw<T, R>(na[it], nb, nh[it], sum, iat, spin, nkb, dx, dy, dz, d, ps, becp, s);
-        B200_CHECK(sum == nkb, kInvalidArgument, "sum of na*nh over types differs from nkb");
-        // hpsi += vkb ps^T (nonlocal_pw.cpp:190-205)
-        B200_CUBLAS(Blas<T>::gemm(cublas, CUBLAS_OP_N, CUBLAS_OP_T, npw, nb, nkb, &one, vkb, k.npwx, ps, nb, &one, hpsi,
-                                  ld));
-    } else {
-        // mixed precision: both projector products on the tensor cores (3xTF32), ps kept in becp's layout
-        const float2* psi_b = psi;
-        int ldb = ld;
-        if (ld & 1) {  // the TMA row pitch must be a multiple of 16 bytes: stage psi with an even pitch
-            ldb = ld + 1;
-            psi_pad32.resize(size_t(nb) * ldb);
-            B200_CUDA(cudaMemcpy2DAsync(psi_pad32.ptr, size_t(ldb) * sizeof(float2), psi, size_t(ld) * sizeof(float2),
-                                        size_t(npw) * sizeof(float2), nb, cudaMemcpyDeviceToDevice, s));
-            psi_b = psi_pad32.ptr;
-        }
-        const int ldps = nkb + (nkb & 1);
+    const int ldps = f64 ? nkb : nkb + (nkb & 1);
+    if constexpr (!f64) {
         if (ldps != nkb) {
             becp32.resize(size_t(ldps) * nb);
             ps32.resize(size_t(ldps) * nb);
             becp = becp32.ptr;
             ps = ps32.ptr;
         }
-        tc_cgemm('C', nkb, nb, npw, one, k.vkbf.ptr, k.ldf, psi_b, ldb, zero, becp, ldps, tcw, s);
-        int sum = 0, iat = 0;
-        for (int it = 0; it < ntype; ++it) {
-            const long total = long(na[it]) * nh[it] * nb;
-            if (total > 0) {
-                int blocks = int((total + 255) / 256);
-                if (blocks > 148 * 8) blocks = 148 * 8;
-                k_nonlocal_kmajor<T, R><<<blocks, 256, 0, s>>>(na[it], nb, nh[it], sum, iat, spin, ldps, dx, dy, dz, d, ps,
-                                                              becp);
-                note_launch();
-                B200_CUDA(cudaGetLastError());
+    }
+    // first half of Nonlocal::act, which reads only psi: becp = vkb^H psi (nonlocal_pw.cpp:261-276) and
+    // ps = D becp per atom type (add_nonlocal_pp, nonlocal_pw.cpp:64-110)
+    auto projections = [&](cudaStream_t st) {
+        if constexpr (f64) {
+            const T* vkb = (const T*)k.vkb.ptr;
+            B200_CUBLAS(cublasSetStream(cublas, st));
+            B200_CUBLAS(Blas<T>::gemm(cublas, CUBLAS_OP_C, CUBLAS_OP_N, nkb, nb, npw, &one, vkb, k.npwx, psi, ld, &zero,
+                                      becp, nkb));
+            B200_CUDA(cudaMemsetAsync(ps, 0, size_t(nkb) * nb * sizeof(T), st));
+            int sum = 0, iat = 0;
+            for (int it = 0; it < ntype; ++it)
+                nonlocal_pw<T, R>(na[it], nb, nh[it], sum, iat, spin, nkb, dx, dy, dz, d, ps, becp, st);
+            B200_CHECK(sum == nkb, kInvalidArgument, "sum of na*nh over types differs from nkb");
+        } else {
+            // mixed precision: both projector products on the tensor cores (3xTF32), ps kept in becp's layout
+            const float2* psi_b = psi;
+            int ldb = ld;
+            if (ld & 1) {  // the TMA row pitch must be a multiple of 16 bytes: stage psi with an even pitch
+                ldb = ld + 1;
+                psi_pad32.resize(size_t(nb) * ldb);
+                B200_CUDA(cudaMemcpy2DAsync(psi_pad32.ptr, size_t(ldb) * sizeof(float2), psi, size_t(ld) * sizeof(float2),
+                                            size_t(npw) * sizeof(float2), nb, cudaMemcpyDeviceToDevice, st));
+                psi_b = psi_pad32.ptr;
             }
-            sum += na[it] * nh[it];
-            iat += na[it];
+            tc_cgemm('C', nkb, nb, npw, one, k.vkbf.ptr, k.ldf, psi_b, ldb, zero, becp, ldps, tcw, st);
+            int sum = 0, iat = 0;
+            for (int it = 0; it < ntype; ++it) {
+                const long total = long(na[it]) * nh[it] * nb;
+                if (total > 0) {
+                    int blocks = int((total + 255) / 256);
+                    if (blocks > 148 * 8) blocks = 148 * 8;
+                    k_nonlocal_kmajor<T, R><<<blocks, 256, 0, st>>>(na[it], nb, nh[it], sum, iat, spin, ldps, dx, dy, dz,
+                                                                   d, ps, becp);
+                    note_launch();
+                    B200_CUDA(cudaGetLastError());
+                }
+                sum += na[it] * nh[it];
+                iat += na[it];
+            }
+            B200_CHECK(sum == nkb, kInvalidArgument, "sum of na*nh over types differs from nkb");
         }
-        B200_CHECK(sum == nkb, kInvalidArgument, "sum of na*nh over types differs from nkb");
+    };
+    if (mode == 2) {
+        projections(s);
+    } else {
+        // the projections run on a second stream beside the local pass (they read psi only); hpsi += vkb ps
+        // waits for both
+        W.ensure_side();
+        B200_CUDA(cudaEventRecord(W.ev_fork, s));
+        B200_CUDA(cudaStreamWaitEvent(W.side, W.ev_fork, 0));
+        projections(W.side);
+        B200_CUDA(cudaEventRecord(W.ev_join, W.side));
+        local_pass(s);
+        B200_CUDA(cudaStreamWaitEvent(s, W.ev_join, 0));
+    }
+    // hpsi += vkb ps^T (nonlocal_pw.cpp:190-205)
+    if constexpr (f64) {
+        B200_CUBLAS(cublasSetStream(cublas, s));
+        B200_CUBLAS(Blas<T>::gemm(cublas, CUBLAS_OP_N, CUBLAS_OP_T, npw, nb, nkb, &one, (const T*)k.vkb.ptr, k.npwx, ps,
+                                  nb, &one, hpsi, ld));
+    } else {
         tc_cgemm('N', npw, nb, nkb, one, k.vkbf.ptr, k.ldf, ps, ldps, one, hpsi, ld, tcw, s);
     }
 }

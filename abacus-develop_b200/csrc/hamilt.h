@@ -33,6 +33,10 @@ struct HpsiWork {
     DeviceArray<float2> sb32, becp32, ps32, psi_pad32;
     cublasHandle_t cublas = nullptr;
     TcGemmWorkspace tcw;
+    // second stream of an H|psi>: the projections (becp, D becp) run on it beside the local pass
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    void ensure_side();
     HpsiWork();
     ~HpsiWork();
     HpsiWork(const HpsiWork&) = delete;
