@@ -44,9 +44,16 @@ extern "C" int b200_hamilt_hpsi_host(b200_hamilt* h, int ik, int spin, int nband
         }
         const bool f64 = H->precision == B200_PREC_FP64;
         const size_t row = size_t(ld) * (f64 ? sizeof(double2) : sizeof(float2));  // bytes of one band
+        // piece boundaries: the first and the last piece are half as large as the others (the first upload
+        // and the last download are the two copies nothing overlaps), so the P pieces weigh 1, 2, ..., 2, 1
+        auto bound = [&](int p) -> int {
+            if (p <= 0) return 0;
+            if (p >= P) return nbands;
+            return int(long(nbands) * (2 * p - 1) / (2 * (P - 1)));
+        };
         auto piece = [&](int p, int& b0, int& b1) {
-            b0 = int(long(p) * nbands / P);
-            b1 = int(long(p + 1) * nbands / P);
+            b0 = bound(p);
+            b1 = bound(p + 1);
         };
         // the copies start after the work already queued on the caller's stream (which may still use the
         // device buffers)

@@ -48,9 +48,10 @@ ROOT = Path(__file__).resolve().parent
 WORKLOAD_NAME = ("64-atom diamond supercell a=20.52 bohr, ecut 50 Ry, 96^3 grid, npw 51627, "
                  "160 bands, 512 projectors, Gamma")
 METRIC = "H|psi> bands/s (FP64) + Davidson time-to-1e-8 Ry, mixed vs FP64"
-# band pieces of the end-to-end H|psi> pipeline: 5 pieces of 32 bands (about two 48 MB band chunks of the
-# local pass each; 4, 8 or 10 pieces measured 13-19 % slower on B200)
-E2E_PIECES = 5
+# band pieces of the end-to-end H|psi> pipeline: 6 pieces of 16, 32, 32, 32, 32, 16 bands (the pipeline
+# halves the first and last piece; 32 bands are about two 48 MB band chunks of the local pass); 4, 5, 7, 8,
+# 9 or 11 pieces measured 9-25 % slower on B200
+E2E_PIECES = 6
 # dram__bytes_read.sum + dram__bytes_write.sum of the fused local H|psi> kernels (27 launches: 9 band
 # chunks x 3 passes) for one 160-band FP64 application, from an ncu capture without cache flush (the
 # local-pass traffic summary under profiles/)

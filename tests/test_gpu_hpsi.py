@@ -122,8 +122,12 @@ def test_hpsi_host_pipeline_equals_device_hpsi(pkg, prec, pieces, pinned):
     pdev = ph.cuda()
     h.hpsi(0, pdev, whole, nb, ld)
     P_ = min(pieces, nb)
+
+    def bound(q):  # the pipeline's pieces weigh 1, 2, ..., 2, 1 (half-size first and last pieces)
+        return 0 if q <= 0 else nb if q >= P_ else nb * (2 * q - 1) // (2 * (P_ - 1))
+
     for q in range(P_):
-        b0, b1 = q * nb // P_, (q + 1) * nb // P_
+        b0, b1 = bound(q), bound(q + 1)
         h.hpsi(0, pdev[b0 * ld:], ref_d[b0 * ld:], b1 - b0, ld)
     if pinned:
         ph = ph.pin_memory()
