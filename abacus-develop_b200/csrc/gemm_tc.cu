@@ -40,6 +40,7 @@ namespace {
 constexpr int kBM = 128;     // real rows of C per tile
 constexpr int kBK = 32;      // real K per stage (one 128-byte swizzle row of fp32)
 constexpr int kStages = 4;
+constexpr int kAcc = 2;      // K stages accumulated in one TMEM buffer before it is drained
 constexpr int kThreads = 320;   // warp 0 TMA, warp 1 MMA, warps 2-9 split / drain / store
 constexpr unsigned long long kWaitNs = 2000000000ull;  // 2 s bound on any single wait
 
@@ -167,10 +168,10 @@ static_assert(2 * 128 + 64 * kStages <= 512, "TMEM columns");
 // PRE: B arrives already split (hi and lo tiles from HBM, written once per call by k_split_b)
 //
 // Accumulation: the tensor-core accumulator truncates on every accumulate, so a long
-// chain of MMAs into one TMEM accumulator drifts (about 2e-8 relative per MMA).  Each
-// K stage therefore starts a fresh accumulator in one of two TMEM buffers; the
-// epilogue warps drain the finished buffer into FP32 registers (IEEE round-to-nearest
-// adds) while the next stage runs in the other buffer.
+// chain of MMAs into one TMEM accumulator drifts (about 2e-8 relative per MMA).  Every
+// kAcc K stages (24 MMAs) therefore start a fresh accumulator in one of two TMEM buffers;
+// the epilogue warps drain the finished buffer into FP32 registers (IEEE round-to-nearest
+// adds) while the next group runs in the other buffer.
 template <int BN, int OPA, int PRE>
 __global__ void __launch_bounds__(kThreads, 1)
     k_tc_cgemm(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
@@ -259,13 +260,17 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
     } else if (warp == 1) {
         if (lane == 0) {
-            // MMA issuer: stage i accumulates (fresh) into TMEM buffer i & 1; A from TMEM, B from shared memory
+            // MMA issuer: the kAcc stages of group i / kAcc accumulate (fresh at the group's first stage) into
+            // TMEM buffer (i / kAcc) & 1; A from TMEM, B from shared memory
             const unsigned idesc =
                 (1u << 4) | (2u << 7) | (2u << 10) | (unsigned(BN >> 3) << 17) | (unsigned(kBM >> 4) << 24);
             for (int i = 0; i < nk && !*abort_flag; ++i) {
                 const int s = i % kStages;
-                const int bf = i & 1;
-                if (i >= 2 && !mbar_wait(smem_u32(&acc_empty[bf]), ((i >> 1) - 1) & 1)) {
+                const int grp = i / kAcc;
+                const int bf = grp & 1;
+                const bool first = (i % kAcc) == 0;
+                const bool last = (i % kAcc) == kAcc - 1 || i == nk - 1;
+                if (first && grp >= 2 && !mbar_wait(smem_u32(&acc_empty[bf]), ((grp >> 1) - 1) & 1)) {
                     fail(32);
                     break;
                 }
@@ -285,12 +290,12 @@ __global__ void __launch_bounds__(kThreads, 1)
                     const unsigned long long dbh = sdesc(b_hi + kk * 32, 16, 1024, 2);
                     const unsigned long long dbl = sdesc(b_lo + kk * 32, 16, 1024, 2);
                     // small terms first, then the leading product
-                    mma_tf32_ta(d, a_hi + kk * 8, dbl, idesc, kk > 0 ? 1u : 0u);
+                    mma_tf32_ta(d, a_hi + kk * 8, dbl, idesc, (kk > 0 || !first) ? 1u : 0u);
                     mma_tf32_ta(d, a_lo + kk * 8, dbh, idesc, 1u);
                     mma_tf32_ta(d, a_hi + kk * 8, dbh, idesc, 1u);
                 }
                 mma_commit(smem_u32(&empty[s]));
-                mma_commit(smem_u32(&acc_full[bf]));
+                if (last) mma_commit(smem_u32(&acc_full[bf]));
             }
         }
     } else {
@@ -310,9 +315,9 @@ __global__ void __launch_bounds__(kThreads, 1)
 #pragma unroll
         for (int j = 0; j < HB; ++j) acc[j] = 0.f;
         bool ok = true;
-        auto drain = [&](int i) {
-            const int bf = i & 1;
-            ok = ok && mbar_wait(smem_u32(&acc_full[bf]), (i >> 1) & 1);
+        auto drain = [&](int grp) {  // the accumulator of stage group grp
+            const int bf = grp & 1;
+            ok = ok && mbar_wait(smem_u32(&acc_full[bf]), (grp >> 1) & 1);
             if (!ok) {
                 fail(16);
                 return;
@@ -389,10 +394,10 @@ __global__ void __launch_bounds__(kThreads, 1)
             tmem_st_wait();
             tc_fence_before();
             mbar_arrive(smem_u32(&ready[s]));
-            if (i > 0) drain(i - 1);
+            if (i > 0 && i % kAcc == 0) drain(i / kAcc - 1);
             if (!ok) break;
         }
-        if (ok && !*abort_flag && nk > 0) drain(nk - 1);
+        if (ok && !*abort_flag && nk > 0) drain((nk - 1) / kAcc);
         // store (warp-uniform: the shuffles are collective)
         const bool go = __all_sync(0xffffffffu, ok && !*abort_flag && nk > 0);
         if (go) {
