@@ -87,6 +87,32 @@ __global__ void k_gather_cols(int nbase, int nbase_x, int nc, int ldv, const int
     }
 }
 
+// squared norm of each of the nc columns of X (dim rows, stride ld), in FP64; one block per column
+template <typename T>
+__global__ void k_colnorm2(long dim, long ld, const T* __restrict__ X, double* __restrict__ out) {
+    __shared__ double part[32];
+    const T* x = X + long(blockIdx.x) * ld;
+    double acc = 0.0;
+    for (long g = threadIdx.x; g < dim; g += blockDim.x) acc += double(x[g].x) * x[g].x + double(x[g].y) * x[g].y;
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        acc = threadIdx.x < (blockDim.x >> 5) ? part[threadIdx.x] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if (threadIdx.x == 0) out[blockIdx.x] = acc;
+    }
+}
+
+// flag = 1 if a column kept less than a quarter of its squared norm through the projection (G(j, j) is its
+// squared norm after it, n2 before it): the projection cancelled most of the column, so what is left is
+// dominated by rounding and needs a second pass ("twice is enough")
+__global__ void k_reorth_flag(int nc, int ldg, const double2* __restrict__ G, const double* __restrict__ n2,
+                              int* __restrict__ flag) {
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < nc; j += gridDim.x * blockDim.x)
+        if (G[long(j) * ldg + j].x < 0.25 * n2[j]) atomicOr(flag, 1);
+}
+
 template <typename T>
 __global__ void k_refresh_diag(int nband, int nbase_x, const double* __restrict__ e, T* __restrict__ hcc,
                                T* __restrict__ vcc) {
@@ -167,6 +193,8 @@ template <typename T> struct Engine {
     DeviceArray<double> w, ein;
     DeviceArray<R> pc;
     DeviceArray<int> unconv_d, info;
+    DeviceArray<double> cn2;  // FP32 engine: squared column norms before the projection
+    int reorth = 0;           // FP32 engine: second projection passes taken (counted per solve)
     TcGemmWorkspace tcw;
     int lwork = 0;
     std::vector<double> eig_h;
@@ -219,6 +247,7 @@ template <typename T> struct Engine {
         pc.resize(dim);
         unconv_d.resize(nband);
         info.resize(4);
+        if constexpr (kF32) cn2.resize(nband);
         B200_CUDA(cudaMemsetAsync(hcc.ptr, 0, hcc.n * sizeof(T), s));
         B200_CUDA(cudaMemsetAsync(vcc.ptr, 0, vcc.n * sizeof(T), s));
         B200_CUDA(cudaMemsetAsync(basis.ptr, 0, basis.n * sizeof(T), s));
@@ -321,8 +350,9 @@ template <typename T> struct Engine {
         Lin<T>::gemm(cb, a, b, m, n, k, al, A, lda, B, ldb, be, C, ldc);
     }
 
-    // X (dim x nc, stride ld) <- X U^-1 with X^H X = U^H U, U from an FP64 Cholesky
-    void cholqr(T* X, int nc) {
+    // X (dim x nc, stride ld) <- X U^-1 with X^H X = U^H U, U from an FP64 Cholesky; with check, info[2] is
+    // set when a column's squared norm fell below a quarter of cn2 (its value before a projection)
+    void cholqr(T* X, int nc, bool check = false) {
         const T one = cmake<T>(1, 0), zero = cmake<T>(0, 0);
         const long n2 = long(ncp) * nc;
         double2* G = gram64.ptr;
@@ -332,6 +362,11 @@ template <typename T> struct Engine {
         } else {
             gemm(CUBLAS_OP_C, CUBLAS_OP_N, nc, nc, dim, one, X, ld, X, ld, zero, gram.ptr, ncp);
             k_convert<T, double2><<<grid_of(n2), kT, 0, s>>>(n2, gram.ptr, G);
+            note_launch();
+            B200_CUDA(cudaGetLastError());
+        }
+        if (check) {
+            k_reorth_flag<<<grid_of(nc), kT, 0, s>>>(nc, ncp, G, cn2.ptr, info.ptr + 2);
             note_launch();
             B200_CUDA(cudaGetLastError());
         }
@@ -356,15 +391,36 @@ template <typename T> struct Engine {
         }
     }
 
-    // orthonormalise X (dim x nc) against basis[:, :nprev] and within itself
+    // orthonormalise X (dim x nc) against basis[:, :nprev] and within itself: block classical Gram-Schmidt
+    // and Cholesky-QR, twice in the FP64 engine; the FP32 engine (whose result is refined in FP64) takes the
+    // second pass on blocks of 128 bands or more only when the first projection cancelled most of some
+    // column or its Cholesky failed.  The reference orthogonalises each new vector once
+    // (diago_david.cpp, SchmidtOrth); the 216-atom FP32 stage runs the same iterations with one pass as with
+    // two and 10 % faster.
     void orth_block(T* X, int nc, int nprev) {
         const T one = cmake<T>(1, 0), zero = cmake<T>(0, 0), mone = cmake<T>(-1, 0);
+        // small blocks always take both passes: their products are latency-bound, the second pass costs
+        // little, and k-point solves of 32 bands took 15 % more iterations with one
+        const bool adaptive = kF32 && nprev > 0 && nband >= 128;
+        if (adaptive) {
+            k_colnorm2<T><<<nc, 256, 0, s>>>(dim, ld, X, cn2.ptr);
+            note_launch();
+            B200_CUDA(cudaGetLastError());
+            B200_CUDA(cudaMemsetAsync(info.ptr + 2, 0, sizeof(int), s));
+        }
         for (int pass = 0; pass < 2; ++pass) {
             if (nprev > 0) {
                 gemm(CUBLAS_OP_C, CUBLAS_OP_N, nprev, nc, dim, one, basis.ptr, ld, X, ld, zero, lag.ptr, L);
                 gemm(CUBLAS_OP_N, CUBLAS_OP_N, dim, nc, nprev, mone, basis.ptr, ld, lag.ptr, L, one, X, ld);
             }
-            cholqr(X, nc);
+            cholqr(X, nc, adaptive && pass == 0);
+            if (adaptive && pass == 0) {
+                int fl[2] = {0, 0};  // Cholesky info, cancellation flag: either asks for the second pass
+                B200_CUDA(cudaMemcpyAsync(fl, info.ptr + 1, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
+                B200_CUDA(cudaStreamSynchronize(s));
+                if (!fl[0] && !fl[1]) break;
+                ++reorth;
+            }
         }
     }
 
@@ -492,8 +548,10 @@ template <typename T> struct Engine {
                 eig_in[m] = eig_h[m];
             }
             if (verbosity > 0)
-                std::fprintf(stderr, "[david %s] iter %3d nbase %4d notconv %4d max|dE| %.3e  t(hpsi/lin/eig) %.3f %.3f %.3f\n",
-                             kF32 ? "fp32" : "fp64", iter, nbase, notconv, dmax, t_hpsi, t_lin, t_eig);
+                std::fprintf(stderr,
+                             "[david %s] iter %3d nbase %4d notconv %4d max|dE| %.3e  t(hpsi/lin/eig) %.3f %.3f %.3f  "
+                             "second passes %d\n",
+                             kF32 ? "fp32" : "fp64", iter, nbase, notconv, dmax, t_hpsi, t_lin, t_eig, reorth);
             if (notconv == 0 || nbase + notconv > nbase_x || iter == maxiter) {
                 B200_CUDA(cudaMemsetAsync(psi, 0, size_t(nband) * ldpsi * sizeof(T), s));
                 gemm(CUBLAS_OP_N, CUBLAS_OP_N, dim, nband, nbase, one, basis.ptr, ld, vcc.ptr, nbase_x, zero, psi, ldpsi);
@@ -510,6 +568,7 @@ template <typename T> struct Engine {
              int& notconv) {
         int ntry = 0, total = 0;
         notconv = 0;
+        reorth = 0;
         // a fresh subspace, as a newly constructed DiagoDavid has (diago_david.cpp:34-148): the refresh reads
         // columns of vcc that this solve may not have written, so a reused solver must start from zeros
         B200_CUDA(cudaMemsetAsync(hcc.ptr, 0, hcc.n * sizeof(T), s));
@@ -567,10 +626,11 @@ class David : public DavidBase {
                 e32_->set_stream(stream_);
                 e32_->retarget(dim_, pc_.ptr);
             }
-            // the FP32 stage is not the reference's iteration, so its restarts start from the exact Ritz
-            // basis (vcc = I); keeping the reference's stale off-diagonal vcc entries there makes the first
-            // residuals after each restart those of mixed vectors and costs iterations
-            e32_->ref_refresh = false;
+            // the FP32 stage of a block of 128 bands or more restarts from the exact Ritz basis (vcc = I): with
+            // the reference's stale off-diagonal vcc entries the first residuals after each restart are those of
+            // mixed vectors (the 216-atom stage ran 20 % longer); smaller blocks keep the reference's refresh,
+            // with which 32-band k-point solves took 25 iterations instead of 29
+            e32_->ref_refresh = e64_->ref_refresh && nband_ < 128;
             e32_->trace = &trace_;
             e32_->verbosity = verbosity_;
             e32_->hpsi_bands = 0;

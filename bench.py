@@ -651,12 +651,18 @@ def kbatch_bench(pkg, steps):
     h = P.device_hamilt(wl, P.PREC_FP64)
     pcs = [P.precondition_d(wl.basis, ik) for ik in iks]
     for name, prec in (("fp64", P.PREC_FP64), ("mixed", P.PREC_MIXED)):
-        psis = [torch.from_numpy(wl.psi0_h[ik].reshape(-1).copy()).cuda() for ik in iks]
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        eig, its = h.solve_kpoints(iks, pcs, psis, ld, nb, 1e-9, 200, precision=prec, nworkers=8)
-        torch.cuda.synchronize()
-        res[name]["solve_all_k_s"] = time.perf_counter() - t0
+        # two calls, the faster reported: each call builds its 8 workers' solvers (handles, buffers) and drives
+        # 8 host threads that synchronise every iteration, so single calls vary with the shared host cores
+        runs = []
+        for _ in range(2):
+            psis = [torch.from_numpy(wl.psi0_h[ik].reshape(-1).copy()).cuda() for ik in iks]
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            eig, its = h.solve_kpoints(iks, pcs, psis, ld, nb, 1e-9, 200, precision=prec, nworkers=8)
+            torch.cuda.synchronize()
+            runs.append(time.perf_counter() - t0)
+        res[name]["solve_all_k_s"] = min(runs)
+        res[name]["solve_all_k_runs_s"] = runs
         res[name]["solve_iters_mean"] = float(np.mean(its))
         if name == "fp64":
             e64 = eig
