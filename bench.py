@@ -55,7 +55,7 @@ E2E_PIECES = 6
 # dram__bytes_read.sum + dram__bytes_write.sum of the fused local H|psi> kernels (27 launches: 9 band
 # chunks x 3 passes) for one 160-band FP64 application, from an ncu capture without cache flush (the
 # local-pass traffic summary under profiles/)
-NCU_TRAFFIC_LOCAL_FP64 = 643307264
+NCU_TRAFFIC_LOCAL_FP64 = 591453440
 
 
 def load_package():
