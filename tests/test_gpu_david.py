@@ -110,3 +110,43 @@ def test_david_diamond8(pkg, diamond8, prec):
     HX = hp.cpu().numpy().reshape(nband, ld)
     res = np.linalg.norm(HX - e[:, None] * X, axis=1)
     assert np.max(res) < 1e-3
+
+
+@pytest.fixture(scope="module")
+def diamond8_dense(pkg):
+    """8-atom cell: the oracle's H assembled column by column and diagonalised densely (npw 2945)."""
+    spec = pkg.synth.config(0)
+    P = pkg.pwdft
+    wl = P.build_workload(spec)
+    ld = wl.basis.npwk_max
+    npw = int(wl.basis.npwk[0])
+    ref_b = PWBasisKRef(spec.a, wl.cell.latvec, spec.ecut, np.zeros((1, 3)))
+    ref = H.HamiltPWRef(ref_b, 0, wl.veff_h, wl.vkb_h[0][:, :ld], wl.deeq_h, [8], [wl.cell.nat])
+    eye = np.zeros((npw, ld), complex)
+    eye[np.arange(npw), np.arange(npw)] = 1.0
+    hm = np.zeros((npw, npw), complex)
+    for i in range(0, npw, 256):
+        nb = min(256, npw - i)
+        hm[:, i:i + nb] = ref.hpsi(eye[i:i + nb].reshape(-1), nb, ld).reshape(nb, ld)[:, :npw].T
+    return wl, np.linalg.eigvalsh(hm)
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_david_136_bands_match_dense_spectrum(pkg, diamond8_dense, prec):
+    """136 bands (at least 128: the mixed solve's FP32 stage restarts cleanly and orthogonalises each new block
+    once unless the projection cancels most of a column) against the dense spectrum of the oracle's H."""
+    wl, w = diamond8_dense
+    P = pkg.pwdft
+    p = P.PREC_FP64 if prec == "fp64" else P.PREC_MIXED
+    h = P.device_hamilt(wl, p)
+    ld = wl.basis.npwk_max
+    nband = 136
+    pc = P.precondition_d(wl.basis, 0)
+    psi0 = wl.cell.psi0(wl.basis.gplusk_cart(0), nband, ld).reshape(-1)
+    dav = P.DiagoDavid(pc, nband, ld, 4, p)
+    psi = torch.from_numpy(psi0.copy()).cuda()
+    e = np.zeros(nband)
+    dav.diag_hamilt(h, 0, ld, psi, e, 1e-10, 200)
+    assert np.max(np.abs(e - w[:nband])) < 1e-8, np.max(np.abs(e - w[:nband]))
+    it_low, it64, _ = dav.stats()
+    assert (it_low > 0) == (prec == "mixed")
