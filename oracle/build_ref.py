@@ -6,12 +6,15 @@ shared library under oracle/_ref/ (git-ignored) that needs only scipy's bundled 
 
 Compiled from the reference (unchanged, from where they lie):
   source/module_hsolver/diago_david.cpp            the Davidson iteration
+  source/module_hsolver/diago_dav_subspace.cpp     the Davidson-subspace iteration (HSolverPW method "dav_subspace")
+  source/module_hsolver/diag_const_nums.cpp        its constants (one, zero, minus one)
   source/module_hsolver/kernels/math_kernel_op.cpp the CPU BLAS functors it calls (gemm_op, gemv_op, ...)
   source/module_hsolver/kernels/dngvd_op.cpp       dnevx_op / dngvd_op (LAPACK zheevx, zhegvd, ...)
   source/module_base/module_device/memory_op.cpp   resize / set / sync / delete memory ops
   source/module_base/timer.cpp                     ModuleBase::timer::tick
 plus this directory's ref/shim.cpp (process-level services: WARNING_QUIT throws, TITLE is silent, the CPU
-device tag, a one-process reduce_pool) and ref/david_capi.cpp (a C entry point with a callback H|psi>).
+device tag, a one-process reduce_pool, NPROC_IN_POOL = 1, diagH_LAPACK on the reference's dngvd_op) and
+ref/david_capi.cpp, ref/dav_subspace_capi.cpp (C entry points with a callback H|psi>).
 
 The reference calls Fortran BLAS/LAPACK (zgemm_, zheevx_, ...); scipy's OpenBLAS exports the same routines
 under a scipy_ prefix, so the object files' references are renamed with objcopy before linking.
@@ -31,12 +34,14 @@ OUT = HERE / "_ref"
 REF = Path(os.environ.get("ABACUS_REF", "/root/reference")) / "source"
 SOURCES = [
     "module_hsolver/diago_david.cpp",
+    "module_hsolver/diago_dav_subspace.cpp",
+    "module_hsolver/diag_const_nums.cpp",
     "module_hsolver/kernels/math_kernel_op.cpp",
     "module_hsolver/kernels/dngvd_op.cpp",
     "module_base/module_device/memory_op.cpp",
     "module_base/timer.cpp",
 ]
-OWN = [HERE / "ref" / "shim.cpp", HERE / "ref" / "david_capi.cpp"]
+OWN = [HERE / "ref" / "shim.cpp", HERE / "ref" / "david_capi.cpp", HERE / "ref" / "dav_subspace_capi.cpp"]
 
 
 def openblas() -> Path:

@@ -208,6 +208,12 @@ class HamiltPWRef:
         return h.T
 
 
+def precondition_dav_subspace(basis, ik):
+    """h_diag = g2 = |k+G|^2 tpiba2, what update_precondition gives the "dav_subspace" method (hsolver_pw.cpp,
+    update_precondition: the method's own preconditioner is applied in Diago_DavSubspace::cal_grad)."""
+    return basis.gk2_k(ik) * basis.tpiba2
+
+
 def precondition(basis, ik):
     """h_diag = 1 + g2 + sqrt(1 + (g2-1)^2), g2 = |k+G|^2 tpiba2 (hsolver_pw.cpp:567-584)."""
     g2 = basis.gk2_k(ik) * basis.tpiba2

@@ -9,6 +9,11 @@
 // * Parallel_Reduce::reduce_pool (module_base/parallel_reduce.h:21-23): a sum over the processes of a pool;
 //   with one process it leaves the data unchanged.
 // * ModuleBase::Memory::record (module_base/memory.h): bookkeeping of allocated bytes, not kept here.
+// * GlobalV::NPROC_IN_POOL (module_base/global_variable.h): processes in a pool, 1.
+// * DiagoIterAssist<T, CPU>::diagH_LAPACK (module_hsolver/diago_iter_assist.cpp): its body is the
+//   reference's dngvd_op (generalised eigenproblem, all pairs, compiled from dngvd_op.cpp) and a copy of the
+//   first nbands eigenvalues; restated here so that the rest of diago_iter_assist.cpp (the psi / Hamiltonian
+//   layers) is not needed.
 #include <complex>
 #include <stdexcept>
 #include <string>
@@ -18,6 +23,10 @@
 #include "module_base/parallel_reduce.h"
 #include "module_base/tool_quit.h"
 #include "module_base/tool_title.h"
+#include "module_hsolver/diago_iter_assist.h"
+#include "module_hsolver/kernels/dngvd_op.h"
+
+#include <vector>
 
 namespace ModuleBase {
 void WARNING_QUIT(const std::string& file, const std::string& description) {
@@ -40,3 +49,21 @@ template <> void reduce_pool<std::complex<float>>(std::complex<float>*, const in
 template <> void reduce_pool<double>(double&) {}
 template <> void reduce_pool<float>(float&) {}
 }  // namespace Parallel_Reduce
+
+namespace GlobalV {
+int NPROC_IN_POOL = 1;
+}  // namespace GlobalV
+
+namespace hsolver {
+template <typename T, typename Device>
+void DiagoIterAssist<T, Device>::diagH_LAPACK(const int nstart, const int nbands, const T* hcc, const T* scc,
+                                              const int ldh, Real* e, T* vcc) {
+    std::vector<Real> w(nstart, Real(0));
+    dngvd_op<T, Device>()(nullptr, nstart, ldh, hcc, scc, w.data(), vcc);
+    for (int i = 0; i < nbands; ++i) e[i] = w[i];
+}
+template void DiagoIterAssist<std::complex<double>, base_device::DEVICE_CPU>::diagH_LAPACK(
+    int, int, const std::complex<double>*, const std::complex<double>*, int, double*, std::complex<double>*);
+template void DiagoIterAssist<std::complex<float>, base_device::DEVICE_CPU>::diagH_LAPACK(
+    int, int, const std::complex<float>*, const std::complex<float>*, int, float*, std::complex<float>*);
+}  // namespace hsolver

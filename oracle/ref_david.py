@@ -1,5 +1,6 @@
-"""Oracle (test infrastructure only): ctypes access to the reference's own CPU DiagoDavid, compiled from
-the reference sources into oracle/_ref/libref_david.so by oracle/build_ref.py.  Only the tests and the
+"""Oracle (test infrastructure only): ctypes access to the reference's own CPU DiagoDavid and
+Diago_DavSubspace, compiled from the reference sources into oracle/_ref/libref_david.so by
+oracle/build_ref.py.  Only the tests and the
 benchmark's CPU reference arm use it.
 """
 from __future__ import annotations
@@ -51,4 +52,34 @@ def diag(hpsi, precond, nband, dim, david_ndim, ldpsi, psi, eig, thr, maxiter, n
                        eig.ctypes.data_as(C.POINTER(C.c_double)), thr, maxiter, ntry_max, notconv_max, C.byref(it))
     if rc != 0:
         raise RuntimeError("reference DiagoDavid failed: " + lib.ref_last_error().decode())
+    return it.value
+
+
+def dav_subspace(hpsi, precond, nband, dim, david_ndim, ldpsi, psi, eig, thr, maxiter, need_subspace=False, scf=False):
+    """Diago_DavSubspace<complex<double>, CPU>::diag (all bands occupied).  hpsi as for diag; psi and eig are
+    updated in place; returns the iteration count."""
+    lib = _load()
+    if not hasattr(lib, "_ds_ready"):
+        lib.ref_dav_subspace.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_double), _CB, C.c_void_p,
+                                         C.c_void_p, C.POINTER(C.c_double), C.c_double, C.c_int, C.c_int, C.c_int,
+                                         C.POINTER(C.c_int)]
+        lib.ref_dav_subspace.restype = C.c_int
+        lib.ref_dav_subspace_last_error.restype = C.c_char_p
+        lib._ds_ready = True
+    assert psi.dtype == np.complex128 and psi.flags.c_contiguous and eig.dtype == np.float64
+
+    def cb(user, x, hx, nvec, d, i0, i1):
+        m = i1 - i0 + 1
+        X = np.ctypeslib.as_array(C.cast(x, C.POINTER(C.c_double)), shape=(nvec * d * 2,)).view(np.complex128)
+        HX = np.ctypeslib.as_array(C.cast(hx, C.POINTER(C.c_double)), shape=(m * d * 2,)).view(np.complex128)
+        HX[:] = hpsi(X.reshape(nvec, d), nvec, d, i0, i1).reshape(-1)
+
+    fn = _CB(cb)
+    pc = np.ascontiguousarray(precond, dtype=np.float64)
+    it = C.c_int()
+    rc = lib.ref_dav_subspace(nband, dim, david_ndim, ldpsi, pc.ctypes.data_as(C.POINTER(C.c_double)), fn, None,
+                              psi.ctypes.data, eig.ctypes.data_as(C.POINTER(C.c_double)), thr, maxiter,
+                              int(bool(need_subspace)), int(bool(scf)), C.byref(it))
+    if rc != 0:
+        raise RuntimeError("reference Diago_DavSubspace failed: " + lib.ref_dav_subspace_last_error().decode())
     return it.value
