@@ -106,6 +106,13 @@ _SIGS = {
     "b200_david_set_verbosity": ([vp, i32], i32),
     "b200_david_set_stream": ([vp, vp], i32),
     "b200_david_set_mixed_threshold": ([vp, f64], i32),
+    "b200_dav_subspace_create": ([i32, i32, i32, f64, i32, i32, vp, C.POINTER(vp)], i32),
+    "b200_dav_subspace_destroy": ([vp], i32),
+    "b200_dav_subspace_diag": ([vp, HPSI_CB, vp, vp, i32, pf64, pi32, i32, pi32], i32),
+    "b200_dav_subspace_diag_hamilt": ([vp, vp, i32, i32, vp, i32, pf64, pi32, i32, pi32], i32),
+    "b200_dav_subspace_set_stream": ([vp, vp], i32),
+    "b200_dav_subspace_set_verbosity": ([vp, i32], i32),
+    "b200_dav_subspace_stats": ([vp, pi32, pi32], i32),
 }
 
 _lib = None

@@ -431,4 +431,62 @@ int b200_david_diag_hamilt(b200_david* d, b200_hamilt* h, int ik, int spin, int 
     });
 }
 
+// ------------------------------------------------------------------ Davidson with subspace rotation
+int b200_dav_subspace_create(int nband, int dim, int david_ndim, double diag_thr, int diag_nmax, int need_subspace,
+                             const double* precond, b200_dav_subspace** out) {
+    return guarded([&] {
+        B200_CHECK(out && precond, b200::kInvalidArgument, "NULL argument");
+        auto p = std::make_unique<b200_dav_subspace>();
+        p->d = b200::make_dav_subspace(nband, dim, david_ndim, diag_thr, diag_nmax, need_subspace != 0, precond);
+        *out = p.release();
+    });
+}
+int b200_dav_subspace_destroy(b200_dav_subspace* d) {
+    return guarded([&] { delete d; });
+}
+int b200_dav_subspace_diag(b200_dav_subspace* d, b200_hpsi_cb hpsi, void* user, void* psi, int psi_in_dmax, double* eig,
+                           const int* is_occupied, int scf_type, int* iters) {
+    return guarded([&] {
+        B200_CHECK(d && hpsi && psi && eig, b200::kInvalidArgument, "NULL argument");
+        b200::HPsiDevice f = [hpsi, user](const void* x, void* hx, int nvec, int dim, int i0, int i1, cudaStream_t) {
+            hpsi(user, x, hx, nvec, dim, i0, i1);
+        };
+        const int it = d->d->diag(f, psi, psi_in_dmax, eig, is_occupied, scf_type != 0);
+        if (iters) *iters = it;
+    });
+}
+int b200_dav_subspace_diag_hamilt(b200_dav_subspace* d, b200_hamilt* h, int ik, int spin, void* psi, int psi_in_dmax,
+                                  double* eig, const int* is_occupied, int scf_type, int* iters) {
+    return guarded([&] {
+        B200_CHECK(d && h && psi && eig, b200::kInvalidArgument, "NULL argument");
+        b200::Hamilt* H = h->h.get();
+        b200::HpsiWork* W = &d->work;
+        b200::HPsiDevice f = [H, W, ik, spin](const void* x, void* hx, int, int dim, int i0, int i1, cudaStream_t s) {
+            const double2* X = (const double2*)x + size_t(i0) * dim;
+            H->hpsi<double2>(ik, spin, i1 - i0 + 1, dim, X, (double2*)hx, 0, s, W);
+        };
+        const int it = d->d->diag(f, psi, psi_in_dmax, eig, is_occupied, scf_type != 0);
+        if (iters) *iters = it;
+    });
+}
+int b200_dav_subspace_set_stream(b200_dav_subspace* d, void* stream) {
+    return guarded([&] {
+        B200_CHECK(d != nullptr, b200::kInvalidArgument, "NULL argument");
+        d->d->set_stream(S(stream));
+    });
+}
+int b200_dav_subspace_set_verbosity(b200_dav_subspace* d, int level) {
+    return guarded([&] {
+        B200_CHECK(d != nullptr, b200::kInvalidArgument, "NULL argument");
+        d->d->set_verbosity(level);
+    });
+}
+int b200_dav_subspace_stats(const b200_dav_subspace* d, int* notconv, int* hpsi_bands) {
+    return guarded([&] {
+        B200_CHECK(d != nullptr, b200::kInvalidArgument, "NULL argument");
+        if (notconv) *notconv = d->d->notconv();
+        if (hpsi_bands) *hpsi_bands = d->d->hpsi_bands();
+    });
+}
+
 }  // extern "C"

@@ -3,6 +3,7 @@
 #include <memory>
 #include <vector>
 
+#include "dav_subspace.h"
 #include "david.h"
 #include "hamilt.h"
 #include "pw_grid.h"
@@ -34,5 +35,9 @@ struct b200_hamilt {
 };
 struct b200_david {
     std::unique_ptr<b200::DavidBase> d;
+    b200::HpsiWork work;  // H|psi> scratch used when the solver applies a Hamiltonian handle
+};
+struct b200_dav_subspace {
+    std::unique_ptr<b200::DavSubspaceBase> d;
     b200::HpsiWork work;  // H|psi> scratch used when the solver applies a Hamiltonian handle
 };

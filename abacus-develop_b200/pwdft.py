@@ -535,6 +535,76 @@ class DiagoDavid:
             pass
 
 
+class DiagoDavSubspace:
+    """hsolver::Diago_DavSubspace<T, DEVICE_GPU> (diago_dav_subspace.h:20-40), FP64, one rank.
+
+    precondition_d: device float64 array of dim (HSolverPW passes |k+G|^2 tpiba2 for this method)."""
+
+    def __init__(self, precondition_d, nband, dim, david_ndim, diag_thr, diag_nmax, need_subspace=False):
+        h = _lib.vp()
+        call("b200_dav_subspace_create", nband, dim, david_ndim, float(diag_thr), int(diag_nmax),
+             int(bool(need_subspace)), ptr(precondition_d), C.byref(h))
+        self._h = h
+        self._lib = _lib.load()
+        self.nband = nband
+        self.dim = dim
+
+    def _args(self, psi, psi_in_dmax, eigenvalue, is_occupied):
+        _check_block(psi, True, self.nband, psi_in_dmax, "psi")
+        if len(eigenvalue) < self.nband or eigenvalue.dtype != np.float64:
+            raise ValueError("eigenvalue: need a float64 array of nband entries")
+        occ = None
+        if is_occupied is not None:
+            occ = np.ascontiguousarray(np.asarray(is_occupied, dtype=bool).astype(np.int32))
+            if len(occ) < self.nband:
+                raise ValueError("is_occupied: need nband flags")
+        return occ, (occ.ctypes.data_as(_lib.pi32) if occ is not None else None)
+
+    def diag(self, hpsi_func, psi, psi_in_dmax, eigenvalue, is_occupied=None, scf_type=False):
+        """hpsi_func(x_ptr, hx_ptr, nvec, dim, id_start, id_end) with raw device pointers (HPsiFunc contract).
+        eigenvalue: numpy float64 array of nband (in: ignored; out: the eigenvalues).  Returns the total
+        iteration count."""
+
+        def cb(user, x, hx, nvec, dim, i0, i1):
+            hpsi_func(x, hx, nvec, dim, i0, i1)
+
+        occ, occ_p = self._args(psi, psi_in_dmax, eigenvalue, is_occupied)
+        cfn = _lib.HPSI_CB(cb)
+        it = C.c_int()
+        call("b200_dav_subspace_diag", self._h, cfn, None, ptr(psi), psi_in_dmax,
+             eigenvalue.ctypes.data_as(_lib.pf64), occ_p, int(bool(scf_type)), C.byref(it))
+        return it.value
+
+    def diag_hamilt(self, hamilt: HamiltPW, ik, psi, psi_in_dmax, eigenvalue, is_occupied=None, scf_type=False,
+                    spin=0):
+        occ, occ_p = self._args(psi, psi_in_dmax, eigenvalue, is_occupied)
+        it = C.c_int()
+        call("b200_dav_subspace_diag_hamilt", self._h, hamilt.handle, ik, spin, ptr(psi), psi_in_dmax,
+             eigenvalue.ctypes.data_as(_lib.pf64), occ_p, int(bool(scf_type)), C.byref(it))
+        return it.value
+
+    def set_stream(self, stream):
+        sp = stream.cuda_stream if hasattr(stream, "cuda_stream") else stream
+        call("b200_dav_subspace_set_stream", self._h, sp)
+
+    def set_verbosity(self, level):
+        call("b200_dav_subspace_set_verbosity", self._h, int(level))
+
+    def stats(self):
+        """(unconverged bands, single-band H applications) of the last solve."""
+        a, b = C.c_int(), C.c_int()
+        call("b200_dav_subspace_stats", self._h, C.byref(a), C.byref(b))
+        return a.value, b.value
+
+    def __del__(self):
+        try:
+            if getattr(self, "_h", None):
+                self._lib.b200_dav_subspace_destroy(self._h)
+                self._h = None
+        except Exception:
+            pass
+
+
 # ------------------------------------------------------------------ workloads
 @dataclass
 class Workload:
@@ -581,6 +651,13 @@ def device_hamilt(wl: Workload, precision=PREC_FP64) -> HamiltPW:
         h.set_vkb(ik, vd)
     torch.cuda.synchronize()
     return h
+
+
+def precondition_dav_subspace_d(basis: PWBasisK, ik: int):
+    """h_diag = |k+G|^2 tpiba2, the preconditioner HSolverPW gives Diago_DavSubspace (hsolver_pw.cpp:573-580),
+    as a device FP64 tensor."""
+    torch = _torch()
+    return torch.from_numpy(np.ascontiguousarray(basis.gk2_k(ik) * basis.tpiba2)).cuda()
 
 
 def precondition_d(basis: PWBasisK, ik: int):

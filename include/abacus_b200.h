@@ -38,6 +38,7 @@ extern "C" {
 typedef struct b200_pw_basis b200_pw_basis; /* host + device plane-wave basis of one pool */
 typedef struct b200_hamilt b200_hamilt;     /* V_eff, projectors, D and workspaces */
 typedef struct b200_david b200_david;       /* Davidson workspaces */
+typedef struct b200_dav_subspace b200_dav_subspace; /* Davidson-with-subspace-rotation workspaces */
 typedef struct b200_graph b200_graph;       /* an instantiated CUDA graph of a captured call */
 
 /* Message of the last failed call on this thread ("" if none). */
@@ -317,6 +318,34 @@ int b200_david_set_low_ndim(b200_david* d, int ndim);
  * any may be NULL) of the last solve and sets *n_out to the number recorded. */
 int b200_david_set_trace(b200_david* d, int on);
 int b200_david_trace(b200_david* d, int max_iters, int nband, double* t, int* stage, double* eig, int* n_out);
+
+/* ------------------------------------------------------------------ Davidson with subspace rotation
+ * hsolver::Diago_DavSubspace<T, DEVICE_GPU> (module_hsolver/diago_dav_subspace.h:20-40), FP64:
+ * constructor (precondition, nband, nbasis, david_ndim, diag_thr, diag_nmax, need_subspace, comm) with a
+ * single-rank comm; precondition_d is a device array of dim (HSolverPW passes |k+G|^2 tpiba2 for this
+ * method, hsolver_pw.cpp:573-580).  The subspace problem is the generalised (hcc, scc) one of the
+ * reference's CPU branch (diago_dav_subspace.cpp:628-652). */
+int b200_dav_subspace_create(int nband, int dim, int david_ndim, double diag_thr, int diag_nmax, int need_subspace,
+                             const double* precondition_d, b200_dav_subspace** out);
+int b200_dav_subspace_destroy(b200_dav_subspace* d);
+/* diag(hpsi_func, psi_in, psi_in_dmax, eigenvalue_in, is_occupied, scf_type) (diago_dav_subspace.cpp:804-838):
+ * psi_d: nband complex128 vectors at psi_d + m*psi_in_dmax (psi_in_dmax >= dim), replaced by the Ritz
+ * vectors; eigenvalue: host, nband; is_occupied: host, nband flags, or NULL for all occupied (an empty
+ * band converges at max(5 diag_thr, 1e-5)); scf_type: 1 = SCF (stop once at most 5 bands are unconverged),
+ * 0 = NSCF (retry until all converge, up to 6 tries).  hpsi has the b200_hpsi_cb contract, called with the
+ * solver's own block (vectors at stride dim).  Returns the total iterations in *iters. */
+int b200_dav_subspace_diag(b200_dav_subspace* d, b200_hpsi_cb hpsi, void* user, void* psi_d, int psi_in_dmax,
+                           double* eigenvalue, const int* is_occupied, int scf_type, int* iters);
+/* Same, with H|psi> taken from a Hamiltonian handle at k-point ik. */
+int b200_dav_subspace_diag_hamilt(b200_dav_subspace* d, b200_hamilt* h, int ik, int spin, void* psi_d,
+                                  int psi_in_dmax, double* eigenvalue, const int* is_occupied, int scf_type,
+                                  int* iters);
+/* Stream of all the solver's work (default NULL = legacy default stream); verbosity 1 = one line per
+ * iteration on stderr. */
+int b200_dav_subspace_set_stream(b200_dav_subspace* d, void* stream);
+int b200_dav_subspace_set_verbosity(b200_dav_subspace* d, int level);
+/* Last solve: unconverged bands (the reference's notconv) and single-band H applications. */
+int b200_dav_subspace_stats(const b200_dav_subspace* d, int* notconv, int* hpsi_bands);
 
 /* Davidson solves of nk k-points of one Hamiltonian handle, nworkers at a time on separate streams
  * (the k loop of HSolverPW::solve, hsolver_pw.cpp:240-270, with the k-points running concurrently).

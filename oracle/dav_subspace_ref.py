@@ -99,7 +99,7 @@ class DavSubspaceRef:
             self.vcc[i, i] = 1.0
         return nb
 
-    def _diag_once(self, hpsi, psi, eig):
+    def _diag_once(self, hpsi, psi, eig, occupied):
         nb, dim = self.nband, self.dim
         unconv = list(range(nb))
         self.notconv = nb
@@ -115,7 +115,9 @@ class DavSubspaceRef:
             self._cal_grad(hpsi, nbase, unconv, e_iter)
             nbase = self._cal_elem(nbase, self.notconv)
             e_iter[:nb] = self._diag_zhegvx(nbase, False)
-            unconv = [m for m in range(nb) if not abs(e_iter[m] - eig[m]) < self.thr]
+            # an empty band converges at max(5 thr, 1e-5) (:186-194)
+            thr_m = [self.thr if occupied[m] else max(self.thr * 5.0, 1e-5) for m in range(nb)]
+            unconv = [m for m in range(nb) if not abs(e_iter[m] - eig[m]) < thr_m[m]]
             self.notconv = len(unconv)
             eig[:] = e_iter[:nb]
             if self.notconv == 0 or nbase + self.notconv + 1 > self.nbase_x or it == self.maxiter:
@@ -135,15 +137,16 @@ class DavSubspaceRef:
         psi[:, :dim] = v[:, :nb].T @ x
 
     # ---------------------------------------------------------------- driver
-    def diag(self, hpsi, psi, eig, scf=False):
-        """hpsi(X) -> H X for the rows of X (m x dim); psi (nband x ld, ld >= dim) and eig (nband) in place.
-        Returns the total iteration count."""
+    def diag(self, hpsi, psi, eig, scf=False, occupied=None):
+        """hpsi(X) -> H X for the rows of X (m x dim); psi (nband x ld, ld >= dim) and eig (nband) in place;
+        occupied: nband flags (None: all occupied).  Returns the total iteration count."""
+        occupied = [True] * self.nband if occupied is None else [bool(o) for o in occupied]
         total, ntry = 0, 0
         self.notconv = 0
         while True:
             if self.is_subspace or ntry > 0:
                 self._diagh_subspace(hpsi, psi, eig)
-            total += self._diag_once(hpsi, psi, eig)
+            total += self._diag_once(hpsi, psi, eig, occupied)
             ntry += 1
             f1 = ntry <= 5
             f2 = (not scf) and self.notconv > 0
