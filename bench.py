@@ -21,6 +21,8 @@ Besides the headline line, the same JSON line carries:
   davidson      FP64 vs mixed Davidson on the 64-atom cell: wall time to thr 1e-9 and the time after which
                 every eigenvalue stays within 1e-8 Ry of an FP64 solve to 1e-11 (per-iteration traces);
   davidson_216  the same on the 216-atom cell (128^3 grid, 480 bands, 1728 projectors);
+  dav_subspace  Davidson with subspace rotation (Diago_DavSubspace, FP64) on the 64-atom cell next to
+                DiagoDavid FP64, and on the 8-atom cell next to the reference's compiled CPU solver;
   kbatch        64 uneven k-points of the 8-atom cell: batched H|psi>, per-k calls, CUDA-graph replay,
                 concurrent Davidson of all k-points;
   serving       Poisson arrivals on four resident cells: p50 / p99 latency and throughput at the offered
@@ -360,6 +362,7 @@ def run_ours(args, ws, rank, local):
     line["tc_gemm"] = gemm_bench(P)
     if not args.skip_david:
         line["davidson"] = davidson_bench(P, wl, h64)
+        line["dav_subspace"] = dav_subspace_bench(pkg, P, wl, h64, rank == 0 and ws == 1 and not args.skip_cpu)
     del h32, psi32, hpsi32
     if not args.skip_216:
         del h64, psi, hpsi
@@ -531,6 +534,106 @@ def davidson_bench(P, wl, h64):
     pc = P.precondition_d(wl.basis, 0)
     out = solve_pair(P, h64, pc, nb, ld, wl.psi0_h[0][:nb].reshape(-1))
     out["workload"] = WORKLOAD_NAME
+    return out
+
+
+def dav_subspace_bench(pkg, P, wl, h64, with_cpu):
+    """Diago_DavSubspace (FP64) on the 64-atom cell next to DiagoDavid FP64 from the same orthonormal start
+    (160 bands, david_ndim 4, thr 1e-9, NSCF exit rule), and on the 8-atom cell next to the reference's own
+    CPU Diago_DavSubspace (compiled from its sources, oracle/_ref) on the same inputs."""
+    import torch
+    nb, ld = wl.spec.nbands, wl.basis.npwk_max
+    npw = int(wl.basis.npwk[0])
+    q, _ = np.linalg.qr(wl.psi0_h[0][:nb, :npw].T)
+    psi0 = np.zeros((nb, ld), complex)
+    psi0[:, :npw] = q.T
+    pc_ds = P.precondition_dav_subspace_d(wl.basis, 0)
+    pc_dav = P.precondition_d(wl.basis, 0)
+
+    def run_ds():
+        ds = P.DiagoDavSubspace(pc_ds, nb, npw, 4, 1e-9, 300)
+        x = torch.from_numpy(psi0.reshape(-1).copy()).cuda()
+        e = np.zeros(nb)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        it = ds.diag_hamilt(h64, 0, x, ld, e)
+        torch.cuda.synchronize()
+        return time.perf_counter() - t0, it, e, ds.stats()
+
+    def run_dav():
+        dav = P.DiagoDavid(pc_dav, nb, ld, 4, P.PREC_FP64)
+        x = torch.from_numpy(psi0.reshape(-1).copy()).cuda()
+        e = np.zeros(nb)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        it = dav.diag_hamilt(h64, 0, ld, x, e, 1e-9, 300)
+        torch.cuda.synchronize()
+        return time.perf_counter() - t0, it, e, dav.stats()
+
+    run_ds()  # warm-up
+    ds_runs = [run_ds() for _ in range(2)]
+    dav_runs = [run_dav() for _ in range(2)]
+    ds, dv = min(ds_runs, key=lambda r: r[0]), min(dav_runs, key=lambda r: r[0])
+    out = {"workload": WORKLOAD_NAME + ", thr 1e-9", "dav_subspace_s": ds[0], "dav_subspace_iters": ds[1],
+           "dav_subspace_hpsi_bands": ds[3][1], "david_fp64_s": dv[0], "david_fp64_iters": dv[1],
+           "david_fp64_hpsi_bands": dv[3][2], "max_abs_diff_vs_david_ry": float(np.max(np.abs(ds[2] - dv[2])))}
+    if with_cpu:
+        out["8atom"] = dav_subspace_8atom(pkg)
+    return out
+
+
+def dav_subspace_8atom(pkg):
+    """8-atom cell (npw 2945, 32 bands, thr 1e-9): the device solver against the reference's CPU
+    Diago_DavSubspace on the same orthonormal start, H|psi> of the CPU arm by the numpy port on all cores."""
+    import torch
+    sys.path.insert(0, str(ROOT))
+    from oracle import hamilt_ref as H
+    from oracle import ref_david
+    from oracle.pw_basis_ref import PWBasisKRef
+    P = pkg.pwdft
+    spec = pkg.synth.config(0)
+    wl = P.build_workload(spec)
+    h = P.device_hamilt(wl, P.PREC_FP64)
+    ld, nb = wl.basis.npwk_max, spec.nbands
+    npw = int(wl.basis.npwk[0])
+    q, _ = np.linalg.qr(wl.psi0_h[0][:nb, :npw].T)
+    psi0 = np.zeros((nb, ld), complex)
+    psi0[:, :npw] = q.T
+    pc = P.precondition_dav_subspace_d(wl.basis, 0)
+    best = None
+    for _ in range(3):
+        ds = P.DiagoDavSubspace(pc, nb, npw, 4, 1e-9, 200)
+        x = torch.from_numpy(psi0.reshape(-1).copy()).cuda()
+        e = np.zeros(nb)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        it = ds.diag_hamilt(h, 0, x, ld, e)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        best = dt if best is None else min(best, dt)
+    out = {"gpu_s": best, "gpu_iters": it}
+    if not ref_david.available():
+        return out
+    H.FFT_WORKERS = os.cpu_count() or 1
+    b = PWBasisKRef(spec.a, wl.cell.latvec, spec.ecut, np.zeros((1, 3)))
+    ham = H.HamiltPWRef(b, 0, wl.veff_h, wl.vkb_h[0][:, :ld], wl.deeq_h, [8], [wl.cell.nat])
+
+    def hp(x, nv, d, i0, i1):
+        m = i1 - i0 + 1
+        y = np.zeros((m, ld), complex)
+        y[:, :npw] = x[i0:i1 + 1, :npw]
+        return ham.hpsi(y.reshape(-1), m, ld).reshape(m, ld)[:, :npw]
+
+    e_r, p_r = np.zeros(nb), psi0.copy()
+    t0 = time.perf_counter()
+    it_r = ref_david.dav_subspace(hp, H.precondition_dav_subspace(b, 0), nb, npw, 4, ld, p_r, e_r, 1e-9, 200)
+    cpu_s = time.perf_counter() - t0
+    out.update({"cpu_reference_s": cpu_s, "cpu_reference_iters": it_r,
+                "cpu_reference_cores": H.FFT_WORKERS, "max_abs_diff_vs_reference_ry": float(np.max(np.abs(e - e_r))),
+                "gpu_speedup_vs_cpu_reference": cpu_s / best,
+                "cpu_reference": "Diago_DavSubspace<complex<double>, CPU> compiled from the reference sources "
+                                 "(diago_dav_subspace.cpp, dngvd_op.cpp; scipy OpenBLAS), H|psi> by the numpy port "
+                                 "of the reference functors"})
     return out
 
 
