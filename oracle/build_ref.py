@@ -12,9 +12,16 @@ Compiled from the reference (unchanged, from where they lie):
   source/module_hsolver/kernels/dngvd_op.cpp       dnevx_op / dngvd_op (LAPACK zheevx, zhegvd, ...)
   source/module_base/module_device/memory_op.cpp   resize / set / sync / delete memory ops
   source/module_base/timer.cpp                     ModuleBase::timer::tick
+  source/module_hsolver/diago_bpcg.cpp             the band-parallel CG iteration (HSolverPW method "bpcg")
+  source/module_psi/psi.cpp, module_parameter/parameter.cpp, module_hamilt_general/operator.cpp
+                                                   the psi / global-parameter / operator layer BPCG calls
+  source/module_base/module_container/{ATen/core,ATen/ops,ATen/kernels,base/core}/*.cpp
+                                                   the tensor library BPCG is written in (einsum, BLAS, LAPACK)
 plus this directory's ref/shim.cpp (process-level services: WARNING_QUIT throws, TITLE is silent, the CPU
 device tag, a one-process reduce_pool, NPROC_IN_POOL = 1, diagH_LAPACK on the reference's dngvd_op) and
-ref/david_capi.cpp, ref/dav_subspace_capi.cpp (C entry points with a callback H|psi>).
+ref/david_capi.cpp, ref/dav_subspace_capi.cpp, ref/bpcg_capi.cpp (C entry points with a callback H|psi>).
+ref/include/fftw3.h gives the FFTW type names that a header on BPCG's include chain declares members with
+(FFTW is absent; no FFTW routine is called or linked).
 
 The reference calls Fortran BLAS/LAPACK (zgemm_, zheevx_, ...); scipy's OpenBLAS exports the same routines
 under a scipy_ prefix, so the object files' references are renamed with objcopy before linking.
@@ -40,8 +47,27 @@ SOURCES = [
     "module_hsolver/kernels/dngvd_op.cpp",
     "module_base/module_device/memory_op.cpp",
     "module_base/timer.cpp",
+    # DiagoBPCG and what it stands on: the psi / operator layer and the container tensor library
+    "module_hsolver/diago_bpcg.cpp",
+    "module_psi/psi.cpp",
+    "module_parameter/parameter.cpp",
+    "module_hamilt_general/operator.cpp",
+    "module_base/module_container/ATen/core/tensor.cpp",
+    "module_base/module_container/ATen/core/tensor_map.cpp",
+    "module_base/module_container/ATen/core/tensor_shape.cpp",
+    "module_base/module_container/ATen/core/tensor_buffer.cpp",
+    "module_base/module_container/ATen/core/tensor_types.cpp",
+    "module_base/module_container/ATen/ops/einsum_op.cpp",
+    "module_base/module_container/ATen/ops/linalg_op.cpp",
+    "module_base/module_container/ATen/kernels/blas.cpp",
+    "module_base/module_container/ATen/kernels/lapack.cpp",
+    "module_base/module_container/ATen/kernels/linalg.cpp",
+    "module_base/module_container/ATen/kernels/memory_impl.cpp",
+    "module_base/module_container/base/core/cpu_allocator.cpp",
+    "module_base/module_container/base/core/refcount.cpp",
 ]
-OWN = [HERE / "ref" / "shim.cpp", HERE / "ref" / "david_capi.cpp", HERE / "ref" / "dav_subspace_capi.cpp"]
+OWN = [HERE / "ref" / "shim.cpp", HERE / "ref" / "david_capi.cpp", HERE / "ref" / "dav_subspace_capi.cpp",
+       HERE / "ref" / "bpcg_capi.cpp"]
 
 
 def openblas() -> Path:
@@ -67,10 +93,11 @@ def build(quiet: bool = False) -> Path | None:
     OUT.mkdir(exist_ok=True)
     tmp = OUT / "obj"
     tmp.mkdir(exist_ok=True)
-    flags = ["-std=c++14", "-O2", "-fPIC", "-fopenmp", f"-I{REF}", f"-I{REF / 'module_base/module_container'}"]
+    flags = ["-std=c++14", "-O2", "-fPIC", "-fopenmp", f"-I{HERE / 'ref' / 'include'}", f"-I{REF}",
+             f"-I{REF / 'module_base/module_container'}"]
     objs = []
     for src in [REF / s for s in SOURCES] + OWN:
-        obj = tmp / (src.stem + ".o")
+        obj = tmp / (src.parent.name + "_" + src.stem + ".o")
         run(["g++", *flags, "-c", str(src), "-o", str(obj)])
         objs.append(obj)
     # Fortran BLAS / LAPACK references -> scipy_ names

@@ -1,5 +1,5 @@
-"""Oracle (test infrastructure only): ctypes access to the reference's own CPU DiagoDavid and
-Diago_DavSubspace, compiled from the reference sources into oracle/_ref/libref_david.so by
+"""Oracle (test infrastructure only): ctypes access to the reference's own CPU DiagoDavid,
+Diago_DavSubspace and DiagoBPCG, compiled from the reference sources into oracle/_ref/libref_david.so by
 oracle/build_ref.py.  Only the tests and the
 benchmark's CPU reference arm use it.
 """
@@ -83,3 +83,30 @@ def dav_subspace(hpsi, precond, nband, dim, david_ndim, ldpsi, psi, eig, thr, ma
     if rc != 0:
         raise RuntimeError("reference Diago_DavSubspace failed: " + lib.ref_dav_subspace_last_error().decode())
     return it.value
+
+
+def bpcg(hpsi, precond, nband, nbasis, psi, eig, scf_iter=1, ncalls=1):
+    """DiagoBPCG<complex<double>, CPU>: init_iter on psi (nband x nbasis) and ncalls diag calls with
+    DiagoIterAssist::SCF_ITER = scf_iter.  hpsi(X, nvec, dim, i0, i1) -> H applied to rows i0..i1 of X; psi and
+    eig updated in place."""
+    lib = _load()
+    if not hasattr(lib, "_bp_ready"):
+        lib.ref_bpcg.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_double), _CB, C.c_void_p, C.c_void_p,
+                                 C.POINTER(C.c_double), C.c_int, C.c_int]
+        lib.ref_bpcg.restype = C.c_int
+        lib.ref_bpcg_last_error.restype = C.c_char_p
+        lib._bp_ready = True
+    assert psi.dtype == np.complex128 and psi.flags.c_contiguous and eig.dtype == np.float64
+
+    def cb(user, x, hx, nvec, d, i0, i1):
+        m = i1 - i0 + 1
+        X = np.ctypeslib.as_array(C.cast(x, C.POINTER(C.c_double)), shape=(nvec * d * 2,)).view(np.complex128)
+        HX = np.ctypeslib.as_array(C.cast(hx, C.POINTER(C.c_double)), shape=(m * d * 2,)).view(np.complex128)
+        HX[:] = hpsi(X.reshape(nvec, d), nvec, d, i0, i1).reshape(-1)
+
+    fn = _CB(cb)
+    pc = np.ascontiguousarray(precond, dtype=np.float64)
+    rc = lib.ref_bpcg(nband, nbasis, pc.ctypes.data_as(C.POINTER(C.c_double)), fn, None, psi.ctypes.data,
+                      eig.ctypes.data_as(C.POINTER(C.c_double)), int(scf_iter), int(ncalls))
+    if rc != 0:
+        raise RuntimeError("reference DiagoBPCG failed: " + lib.ref_bpcg_last_error().decode())
