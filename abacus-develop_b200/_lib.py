@@ -113,6 +113,12 @@ _SIGS = {
     "b200_dav_subspace_set_stream": ([vp, vp], i32),
     "b200_dav_subspace_set_verbosity": ([vp, i32], i32),
     "b200_dav_subspace_stats": ([vp, pi32, pi32], i32),
+    "b200_bpcg_create": ([vp, i32, i32, C.POINTER(vp)], i32),
+    "b200_bpcg_destroy": ([vp], i32),
+    "b200_bpcg_diag": ([vp, HPSI_CB, vp, vp, pf64, i32, pi32], i32),
+    "b200_bpcg_diag_hamilt": ([vp, vp, i32, i32, vp, pf64, i32, pi32], i32),
+    "b200_bpcg_set_stream": ([vp, vp], i32),
+    "b200_bpcg_stats": ([vp, pf64, pi32], i32),
 }
 
 _lib = None

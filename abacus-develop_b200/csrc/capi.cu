@@ -489,4 +489,61 @@ int b200_dav_subspace_stats(const b200_dav_subspace* d, int* notconv, int* hpsi_
     });
 }
 
+// ------------------------------------------------------------------ band-parallel CG
+int b200_bpcg_create(const double* precond, int nband, int nbasis, b200_bpcg** out) {
+    return guarded([&] {
+        B200_CHECK(out && precond, b200::kInvalidArgument, "NULL argument");
+        auto p = std::make_unique<b200_bpcg>();
+        p->d = b200::make_bpcg(nband, nbasis, precond);
+        *out = p.release();
+    });
+}
+int b200_bpcg_destroy(b200_bpcg* d) {
+    return guarded([&] { delete d; });
+}
+int b200_bpcg_diag(b200_bpcg* d, b200_hpsi_cb hpsi, void* user, void* psi, double* eig, int scf_iter, int* iters) {
+    return guarded([&] {
+        B200_CHECK(d && hpsi && psi && eig, b200::kInvalidArgument, "NULL argument");
+        b200::HPsiDevice f = [hpsi, user](const void* x, void* hx, int nvec, int dim, int i0, int i1, cudaStream_t) {
+            hpsi(user, x, hx, nvec, dim, i0, i1);
+        };
+        const int it = d->d->diag(f, psi, eig, scf_iter);
+        if (iters) *iters = it;
+    });
+}
+int b200_bpcg_diag_hamilt(b200_bpcg* d, b200_hamilt* h, int ik, int spin, void* psi, double* eig, int scf_iter,
+                          int* iters) {
+    return guarded([&] {
+        B200_CHECK(d && h && psi && eig, b200::kInvalidArgument, "NULL argument");
+        b200::Hamilt* H = h->h.get();
+        B200_CHECK(ik >= 0 && ik < int(H->grid->kmaps.size()), b200::kInvalidArgument, "k-point index out of range");
+        const int npw = H->grid->kmaps[ik].npw;
+        b200::HpsiWork* W = &d->work;
+        b200::HPsiDevice f = [H, W, ik, spin, npw](const void* x, void* hx, int, int dim, int i0, int i1,
+                                                   cudaStream_t s) {
+            const int nb = i1 - i0 + 1;
+            const double2* X = (const double2*)x + size_t(i0) * dim;
+            H->hpsi<double2>(ik, spin, nb, dim, X, (double2*)hx, 0, s, W);
+            if (dim > npw)
+                B200_CUDA(cudaMemset2DAsync((double2*)hx + npw, size_t(dim) * sizeof(double2), 0,
+                                            size_t(dim - npw) * sizeof(double2), nb, s));
+        };
+        const int it = d->d->diag(f, psi, eig, scf_iter);
+        if (iters) *iters = it;
+    });
+}
+int b200_bpcg_set_stream(b200_bpcg* d, void* stream) {
+    return guarded([&] {
+        B200_CHECK(d != nullptr, b200::kInvalidArgument, "NULL argument");
+        d->d->set_stream(S(stream));
+    });
+}
+int b200_bpcg_stats(const b200_bpcg* d, double* max_err, int* hpsi_bands) {
+    return guarded([&] {
+        B200_CHECK(d != nullptr, b200::kInvalidArgument, "NULL argument");
+        if (max_err) *max_err = d->d->max_err();
+        if (hpsi_bands) *hpsi_bands = d->d->hpsi_bands();
+    });
+}
+
 }  // extern "C"

@@ -3,6 +3,7 @@
 #include <memory>
 #include <vector>
 
+#include "bpcg.h"
 #include "dav_subspace.h"
 #include "david.h"
 #include "hamilt.h"
@@ -39,5 +40,9 @@ struct b200_david {
 };
 struct b200_dav_subspace {
     std::unique_ptr<b200::DavSubspaceBase> d;
+    b200::HpsiWork work;  // H|psi> scratch used when the solver applies a Hamiltonian handle
+};
+struct b200_bpcg {
+    std::unique_ptr<b200::BpcgBase> d;
     b200::HpsiWork work;  // H|psi> scratch used when the solver applies a Hamiltonian handle
 };

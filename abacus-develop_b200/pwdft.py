@@ -605,6 +605,63 @@ class DiagoDavSubspace:
             pass
 
 
+class DiagoBPCG:
+    """hsolver::DiagoBPCG<T, DEVICE_GPU> (diago_bpcg.h:18-337), FP64, one rank: the constructor and
+    init_iter(psi) in one (nband, nbasis).  precondition_d: device float64 array of nbasis."""
+
+    def __init__(self, precondition_d, nband, nbasis):
+        h = _lib.vp()
+        call("b200_bpcg_create", ptr(precondition_d), nband, nbasis, C.byref(h))
+        self._h = h
+        self._lib = _lib.load()
+        self.nband = nband
+        self.nbasis = nbasis
+
+    def _check(self, psi, eigenvalue):
+        _check_block(psi, True, self.nband, self.nbasis, "psi")
+        if len(eigenvalue) < self.nband or eigenvalue.dtype != np.float64:
+            raise ValueError("eigenvalue: need a float64 array of nband entries")
+
+    def diag(self, hpsi_func, psi, eigenvalue, scf_iter=1):
+        """hpsi_func(x_ptr, hx_ptr, nvec, dim, id_start, id_end) with raw device pointers (HPsiFunc contract),
+        called for all bands.  scf_iter: DiagoIterAssist::SCF_ITER.  Returns the CG iterations."""
+
+        def cb(user, x, hx, nvec, dim, i0, i1):
+            hpsi_func(x, hx, nvec, dim, i0, i1)
+
+        self._check(psi, eigenvalue)
+        cfn = _lib.HPSI_CB(cb)
+        it = C.c_int()
+        call("b200_bpcg_diag", self._h, cfn, None, ptr(psi), eigenvalue.ctypes.data_as(_lib.pf64), int(scf_iter),
+             C.byref(it))
+        return it.value
+
+    def diag_hamilt(self, hamilt: HamiltPW, ik, psi, eigenvalue, scf_iter=1, spin=0):
+        self._check(psi, eigenvalue)
+        it = C.c_int()
+        call("b200_bpcg_diag_hamilt", self._h, hamilt.handle, ik, spin, ptr(psi),
+             eigenvalue.ctypes.data_as(_lib.pf64), int(scf_iter), C.byref(it))
+        return it.value
+
+    def set_stream(self, stream):
+        sp = stream.cuda_stream if hasattr(stream, "cuda_stream") else stream
+        call("b200_bpcg_set_stream", self._h, sp)
+
+    def stats(self):
+        """(largest residual norm of the last iteration, single-band H applications) of the last diag."""
+        e, n = C.c_double(), C.c_int()
+        call("b200_bpcg_stats", self._h, C.byref(e), C.byref(n))
+        return e.value, n.value
+
+    def __del__(self):
+        try:
+            if getattr(self, "_h", None):
+                self._lib.b200_bpcg_destroy(self._h)
+                self._h = None
+        except Exception:
+            pass
+
+
 # ------------------------------------------------------------------ workloads
 @dataclass
 class Workload:

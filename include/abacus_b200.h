@@ -39,6 +39,7 @@ typedef struct b200_pw_basis b200_pw_basis; /* host + device plane-wave basis of
 typedef struct b200_hamilt b200_hamilt;     /* V_eff, projectors, D and workspaces */
 typedef struct b200_david b200_david;       /* Davidson workspaces */
 typedef struct b200_dav_subspace b200_dav_subspace; /* Davidson-with-subspace-rotation workspaces */
+typedef struct b200_bpcg b200_bpcg;         /* band-parallel CG workspaces */
 typedef struct b200_graph b200_graph;       /* an instantiated CUDA graph of a captured call */
 
 /* Message of the last failed call on this thread ("" if none). */
@@ -346,6 +347,27 @@ int b200_dav_subspace_set_stream(b200_dav_subspace* d, void* stream);
 int b200_dav_subspace_set_verbosity(b200_dav_subspace* d, int level);
 /* Last solve: unconverged bands (the reference's notconv) and single-band H applications. */
 int b200_dav_subspace_stats(const b200_dav_subspace* d, int* notconv, int* hpsi_bands);
+
+/* ------------------------------------------------------------------ band-parallel CG
+ * hsolver::DiagoBPCG<T, DEVICE_GPU> (module_hsolver/diago_bpcg.h:18-337), FP64: the constructor
+ * DiagoBPCG(precondition) and init_iter(psi) (nband, nbasis) in one call; precondition_d: device array
+ * of nbasis (HSolverPW: 1 + g2 + sqrt(1 + (g2 - 1)^2) on the plane waves, 1 on the padding). */
+int b200_bpcg_create(const double* precondition_d, int nband, int nbasis, b200_bpcg** out);
+int b200_bpcg_destroy(b200_bpcg* d);
+/* diag(hamilt, psi, eigenvalue) (diago_bpcg.cpp:254-306) with DiagoIterAssist::SCF_ITER = scf_iter
+ * (1 = the first SCF step: up to 24 iterations with a Rayleigh-Ritz every 4; otherwise up to 4):
+ * psi_d: nband complex128 vectors of nbasis entries, contiguous, replaced; eigenvalue: host, nband;
+ * hpsi: the b200_hpsi_cb contract, always called for all nband vectors (id_start 0, id_end nband-1,
+ * dim = nbasis).  *iters (or NULL): iterations of the CG loop. */
+int b200_bpcg_diag(b200_bpcg* d, b200_hpsi_cb hpsi, void* user, void* psi_d, double* eigenvalue, int scf_iter,
+                   int* iters);
+/* Same, with H|psi> taken from a Hamiltonian handle at k-point ik (entries npwk..nbasis-1 of every H|psi>
+ * zeroed, as the reference's operator chain leaves them). */
+int b200_bpcg_diag_hamilt(b200_bpcg* d, b200_hamilt* h, int ik, int spin, void* psi_d, double* eigenvalue,
+                          int scf_iter, int* iters);
+int b200_bpcg_set_stream(b200_bpcg* d, void* stream);
+/* Last diag: largest residual norm of its last iteration and the single-band H applications. */
+int b200_bpcg_stats(const b200_bpcg* d, double* max_err, int* hpsi_bands);
 
 /* Davidson solves of nk k-points of one Hamiltonian handle, nworkers at a time on separate streams
  * (the k loop of HSolverPW::solve, hsolver_pw.cpp:240-270, with the k-points running concurrently).

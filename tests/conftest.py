@@ -42,3 +42,25 @@ def golden():
     def _load(name):
         return np.load(ROOT / "tests" / "golden" / f"{name}.npz")
     return _load
+
+
+@pytest.fixture(scope="session")
+def diamond8_dense_h(pkg):
+    """8-atom cell (config 0): workload, the oracle's H assembled column by column (npw 2945), its spectrum
+    and the oracle's basis (for the preconditioners)."""
+    import numpy as np
+    from oracle import hamilt_ref as H
+    from oracle.pw_basis_ref import PWBasisKRef
+    spec = pkg.synth.config(0)
+    wl = pkg.pwdft.build_workload(spec)
+    ld = wl.basis.npwk_max
+    npw = int(wl.basis.npwk[0])
+    ref_b = PWBasisKRef(spec.a, wl.cell.latvec, spec.ecut, np.zeros((1, 3)))
+    ref = H.HamiltPWRef(ref_b, 0, wl.veff_h, wl.vkb_h[0][:, :ld], wl.deeq_h, [8], [wl.cell.nat])
+    eye = np.zeros((npw, ld), complex)
+    eye[np.arange(npw), np.arange(npw)] = 1.0
+    hm = np.zeros((npw, npw), complex)
+    for i in range(0, npw, 256):
+        nb = min(256, npw - i)
+        hm[:, i:i + nb] = ref.hpsi(eye[i:i + nb].reshape(-1), nb, ld).reshape(nb, ld)[:, :npw].T
+    return wl, hm, np.linalg.eigvalsh(hm), ref_b

@@ -18,7 +18,6 @@ import scipy.sparse
 
 from oracle import hamilt_ref as H
 from oracle.dav_subspace_ref import DavSubspaceRef
-from oracle.pw_basis_ref import PWBasisKRef
 
 pytestmark = pytest.mark.gpu
 torch = pytest.importorskip("torch")
@@ -102,27 +101,9 @@ def test_dav_subspace_si2_empty_bands(pkg, si2):
     assert abs(it - it_o) <= max(3, it_o // 20), (it, it_o)
 
 
-@pytest.fixture(scope="module")
-def diamond8_dense_h(pkg):
-    """8-atom cell: the oracle's H assembled column by column (npw 2945) and its spectrum."""
-    spec = pkg.synth.config(0)
-    P = pkg.pwdft
-    wl = P.build_workload(spec)
-    ld = wl.basis.npwk_max
-    npw = int(wl.basis.npwk[0])
-    ref_b = PWBasisKRef(spec.a, wl.cell.latvec, spec.ecut, np.zeros((1, 3)))
-    ref = H.HamiltPWRef(ref_b, 0, wl.veff_h, wl.vkb_h[0][:, :ld], wl.deeq_h, [8], [wl.cell.nat])
-    eye = np.zeros((npw, ld), complex)
-    eye[np.arange(npw), np.arange(npw)] = 1.0
-    hm = np.zeros((npw, npw), complex)
-    for i in range(0, npw, 256):
-        nb = min(256, npw - i)
-        hm[:, i:i + nb] = ref.hpsi(eye[i:i + nb].reshape(-1), nb, ld).reshape(nb, ld)[:, :npw].T
-    return wl, hm, np.linalg.eigvalsh(hm), H.precondition_dav_subspace(ref_b, 0)
-
-
 def test_dav_subspace_diamond8_hamilt(pkg, diamond8_dense_h):
-    wl, hm, w, pc_ref = diamond8_dense_h
+    wl, hm, w, ref_b = diamond8_dense_h
+    pc_ref = H.precondition_dav_subspace(ref_b, 0)
     P = pkg.pwdft
     ld = wl.basis.npwk_max
     npw = int(wl.basis.npwk[0])
