@@ -10,10 +10,17 @@ namespace {
 
 constexpr double kTwoPi = 6.283185307179586476925286766559;
 
-// 3x3 helpers on row-major arrays
+// 3x3 helpers on row-major arrays.  The determinant is expanded in ModuleBase::Matrix3::Det's order
+// (module_base/matrix3.cpp:29-37) and a zero determinant replaced by 1 as Matrix3::Inverse does (:44-59), so
+// that G, kvec_c, tpiba and omega carry the reference's bits (a wavefunction file is checked against them
+// exactly, read_wfc_pw.cpp:121-160).
+double det3(const double* a) {
+    return a[0] * a[4] * a[8] - a[0] * a[7] * a[5] + a[3] * a[7] * a[2] - a[3] * a[1] * a[8] + a[6] * a[1] * a[5] -
+           a[6] * a[4] * a[2];
+}
 void inv3(const double* a, double* r) {
-    const double det = a[0] * (a[4] * a[8] - a[5] * a[7]) - a[1] * (a[3] * a[8] - a[5] * a[6]) +
-                       a[2] * (a[3] * a[7] - a[4] * a[6]);
+    double det = det3(a);
+    if (det == 0.0) det = 1.0;
     r[0] = (a[4] * a[8] - a[5] * a[7]) / det;
     r[1] = (a[2] * a[7] - a[1] * a[8]) / det;
     r[2] = (a[1] * a[5] - a[2] * a[4]) / det;
@@ -23,10 +30,6 @@ void inv3(const double* a, double* r) {
     r[6] = (a[3] * a[7] - a[4] * a[6]) / det;
     r[7] = (a[1] * a[6] - a[0] * a[7]) / det;
     r[8] = (a[0] * a[4] - a[1] * a[3]) / det;
-}
-double det3(const double* a) {
-    return a[0] * (a[4] * a[8] - a[5] * a[7]) - a[1] * (a[3] * a[8] - a[5] * a[6]) +
-           a[2] * (a[3] * a[7] - a[4] * a[6]);
 }
 // f . (M f) with M row-major, evaluated as (M*f) then the dot product
 double quad(const double* M, double x, double y, double z) {
@@ -73,6 +76,22 @@ int PWBasisK::setup(double lat0_in, const double* latvec_in, double ecutwfc_in, 
             GGT[i * 3 + j] = s;
         }
     gridecut_lat = ecutrho / tpiba2;
+    const bool explicit_grid = nx_in > 0 && ny_in > 0 && nz_in > 0;
+    if (ecutrho_in < 0.0) {
+        // the cutoff an explicit grid holds (initgrids(lat0, latvec, nx, ny, nz), pw_init.cpp:157-207): the
+        // smallest |G|^2 on the shell just outside the box of half-widths (n-1)/2, less 1e-6
+        if (!explicit_grid) return 1;
+        const int bx = (nx_in - 1) / 2 + 1, by = (ny_in - 1) / 2 + 1, bz = (nz_in - 1) / 2 + 1;
+        double m = 1e20;
+        for (int igz = -bz; igz <= bz; ++igz)
+            for (int igy = -by; igy <= by; ++igy)
+                for (int igx = -bx; igx <= bx; ++igx) {
+                    if (std::abs(igx) <= bx - 1 && std::abs(igy) <= by - 1 && std::abs(igz) <= bz - 1) continue;
+                    m = std::min(m, quad(GGT, igx, igy, igz));
+                }
+        gridecut_lat = m - 1e-6;
+        ecutrho = gridecut_lat * tpiba2;
+    }
     int ibox[3];
     for (int i = 0; i < 3; ++i) {
         const double* l = latvec + 3 * i;
@@ -88,7 +107,7 @@ int PWBasisK::setup(double lat0_in, const double* latvec_in, double ecutwfc_in, 
                     n3 = std::max(n3, std::abs(igz));
                 }
             }
-    if (nx_in > 0 && ny_in > 0 && nz_in > 0) {
+    if (explicit_grid) {
         nx = nx_in;
         ny = ny_in;
         nz = nz_in;

@@ -246,6 +246,10 @@ class PWBasisK:
     def ig2ixyz(self, ik):
         return self._k(ik)[0].astype(np.int64)
 
+    def kvec_c(self, ik):
+        """k-point ik in cartesian units of 2 pi / lat0 (PW_Basis_K::kvec_c)."""
+        return self._k(ik)[3].copy()
+
     def gk2_k(self, ik):
         return self._k(ik)[1]
 

@@ -101,7 +101,8 @@ int b200_set_real_to_recip_output_op_f32(int npw_k, int nxyz, int add, float fac
  * initparameters (pw_basis_k.cpp:53-116), setuptransform + setupIndGk (pw_basis_k.cpp:118-187),
  * collect_local_pw (:189-265) and get_ig2ixyz_k (:319-344).  Builds the host maps and
  * uploads the device stick maps.  nx = ny = nz = 0 selects the reference's 2,3,5-smooth
- * grid rule; ecutrho <= 0 means 4*ecutwfc.  latvec is row-major (rows = a1, a2, a3 in
+ * grid rule; ecutrho == 0 means 4*ecutwfc; ecutrho < 0 with an explicit grid means the cutoff that
+ * grid holds (initgrids(lat0, latvec, nx, ny, nz), pw_init.cpp:157-207).  latvec is row-major (rows = a1, a2, a3 in
  * units of lat0), kvec_d is nks x 3 direct coordinates. */
 int b200_pw_basis_create(double lat0, const double* latvec, double ecutwfc, double ecutrho, int nx, int ny, int nz,
                          int nks, const double* kvec_d, b200_pw_basis** out);

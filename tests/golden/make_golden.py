@@ -13,6 +13,12 @@ reference's unit tests as text and writes ``tests/golden/*.npz``:
   ylm_op.npz       <- source/module_base/kernels/test/math_op_test.cpp
   elecstate_op.npz <- source/module_elecstate/kernels/test/elecstate_op_test.cpp
   pyabacus_si2.npz <- python/pyabacus/tests/test_diag/Si2.mat (sparse H, CSC arrays)
+  wfc_pw.npz       <- source/module_io/test/support/WAVEFUNC1.dat (bytes) + read_wfc_pw_test.cpp's
+                      basis set-up and expected coefficients (one process per pool)
+  cube_chg.npz     <- source/module_io/test_serial/support/SPIN1_CHG.cube (bytes, zlib) + rho_io_test.cpp's
+                      expected Fermi energy, values and trilinear-interpolation values
+  nscf_band.npz    <- source/module_io/test_serial/nscf_band_test.cpp: band energies, k-points and the
+                      expected output line
 
 The fixtures are committed; tests never read the reference tree.
 """
@@ -134,7 +140,62 @@ def main():
                             shape=np.array(csc.shape))
     except Exception as exc:  # pragma: no cover
         print("Si2.mat skipped:", exc, file=sys.stderr)
+    io_fixtures()
     print("golden fixtures written to", OUT)
+
+
+def _expect_doubles(src: str):
+    """(expression, value) of every EXPECT_DOUBLE_EQ(expr, value) in src, in order."""
+    return [(a.strip(), float(b)) for a, b in re.findall(r"EXPECT_DOUBLE_EQ\((.*),\s*(" + _num + r")\s*\);", src)]
+
+
+def io_fixtures():
+    import zlib
+    # plane-wave wavefunction file and the reader's known answers (read_wfc_pw_test.cpp, one process)
+    test = (REF / "source/module_io/test/read_wfc_pw_test.cpp").read_text()
+    body = test[test.index("TEST_F(ReadWfcPwTest, ReadWfcPw)"):test.index("else if (GlobalV::NPROC_IN_POOL == 4)")]
+    exp = _expect_doubles(body)
+    m = re.search(r"initgrids\(\s*(" + _num + r")\s*,\s*ModuleBase::Matrix3\(([^)]*)\)\s*,\s*(\d+)\s*,\s*(\d+)\s*,\s*(\d+)\)", body)
+    lat0, latvec = float(m.group(1)), np.array([float(x) for x in m.group(2).split(",")]).reshape(3, 3)
+    grid = np.array([int(m.group(3)), int(m.group(4)), int(m.group(5))])
+    m2 = re.search(r"initparameters\(\s*false\s*,\s*(" + _num + r")\s*,\s*(\d+)", body)
+    nbands = int(re.search(r"GlobalV::NBANDS\s*=\s*(\d+)", body).group(1))
+    nkstot = int(re.search(r"int nkstot\s*=\s*(\d+)", test).group(1))
+    # wfcatom(ib, ig) with ig = 0 or npwk-1 ("last"): band, which, real/imag, value
+    rows = []
+    for expr, val in exp:
+        mm = re.match(r"wfcatom\((\d+),\s*(0|wfcpw->npwk\[0\] - 1)\)\.(real|imag)\(\)", expr)
+        rows.append((int(mm.group(1)), 0 if mm.group(2) == "0" else -1, 0 if mm.group(3) == "real" else 1, val))
+    raw = (REF / "source/module_io/test/support/WAVEFUNC1.dat").read_bytes()
+    np.savez(OUT / "wfc_pw.npz", raw=np.frombuffer(raw, dtype=np.uint8), lat0=lat0, latvec=latvec, grid=grid,
+             ecutwfc=float(m2.group(1)), nks=int(m2.group(2)), nkstot=nkstot, nbands=nbands,
+             expect=np.array(rows, dtype=np.float64))
+
+    # cube file and the reader's known answers (rho_io_test.cpp)
+    test = (REF / "source/module_io/test_serial/rho_io_test.cpp").read_text()
+    read = _expect_doubles(test[test.index("TEST_F(RhoIOTest, Read)"):test.index("TEST_F(RhoIOTest, TrilinearInterpolate)")])
+    interp = _expect_doubles(test[test.index("TEST_F(RhoIOTest, TrilinearInterpolate)"):])
+    dims = re.findall(r"int n([xyz])(?:_read)?\s*=\s*(\d+);", test[test.index("TEST_F(RhoIOTest, TrilinearInterpolate)"):])
+    raw = (REF / "source/module_io/test_serial/support/SPIN1_CHG.cube").read_bytes()
+    np.savez(OUT / "cube_chg.npz", zraw=np.frombuffer(zlib.compress(raw, 9), dtype=np.uint8),
+             ef=read[0][1], rho_idx=np.array([int(re.search(r"\[(\d+)\]$", e).group(1)) for e, _ in read[1:]]),
+             rho_val=np.array([v for _, v in read[1:]]),
+             interp_dims=np.array([int(v) for _, v in dims[:3]]),
+             interp_idx=np.array([int(re.search(r"\[(\d+)\]", e).group(1)) for e, _ in interp]),
+             interp_val=np.array([v for _, v in interp]))
+
+    # band-structure file line (nscf_band_test.cpp)
+    test = (REF / "source/module_io/test_serial/nscf_band_test.cpp").read_text()
+    ekb = {(int(a), int(b)): float(c) for a, b, c in re.findall(r"ekb\((\d+),\s*(\d+)\)\s*=\s*(" + _num + r");", test)}
+    nks = 1 + max(k[0] for k in ekb)
+    nband = 1 + max(k[1] for k in ekb)
+    kv = [tuple(float(x) for x in g) for g in re.findall(r"kvec_c\[\d\] = ModuleBase::Vector3<double>\((" + _num +
+                                                         r"),\s*(" + _num + r"),\s*(" + _num + r")\)", test)]
+    seg = [int(x) for x in re.findall(r"kl_segids\[\d\] = (\d+);", test)]
+    line = re.search(r'HasSubstr\("([^"]*)"\)', test[test.index("TEST_F(BandTest, nscf_band)"):]).group(1)
+    prec = int(re.search(r"nscf_band\(is, out_band_dir, nband, fermie, (\d+),", test).group(1))
+    np.savez(OUT / "nscf_band.npz", ekb=np.array([[ekb[(k, b)] for b in range(nband)] for k in range(nks)]),
+             kvec_c=np.array(kv), kl_segids=np.array(seg), precision=prec, fermie=0.0, line=np.array(line))
 
 
 if __name__ == "__main__":
