@@ -1,0 +1,101 @@
+"""Non-self-consistent band solve on the device: ESolver_KS_PW::nscf (module_esolver/pw_nscf.cpp:54-200) for one
+pool, norm-conserving pseudopotentials, nspin = 1, fixed occupations.
+
+  1. V_eff from a cube file (``out_pot``; interpolated when its grid differs, read_cube.cpp) or an array;
+  2. the solver threshold from pw_diag_thr / scf_thr / nelec (pw_nscf.cpp:63-68);
+  3. Davidson solves of all k-points on the device (HSolverPW::solve's k loop, the k-points concurrent;
+     NSCF exit rule: every band converged, up to 5 retries, hsolver_pw.cpp:580-593), start vectors from
+     wavefunction files (``init_wfc file``, read_wfc_pw.cpp) or given arrays;
+  4. occupations of an insulator (Occupy::iweights, occupy.cpp:132-186) and the Fermi energy;
+  5. outputs: the eigenvalue block of the running log, the band-structure file (nscf_band.cpp) and, on
+     request, the wavefunction files (write_wfc_pw.cpp).
+The band solve is the library's (b200_solve_kpoints); this module is the host-side driver around it.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+from pathlib import Path
+
+import numpy as np
+
+from . import nscf_io
+from . import pwdft as P
+
+
+def occupation_weights(ekb, wk, nelec):
+    """Occupy::iweights for nspin = 1 (is = -1): the lowest nelec / 2 bands of every k-point carry the k
+    weight, the rest none; E_F is the highest occupied eigenvalue.  Metals (nelec / 2 not an integer) are
+    refused, as the reference refuses fixed occupations for them."""
+    ekb = np.asarray(ekb, dtype=np.float64)
+    ib_mind = nelec / 2.0
+    ib_min = math.ceil(ib_mind)
+    if ib_min != int(ib_mind):
+        raise ValueError("It is not a semiconductor or insulator. Please do not set 'smearing_method=fixed', "
+                         "and try other options.")
+    wg = np.zeros_like(ekb)
+    wg[:, :ib_min] = np.asarray(wk, dtype=np.float64)[:, None]
+    ef = float(np.max(ekb[:, :ib_min])) if ib_min > 0 else -1e10
+    return wg, ef
+
+
+def load_veff_cube(fn, basis):
+    """V_eff(r) of a cube file on the basis's grid (r order), interpolated when the grids differ."""
+    return nscf_io.read_cube(fn, basis.nx, basis.ny, basis.nz).data
+
+
+def read_start_wavefunctions(prefix, basis, nbands, nkstot, latvec):
+    """The start vectors of every k-point from ``<prefix><ik+1>.dat`` (init_wfc file)."""
+    return [nscf_io.read_wfc_pw(f"{prefix}{ik + 1}.dat", basis, ik, nkstot, nbands, latvec) for ik in range(basis.nks)]
+
+
+@dataclass
+class NscfResult:
+    ekb: np.ndarray            # (nks, nbands) Ry
+    wg: np.ndarray             # (nks, nbands) occupation weights
+    ef: float                  # Ry
+    iters: np.ndarray          # Davidson iterations per k-point
+    diag_thr: float
+    psis: list = field(default_factory=list)       # host eigenvectors, (nbands, npwk) per k-point
+    files: dict = field(default_factory=dict)      # written outputs
+    running_lines: list = field(default_factory=list)
+
+
+def run_nscf(hamilt, nbands, psi_init, *, wk, nelec, latvec, ecutwfc, pw_diag_thr=1e-2, scf_thr=1e-9,
+             precision=P.PREC_FP64, david_ndim=4, maxiter=50, nworkers=4, out_dir=None, out_wfc_pw=0,
+             kl_segids=None, band_precision=8):
+    """Solve nbands bands at every k-point of hamilt's basis (V_eff, D and the projectors already set) from the
+    start vectors psi_init[ik] ((nbands, npwk) arrays in the basis's order).  Outputs go to out_dir when it is
+    given: BANDS_1.dat (nscf_band.cpp), running_nscf.log (the eigenvalue block), WAVEFUNC<ik>.dat / .txt
+    (out_wfc_pw 2 / 1)."""
+    import torch
+    basis = hamilt.basis
+    nks, ld = basis.nks, basis.npwk_max
+    thr = nscf_io.nscf_diag_thr(pw_diag_thr, scf_thr, nelec)
+    psis_d, pcs = [], []
+    for ik in range(nks):
+        npw = int(basis.npwk[ik])
+        x = np.zeros((nbands, ld), dtype=np.complex128)
+        x[:, :npw] = np.asarray(psi_init[ik])[:nbands, :npw]
+        psis_d.append(torch.from_numpy(x.reshape(-1)).cuda())
+        pcs.append(P.precondition_d(basis, ik))
+    ekb, its = hamilt.solve_kpoints(list(range(nks)), pcs, psis_d, ld, nbands, thr, maxiter, david_ndim=david_ndim,
+                                    precision=precision, nworkers=nworkers, ntry_max=5, notconv_max=0)
+    torch.cuda.synchronize()
+    psis = [p.cpu().numpy().reshape(nbands, ld)[:, :int(basis.npwk[ik])].copy() for ik, p in enumerate(psis_d)]
+    wg, ef = occupation_weights(ekb, wk, nelec)
+    kvec_c = np.array([basis.kvec_c(ik) for ik in range(nks)])
+    res = NscfResult(ekb=ekb, wg=wg, ef=ef, iters=its, diag_thr=thr, psis=psis)
+    res.running_lines = [f" PW_DIAG_THR  = {thr:g}\n"] + nscf_io.running_band_lines(ekb, wg, kvec_c, nks)
+    if out_dir is not None:
+        d = Path(out_dir)
+        d.mkdir(parents=True, exist_ok=True)
+        seg = np.zeros(nks, dtype=int) if kl_segids is None else kl_segids
+        nscf_io.nscf_band(d / "BANDS_1.dat", ekb, kvec_c, seg, ef, band_precision)
+        res.files["band"] = str(d / "BANDS_1.dat")
+        (d / "running_nscf.log").write_text("".join(res.running_lines))
+        res.files["running"] = str(d / "running_nscf.log")
+        if out_wfc_pw in (1, 2):
+            res.files["wfc"] = nscf_io.write_wfc_pw(str(d / "WAVEFUNC"), basis, psis, kvec_c, wk, ecutwfc, latvec,
+                                                    nbands=nbands, fmt=out_wfc_pw)
+    return res
