@@ -10,8 +10,8 @@
 //    grad = -r / prec + beta / beta_old grad_old (k_bp_grad); grad projected off span(psi) (two GEMMs);
 //    grad_old = grad; H grad; per band grad and H grad normalised and psi <- cos(theta) psi + sin(theta) grad
 //    with theta = |atan(2 e1 / (e0 - e2))| / 2 (k_bp_line_min); psi and H psi made orthonormal through the
-//    upper Cholesky factor of psi^H psi (the reference inverts it with trtri and multiplies; here a
-//    triangular solve applies the inverse); on the first SCF step a Rayleigh-Ritz every 4 iterations;
+//    inverse of the upper Cholesky factor of psi^H psi, as the reference does (trtri, then a GEMM; here the
+//    inverse comes from a triangular solve against I); on the first SCF step a Rayleigh-Ritz every 4 iterations;
 //    stop once no band's err exceeds 1e-5;
 //  * the exit Rayleigh-Ritz (:235-250) on the loop's H psi, psi rotated, its Ritz values returned.
 // Per-band reductions run one CTA per band in a fixed order (deterministic); one host read of the nband
@@ -47,7 +47,7 @@ namespace b200 {
 
 namespace {
 
-constexpr int kBpThreads = 512;
+constexpr int kBpThreads = 1024;
 
 // sum over the CTA of K values per thread (fixed order); every thread gets the sums
 template <int K> __device__ void bp_block_sum(double (&v)[K]) {
@@ -80,10 +80,12 @@ __global__ void __launch_bounds__(kBpThreads) k_bp_grad(long n, const double* __
     double2* p = psi + off;
     double2* hp = hpsi + off;
     double s[1] = {0.0};
+#pragma unroll 4
     for (long i = threadIdx.x; i < n; i += kBpThreads) s[0] += p[i].x * p[i].x + p[i].y * p[i].y;
     bp_block_sum<1>(s);
     const double nrm = 1.0 / sqrt(s[0]);
     double e[1] = {0.0};
+#pragma unroll 4
     for (long i = threadIdx.x; i < n; i += kBpThreads) {
         const double2 a = make_double2(p[i].x * nrm, p[i].y * nrm), b = make_double2(hp[i].x * nrm, hp[i].y * nrm);
         p[i] = a;
@@ -93,6 +95,7 @@ __global__ void __launch_bounds__(kBpThreads) k_bp_grad(long n, const double* __
     bp_block_sum<1>(e);
     const double eps = e[0];
     double rb[2] = {0.0, 0.0};  // sum |r|^2, sum |r|^2 / prec
+#pragma unroll 4
     for (long i = threadIdx.x; i < n; i += kBpThreads) {
         const double rx = hp[i].x - eps * p[i].x, ry = hp[i].y - eps * p[i].y;
         const double r2 = rx * rx + ry * ry;
@@ -103,6 +106,7 @@ __global__ void __launch_bounds__(kBpThreads) k_bp_grad(long n, const double* __
     const double ratio = rb[1] / beta_old;
     double2* g = grad + off;
     const double2* go = grad_old + off;
+#pragma unroll 4
     for (long i = threadIdx.x; i < n; i += kBpThreads) {
         const double rx = hp[i].x - eps * p[i].x, ry = hp[i].y - eps * p[i].y;
         const double q = prec[i];
@@ -124,10 +128,12 @@ __global__ void __launch_bounds__(kBpThreads) k_bp_line_min(long n, double2* __r
     double2* p = psi + off;
     double2* hp = hpsi + off;
     double s[1] = {0.0};
+#pragma unroll 4
     for (long i = threadIdx.x; i < n; i += kBpThreads) s[0] += g[i].x * g[i].x + g[i].y * g[i].y;
     bp_block_sum<1>(s);
     const double nrm = 1.0 / sqrt(s[0]);
     double e[3] = {0.0, 0.0, 0.0};
+#pragma unroll 4
     for (long i = threadIdx.x; i < n; i += kBpThreads) {
         const double2 a = make_double2(g[i].x * nrm, g[i].y * nrm), b = make_double2(hg[i].x * nrm, hg[i].y * nrm);
         g[i] = a;
@@ -140,6 +146,7 @@ __global__ void __launch_bounds__(kBpThreads) k_bp_line_min(long n, double2* __r
     bp_block_sum<3>(e);
     const double theta = 0.5 * fabs(atan(2.0 * e[1] / (e[0] - e[2])));
     const double c = cos(theta), sn = sin(theta);
+#pragma unroll 4
     for (long i = threadIdx.x; i < n; i += kBpThreads) {
         p[i] = make_double2(p[i].x * c + g[i].x * sn, p[i].y * c + g[i].y * sn);
         hp[i] = make_double2(hp[i].x * c + hg[i].x * sn, hp[i].y * c + hg[i].y * sn);
@@ -148,6 +155,11 @@ __global__ void __launch_bounds__(kBpThreads) k_bp_line_min(long n, double2* __r
 
 __global__ void k_bp_fill(long n, double v, double* __restrict__ x) {
     for (long i = blockIdx.x * long(blockDim.x) + threadIdx.x; i < n; i += long(gridDim.x) * blockDim.x) x[i] = v;
+}
+
+__global__ void k_bp_identity(int n, double2* __restrict__ a) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n * n; i += gridDim.x * blockDim.x)
+        a[i] = make_double2(i % n == i / n ? 1.0 : 0.0, 0.0);
 }
 
 class Bpcg : public BpcgBase {
@@ -164,6 +176,7 @@ class Bpcg : public BpcgBase {
         grad_old_.resize(blk);
         work_.resize(blk);
         hsub_.resize(size_t(nb_) * nb_);
+        uinv_.resize(size_t(nb_) * nb_);
         prec_.resize(n_);
         eig_d_.resize(nb_);
         beta_.resize(nb_);
@@ -237,7 +250,7 @@ class Bpcg : public BpcgBase {
     double max_err() const override { return err_h_.empty() ? 0.0 : *std::max_element(err_h_.begin(), err_h_.end()); }
     int hpsi_bands() const override { return hpsi_bands_; }
     size_t device_bytes() const override {
-        return (hpsi_.n + grad_.n + hgrad_.n + grad_old_.n + work_.n + hsub_.n + lw_.n) * sizeof(double2) +
+        return (hpsi_.n + grad_.n + hgrad_.n + grad_old_.n + work_.n + hsub_.n + uinv_.n + lw_.n) * sizeof(double2) +
                (prec_.n + eig_d_.n + beta_.n + err_.n) * sizeof(double);
     }
 
@@ -249,7 +262,7 @@ class Bpcg : public BpcgBase {
     cudaStream_t s_ = 0;
     cublasHandle_t cb_ = nullptr;
     cusolverDnHandle_t cs_ = nullptr;
-    DeviceArray<double2> hpsi_, grad_, hgrad_, grad_old_, work_, hsub_, lw_;
+    DeviceArray<double2> hpsi_, grad_, hgrad_, grad_old_, work_, hsub_, uinv_, lw_;
     DeviceArray<double> prec_, eig_d_, beta_, err_;
     DeviceArray<int> info_;
     int lwork_ = 0;
@@ -301,18 +314,24 @@ class Bpcg : public BpcgBase {
 
     // orth_cholesky (:86-106): psi^H psi = U^H U; psi <- psi U^-1, H psi <- H psi U^-1
     void orth_cholesky(double2* psi) {
-        const double one = 1.0, zero = 0.0;
         auto* S = reinterpret_cast<cuDoubleComplex*>(hsub_.ptr);
-        B200_BP_CUBLAS(cublasZherk(cb_, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_C, nb_, n_, &one,
-                                   reinterpret_cast<const cuDoubleComplex*>(psi), n_, &zero, S, nb_));
+        // S = psi^H psi as a full GEMM (Zgemm3m runs faster than Zherk on these tall shapes; potrf reads the
+        // upper triangle only)
+        gemm(CUBLAS_OP_C, nb_, nb_, n_, 1.0, psi, n_, psi, n_, 0.0, hsub_.ptr, nb_);
         B200_CUDA(cudaMemsetAsync(info_.ptr, 0, sizeof(int), s_));
         B200_BP_CUSOLVER(cusolverDnZpotrf(cs_, CUBLAS_FILL_MODE_UPPER, nb_, S, nb_,
                                           reinterpret_cast<cuDoubleComplex*>(lw_.ptr), lwork_, info_.ptr));
+        // U^-1 (upper, exact zeros below) by a triangular solve against I, then two GEMMs: the tall
+        // triangular solves psi U^-1, H psi U^-1 themselves run well below GEMM speed
         const cuDoubleComplex c1 = make_cuDoubleComplex(1.0, 0.0);
-        B200_BP_CUBLAS(cublasZtrsm(cb_, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, n_,
-                                   nb_, &c1, S, nb_, reinterpret_cast<cuDoubleComplex*>(psi), n_));
-        B200_BP_CUBLAS(cublasZtrsm(cb_, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, n_,
-                                   nb_, &c1, S, nb_, reinterpret_cast<cuDoubleComplex*>(hpsi_.ptr), n_));
+        k_bp_identity<<<ceil_div(long(nb_) * nb_, 256), 256, 0, s_>>>(nb_, uinv_.ptr);
+        check_launch();
+        B200_BP_CUBLAS(cublasZtrsm(cb_, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, nb_,
+                                   nb_, &c1, S, nb_, reinterpret_cast<cuDoubleComplex*>(uinv_.ptr), nb_));
+        gemm(CUBLAS_OP_N, n_, nb_, nb_, 1.0, psi, n_, uinv_.ptr, nb_, 0.0, work_.ptr, n_);
+        B200_CUDA(cudaMemcpyAsync(psi, work_.ptr, work_.n * sizeof(double2), cudaMemcpyDeviceToDevice, s_));
+        gemm(CUBLAS_OP_N, n_, nb_, nb_, 1.0, hpsi_.ptr, n_, uinv_.ptr, nb_, 0.0, work_.ptr, n_);
+        std::swap(hpsi_, work_);
         // info_ is read with the residual norms at the end of the iteration
     }
 };

@@ -100,11 +100,14 @@ __device__ double block_sum(double v) {
 
 // Preconditioned, normalised residual of column m (one block per column, :384-421): x / d(lambda_m), then
 // divided by its 2-norm.  The first pass only reads (the norm), the second reads and writes.
-__global__ void k_ds_precond_normalise(long dim, double2* __restrict__ X, const double* __restrict__ pc,
-                                       const double* __restrict__ lam) {
+constexpr int kDsNormThreads = 1024;
+__global__ void __launch_bounds__(kDsNormThreads) k_ds_precond_normalise(long dim, double2* __restrict__ X,
+                                                                          const double* __restrict__ pc,
+                                                                          const double* __restrict__ lam) {
     double2* x = X + long(blockIdx.x) * dim;
     const double e = lam[blockIdx.x];
     double acc = 0.0;
+#pragma unroll 4
     for (long g = threadIdx.x; g < dim; g += blockDim.x) {
         const double d = ds_denominator(pc[g], e);
         const double2 v = x[g];
@@ -112,6 +115,7 @@ __global__ void k_ds_precond_normalise(long dim, double2* __restrict__ X, const 
         acc += re * re + im * im;
     }
     const double nrm = sqrt(block_sum(acc));
+#pragma unroll 4
     for (long g = threadIdx.x; g < dim; g += blockDim.x) {
         const double d = ds_denominator(pc[g], e);
         const double2 v = x[g];
@@ -349,7 +353,7 @@ class DavSubspace : public DavSubspaceBase {
         double2* X = psi_iter_.ptr + size_t(nbase) * dim_;
         gemm(CUBLAS_OP_N, dim_, nc, nbase, 1.0, psi_iter_.ptr, dim_, vcl_.ptr, nx_, 0.0, X, dim_);
         gemm(CUBLAS_OP_N, dim_, nc, nbase, 1.0, hphi_.ptr, dim_, vc_.ptr, nx_, 1.0, X, dim_);
-        k_ds_precond_normalise<<<nc, kT, 0, s_>>>(dim_, X, pc_.ptr, lam_.ptr);
+        k_ds_precond_normalise<<<nc, kDsNormThreads, 0, s_>>>(dim_, X, pc_.ptr, lam_.ptr);
         check_launch();
         apply_h(f, psi_iter_.ptr, hphi_.ptr + size_t(nbase) * dim_, nbase, nbase + nc - 1);
     }
