@@ -27,23 +27,9 @@
 
 #include "bpcg.h"
 #include "common.h"
+#include "linalg_status.h"
 
 namespace b200 {
-
-#define B200_BP_CUSOLVER(call)                                                                                \
-    do {                                                                                                      \
-        cusolverStatus_t st_ = (call);                                                                        \
-        if (st_ != CUSOLVER_STATUS_SUCCESS)                                                                   \
-            throw ::b200::Error(::b200::kCusolverError, std::string(#call) + " failed with status " +       \
-                                                            std::to_string(int(st_)));                       \
-    } while (0)
-#define B200_BP_CUBLAS(call)                                                                                  \
-    do {                                                                                                      \
-        cublasStatus_t st_ = (call);                                                                          \
-        if (st_ != CUBLAS_STATUS_SUCCESS)                                                                     \
-            throw ::b200::Error(::b200::kCublasError, std::string(#call) + " failed with status " +         \
-                                                          std::to_string(int(st_)));                         \
-    } while (0)
 
 namespace {
 
@@ -166,8 +152,8 @@ class Bpcg : public BpcgBase {
   public:
     Bpcg(int nband, int nbasis, const double* precond_d) : nb_(nband), n_(nbasis) {
         B200_CHECK(nband > 0 && nbasis >= nband, kInvalidArgument, "need 0 < nband <= nbasis");
-        B200_BP_CUBLAS(cublasCreate(&cb_));
-        B200_BP_CUSOLVER(cusolverDnCreate(&cs_));
+        B200_CUBLAS(cublasCreate(&cb_));
+        B200_CUSOLVER(cusolverDnCreate(&cs_));
         set_handles_stream();
         const size_t blk = size_t(nb_) * n_;
         hpsi_.resize(blk);
@@ -185,9 +171,9 @@ class Bpcg : public BpcgBase {
         B200_CUDA(cudaMemcpyAsync(prec_.ptr, precond_d, size_t(n_) * sizeof(double), cudaMemcpyDeviceToDevice, s_));
         int l1 = 0, l2 = 0;
         auto* H = reinterpret_cast<cuDoubleComplex*>(hsub_.ptr);
-        B200_BP_CUSOLVER(cusolverDnZheevd_bufferSize(cs_, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, nb_, H, nb_,
+        B200_CUSOLVER(cusolverDnZheevd_bufferSize(cs_, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, nb_, H, nb_,
                                                      eig_d_.ptr, &l1));
-        B200_BP_CUSOLVER(cusolverDnZpotrf_bufferSize(cs_, CUBLAS_FILL_MODE_UPPER, nb_, H, nb_, &l2));
+        B200_CUSOLVER(cusolverDnZpotrf_bufferSize(cs_, CUBLAS_FILL_MODE_UPPER, nb_, H, nb_, &l2));
         lwork_ = std::max(1, std::max(l1, l2));
         lw_.resize(size_t(lwork_));
         err_h_.assign(nb_, 0.0);
@@ -269,8 +255,8 @@ class Bpcg : public BpcgBase {
     std::vector<double> err_h_;
 
     void set_handles_stream() {
-        B200_BP_CUBLAS(cublasSetStream(cb_, s_));
-        B200_BP_CUSOLVER(cusolverDnSetStream(cs_, s_));
+        B200_CUBLAS(cublasSetStream(cb_, s_));
+        B200_CUSOLVER(cusolverDnSetStream(cs_, s_));
     }
     void check_launch() {
         note_launch();
@@ -279,7 +265,7 @@ class Bpcg : public BpcgBase {
     void gemm(cublasOperation_t a, int m, int n, int k, double al_re, const double2* A, int lda, const double2* B,
               int ldb, double be_re, double2* C, int ldc) {
         const cuDoubleComplex al = make_cuDoubleComplex(al_re, 0.0), be = make_cuDoubleComplex(be_re, 0.0);
-        B200_BP_CUBLAS(cublasZgemm3m(cb_, a, CUBLAS_OP_N, m, n, k, &al, reinterpret_cast<const cuDoubleComplex*>(A), lda,
+        B200_CUBLAS(cublasZgemm3m(cb_, a, CUBLAS_OP_N, m, n, k, &al, reinterpret_cast<const cuDoubleComplex*>(A), lda,
                                      reinterpret_cast<const cuDoubleComplex*>(B), ldb, &be,
                                      reinterpret_cast<cuDoubleComplex*>(C), ldc));
     }
@@ -300,7 +286,7 @@ class Bpcg : public BpcgBase {
         if (apply) apply_h(f, psi, hpsi_.ptr);
         gemm(CUBLAS_OP_C, nb_, nb_, n_, 1.0, psi, n_, hpsi_.ptr, n_, 0.0, hsub_.ptr, nb_);
         B200_CUDA(cudaMemsetAsync(info_.ptr, 0, sizeof(int), s_));
-        B200_BP_CUSOLVER(cusolverDnZheevd(cs_, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, nb_,
+        B200_CUSOLVER(cusolverDnZheevd(cs_, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, nb_,
                                           reinterpret_cast<cuDoubleComplex*>(hsub_.ptr), nb_, eig_d_.ptr,
                                           reinterpret_cast<cuDoubleComplex*>(lw_.ptr), lwork_, info_.ptr));
         gemm(CUBLAS_OP_N, n_, nb_, nb_, 1.0, psi, n_, hsub_.ptr, nb_, 0.0, work_.ptr, n_);
@@ -319,14 +305,14 @@ class Bpcg : public BpcgBase {
         // upper triangle only)
         gemm(CUBLAS_OP_C, nb_, nb_, n_, 1.0, psi, n_, psi, n_, 0.0, hsub_.ptr, nb_);
         B200_CUDA(cudaMemsetAsync(info_.ptr, 0, sizeof(int), s_));
-        B200_BP_CUSOLVER(cusolverDnZpotrf(cs_, CUBLAS_FILL_MODE_UPPER, nb_, S, nb_,
+        B200_CUSOLVER(cusolverDnZpotrf(cs_, CUBLAS_FILL_MODE_UPPER, nb_, S, nb_,
                                           reinterpret_cast<cuDoubleComplex*>(lw_.ptr), lwork_, info_.ptr));
         // U^-1 (upper, exact zeros below) by a triangular solve against I, then two GEMMs: the tall
         // triangular solves psi U^-1, H psi U^-1 themselves run well below GEMM speed
         const cuDoubleComplex c1 = make_cuDoubleComplex(1.0, 0.0);
         k_bp_identity<<<ceil_div(long(nb_) * nb_, 256), 256, 0, s_>>>(nb_, uinv_.ptr);
         check_launch();
-        B200_BP_CUBLAS(cublasZtrsm(cb_, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, nb_,
+        B200_CUBLAS(cublasZtrsm(cb_, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, nb_,
                                    nb_, &c1, S, nb_, reinterpret_cast<cuDoubleComplex*>(uinv_.ptr), nb_));
         gemm(CUBLAS_OP_N, n_, nb_, nb_, 1.0, psi, n_, uinv_.ptr, nb_, 0.0, work_.ptr, n_);
         B200_CUDA(cudaMemcpyAsync(psi, work_.ptr, work_.n * sizeof(double2), cudaMemcpyDeviceToDevice, s_));

@@ -5,6 +5,7 @@
 #include <memory>
 #include <string>
 
+#include "capi_guard.h"
 #include "../../include/abacus_b200.h"
 #include "david.h"
 #include "functors.h"
@@ -28,19 +29,7 @@ unsigned long long launches() { return g_launches.load(std::memory_order_relaxed
 }  // namespace b200
 
 namespace {
-template <typename F> int guarded(F&& f) {
-    try {
-        f();
-        b200::set_last_error("");
-        return B200_STATUS_OK;
-    } catch (const b200::Error& e) {
-        b200::set_last_error(e.what());
-        return e.code;
-    } catch (const std::exception& e) {
-        b200::set_last_error(e.what());
-        return B200_STATUS_INVALID_ARGUMENT;
-    }
-}
+using b200::guarded;
 inline cudaStream_t S(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 }  // namespace
 

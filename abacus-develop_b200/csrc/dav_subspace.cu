@@ -31,24 +31,10 @@
 #include <vector>
 
 #include "common.h"
+#include "linalg_status.h"
 #include "dav_subspace.h"
 
 namespace b200 {
-
-#define B200_DS_CUSOLVER(call)                                                                                \
-    do {                                                                                                      \
-        cusolverStatus_t st_ = (call);                                                                        \
-        if (st_ != CUSOLVER_STATUS_SUCCESS)                                                                   \
-            throw ::b200::Error(::b200::kCusolverError, std::string(#call) + " failed with status " +       \
-                                                            std::to_string(int(st_)));                       \
-    } while (0)
-#define B200_DS_CUBLAS(call)                                                                                  \
-    do {                                                                                                      \
-        cublasStatus_t st_ = (call);                                                                          \
-        if (st_ != CUBLAS_STATUS_SUCCESS)                                                                     \
-            throw ::b200::Error(::b200::kCublasError, std::string(#call) + " failed with status " +         \
-                                                          std::to_string(int(st_)));                         \
-    } while (0)
 
 namespace {
 
@@ -169,8 +155,8 @@ class DavSubspace : public DavSubspaceBase {
         B200_CHECK(ndim > 1 && nband > 0 && ndim * nband < dim, kInvalidArgument,
                    "need david_ndim > 1 and david_ndim*nband < dim");
         B200_CHECK(maxiter > 0 && thr > 0.0, kInvalidArgument, "need diag_nmax > 0 and diag_thr > 0");
-        B200_DS_CUBLAS(cublasCreate(&cb_));
-        B200_DS_CUSOLVER(cusolverDnCreate(&cs_));
+        B200_CUBLAS(cublasCreate(&cb_));
+        B200_CUSOLVER(cusolverDnCreate(&cs_));
         set_handles_stream();
         const size_t nx = size_t(nx_);
         psi_iter_.resize(nx * dim_);
@@ -194,12 +180,12 @@ class DavSubspace : public DavSubspaceBase {
         auto* A = reinterpret_cast<cuDoubleComplex*>(a_.ptr);
         auto* B = reinterpret_cast<cuDoubleComplex*>(b_.ptr);
         int l1 = 0, l2 = 0, l3 = 0, meig = 0;
-        B200_DS_CUSOLVER(cusolverDnZheevd_bufferSize(cs_, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, nb_, A, nx_,
+        B200_CUSOLVER(cusolverDnZheevd_bufferSize(cs_, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, nb_, A, nx_,
                                                      w_.ptr, &l1));
-        B200_DS_CUSOLVER(cusolverDnZhegvdx_bufferSize(cs_, CUSOLVER_EIG_TYPE_1, CUSOLVER_EIG_MODE_VECTOR,
+        B200_CUSOLVER(cusolverDnZhegvdx_bufferSize(cs_, CUSOLVER_EIG_TYPE_1, CUSOLVER_EIG_MODE_VECTOR,
                                                       CUSOLVER_EIG_RANGE_I, CUBLAS_FILL_MODE_UPPER, nx_, A, nx_, B, nx_,
                                                       0.0, 0.0, 1, nb_, &meig, w_.ptr, &l2));
-        B200_DS_CUSOLVER(cusolverDnZhegvd_bufferSize(cs_, CUSOLVER_EIG_TYPE_1, CUSOLVER_EIG_MODE_VECTOR,
+        B200_CUSOLVER(cusolverDnZhegvd_bufferSize(cs_, CUSOLVER_EIG_TYPE_1, CUSOLVER_EIG_MODE_VECTOR,
                                                      CUBLAS_FILL_MODE_UPPER, nb_, A, nb_, B, nb_, w_.ptr, &l3));
         lwork_ = std::max(1, std::max(l1, std::max(l2, l3)));
         work_.resize(size_t(lwork_));
@@ -267,8 +253,8 @@ class DavSubspace : public DavSubspaceBase {
     std::vector<int> unconv_, occ_;
 
     void set_handles_stream() {
-        B200_DS_CUBLAS(cublasSetStream(cb_, s_));
-        B200_DS_CUSOLVER(cusolverDnSetStream(cs_, s_));
+        B200_CUBLAS(cublasSetStream(cb_, s_));
+        B200_CUSOLVER(cusolverDnSetStream(cs_, s_));
     }
     void check_launch() {
         note_launch();
@@ -279,7 +265,7 @@ class DavSubspace : public DavSubspaceBase {
               int ldb, double be_re, double2* C, int ldc) {
         if (m <= 0 || n <= 0) return;
         const cuDoubleComplex al = make_cuDoubleComplex(al_re, 0.0), be = make_cuDoubleComplex(be_re, 0.0);
-        B200_DS_CUBLAS(cublasZgemm3m(cb_, a, CUBLAS_OP_N, m, n, k, &al, reinterpret_cast<const cuDoubleComplex*>(A), lda,
+        B200_CUBLAS(cublasZgemm3m(cb_, a, CUBLAS_OP_N, m, n, k, &al, reinterpret_cast<const cuDoubleComplex*>(A), lda,
                                      reinterpret_cast<const cuDoubleComplex*>(B), ldb, &be,
                                      reinterpret_cast<cuDoubleComplex*>(C), ldc));
     }
@@ -327,13 +313,13 @@ class DavSubspace : public DavSubspaceBase {
                                     cudaMemcpyDeviceToDevice, s_));
         if (init) {
             // standard problem of the nband input vectors (dnevx, :646-655); nbase == nband here
-            B200_DS_CUSOLVER(cusolverDnZheevd(cs_, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, nbase, A, nx_,
+            B200_CUSOLVER(cusolverDnZheevd(cs_, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, nbase, A, nx_,
                                               w_.ptr, reinterpret_cast<cuDoubleComplex*>(work_.ptr), lwork_, info_.ptr));
         } else {
             B200_CUDA(cudaMemcpy2DAsync(b_.ptr, pitch, scc_.ptr, pitch, size_t(nbase) * sizeof(double2), nbase,
                                         cudaMemcpyDeviceToDevice, s_));
             int meig = 0;
-            B200_DS_CUSOLVER(cusolverDnZhegvdx(cs_, CUSOLVER_EIG_TYPE_1, CUSOLVER_EIG_MODE_VECTOR, CUSOLVER_EIG_RANGE_I,
+            B200_CUSOLVER(cusolverDnZhegvdx(cs_, CUSOLVER_EIG_TYPE_1, CUSOLVER_EIG_MODE_VECTOR, CUSOLVER_EIG_RANGE_I,
                                                CUBLAS_FILL_MODE_UPPER, nbase, A, nx_, B, nx_, 0.0, 0.0, 1, nb_, &meig,
                                                w_.ptr, reinterpret_cast<cuDoubleComplex*>(work_.ptr), lwork_,
                                                info_.ptr));
@@ -425,7 +411,7 @@ class DavSubspace : public DavSubspaceBase {
         gemm(CUBLAS_OP_C, nb_, nb_, dim_, 1.0, psi_iter_.ptr, dim_, hphi_.ptr, dim_, 0.0, a_.ptr, nb_);
         gemm(CUBLAS_OP_C, nb_, nb_, dim_, 1.0, psi_iter_.ptr, dim_, psi_iter_.ptr, dim_, 0.0, b_.ptr, nb_);
         B200_CUDA(cudaMemsetAsync(info_.ptr, 0, sizeof(int), s_));
-        B200_DS_CUSOLVER(cusolverDnZhegvd(cs_, CUSOLVER_EIG_TYPE_1, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, nb_,
+        B200_CUSOLVER(cusolverDnZhegvd(cs_, CUSOLVER_EIG_TYPE_1, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, nb_,
                                           reinterpret_cast<cuDoubleComplex*>(a_.ptr), nb_,
                                           reinterpret_cast<cuDoubleComplex*>(b_.ptr), nb_, w_.ptr,
                                           reinterpret_cast<cuDoubleComplex*>(work_.ptr), lwork_, info_.ptr));

@@ -28,26 +28,12 @@
 #include <vector>
 
 #include "common.h"
+#include "linalg_status.h"
 #include "david.h"
 #include "fft_core.cuh"
 #include "gemm_tc.h"
 
 namespace b200 {
-
-#define B200_CUSOLVER(call)                                                                                   \
-    do {                                                                                                      \
-        cusolverStatus_t st_ = (call);                                                                        \
-        if (st_ != CUSOLVER_STATUS_SUCCESS)                                                                   \
-            throw ::b200::Error(::b200::kCusolverError, std::string(#call) + " failed with status " +       \
-                                                            std::to_string(int(st_)));                       \
-    } while (0)
-#define B200_CUBLAS_D(call)                                                                                   \
-    do {                                                                                                      \
-        cublasStatus_t st_ = (call);                                                                          \
-        if (st_ != CUBLAS_STATUS_SUCCESS)                                                                     \
-            throw ::b200::Error(::b200::kCublasError, std::string(#call) + " failed with status " +         \
-                                                          std::to_string(int(st_)));                         \
-    } while (0)
 
 namespace {
 
@@ -136,34 +122,34 @@ template <> struct Lin<double2> {
     // cublasZgemm3m: the same bits as cublasZgemm on these shapes with B200's cuBLAS 12.9, 18-20 % faster
     static void gemm(cublasHandle_t h, cublasOperation_t a, cublasOperation_t b, int m, int n, int k, double2 al,
                      const double2* A, int lda, const double2* B, int ldb, double2 be, double2* C, int ldc) {
-        B200_CUBLAS_D(cublasZgemm3m(h, a, b, m, n, k, (const cuDoubleComplex*)&al, (const cuDoubleComplex*)A, lda,
+        B200_CUBLAS(cublasZgemm3m(h, a, b, m, n, k, (const cuDoubleComplex*)&al, (const cuDoubleComplex*)A, lda,
                                   (const cuDoubleComplex*)B, ldb, (const cuDoubleComplex*)&be, (cuDoubleComplex*)C, ldc));
     }
     static void herk(cublasHandle_t h, int n, int k, const double2* A, int lda, double2* C, int ldc) {
         const double one = 1.0, zero = 0.0;
-        B200_CUBLAS_D(cublasZherk(h, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_C, n, k, &one, (const cuDoubleComplex*)A, lda, &zero,
+        B200_CUBLAS(cublasZherk(h, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_C, n, k, &one, (const cuDoubleComplex*)A, lda, &zero,
                                   (cuDoubleComplex*)C, ldc));
     }
     static void trsm(cublasHandle_t h, int m, int n, const double2* U, int ldu, double2* X, int ldx) {
         const double2 one = make_double2(1.0, 0.0);
-        B200_CUBLAS_D(cublasZtrsm(h, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, m, n,
+        B200_CUBLAS(cublasZtrsm(h, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, m, n,
                                   (const cuDoubleComplex*)&one, (const cuDoubleComplex*)U, ldu, (cuDoubleComplex*)X, ldx));
     }
 };
 template <> struct Lin<float2> {
     static void gemm(cublasHandle_t h, cublasOperation_t a, cublasOperation_t b, int m, int n, int k, float2 al,
                      const float2* A, int lda, const float2* B, int ldb, float2 be, float2* C, int ldc) {
-        B200_CUBLAS_D(cublasCgemm(h, a, b, m, n, k, (const cuComplex*)&al, (const cuComplex*)A, lda, (const cuComplex*)B,
+        B200_CUBLAS(cublasCgemm(h, a, b, m, n, k, (const cuComplex*)&al, (const cuComplex*)A, lda, (const cuComplex*)B,
                                   ldb, (const cuComplex*)&be, (cuComplex*)C, ldc));
     }
     static void herk(cublasHandle_t h, int n, int k, const float2* A, int lda, float2* C, int ldc) {
         const float one = 1.f, zero = 0.f;
-        B200_CUBLAS_D(cublasCherk(h, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_C, n, k, &one, (const cuComplex*)A, lda, &zero,
+        B200_CUBLAS(cublasCherk(h, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_C, n, k, &one, (const cuComplex*)A, lda, &zero,
                                   (cuComplex*)C, ldc));
     }
     static void trsm(cublasHandle_t h, int m, int n, const float2* U, int ldu, float2* X, int ldx) {
         const float2 one = make_float2(1.f, 0.f);
-        B200_CUBLAS_D(cublasCtrsm(h, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, m, n,
+        B200_CUBLAS(cublasCtrsm(h, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, m, n,
                                   (const cuComplex*)&one, (const cuComplex*)U, ldu, (cuComplex*)X, ldx));
     }
 };
@@ -226,9 +212,9 @@ template <typename T> struct Engine {
     Engine(int nb, int d, int ndim, const double* precond_d)
         : nband(nb), dim(d), nbase_x(ndim * nb), ld(kF32 ? even(d) : d), L(even(ndim * nb)), ncp(even(nb)), dim_cap(d) {
         B200_CHECK(ndim > 1 && nb > 0 && ndim * nb < d, kInvalidArgument, "need david_ndim > 1 and david_ndim*nband < dim");
-        B200_CUBLAS_D(cublasCreate(&cb));
+        B200_CUBLAS(cublasCreate(&cb));
         B200_CUSOLVER(cusolverDnCreate(&cs));
-        B200_CUBLAS_D(cublasSetStream(cb, s));
+        B200_CUBLAS(cublasSetStream(cb, s));
         B200_CUSOLVER(cusolverDnSetStream(cs, s));
         basis.resize(size_t(nbase_x) * ld);
         hp.resize(size_t(nbase_x) * ld);
@@ -307,7 +293,7 @@ template <typename T> struct Engine {
     void set_stream(cudaStream_t st) {
         B200_CUDA(cudaStreamSynchronize(s));
         s = st;
-        B200_CUBLAS_D(cublasSetStream(cb, s));
+        B200_CUBLAS(cublasSetStream(cb, s));
         B200_CUSOLVER(cusolverDnSetStream(cs, s));
     }
 
@@ -380,7 +366,7 @@ template <typename T> struct Engine {
             note_launch();
             B200_CUDA(cudaGetLastError());
             const double2 done = make_double2(1.0, 0.0);
-            B200_CUBLAS_D(cublasZtrsm(cb, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, nc, nc,
+            B200_CUBLAS(cublasZtrsm(cb, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, nc, nc,
                                       (const cuDoubleComplex*)&done, (const cuDoubleComplex*)G, ncp,
                                       (cuDoubleComplex*)winv.ptr, ncp));
             k_convert<double2, T><<<grid_of(n2), kT, 0, s>>>(n2, winv.ptr, gram.ptr);

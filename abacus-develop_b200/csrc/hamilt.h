@@ -6,17 +6,10 @@
 
 #include "common.h"
 #include "gemm_tc.h"
+#include "linalg_status.h"
 #include "pw_grid.h"
 
 namespace b200 {
-
-#define B200_CUBLAS(call)                                                                                       \
-    do {                                                                                                        \
-        cublasStatus_t st_ = (call);                                                                            \
-        if (st_ != CUBLAS_STATUS_SUCCESS)                                                                       \
-            throw ::b200::Error(::b200::kCublasError, std::string(#call) + " failed with status " +           \
-                                                          std::to_string(int(st_)));                           \
-    } while (0)
 
 struct NonlocalK {
     int nkb = 0, npwx = 0;

@@ -6,28 +6,17 @@
 // program uses when psi lives in host memory.
 #include <algorithm>
 
+#include "capi_guard.h"
 #include "../../include/abacus_b200.h"
 #include "capi_handles.h"
 
 namespace {
-template <typename F> int guarded_h(F&& f) {
-    try {
-        f();
-        b200::set_last_error("");
-        return B200_STATUS_OK;
-    } catch (const b200::Error& e) {
-        b200::set_last_error(e.what());
-        return e.code;
-    } catch (const std::exception& e) {
-        b200::set_last_error(e.what());
-        return B200_STATUS_INVALID_ARGUMENT;
-    }
-}
+using b200::guarded;
 }  // namespace
 
 extern "C" int b200_hamilt_hpsi_host(b200_hamilt* h, int ik, int spin, int nbands, int ld, const void* psi_host,
                                      void* hpsi_host, void* psi_dev, void* hpsi_dev, int npieces, void* stream) {
-    return guarded_h([&] {
+    return guarded([&] {
         B200_CHECK(h && psi_host && hpsi_host && psi_dev && hpsi_dev, b200::kInvalidArgument, "NULL argument");
         B200_CHECK(nbands >= 1 && ld >= 1 && npieces >= 1, b200::kInvalidArgument, "need nbands, ld, npieces >= 1");
         b200::Hamilt* H = h->h.get();

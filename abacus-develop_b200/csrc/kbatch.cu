@@ -14,6 +14,7 @@
 #include <thread>
 #include <vector>
 
+#include "capi_guard.h"
 #include "../../include/abacus_b200.h"
 #include "capi_handles.h"
 
@@ -28,19 +29,7 @@ struct b200_graph {
 
 namespace {
 
-template <typename F> int guarded_k(F&& f) {
-    try {
-        f();
-        b200::set_last_error("");
-        return B200_STATUS_OK;
-    } catch (const b200::Error& e) {
-        b200::set_last_error(e.what());
-        return e.code;
-    } catch (const std::exception& e) {
-        b200::set_last_error(e.what());
-        return B200_STATUS_INVALID_ARGUMENT;
-    }
-}
+using b200::guarded;
 
 void kbatch_call(b200_hamilt* h, int nk, const int* iks, int spin, int nb, int ld, void* const* psi, void* const* hpsi,
                  cudaStream_t s) {
@@ -59,12 +48,12 @@ extern "C" {
 
 int b200_hamilt_hpsi_kbatch(b200_hamilt* h, int nk, const int* iks, int spin, int nbands, int ld, void* const* psi_d,
                             void* const* hpsi_d, void* stream) {
-    return guarded_k([&] { kbatch_call(h, nk, iks, spin, nbands, ld, psi_d, hpsi_d, reinterpret_cast<cudaStream_t>(stream)); });
+    return guarded([&] { kbatch_call(h, nk, iks, spin, nbands, ld, psi_d, hpsi_d, reinterpret_cast<cudaStream_t>(stream)); });
 }
 
 int b200_graph_capture_hpsi_kbatch(b200_hamilt* h, int nk, const int* iks, int spin, int nbands, int ld,
                                    void* const* psi_d, void* const* hpsi_d, void* stream, b200_graph** out) {
-    return guarded_k([&] {
+    return guarded([&] {
         B200_CHECK(out != nullptr, b200::kInvalidArgument, "NULL argument");
         cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
         B200_CHECK(s != nullptr, b200::kInvalidArgument, "capture needs a non-default stream");
@@ -88,19 +77,19 @@ int b200_graph_capture_hpsi_kbatch(b200_hamilt* h, int nk, const int* iks, int s
 }
 
 int b200_graph_launch(b200_graph* g, void* stream) {
-    return guarded_k([&] {
+    return guarded([&] {
         B200_CHECK(g && g->exec, b200::kInvalidArgument, "NULL graph");
         B200_CUDA(cudaGraphLaunch(g->exec, reinterpret_cast<cudaStream_t>(stream)));
     });
 }
 
 int b200_graph_destroy(b200_graph* g) {
-    return guarded_k([&] { delete g; });
+    return guarded([&] { delete g; });
 }
 
 int b200_hamilt_autotune(b200_hamilt* h, int ik, int nbands, int ld, const void* psi_d, void* hpsi_d, void* stream,
                          int* best_chunk) {
-    return guarded_k([&] {
+    return guarded([&] {
         B200_CHECK(h && psi_d && hpsi_d, b200::kInvalidArgument, "NULL argument");
         cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
         b200::Hamilt& H = *h->h;
@@ -146,7 +135,7 @@ int b200_hamilt_autotune(b200_hamilt* h, int ik, int nbands, int ld, const void*
 int b200_solve_kpoints(b200_hamilt* h, int nk, const int* iks, int spin, int nband, int david_ndim, int precision,
                        const double* const* precond_d, void* const* psi_d, int ldpsi, double* eigenvalues,
                        double thr, int maxiter, int ntry_max, int notconv_max, int nworkers, int* iters) {
-    return guarded_k([&] {
+    return guarded([&] {
         B200_CHECK(h && iks && precond_d && psi_d && eigenvalues, b200::kInvalidArgument, "NULL argument");
         B200_CHECK(nk >= 1 && nworkers >= 1, b200::kInvalidArgument, "need nk >= 1 and nworkers >= 1");
         b200::Hamilt* H = h->h.get();

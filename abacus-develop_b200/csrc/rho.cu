@@ -11,6 +11,7 @@
 #include <algorithm>
 #include <vector>
 
+#include "capi_guard.h"
 #include "../../include/abacus_b200.h"
 #include "capi_handles.h"
 
@@ -82,19 +83,7 @@ void elecstate_nc_call(int domag, int domag_z, int nrxx, R w1, R* const* rho, co
 }  // namespace b200
 
 namespace {
-template <typename F> int guarded_r(F&& f) {
-    try {
-        f();
-        b200::set_last_error("");
-        return B200_STATUS_OK;
-    } catch (const b200::Error& e) {
-        b200::set_last_error(e.what());
-        return e.code;
-    } catch (const std::exception& e) {
-        b200::set_last_error(e.what());
-        return B200_STATUS_INVALID_ARGUMENT;
-    }
-}
+using b200::guarded;
 
 template <typename T, typename R>
 void psi_to_rho(b200_pw_basis* b, b200::DeviceArray<T>& box, b200::DeviceArray<T>& aux, b200::DeviceArray<T>& sbuf,
@@ -147,25 +136,25 @@ void psi_to_rho(b200_pw_basis* b, b200::DeviceArray<T>& box, b200::DeviceArray<T
 extern "C" {
 
 int b200_elecstate_pw_op_f64(int spin, int nrxx, double w1, double* const* rho, const void* wfcr_d, void* stream) {
-    return guarded_r([&] {
+    return guarded([&] {
         b200::elecstate_call<double2, double>(spin, nrxx, w1, rho, (const double2*)wfcr_d, (cudaStream_t)stream);
     });
 }
 int b200_elecstate_pw_op_f32(int spin, int nrxx, float w1, float* const* rho, const void* wfcr_d, void* stream) {
-    return guarded_r([&] {
+    return guarded([&] {
         b200::elecstate_call<float2, float>(spin, nrxx, w1, rho, (const float2*)wfcr_d, (cudaStream_t)stream);
     });
 }
 int b200_elecstate_pw_op_nc_f64(int domag, int domag_z, int nrxx, double w1, double* const* rho, const void* wfcr_d,
                                 const void* wfcr_another_spin_d, void* stream) {
-    return guarded_r([&] {
+    return guarded([&] {
         b200::elecstate_nc_call<double2, double>(domag, domag_z, nrxx, w1, rho, (const double2*)wfcr_d,
                                                  (const double2*)wfcr_another_spin_d, (cudaStream_t)stream);
     });
 }
 int b200_elecstate_pw_op_nc_f32(int domag, int domag_z, int nrxx, float w1, float* const* rho, const void* wfcr_d,
                                 const void* wfcr_another_spin_d, void* stream) {
-    return guarded_r([&] {
+    return guarded([&] {
         b200::elecstate_nc_call<float2, float>(domag, domag_z, nrxx, w1, rho, (const float2*)wfcr_d,
                                                (const float2*)wfcr_another_spin_d, (cudaStream_t)stream);
     });
@@ -173,7 +162,7 @@ int b200_elecstate_pw_op_nc_f32(int domag, int domag_z, int nrxx, float w1, floa
 
 int b200_pw_basis_psi_to_rho_f64(b200_pw_basis* b, int ik, int nbands, int ld, const void* psi_d, const double* w1,
                                  double* rho_d, void* stream) {
-    return guarded_r([&] {
+    return guarded([&] {
         B200_CHECK(b != nullptr, b200::kInvalidArgument, "NULL basis");
         psi_to_rho<double2, double>(b, b->rho_box64, b->aux64, b->rho_sb64, b->rho_ws64, ik, nbands, ld,
                                     (const double2*)psi_d, w1, rho_d, (cudaStream_t)stream);
@@ -181,7 +170,7 @@ int b200_pw_basis_psi_to_rho_f64(b200_pw_basis* b, int ik, int nbands, int ld, c
 }
 int b200_pw_basis_psi_to_rho_f32(b200_pw_basis* b, int ik, int nbands, int ld, const void* psi_d, const double* w1,
                                  float* rho_d, void* stream) {
-    return guarded_r([&] {
+    return guarded([&] {
         B200_CHECK(b != nullptr, b200::kInvalidArgument, "NULL basis");
         psi_to_rho<float2, float>(b, b->rho_box32, b->aux32, b->rho_sb32, b->rho_ws32, ik, nbands, ld,
                                   (const float2*)psi_d, w1, rho_d, (cudaStream_t)stream);

@@ -32,6 +32,7 @@
 #include <unordered_map>
 #include <vector>
 
+#include "capi_guard.h"
 #include "../../include/abacus_b200.h"
 #include "capi_handles.h"
 
@@ -444,25 +445,13 @@ struct b200_server {
 };
 
 namespace {
-template <typename F> int guarded_s(F&& f) {
-    try {
-        f();
-        b200::set_last_error("");
-        return B200_STATUS_OK;
-    } catch (const b200::Error& e) {
-        b200::set_last_error(e.what());
-        return e.code;
-    } catch (const std::exception& e) {
-        b200::set_last_error(e.what());
-        return B200_STATUS_INVALID_ARGUMENT;
-    }
-}
+using b200::guarded;
 }  // namespace
 
 extern "C" {
 
 int b200_server_create(unsigned long long hbm_budget_bytes, int nworkers, int david_ndim, b200_server** out) {
-    return guarded_s([&] {
+    return guarded([&] {
         B200_CHECK(out != nullptr, b200::kInvalidArgument, "NULL argument");
         auto p = std::make_unique<b200_server>();
         p->s = std::make_unique<b200::Server>(size_t(hbm_budget_bytes), nworkers, david_ndim);
@@ -471,11 +460,11 @@ int b200_server_create(unsigned long long hbm_budget_bytes, int nworkers, int da
 }
 
 int b200_server_destroy(b200_server* s) {
-    return guarded_s([&] { delete s; });
+    return guarded([&] { delete s; });
 }
 
 int b200_server_add_cell(b200_server* s, b200_hamilt* h, int max_inflight, int* cell_id) {
-    return guarded_s([&] {
+    return guarded([&] {
         B200_CHECK(s && h && cell_id, b200::kInvalidArgument, "NULL argument");
         *cell_id = s->s->add_cell(h, max_inflight);
     });
@@ -483,7 +472,7 @@ int b200_server_add_cell(b200_server* s, b200_hamilt* h, int max_inflight, int* 
 
 int b200_server_submit(b200_server* s, int cell, int ik, int nbands, int precision, double thr, int maxiter,
                        unsigned long long seed, double* eig_out, long long* req_id) {
-    return guarded_s([&] {
+    return guarded([&] {
         B200_CHECK(s && req_id, b200::kInvalidArgument, "NULL argument");
         *req_id = s->s->submit(cell, ik, nbands, precision, thr, maxiter, seed, eig_out);
     });
@@ -504,14 +493,14 @@ int b200_server_poll(b200_server* s, int max_out, int wait, long long* ids, int*
 }
 
 int b200_server_drain(b200_server* s) {
-    return guarded_s([&] {
+    return guarded([&] {
         B200_CHECK(s != nullptr, b200::kInvalidArgument, "NULL argument");
         s->s->drain();
     });
 }
 
 int b200_server_stats(b200_server* s, double* out6) {
-    return guarded_s([&] {
+    return guarded([&] {
         B200_CHECK(s && out6, b200::kInvalidArgument, "NULL argument");
         s->s->stats(out6);
     });

@@ -11,6 +11,7 @@
 #include <cmath>
 #include <string>
 
+#include "capi_guard.h"
 #include "../../include/abacus_b200.h"
 #include "capi_handles.h"
 
@@ -283,19 +284,7 @@ void Hamilt::build_vkb(int ik, cudaStream_t s) {
 }  // namespace b200
 
 namespace {
-template <typename F> int guarded_v(F&& f) {
-    try {
-        f();
-        b200::set_last_error("");
-        return B200_STATUS_OK;
-    } catch (const b200::Error& e) {
-        b200::set_last_error(e.what());
-        return e.code;
-    } catch (const std::exception& e) {
-        b200::set_last_error(e.what());
-        return B200_STATUS_INVALID_ARGUMENT;
-    }
-}
+using b200::guarded;
 
 template <typename R>
 void ylm_call(int ng, int lmax, const R* g, R* ylm, cudaStream_t s) {
@@ -355,10 +344,10 @@ void vnl_call(int ntype, int npw, int npwx, int nhm, int tab_2, int tab_3, const
 extern "C" {
 
 int b200_cal_ylm_real_op_f64(int ng, int lmax, const double* g_d, double* ylm_d, void* stream) {
-    return guarded_v([&] { ylm_call<double>(ng, lmax, g_d, ylm_d, (cudaStream_t)stream); });
+    return guarded([&] { ylm_call<double>(ng, lmax, g_d, ylm_d, (cudaStream_t)stream); });
 }
 int b200_cal_ylm_real_op_f32(int ng, int lmax, const float* g_d, float* ylm_d, void* stream) {
-    return guarded_v([&] { ylm_call<float>(ng, lmax, g_d, ylm_d, (cudaStream_t)stream); });
+    return guarded([&] { ylm_call<float>(ng, lmax, g_d, ylm_d, (cudaStream_t)stream); });
 }
 
 int b200_cal_sk_op_f64(int ik, int ntype, int nx, int ny, int nz, int rho_nx, int rho_ny, int rho_nz, int npw, int npwx,
@@ -366,7 +355,7 @@ int b200_cal_sk_op_f64(int ik, int ntype, int nx, int ny, int nz, int rho_nx, in
                        const int* igl2isz_d, const int* is2fftixy_d, double two_pi, const double* kvec_c_d,
                        const double* atom_tau_d, const void* eigts1_d, const void* eigts2_d, const void* eigts3_d,
                        void* sk_d, void* stream) {
-    return guarded_v([&] {
+    return guarded([&] {
         sk_call<double, double2>(ik, ntype, nx, ny, nz, rho_nx, rho_ny, rho_nz, npw, npwx, fftny, eigts1_nc, eigts2_nc,
                                  eigts3_nc, atom_na, igl2isz_d, is2fftixy_d, two_pi, kvec_c_d, atom_tau_d,
                                  (const double2*)eigts1_d, (const double2*)eigts2_d, (const double2*)eigts3_d,
@@ -378,7 +367,7 @@ int b200_cal_sk_op_f32(int ik, int ntype, int nx, int ny, int nz, int rho_nx, in
                        const int* igl2isz_d, const int* is2fftixy_d, float two_pi, const float* kvec_c_d,
                        const float* atom_tau_d, const void* eigts1_d, const void* eigts2_d, const void* eigts3_d,
                        void* sk_d, void* stream) {
-    return guarded_v([&] {
+    return guarded([&] {
         sk_call<float, float2>(ik, ntype, nx, ny, nz, rho_nx, rho_ny, rho_nz, npw, npwx, fftny, eigts1_nc, eigts2_nc,
                                eigts3_nc, atom_na, igl2isz_d, is2fftixy_d, two_pi, kvec_c_d, atom_tau_d,
                                (const float2*)eigts1_d, (const float2*)eigts2_d, (const float2*)eigts3_d, (float2*)sk_d,
@@ -391,7 +380,7 @@ int b200_cal_vnl_op_f64(int ntype, int npw, int npwx, int nhm, int tab_2, int ta
                         const double* ylm_d, const double* indv_d, const double* nhtol_d, const double* nhtolm_d,
                         const double* tab_d, double* vkb1_d, const void* sk_d, void* vkb_d, void* stream) {
     (void)vkb1_d;
-    return guarded_v([&] {
+    return guarded([&] {
         vnl_call<double, double2>(ntype, npw, npwx, nhm, tab_2, tab_3, atom_na, atom_nb, atom_nh, dq, tpiba, gk_d, ylm_d,
                                   indv_d, nhtol_d, nhtolm_d, tab_d, (const double2*)sk_d, (double2*)vkb_d,
                                   (cudaStream_t)stream);
@@ -402,7 +391,7 @@ int b200_cal_vnl_op_f32(int ntype, int npw, int npwx, int nhm, int tab_2, int ta
                         const float* ylm_d, const float* indv_d, const float* nhtol_d, const float* nhtolm_d,
                         const float* tab_d, float* vkb1_d, const void* sk_d, void* vkb_d, void* stream) {
     (void)vkb1_d;
-    return guarded_v([&] {
+    return guarded([&] {
         vnl_call<float, float2>(ntype, npw, npwx, nhm, tab_2, tab_3, atom_na, atom_nb, atom_nh, dq, tpiba, gk_d, ylm_d,
                                 indv_d, nhtol_d, nhtolm_d, tab_d, (const float2*)sk_d, (float2*)vkb_d,
                                 (cudaStream_t)stream);
@@ -412,21 +401,21 @@ int b200_cal_vnl_op_f32(int ntype, int npw, int npwx, int nhm, int tab_2, int ta
 int b200_hamilt_set_projectors(b200_hamilt* h, int ntype, const int* na, const int* nbeta, const int* nh, int nhm,
                                int lmax, const int* indv, const int* nhtol, const int* nhtolm, int tab_2, int tab_3,
                                double dq, const double* tab, const double* tau) {
-    return guarded_v([&] {
+    return guarded([&] {
         B200_CHECK(h != nullptr, b200::kInvalidArgument, "NULL handle");
         h->h->set_projectors(ntype, na, nbeta, nh, nhm, lmax, indv, nhtol, nhtolm, tab_2, tab_3, dq, tab, tau);
     });
 }
 
 int b200_hamilt_build_vkb(b200_hamilt* h, int ik, void* stream) {
-    return guarded_v([&] {
+    return guarded([&] {
         B200_CHECK(h != nullptr, b200::kInvalidArgument, "NULL handle");
         h->h->build_vkb(ik, (cudaStream_t)stream);
     });
 }
 
 int b200_hamilt_copy_vkb(const b200_hamilt* h, int ik, void* vkb_d, void* stream) {
-    return guarded_v([&] {
+    return guarded([&] {
         B200_CHECK(h != nullptr && vkb_d != nullptr, b200::kInvalidArgument, "NULL argument");
         B200_CHECK(ik >= 0 && ik < int(h->h->nl.size()), b200::kInvalidArgument, "k-point index out of range");
         const b200::NonlocalK& k = h->h->nl[ik];
