@@ -56,46 +56,89 @@ class NscfResult:
     ef: float                  # Ry
     iters: np.ndarray          # Davidson iterations per k-point
     diag_thr: float
-    psis: list = field(default_factory=list)       # host eigenvectors, (nbands, npwk) per k-point
+    psis: list = field(default_factory=list)       # host eigenvectors of this rank's k-points, (nbands, npwk)
     files: dict = field(default_factory=dict)      # written outputs
     running_lines: list = field(default_factory=list)
+    iks: list = field(default_factory=list)        # the k-points this rank solved (psis follow this order)
 
 
-def run_nscf(hamilt, nbands, psi_init, *, wk, nelec, latvec, ecutwfc, pw_diag_thr=1e-2, scf_thr=1e-9,
-             precision=P.PREC_FP64, david_ndim=4, maxiter=50, nworkers=4, out_dir=None, out_wfc_pw=0,
-             kl_segids=None, band_precision=8):
-    """Solve nbands bands at every k-point of hamilt's basis (V_eff, D and the projectors already set) from the
-    start vectors psi_init[ik] ((nbands, npwk) arrays in the basis's order).  Outputs go to out_dir when it is
-    given: BANDS_1.dat (nscf_band.cpp), running_nscf.log (the eigenvalue block), WAVEFUNC<ik>.dat / .txt
-    (out_wfc_pw 2 / 1)."""
-    import torch
-    basis = hamilt.basis
-    nks, ld = basis.nks, basis.npwk_max
+def device_solve(hamilt, *, precision=P.PREC_FP64, david_ndim=4, maxiter=50, nworkers=4):
+    """The band solve of run_nscf_pool on this rank's GPU: b200_solve_kpoints over the rank's k-points, NSCF
+    exit rule (ntry_max 5, notconv_max 0, hsolver_pw.cpp:580-593)."""
+    def solve(iks, psi_init, nbands, thr):
+        import torch
+        basis = hamilt.basis
+        ld = basis.npwk_max
+        if not iks:
+            return np.zeros((0, nbands)), np.zeros(0, dtype=np.int32), []
+        psis_d, pcs = [], []
+        for q, ik in enumerate(iks):
+            npw = int(basis.npwk[ik])
+            x = np.zeros((nbands, ld), dtype=np.complex128)
+            x[:, :npw] = np.asarray(psi_init[q])[:nbands, :npw]
+            psis_d.append(torch.from_numpy(x.reshape(-1)).cuda())
+            pcs.append(P.precondition_d(basis, ik))
+        ekb, its = hamilt.solve_kpoints(list(iks), pcs, psis_d, ld, nbands, thr, maxiter, david_ndim=david_ndim,
+                                        precision=precision, nworkers=nworkers, ntry_max=5, notconv_max=0)
+        torch.cuda.synchronize()
+        psis = [p.cpu().numpy().reshape(nbands, ld)[:, :int(basis.npwk[ik])].copy() for ik, p in zip(iks, psis_d)]
+        return ekb, its, psis
+    return solve
+
+
+def run_nscf_pool(basis, nbands, psi_init, solve, *, wk, nelec, latvec, ecutwfc, pw_diag_thr=1e-2, scf_thr=1e-9,
+                  out_dir=None, out_wfc_pw=0, kl_segids=None, band_precision=8, group=None):
+    """The NSCF run of one rank of a k-point pool split (one pool per GPU, module_base/module_device/
+    device.cpp:195-217): this rank solves its share of the k-points (kpool.partition, cost npwk * nbands^2)
+    with solve(iks, psi_init_of_those, nbands, thr) -> (ekb, iters, eigenvectors); the eigenvalues are
+    all-gathered (the only collective); occupations, the Fermi energy and the band / running-log files come
+    from the gathered eigenvalues (files on rank 0), each rank writes the wavefunction files of its own
+    k-points.  psi_init[ik] is indexed by global k-point (entries of other ranks' k-points are not read)."""
+    from . import kpool
+    ws, rank = 1, 0
+    try:
+        import torch.distributed as dist
+        if dist.is_initialized():
+            ws, rank = dist.get_world_size(group), dist.get_rank(group)
+    except ImportError:
+        pass
+    nks = basis.nks
     thr = nscf_io.nscf_diag_thr(pw_diag_thr, scf_thr, nelec)
-    psis_d, pcs = [], []
-    for ik in range(nks):
-        npw = int(basis.npwk[ik])
-        x = np.zeros((nbands, ld), dtype=np.complex128)
-        x[:, :npw] = np.asarray(psi_init[ik])[:nbands, :npw]
-        psis_d.append(torch.from_numpy(x.reshape(-1)).cuda())
-        pcs.append(P.precondition_d(basis, ik))
-    ekb, its = hamilt.solve_kpoints(list(range(nks)), pcs, psis_d, ld, nbands, thr, maxiter, david_ndim=david_ndim,
-                                    precision=precision, nworkers=nworkers, ntry_max=5, notconv_max=0)
-    torch.cuda.synchronize()
-    psis = [p.cpu().numpy().reshape(nbands, ld)[:, :int(basis.npwk[ik])].copy() for ik, p in enumerate(psis_d)]
+    mine = kpool.partition(basis.npwk, nbands, ws)[rank]
+    ekb_l, its_l, psis_l = solve(mine, [psi_init[ik] for ik in mine], nbands, thr)
+    ekb = kpool.gather_eigenvalues({ik: ekb_l[q] for q, ik in enumerate(mine)}, nks, nbands, group)
+    its = kpool.gather_eigenvalues({ik: [float(its_l[q])] for q, ik in enumerate(mine)}, nks, 1, group)[:, 0]
     wg, ef = occupation_weights(ekb, wk, nelec)
     kvec_c = np.array([basis.kvec_c(ik) for ik in range(nks)])
-    res = NscfResult(ekb=ekb, wg=wg, ef=ef, iters=its, diag_thr=thr, psis=psis)
+    res = NscfResult(ekb=ekb, wg=wg, ef=ef, iters=its.astype(np.int64), diag_thr=thr, psis=psis_l, iks=list(mine))
     res.running_lines = [f" PW_DIAG_THR  = {thr:g}\n"] + nscf_io.running_band_lines(ekb, wg, kvec_c, nks)
     if out_dir is not None:
         d = Path(out_dir)
         d.mkdir(parents=True, exist_ok=True)
-        seg = np.zeros(nks, dtype=int) if kl_segids is None else kl_segids
-        nscf_io.nscf_band(d / "BANDS_1.dat", ekb, kvec_c, seg, ef, band_precision)
-        res.files["band"] = str(d / "BANDS_1.dat")
-        (d / "running_nscf.log").write_text("".join(res.running_lines))
-        res.files["running"] = str(d / "running_nscf.log")
+        if rank == 0:
+            seg = np.zeros(nks, dtype=int) if kl_segids is None else kl_segids
+            nscf_io.nscf_band(d / "BANDS_1.dat", ekb, kvec_c, seg, ef, band_precision)
+            (d / "running_nscf.log").write_text("".join(res.running_lines))
+            res.files["band"] = str(d / "BANDS_1.dat")
+            res.files["running"] = str(d / "running_nscf.log")
         if out_wfc_pw in (1, 2):
-            res.files["wfc"] = nscf_io.write_wfc_pw(str(d / "WAVEFUNC"), basis, psis, kvec_c, wk, ecutwfc, latvec,
-                                                    nbands=nbands, fmt=out_wfc_pw)
+            res.files["wfc"] = []
+            for q, ik in enumerate(mine):
+                res.files["wfc"].append(nscf_io.write_wfc_pw_k(str(d / "WAVEFUNC"), basis, ik, psis_l[q],
+                                                               kvec_c[ik], wk[ik], ecutwfc, latvec, nbands,
+                                                               out_wfc_pw, nks))
     return res
+
+
+def run_nscf(hamilt, nbands, psi_init, *, wk, nelec, latvec, ecutwfc, pw_diag_thr=1e-2, scf_thr=1e-9,
+             precision=P.PREC_FP64, david_ndim=4, maxiter=50, nworkers=4, out_dir=None, out_wfc_pw=0,
+             kl_segids=None, band_precision=8, group=None):
+    """Solve nbands bands at every k-point of hamilt's basis (V_eff, D and the projectors already set) from the
+    start vectors psi_init[ik] ((nbands, npwk) arrays in the basis's order), on this GPU or, under
+    torch.distributed, on this rank's share of a k-point pool split.  Outputs go to out_dir when it is
+    given: BANDS_1.dat (nscf_band.cpp), running_nscf.log (the eigenvalue block), WAVEFUNC<ik>.dat / .txt
+    (out_wfc_pw 2 / 1)."""
+    solve = device_solve(hamilt, precision=precision, david_ndim=david_ndim, maxiter=maxiter, nworkers=nworkers)
+    return run_nscf_pool(hamilt.basis, nbands, psi_init, solve, wk=wk, nelec=nelec, latvec=latvec,
+                         ecutwfc=ecutwfc, pw_diag_thr=pw_diag_thr, scf_thr=scf_thr, out_dir=out_dir,
+                         out_wfc_pw=out_wfc_pw, kl_segids=kl_segids, band_precision=band_precision, group=group)

@@ -92,53 +92,57 @@ def write_wfc_pw(prefix, basis, psis, kvec_c, wk, ecutwfc, latvec, nbands=None, 
     Returns the file names."""
     nks = basis.nks
     nkstot = nks if nkstot is None else nkstot
+    return [write_wfc_pw_k(prefix, basis, ik, psis[ik], kvec_c[ik], wk[ik], ecutwfc, latvec, nbands, fmt, nkstot)
+            for ik in range(nks)]
+
+
+def write_wfc_pw_k(prefix, basis, ik, psi, kvec_c, wk, ecutwfc, latvec, nbands=None, fmt=2, nkstot=None):
+    """The file of k-point ik alone (write_wfc_pw.cpp:62-280 for one ik); returns its name."""
+    nkstot = basis.nks if nkstot is None else nkstot
     G = reciprocal_lattice(latvec)
     tpiba = TWO_PI / basis.lat0
-    names = []
-    for ik in range(nks):
-        psi = np.asarray(psis[ik])
-        nb = psi.shape[0] if nbands is None else nbands
-        ng = int(basis.npwk[ik])
-        ix, iy, iz = _box_indices(basis, ik)
-        fn = wfc_filename(prefix, ik, fmt)
-        names.append(fn)
-        kx, ky, kz = (float(v) for v in kvec_c[ik])
-        if fmt == 2:
-            with open(fn, "wb") as f:
-                f.write(struct.pack("<iii3ddiidddi", 72, ik + 1, nkstot, kx, ky, kz, float(wk[ik]), ng, nb,
-                                    float(ecutwfc), float(basis.lat0), tpiba, 72))
-                f.write(struct.pack("<i9di", 72, *[float(v) for v in G.reshape(9)], 72))
-                mill = np.stack([ix, iy, iz], axis=1).astype("<i4")
-                f.write(struct.pack("<i", ng * 12) + mill.tobytes() + struct.pack("<i", ng * 12))
-                rec = struct.pack("<i", ng * 16)
-                for ib in range(nb):
-                    f.write(rec + np.ascontiguousarray(psi[ib, :ng], dtype="<c16").tobytes() + rec)
-        elif fmt == 1:
-            lines = ["".join(f"{s:>10}" for s in ("Kpoint", "nKpoint", "kv.x", "kv.y", "kv.z", "weight", "ngtot",
-                                                  "nband", "ecut", "lat0", "2pi/lat0")) + "\n"]
-            lines.append(f"{ik + 1:10d}{nkstot:10d}" + "".join(_cxx_g(v) for v in (kx, ky, kz, float(wk[ik])))
-                         + f"{ng:10d}{nb:10d}" + "".join(_cxx_g(v) for v in (float(ecutwfc), basis.lat0, tpiba))
-                         + "\n")
-            lines.append("\n<Reciprocal Lattice Vector>\n")
-            for r in range(3):
-                lines.append("".join(_cxx_g(float(v)) for v in G[r]) + "\n")
-            lines.append("<Reciprocal Lattice Vector>\n\n")
-            lines.append("<G vectors>\n")
-            lines.extend(f"{a:10d}{b:10d}{c:10d}\n" for a, b, c in zip(ix, iy, iz))
-            lines.append("<G vectors>\n\n")
+    psi = np.asarray(psi)
+    nb = psi.shape[0] if nbands is None else nbands
+    ng = int(basis.npwk[ik])
+    ix, iy, iz = _box_indices(basis, ik)
+    fn = wfc_filename(prefix, ik, fmt)
+    kx, ky, kz = (float(v) for v in kvec_c)
+    if fmt == 2:
+        with open(fn, "wb") as f:
+            f.write(struct.pack("<iii3ddiidddi", 72, ik + 1, nkstot, kx, ky, kz, float(wk), ng, nb,
+                                float(ecutwfc), float(basis.lat0), tpiba, 72))
+            f.write(struct.pack("<i9di", 72, *[float(v) for v in G.reshape(9)], 72))
+            mill = np.stack([ix, iy, iz], axis=1).astype("<i4")
+            f.write(struct.pack("<i", ng * 12) + mill.tobytes() + struct.pack("<i", ng * 12))
+            rec = struct.pack("<i", ng * 16)
             for ib in range(nb):
-                lines.append(f"\n< Band {ib + 1} >\n")
-                v = np.empty(2 * ng)
-                v[0::2], v[1::2] = psi[ib, :ng].real, psi[ib, :ng].imag
-                cells = [f"{x:15.6e}" for x in v]
-                rows = ["".join(cells[i:i + 8]) for i in range(0, len(cells), 8)]  # 4 complex numbers per row
-                lines.append("\n".join(rows))
-                lines.append(f"\n< Band {ib + 1} >\n")
-            with open(fn, "w") as f:
-                f.write("".join(lines))
-        else:
-            raise ValueError("fmt must be 1 (txt) or 2 (dat)")
-    return names
+                f.write(rec + np.ascontiguousarray(psi[ib, :ng], dtype="<c16").tobytes() + rec)
+    elif fmt == 1:
+        lines = ["".join(f"{s:>10}" for s in ("Kpoint", "nKpoint", "kv.x", "kv.y", "kv.z", "weight", "ngtot",
+                                              "nband", "ecut", "lat0", "2pi/lat0")) + "\n"]
+        lines.append(f"{ik + 1:10d}{nkstot:10d}" + "".join(_cxx_g(v) for v in (kx, ky, kz, float(wk)))
+                     + f"{ng:10d}{nb:10d}" + "".join(_cxx_g(v) for v in (float(ecutwfc), basis.lat0, tpiba))
+                     + "\n")
+        lines.append("\n<Reciprocal Lattice Vector>\n")
+        for r in range(3):
+            lines.append("".join(_cxx_g(float(v)) for v in G[r]) + "\n")
+        lines.append("<Reciprocal Lattice Vector>\n\n")
+        lines.append("<G vectors>\n")
+        lines.extend(f"{a:10d}{b:10d}{c:10d}\n" for a, b, c in zip(ix, iy, iz))
+        lines.append("<G vectors>\n\n")
+        for ib in range(nb):
+            lines.append(f"\n< Band {ib + 1} >\n")
+            v = np.empty(2 * ng)
+            v[0::2], v[1::2] = psi[ib, :ng].real, psi[ib, :ng].imag
+            cells = [f"{x:15.6e}" for x in v]
+            rows = ["".join(cells[i:i + 8]) for i in range(0, len(cells), 8)]  # 4 complex numbers per row
+            lines.append("\n".join(rows))
+            lines.append(f"\n< Band {ib + 1} >\n")
+        with open(fn, "w") as f:
+            f.write("".join(lines))
+    else:
+        raise ValueError("fmt must be 1 (txt) or 2 (dat)")
+    return fn
 
 
 def read_wfc_pw_header(filename) -> WfcHeader:
