@@ -23,10 +23,11 @@ const char* ref_dav_subspace_last_error() { return g_err_ds.c_str(); }
 
 // psi (in/out): nband vectors of dim complex entries at psi + m*ldpsi; eig: nband doubles (in: the previous
 // eigenvalues, out); precond: dim doubles (HSolverPW passes g2kin for this method, hsolver_pw.cpp:550-593);
-// all bands occupied; returns 0 on success and the total iteration count in *iters.
+// occupied: nband flags, or NULL for all bands occupied (as HSolverPW passes them); returns 0 on success and
+// the total iteration count in *iters.
 int ref_dav_subspace(int nband, int dim, int david_ndim, int ldpsi, const double* precond, ref_hpsi_cb_ds cb,
                      void* user, void* psi, double* eig, double thr, int maxiter, int need_subspace, int scf,
-                     int* iters) {
+                     const int* occupied, int* iters) {
     using T = std::complex<double>;
     try {
         hsolver::diag_comm_info comm(0, 1);
@@ -36,7 +37,9 @@ int ref_dav_subspace(int nband, int dim, int david_ndim, int ldpsi, const double
         auto hpsi = [cb, user](T* x, T* hx, const int nvec, const int d, const int i0, const int i1) {
             cb(user, x, hx, nvec, d, i0, i1);
         };
-        const std::vector<bool> occ(nband, true);
+        std::vector<bool> occ(nband, true);
+        if (occupied)
+            for (int m = 0; m < nband; ++m) occ[m] = occupied[m] != 0;
         const int it = dav.diag(hpsi, static_cast<T*>(psi), ldpsi, eig, occ, scf != 0);
         if (iters) *iters = it;
         g_err_ds.clear();

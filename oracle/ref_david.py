@@ -55,14 +55,15 @@ def diag(hpsi, precond, nband, dim, david_ndim, ldpsi, psi, eig, thr, maxiter, n
     return it.value
 
 
-def dav_subspace(hpsi, precond, nband, dim, david_ndim, ldpsi, psi, eig, thr, maxiter, need_subspace=False, scf=False):
-    """Diago_DavSubspace<complex<double>, CPU>::diag (all bands occupied).  hpsi as for diag; psi and eig are
-    updated in place; returns the iteration count."""
+def dav_subspace(hpsi, precond, nband, dim, david_ndim, ldpsi, psi, eig, thr, maxiter, need_subspace=False, scf=False,
+                 occupied=None):
+    """Diago_DavSubspace<complex<double>, CPU>::diag; occupied: nband flags (None: all bands occupied).  hpsi as
+    for diag; psi and eig are updated in place; returns the iteration count."""
     lib = _load()
     if not hasattr(lib, "_ds_ready"):
         lib.ref_dav_subspace.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_double), _CB, C.c_void_p,
                                          C.c_void_p, C.POINTER(C.c_double), C.c_double, C.c_int, C.c_int, C.c_int,
-                                         C.POINTER(C.c_int)]
+                                         C.POINTER(C.c_int), C.POINTER(C.c_int)]
         lib.ref_dav_subspace.restype = C.c_int
         lib.ref_dav_subspace_last_error.restype = C.c_char_p
         lib._ds_ready = True
@@ -77,9 +78,11 @@ def dav_subspace(hpsi, precond, nband, dim, david_ndim, ldpsi, psi, eig, thr, ma
     fn = _CB(cb)
     pc = np.ascontiguousarray(precond, dtype=np.float64)
     it = C.c_int()
+    occ = None if occupied is None else np.ascontiguousarray(np.asarray(occupied, dtype=bool).astype(np.int32))
     rc = lib.ref_dav_subspace(nband, dim, david_ndim, ldpsi, pc.ctypes.data_as(C.POINTER(C.c_double)), fn, None,
                               psi.ctypes.data, eig.ctypes.data_as(C.POINTER(C.c_double)), thr, maxiter,
-                              int(bool(need_subspace)), int(bool(scf)), C.byref(it))
+                              int(bool(need_subspace)), int(bool(scf)),
+                              None if occ is None else occ.ctypes.data_as(C.POINTER(C.c_int)), C.byref(it))
     if rc != 0:
         raise RuntimeError("reference Diago_DavSubspace failed: " + lib.ref_dav_subspace_last_error().decode())
     return it.value

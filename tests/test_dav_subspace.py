@@ -75,3 +75,30 @@ def test_reference_dav_subspace_pins_the_oracle_on_a_plane_wave_cell():
     it_o = DavSubspaceRef(pc, nb, npw, 4, 1e-9, 100).diag(hp, p_o, e_o)
     assert it_o == it_r
     assert np.max(np.abs(e_o - e_r)) < 1e-11
+
+
+@pytest.mark.parametrize("scf", [False, True])
+def test_reference_dav_subspace_pins_the_empty_band_rule(scf):
+    """Empty bands converge at max(5 thr, 1e-5) (diago_dav_subspace.cpp:186-194): the oracle and the compiled
+    reference with the same occupation flags on a seeded Hermitian matrix."""
+    rng = np.random.default_rng(21)
+    n, nband = 240, 6
+    a = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
+    A = 0.05 * (a + a.conj().T) + np.diag(np.linspace(0.0, 20.0, n))
+    pc = np.real(np.diag(A)).copy()
+    q, _ = np.linalg.qr(rng.standard_normal((n, nband)) + 0j)
+    psi0 = np.ascontiguousarray(q.T)
+    occ = [True, True, True, False, False, False]
+    thr = 1e-10
+    psi_r, e_r = psi0.copy(), np.zeros(nband)
+    it_r = ref_david.dav_subspace(lambda x, nv, d, i0, i1: (A @ x[i0:i1 + 1].T).T, pc, nband, n, 4, n, psi_r, e_r,
+                                  thr, 300, False, scf, occupied=occ)
+    psi_o, e_o = psi0.copy(), np.zeros(nband)
+    it_o = DavSubspaceRef(pc, nband, n, 4, thr, 300).diag(lambda x: (A @ x.T).T, psi_o, e_o, scf, occ)
+    assert it_o == it_r
+    assert np.max(np.abs(e_o - e_r)) < 1e-12
+    w = np.linalg.eigvalsh(A)[:nband]
+    assert np.max(np.abs(e_o[:3] - w[:3])) < 1e-8
+    e_all = np.zeros(nband)
+    it_all = DavSubspaceRef(pc, nband, n, 4, thr, 300).diag(lambda x: (A @ x.T).T, psi0.copy(), e_all, scf)
+    assert it_o < it_all  # the empty bands' looser threshold ends the solve earlier (21 against 31 iterations)
