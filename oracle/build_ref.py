@@ -17,9 +17,12 @@ Compiled from the reference (unchanged, from where they lie):
                                                    the psi / global-parameter / operator layer BPCG calls
   source/module_base/module_container/{ATen/core,ATen/ops,ATen/kernels,base/core}/*.cpp
                                                    the tensor library BPCG is written in (einsum, BLAS, LAPACK)
+  source/module_elecstate/occupy.cpp, module_base/matrix.cpp
+                                                   occupations (smearing weights, Fermi energy) of an NSCF run
 plus this directory's ref/shim.cpp (process-level services: WARNING_QUIT throws, TITLE is silent, the CPU
 device tag, a one-process reduce_pool, NPROC_IN_POOL = 1, diagH_LAPACK on the reference's dngvd_op) and
-ref/david_capi.cpp, ref/dav_subspace_capi.cpp, ref/bpcg_capi.cpp (C entry points with a callback H|psi>).
+ref/david_capi.cpp, ref/dav_subspace_capi.cpp, ref/bpcg_capi.cpp (C entry points with a callback H|psi>),
+ref/occupy_capi.cpp (the occupation functions).
 ref/include/fftw3.h gives the FFTW type names that a header on BPCG's include chain declares members with
 (FFTW is absent; no FFTW routine is called or linked).
 
@@ -65,9 +68,12 @@ SOURCES = [
     "module_base/module_container/ATen/kernels/memory_impl.cpp",
     "module_base/module_container/base/core/cpu_allocator.cpp",
     "module_base/module_container/base/core/refcount.cpp",
+    # the occupation code of the NSCF weights and the matrix class it takes
+    "module_elecstate/occupy.cpp",
+    "module_base/matrix.cpp",
 ]
 OWN = [HERE / "ref" / "shim.cpp", HERE / "ref" / "david_capi.cpp", HERE / "ref" / "dav_subspace_capi.cpp",
-       HERE / "ref" / "bpcg_capi.cpp"]
+       HERE / "ref" / "bpcg_capi.cpp", HERE / "ref" / "occupy_capi.cpp"]
 
 
 def openblas() -> Path:

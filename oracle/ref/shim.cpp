@@ -9,12 +9,15 @@
 // * Parallel_Reduce::reduce_pool (module_base/parallel_reduce.h:21-23): a sum over the processes of a pool;
 //   with one process it leaves the data unchanged.
 // * ModuleBase::Memory::record (module_base/memory.h): bookkeeping of allocated bytes, not kept here.
-// * GlobalV::NPROC_IN_POOL (module_base/global_variable.h): processes in a pool, 1.
+// * GlobalV::NPROC_IN_POOL (module_base/global_variable.h): processes in a pool, 1; GlobalV::NBANDS, the
+//   band count the occupation code reads; GlobalV::ofs_warning, an unopened stream (warnings dropped).
+// * ModuleBase::WARNING (module_base/tool_quit.h): a log line, dropped.
 // * DiagoIterAssist<T, CPU>::diagH_LAPACK (module_hsolver/diago_iter_assist.cpp): its body is the
 //   reference's dngvd_op (generalised eigenproblem, all pairs, compiled from dngvd_op.cpp) and a copy of the
 //   first nbands eigenvalues; restated here so that the rest of diago_iter_assist.cpp (the psi / Hamiltonian
 //   layers) is not needed.
 #include <complex>
+#include <fstream>
 #include <stdexcept>
 #include <string>
 
@@ -36,6 +39,7 @@ void WARNING_QUIT(const std::string& file, const std::string& description, int) 
     throw std::runtime_error(file + ": " + description);
 }
 void TITLE(const std::string&, const std::string&, const bool) {}
+void WARNING(const std::string&, const std::string&) {}
 void Memory::record(const std::string&, const size_t&, const bool) {}
 }  // namespace ModuleBase
 
@@ -52,6 +56,8 @@ template <> void reduce_pool<float>(float&) {}
 
 namespace GlobalV {
 int NPROC_IN_POOL = 1;
+int NBANDS = 0;                 // set by the occupation entry point before each call
+std::ofstream ofs_warning;      // never opened: warnings are dropped
 }  // namespace GlobalV
 
 namespace hsolver {

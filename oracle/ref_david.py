@@ -113,3 +113,25 @@ def bpcg(hpsi, precond, nband, nbasis, psi, eig, scf_iter=1, ncalls=1):
                       eig.ctypes.data_as(C.POINTER(C.c_double)), int(scf_iter), int(ncalls))
     if rc != 0:
         raise RuntimeError("reference DiagoBPCG failed: " + lib.ref_bpcg_last_error().decode())
+
+
+def gweights(ekb, wk, nelec, sigma, ngauss):
+    """Occupy::gweights (nspin 1): (wg, ef, demet) from the reference's compiled occupation code."""
+    lib = _load()
+    if not hasattr(lib, "_occ_ready"):
+        pd = C.POINTER(C.c_double)
+        lib.ref_gweights.argtypes = [C.c_int, pd, C.c_int, C.c_double, C.c_double, C.c_int, pd, pd, pd, pd]
+        lib.ref_gweights.restype = C.c_int
+        lib.ref_occupy_last_error.restype = C.c_char_p
+        lib._occ_ready = True
+    e = np.ascontiguousarray(ekb, dtype=np.float64)
+    w = np.ascontiguousarray(wk, dtype=np.float64)
+    nks, nband = e.shape
+    wg = np.zeros_like(e)
+    ef, demet = C.c_double(), C.c_double()
+    pd = C.POINTER(C.c_double)
+    rc = lib.ref_gweights(nks, w.ctypes.data_as(pd), nband, float(nelec), float(sigma), int(ngauss),
+                          e.ctypes.data_as(pd), C.byref(ef), C.byref(demet), wg.ctypes.data_as(pd))
+    if rc != 0:
+        raise RuntimeError("reference Occupy::gweights failed: " + lib.ref_occupy_last_error().decode())
+    return wg, ef.value, demet.value

@@ -1,6 +1,7 @@
 """The NSCF driver's k-point pool split on CPU (gloo, world size 2): each k-point solved by exactly one rank,
 the eigenvalues gathered on every rank, the band file written once (rank 0) with every k-point, the
-wavefunction files written by their owners and readable bit for bit.  The band solve is injected: a small
+wavefunction files written by their owners and readable bit for bit, smeared occupations from the gathered
+eigenvalues.  The band solve is injected: a small
 dense stand-in (exact eigenpairs of a per-k Hermitian matrix), since this test is about the host logic."""
 from __future__ import annotations
 
@@ -56,7 +57,10 @@ def _worker(rank, ws, port, outdir, q):
         psi0 = [np.zeros((nb, int(b.npwk[ik])), complex) for ik in range(b.nks)]
         res = pkg.nscf.run_nscf_pool(b, nb, psi0, _stand_in_solve(b), wk=[0.4] * b.nks, nelec=8.0, latvec=LATVEC,
                                      ecutwfc=8.0, pw_diag_thr=1e-9, out_dir=outdir, out_wfc_pw=2)
-        q.put((rank, res.iks, res.ekb.tolist(), res.ef, res.iters.tolist(), res.files.get("wfc", [])))
+        sm = pkg.nscf.run_nscf_pool(b, nb, psi0, _stand_in_solve(b), wk=[0.4] * b.nks, nelec=7.0, latvec=LATVEC,
+                                    ecutwfc=8.0, pw_diag_thr=1e-9, smearing=("mp", 0.01))
+        q.put((rank, res.iks, res.ekb.tolist(), res.ef, res.iters.tolist(), res.files.get("wfc", []), sm.ef,
+               sm.wg.tolist()))
     finally:
         dist.destroy_process_group()
 
@@ -76,11 +80,13 @@ def test_nscf_pool_two_ranks(pkg, tmp_path):
     nb = 6
     ekb_ref, psi_ref = _stand_in_solve(b)(list(range(b.nks)), [None] * b.nks, nb, 0.0)[0::2]
     owned = []
-    for rank, iks, ekb, ef, iters, wfc in res:
+    wg_s, ef_s, _ = pkg.nscf.smearing_weights(ekb_ref, [0.4] * b.nks, 7.0, 0.01, "mp")
+    for rank, iks, ekb, ef, iters, wfc, sm_ef, sm_wg in res:
         owned += iks
         assert np.array_equal(np.array(ekb), ekb_ref)          # gathered on every rank
         assert ef == float(np.max(ekb_ref[:, :4])) and iters == [7] * b.nks
         assert len(wfc) == len(iks)
+        assert sm_ef == ef_s and np.array_equal(np.array(sm_wg), wg_s)  # smeared occupations from the gather
     assert sorted(owned) == list(range(b.nks))
     band = (tmp_path / "BANDS_1.dat").read_text().rstrip("\n").split("\n")
     assert len(band) == b.nks and band[0].startswith("   1 0.00000000")
