@@ -60,12 +60,15 @@ def _worker(rank, ws, port, outdir, q):
         sm = pkg.nscf.run_nscf_pool(b, nb, psi0, _stand_in_solve(b), wk=[0.4] * b.nks, nelec=7.0, latvec=LATVEC,
                                     ecutwfc=8.0, pw_diag_thr=1e-9, smearing=("mp", 0.01))
         q.put((rank, res.iks, res.ekb.tolist(), res.ef, res.iters.tolist(), res.files.get("wfc", []), sm.ef,
-               sm.wg.tolist()))
+               sm.wg.tolist(), [np.asarray(x) for x in res.psis]))
     finally:
         dist.destroy_process_group()
 
 
-def test_nscf_pool_two_ranks(pkg, tmp_path):
+def test_nscf_pool_two_ranks(pkg, tmp_path, monkeypatch):
+    # one BLAS thread per rank: two ranks whose BLAS pools each span every core spend the test spinning
+    for var in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS"):
+        monkeypatch.setenv(var, "1")
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
@@ -78,19 +81,22 @@ def test_nscf_pool_two_ranks(pkg, tmp_path):
         assert p.exitcode == 0
     b = _basis(pkg)
     nb = 6
-    ekb_ref, psi_ref = _stand_in_solve(b)(list(range(b.nks)), [None] * b.nks, nb, 0.0)[0::2]
-    owned = []
-    wg_s, ef_s, _ = pkg.nscf.smearing_weights(ekb_ref, [0.4] * b.nks, 7.0, 0.01, "mp")
-    for rank, iks, ekb, ef, iters, wfc, sm_ef, sm_wg in res:
+    ekb_ref = _stand_in_solve(b)(list(range(b.nks)), [None] * b.nks, nb, 0.0)[0]
+    gathered = np.array(res[0][2])
+    assert np.max(np.abs(gathered - ekb_ref)) < 1e-12     # the ranks' BLAS threads differ from this process's
+    wg_s, ef_s, _ = pkg.nscf.smearing_weights(gathered, [0.4] * b.nks, 7.0, 0.01, "mp")
+    owned, psi_by_k = [], {}
+    for rank, iks, ekb, ef, iters, wfc, sm_ef, sm_wg, psis in res:
         owned += iks
-        assert np.array_equal(np.array(ekb), ekb_ref)          # gathered on every rank
-        assert ef == float(np.max(ekb_ref[:, :4])) and iters == [7] * b.nks
+        assert np.array_equal(np.array(ekb), gathered)         # the same gathered array on every rank
+        assert ef == float(np.max(gathered[:, :4])) and iters == [7] * b.nks
         assert len(wfc) == len(iks)
         assert sm_ef == ef_s and np.array_equal(np.array(sm_wg), wg_s)  # smeared occupations from the gather
+        psi_by_k.update(zip(iks, psis))
     assert sorted(owned) == list(range(b.nks))
     band = (tmp_path / "BANDS_1.dat").read_text().rstrip("\n").split("\n")
     assert len(band) == b.nks and band[0].startswith("   1 0.00000000")
     io = pkg.nscf_io
     for ik in range(b.nks):
         back = io.read_wfc_pw(tmp_path / f"WAVEFUNC{ik + 1}.dat", b, ik, b.nks, nb, LATVEC)
-        assert np.array_equal(back, psi_ref[ik])
+        assert np.array_equal(back, psi_by_k[ik])
