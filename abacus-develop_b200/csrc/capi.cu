@@ -310,8 +310,9 @@ int b200_hamilt_hpsi_part(b200_hamilt* h, int ik, int spin, int nbands, int ld, 
 int b200_david_create(int nband, int dim, int david_ndim, int precision, const double* precond, b200_david** out) {
     return guarded([&] {
         B200_CHECK(out && precond, b200::kInvalidArgument, "NULL argument");
+        auto d = b200::make_david(nband, dim, david_ndim, precision, precond);  // arguments checked first
         auto p = std::make_unique<b200_david>();
-        p->d = b200::make_david(nband, dim, david_ndim, precision, precond);
+        p->d = std::move(d);
         *out = p.release();
     });
 }
@@ -425,8 +426,10 @@ int b200_dav_subspace_create(int nband, int dim, int david_ndim, double diag_thr
                              const double* precond, b200_dav_subspace** out) {
     return guarded([&] {
         B200_CHECK(out && precond, b200::kInvalidArgument, "NULL argument");
+        // the solver (which checks its arguments before any device call) before the handle's H|psi> scratch
+        auto d = b200::make_dav_subspace(nband, dim, david_ndim, diag_thr, diag_nmax, need_subspace != 0, precond);
         auto p = std::make_unique<b200_dav_subspace>();
-        p->d = b200::make_dav_subspace(nband, dim, david_ndim, diag_thr, diag_nmax, need_subspace != 0, precond);
+        p->d = std::move(d);
         *out = p.release();
     });
 }
@@ -482,8 +485,9 @@ int b200_dav_subspace_stats(const b200_dav_subspace* d, int* notconv, int* hpsi_
 int b200_bpcg_create(const double* precond, int nband, int nbasis, b200_bpcg** out) {
     return guarded([&] {
         B200_CHECK(out && precond, b200::kInvalidArgument, "NULL argument");
+        auto d = b200::make_bpcg(nband, nbasis, precond);  // arguments checked before any device call
         auto p = std::make_unique<b200_bpcg>();
-        p->d = b200::make_bpcg(nband, nbasis, precond);
+        p->d = std::move(d);
         *out = p.release();
     });
 }

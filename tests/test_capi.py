@@ -65,3 +65,31 @@ def test_host_basis_rejects_bad_input(pkg):
         pkg.pwdft.PWBasisK(10.0, np.zeros((3, 3)), 30.0, np.zeros((1, 3)))
     with pytest.raises(pkg._lib.B200Error):
         pkg.pwdft.PWBasisK(10.0, np.eye(3), -1.0, np.zeros((1, 3)))
+
+
+def test_solver_entry_points_reject_bad_arguments_without_gpu_calls(pkg):
+    """The Diago_DavSubspace and DiagoBPCG entry points check their arguments before any device call; a bad
+    one is a B200_STATUS_INVALID_ARGUMENT status with a message, never an exit."""
+    lib = pkg._lib.load()
+    out = ctypes.c_void_p()
+    fake = ctypes.c_void_p(16)  # never dereferenced: every call below fails its checks first
+    no_cb = pkg._lib.HPSI_CB()  # a NULL callback
+    cases = [
+        (lib.b200_dav_subspace_create, (4, 100, 2, 1e-9, 50, 0, None, ctypes.byref(out)), b"NULL"),
+        (lib.b200_dav_subspace_create, (4, 10, 3, 1e-9, 50, 0, fake, ctypes.byref(out)), b"david_ndim"),
+        (lib.b200_dav_subspace_create, (4, 100, 2, 1e-9, 0, 0, fake, ctypes.byref(out)), b"diag_nmax"),
+        (lib.b200_dav_subspace_diag, (None, no_cb, None, fake, 100, None, None, 0, None), b"NULL"),
+        (lib.b200_dav_subspace_diag_hamilt, (None, None, 0, 0, fake, 100, None, None, 0, None), b"NULL"),
+        (lib.b200_dav_subspace_set_stream, (None, None), b"NULL"),
+        (lib.b200_dav_subspace_stats, (None, None, None), b"NULL"),
+        (lib.b200_bpcg_create, (None, 4, 100, ctypes.byref(out)), b"NULL"),
+        (lib.b200_bpcg_create, (fake, 8, 4, ctypes.byref(out)), b"nband"),
+        (lib.b200_bpcg_diag, (None, no_cb, None, fake, None, 1, None), b"NULL"),
+        (lib.b200_bpcg_diag_hamilt, (None, None, 0, 0, fake, None, 1, None), b"NULL"),
+        (lib.b200_bpcg_set_stream, (None, None), b"NULL"),
+        (lib.b200_bpcg_stats, (None, None, None), b"NULL"),
+    ]
+    for fn, args, msg in cases:
+        assert fn(*args) == 1, fn.__name__
+        assert msg in lib.b200_last_error(), (fn.__name__, lib.b200_last_error())
+    assert out.value is None  # nothing was created
