@@ -95,6 +95,10 @@ _SIGS = {
                             i32, i32, i32, pi32], i32),
     "b200_tc_cgemm": ([C.c_char, C.c_char, i32, i32, i32, f32, f32, vp, i32, vp, i32, f32, f32, vp, i32, vp], i32),
     "b200_tc_cgemm_error": ([pi32], i32),
+    "b200_gemm_op_f64": ([C.c_char, C.c_char, i32, i32, i32, pf64, vp, i32, vp, i32, pf64, vp, i32, vp], i32),
+    "b200_gemv_op_f64": ([C.c_char, i32, i32, pf64, vp, i32, vp, i32, pf64, vp, i32, vp], i32),
+    "b200_dot_real_op_f64": ([i32, vp, vp, i32, pf64, vp], i32),
+    "b200_dot_real_op_f32": ([i32, vp, vp, i32, C.POINTER(C.c_float), vp], i32),
     "b200_david_create": ([i32, i32, i32, i32, vp, C.POINTER(vp)], i32),
     "b200_david_destroy": ([vp], i32),
     "b200_david_diag": ([vp, HPSI_CB, vp, i32, vp, pf64, f64, i32, i32, i32, pi32], i32),

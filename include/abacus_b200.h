@@ -278,6 +278,23 @@ int b200_tc_cgemm(char transa, char transb, int m, int n, int k, float alpha_re,
  * wait inside a kernel ran out (the kernel then returned without finishing its tile). */
 int b200_tc_cgemm_error(int* code);
 
+/* ---- FP64 BLAS functors of the Davidson / nonlocal path (module_hsolver/kernels/math_kernel_op.h) ----
+ * gemm_op<std::complex<double>, DEVICE_GPU> (math_kernel_op.h:240-265, cuda/math_kernel_op.cu:815-874):
+ * C = alpha op(A) op(B) + beta C, column-major, trans 'N' / 'T' / 'C'; alpha, beta: host complex
+ * (2 doubles each).  cuBLAS ZGEMM, as the reference. */
+int b200_gemm_op_f64(char transa, char transb, int m, int n, int k, const double* alpha, const void* a_d, int lda,
+                     const void* b_d, int ldb, const double* beta, void* c_d, int ldc, void* stream);
+/* gemv_op<std::complex<double>, DEVICE_GPU> (math_kernel_op.h:214-237, cuda/math_kernel_op.cu:741-792):
+ * y = alpha op(A) x + beta y.  The reference passes incx as y's increment; incy is used here (the same
+ * for the reference's callers, which pass incx == incy). */
+int b200_gemv_op_f64(char trans, int m, int n, const double* alpha, const void* a_d, int lda, const void* x_d,
+                     int incx, const double* beta, void* y_d, int incy, void* stream);
+/* dot_real_op<std::complex<T>, DEVICE_GPU> (math_kernel_op.h:86-104, cuda/math_kernel_op.cu:468-506):
+ * Re sum conj(L) R over dim complex entries, returned on the host (the call synchronises the stream);
+ * reduce (the pool reduction) is the identity with one process per pool.  Deterministic two-pass sum. */
+int b200_dot_real_op_f64(int dim, const void* psi_l_d, const void* psi_r_d, int reduce, double* result, void* stream);
+int b200_dot_real_op_f32(int dim, const void* psi_l_d, const void* psi_r_d, int reduce, float* result, void* stream);
+
 /* ------------------------------------------------------------------ Davidson
  * hsolver::DiagoDavid<T, DEVICE_GPU> (module_hsolver/diago_david.h:19-84):
  * constructor (precondition, nband, dim, david_ndim, use_paw = false) and
