@@ -1,0 +1,72 @@
+// Test infrastructure (oracle): a C entry point to the reference's own PW_Basis_K set-up
+// (module_basis/module_pw/pw_init.cpp, pw_basis.cpp, pw_basis_k.cpp, pw_distributeg*.cpp, compiled from the
+// reference sources by oracle/build_ref.py; FFTW plans through the stand-in of oracle/ref/fftw_stub.cpp, never
+// executed), for comparing its plane-wave spheres and index maps with this library's.  The product never
+// loads it.
+//
+// As ESolver_KS_PW sets the wavefunction basis up: the charge grid from ecutrho (initgrids(lat0, latvec,
+// ecutrho), the 2,3,5-smooth rule) unless an explicit grid is given, then the wavefunction basis on that grid
+// (initgrids(lat0, latvec, nx, ny, nz)), initparameters(gamma_only = false, ecutwfc, nks, kvec_d),
+// setuptransform, collect_local_pw and get_ig2ixyz_k.
+#include <exception>
+#include <string>
+#include <vector>
+
+#include "module_base/matrix3.h"
+#include "module_base/vector3.h"
+#include "module_basis/module_pw/pw_basis.h"
+#include "module_basis/module_pw/pw_basis_k.h"
+
+namespace {
+std::string g_err_pw;
+}
+
+extern "C" {
+
+const char* ref_pw_basis_last_error() { return g_err_pw.c_str(); }
+
+// latvec: 9 doubles, rows a1, a2, a3 in units of lat0; kvec_d: nks x 3.  Outputs: dims = (nx, ny, nz,
+// npwk_max); npwk: nks; ig2ixyz and gk2: nks x cap entries (k-point ik at ik * cap), filled when
+// cap >= npwk_max (otherwise only dims and npwk are written).  Returns 0 on success.
+int ref_pw_basis_k(double lat0, const double* latvec, double ecutwfc, double ecutrho, int nx, int ny, int nz, int nks,
+                   const double* kvec_d, int* dims, int* npwk, int cap, int* ig2ixyz, double* gk2) {
+    try {
+        const ModuleBase::Matrix3 lv(latvec[0], latvec[1], latvec[2], latvec[3], latvec[4], latvec[5], latvec[6],
+                                     latvec[7], latvec[8]);
+        int gx = nx, gy = ny, gz = nz;
+        if (gx <= 0 || gy <= 0 || gz <= 0) {
+            ModulePW::PW_Basis rho;
+            rho.initgrids(lat0, lv, ecutrho);
+            gx = rho.nx;
+            gy = rho.ny;
+            gz = rho.nz;
+        }
+        std::vector<ModuleBase::Vector3<double>> kd(nks);
+        for (int ik = 0; ik < nks; ++ik) kd[ik] = ModuleBase::Vector3<double>(kvec_d[3 * ik], kvec_d[3 * ik + 1], kvec_d[3 * ik + 2]);
+        ModulePW::PW_Basis_K wfc;
+        wfc.initgrids(lat0, lv, gx, gy, gz);
+        wfc.initparameters(false, ecutwfc, nks, kd.data());
+        wfc.setuptransform();
+        wfc.collect_local_pw();
+        wfc.get_ig2ixyz_k();
+        dims[0] = wfc.nx;
+        dims[1] = wfc.ny;
+        dims[2] = wfc.nz;
+        dims[3] = wfc.npwk_max;
+        for (int ik = 0; ik < nks; ++ik) npwk[ik] = wfc.npwk[ik];
+        if (cap >= wfc.npwk_max && ig2ixyz && gk2) {
+            for (int ik = 0; ik < nks; ++ik)
+                for (int ig = 0; ig < wfc.npwk[ik]; ++ig) {
+                    ig2ixyz[ik * cap + ig] = wfc.ig2ixyz_k_[ik * wfc.npwk_max + ig];
+                    gk2[ik * cap + ig] = wfc.gk2[ik * wfc.npwk_max + ig];
+                }
+        }
+        g_err_pw.clear();
+        return 0;
+    } catch (const std::exception& e) {
+        g_err_pw = e.what();
+        return 1;
+    }
+}
+
+}  // extern "C"

@@ -11,7 +11,8 @@
 // * ModuleBase::Memory::record (module_base/memory.h): bookkeeping of allocated bytes, not kept here.
 // * GlobalV::NPROC_IN_POOL (module_base/global_variable.h): processes in a pool, 1; GlobalV::NBANDS, the
 //   band count the occupation code reads; GlobalV::ofs_warning, an unopened stream (warnings dropped).
-// * ModuleBase::WARNING (module_base/tool_quit.h): a log line, dropped.
+// * ModuleBase::WARNING (module_base/tool_quit.h): a log line, dropped; CHECK_WARNING_QUIT throws when its
+//   condition holds, as WARNING_QUIT.
 // * DiagoIterAssist<T, CPU>::diagH_LAPACK (module_hsolver/diago_iter_assist.cpp): its body is the
 //   reference's dngvd_op (generalised eigenproblem, all pairs, compiled from dngvd_op.cpp) and a copy of the
 //   first nbands eigenvalues; restated here so that the rest of diago_iter_assist.cpp (the psi / Hamiltonian
@@ -40,6 +41,10 @@ void WARNING_QUIT(const std::string& file, const std::string& description, int) 
 }
 void TITLE(const std::string&, const std::string&, const bool) {}
 void WARNING(const std::string&, const std::string&) {}
+void CHECK_WARNING_QUIT(const bool error_in, const std::string& file, const std::string& calculation,
+                        const std::string& description) {
+    if (error_in) throw std::runtime_error(file + " (" + calculation + "): " + description);
+}
 void Memory::record(const std::string&, const size_t&, const bool) {}
 }  // namespace ModuleBase
 

@@ -135,3 +135,39 @@ def gweights(ekb, wk, nelec, sigma, ngauss):
     if rc != 0:
         raise RuntimeError("reference Occupy::gweights failed: " + lib.ref_occupy_last_error().decode())
     return wg, ef.value, demet.value
+
+
+def pw_basis_k(lat0, latvec, ecutwfc, kvec_d, ecutrho=None, grid=None):
+    """The reference's own PW_Basis_K set-up (as ESolver_KS_PW builds the wavefunction basis): returns
+    (nx, ny, nz), npwk per k-point, and per k-point ig2ixyz (iz + iy nz + ix ny nz) and gk2 arrays."""
+    lib = _load()
+    pd, pi = C.POINTER(C.c_double), C.POINTER(C.c_int)
+    if not hasattr(lib, "_pw_ready"):
+        lib.ref_pw_basis_k.argtypes = [C.c_double, pd, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, C.c_int,
+                                       pd, pi, pi, C.c_int, pi, pd]
+        lib.ref_pw_basis_k.restype = C.c_int
+        lib.ref_pw_basis_last_error.restype = C.c_char_p
+        lib._pw_ready = True
+    kd = np.ascontiguousarray(np.atleast_2d(kvec_d), dtype=np.float64)
+    nks = len(kd)
+    lv = np.ascontiguousarray(np.asarray(latvec, dtype=np.float64).reshape(9))
+    gx, gy, gz = grid if grid is not None else (0, 0, 0)
+    ecutrho = 4.0 * ecutwfc if ecutrho is None else ecutrho
+    dims = np.zeros(4, dtype=np.int32)
+    npwk = np.zeros(nks, dtype=np.int32)
+
+    def call(cap, ig, g2):
+        rc = lib.ref_pw_basis_k(lat0, lv.ctypes.data_as(pd), ecutwfc, ecutrho, gx, gy, gz, nks, kd.ctypes.data_as(pd),
+                                dims.ctypes.data_as(pi), npwk.ctypes.data_as(pi), cap,
+                                None if ig is None else ig.ctypes.data_as(pi),
+                                None if g2 is None else g2.ctypes.data_as(pd))
+        if rc != 0:
+            raise RuntimeError("reference PW_Basis_K set-up failed: " + lib.ref_pw_basis_last_error().decode())
+
+    call(0, None, None)
+    cap = int(dims[3])
+    ig = np.zeros((nks, cap), dtype=np.int32)
+    g2 = np.zeros((nks, cap))
+    call(cap, ig, g2)
+    return (tuple(int(v) for v in dims[:3]), npwk.astype(np.int64),
+            [ig[ik, :npwk[ik]].astype(np.int64) for ik in range(nks)], [g2[ik, :npwk[ik]].copy() for ik in range(nks)])
