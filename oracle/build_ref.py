@@ -19,14 +19,15 @@ Compiled from the reference (unchanged, from where they lie):
                                                    the tensor library BPCG is written in (einsum, BLAS, LAPACK)
   source/module_elecstate/occupy.cpp, module_base/matrix.cpp
                                                    occupations (smearing weights, Fermi energy) of an NSCF run
-  source/module_basis/module_pw/{pw_basis,pw_basis_k,pw_init,pw_distributeg*,pw_distributer,fft}.cpp,
-  module_base/matrix3.cpp, module_base/mymath.cpp    the plane-wave basis set-up (its FFT plans never executed)
+  source/module_basis/module_pw/{pw_basis,pw_basis_k,pw_init,pw_distributeg*,pw_distributer,fft,
+  pw_transform_k}.cpp, module_base/matrix3.cpp, module_base/mymath.cpp
+                                                   the plane-wave basis and its transforms
 plus this directory's ref/shim.cpp (process-level services: WARNING_QUIT throws, TITLE is silent, the CPU
 device tag, a one-process reduce_pool, NPROC_IN_POOL = 1, diagH_LAPACK on the reference's dngvd_op) and
 ref/david_capi.cpp, ref/dav_subspace_capi.cpp, ref/bpcg_capi.cpp (C entry points with a callback H|psi>),
 ref/occupy_capi.cpp (the occupation functions), ref/pw_basis_capi.cpp (the basis set-up).
-ref/include/fftw3.h declares the FFTW API names those sources use and ref/fftw_stub.cpp stands in for them at
-link time (FFTW is absent): buffers are allocated, plans are placeholders, executing one throws.
+ref/include/fftw3.h declares the FFTW API names those sources use and ref/fftw_stub.cpp stands in for them
+(FFTW is absent): plans record a batch of 1-D complex transforms that executing evaluates as direct DFTs.
 
 The reference calls Fortran BLAS/LAPACK (zgemm_, zheevx_, ...); scipy's OpenBLAS exports the same routines
 under a scipy_ prefix, so the object files' references are renamed with objcopy before linking.
@@ -82,6 +83,7 @@ SOURCES = [
     "module_basis/module_pw/pw_distributeg_method2.cpp",
     "module_basis/module_pw/pw_distributer.cpp",
     "module_basis/module_pw/fft.cpp",
+    "module_basis/module_pw/pw_transform_k.cpp",
     "module_base/matrix3.cpp",
     "module_base/mymath.cpp",
 ]

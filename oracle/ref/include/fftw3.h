@@ -1,9 +1,9 @@
 /* Test infrastructure (oracle build only): compile-time stand-in for FFTW's API, as far as the reference's
- * sources on this library's reference builds name it.  FFTW is absent here.  DiagoBPCG's header reaches
- * module_basis/module_pw/fft.h, which declares FFTW plan members; the PW_Basis_K set-up (pw_basis*.cpp,
- * fft.cpp) is compiled to compare its index maps with this library's, so fft.cpp's plan set-up must link.
- * oracle/ref/fftw_stub.cpp defines these routines as stand-ins that allocate (fftw_malloc / fftw_free) and
- * return placeholder plans; executing a plan throws -- no transform is ever computed through them. */
+ * sources in this oracle's builds name it (FFTW is absent here): DiagoBPCG's header reaches
+ * module_basis/module_pw/fft.h, and the reference's PW_Basis_K set-up and transforms (pw_basis*.cpp, fft.cpp,
+ * pw_transform_k.cpp) are compiled to compare their maps and transforms with this repository's.
+ * oracle/ref/fftw_stub.cpp defines these routines: plans record a batch of one-dimensional complex lines,
+ * executing one evaluates each line's DFT directly (slow, exact enough for the small parity grids). */
 #pragma once
 #include <stddef.h>
 

@@ -8,7 +8,9 @@
 // ecutrho), the 2,3,5-smooth rule) unless an explicit grid is given, then the wavefunction basis on that grid
 // (initgrids(lat0, latvec, nx, ny, nz)), initparameters(gamma_only = false, ecutwfc, nks, kvec_d),
 // setuptransform, collect_local_pw and get_ig2ixyz_k.
+#include <complex>
 #include <exception>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -19,7 +21,31 @@
 
 namespace {
 std::string g_err_pw;
+
+// the wavefunction basis as ESolver_KS_PW builds it (see the file comment)
+std::unique_ptr<ModulePW::PW_Basis_K> make_basis(double lat0, const double* latvec, double ecutwfc, double ecutrho,
+                                                 int nx, int ny, int nz, int nks, const double* kvec_d) {
+    const ModuleBase::Matrix3 lv(latvec[0], latvec[1], latvec[2], latvec[3], latvec[4], latvec[5], latvec[6],
+                                 latvec[7], latvec[8]);
+    int gx = nx, gy = ny, gz = nz;
+    if (gx <= 0 || gy <= 0 || gz <= 0) {
+        ModulePW::PW_Basis rho;
+        rho.initgrids(lat0, lv, ecutrho);
+        gx = rho.nx;
+        gy = rho.ny;
+        gz = rho.nz;
+    }
+    std::vector<ModuleBase::Vector3<double>> kd(nks);
+    for (int ik = 0; ik < nks; ++ik) kd[ik] = ModuleBase::Vector3<double>(kvec_d[3 * ik], kvec_d[3 * ik + 1], kvec_d[3 * ik + 2]);
+    auto wfc = std::make_unique<ModulePW::PW_Basis_K>();
+    wfc->initgrids(lat0, lv, gx, gy, gz);
+    wfc->initparameters(false, ecutwfc, nks, kd.data());
+    wfc->setuptransform();
+    wfc->collect_local_pw();
+    wfc->get_ig2ixyz_k();
+    return wfc;
 }
+}  // namespace
 
 extern "C" {
 
@@ -31,24 +57,8 @@ const char* ref_pw_basis_last_error() { return g_err_pw.c_str(); }
 int ref_pw_basis_k(double lat0, const double* latvec, double ecutwfc, double ecutrho, int nx, int ny, int nz, int nks,
                    const double* kvec_d, int* dims, int* npwk, int cap, int* ig2ixyz, double* gk2) {
     try {
-        const ModuleBase::Matrix3 lv(latvec[0], latvec[1], latvec[2], latvec[3], latvec[4], latvec[5], latvec[6],
-                                     latvec[7], latvec[8]);
-        int gx = nx, gy = ny, gz = nz;
-        if (gx <= 0 || gy <= 0 || gz <= 0) {
-            ModulePW::PW_Basis rho;
-            rho.initgrids(lat0, lv, ecutrho);
-            gx = rho.nx;
-            gy = rho.ny;
-            gz = rho.nz;
-        }
-        std::vector<ModuleBase::Vector3<double>> kd(nks);
-        for (int ik = 0; ik < nks; ++ik) kd[ik] = ModuleBase::Vector3<double>(kvec_d[3 * ik], kvec_d[3 * ik + 1], kvec_d[3 * ik + 2]);
-        ModulePW::PW_Basis_K wfc;
-        wfc.initgrids(lat0, lv, gx, gy, gz);
-        wfc.initparameters(false, ecutwfc, nks, kd.data());
-        wfc.setuptransform();
-        wfc.collect_local_pw();
-        wfc.get_ig2ixyz_k();
+        auto b = make_basis(lat0, latvec, ecutwfc, ecutrho, nx, ny, nz, nks, kvec_d);
+        ModulePW::PW_Basis_K& wfc = *b;
         dims[0] = wfc.nx;
         dims[1] = wfc.ny;
         dims[2] = wfc.nz;
@@ -61,6 +71,27 @@ int ref_pw_basis_k(double lat0, const double* latvec, double ecutwfc, double ecu
                     gk2[ik * cap + ig] = wfc.gk2[ik * wfc.npwk_max + ig];
                 }
         }
+        g_err_pw.clear();
+        return 0;
+    } catch (const std::exception& e) {
+        g_err_pw = e.what();
+        return 1;
+    }
+}
+
+// PW_Basis_K::recip2real (inverse != 0: npwk[ik] coefficients -> nx ny nz box, r order) or real2recip
+// (inverse == 0: box -> coefficients) <double> of k-point ik, with add / factor as the reference
+// (pw_transform_k.cpp:26-213), through its FFT class on the stand-in transforms of oracle/ref/fftw_stub.cpp.
+int ref_pw_transform(double lat0, const double* latvec, double ecutwfc, double ecutrho, int nx, int ny, int nz,
+                     int nks, const double* kvec_d, int ik, int inverse, const void* in, void* out, int add,
+                     double factor) {
+    try {
+        auto b = make_basis(lat0, latvec, ecutwfc, ecutrho, nx, ny, nz, nks, kvec_d);
+        using C = std::complex<double>;
+        if (inverse)
+            b->recip2real<double>(static_cast<const C*>(in), static_cast<C*>(out), ik, add != 0, factor);
+        else
+            b->real2recip<double>(static_cast<const C*>(in), static_cast<C*>(out), ik, add != 0, factor);
         g_err_pw.clear();
         return 0;
     } catch (const std::exception& e) {

@@ -171,3 +171,31 @@ def pw_basis_k(lat0, latvec, ecutwfc, kvec_d, ecutrho=None, grid=None):
     call(cap, ig, g2)
     return (tuple(int(v) for v in dims[:3]), npwk.astype(np.int64),
             [ig[ik, :npwk[ik]].astype(np.int64) for ik in range(nks)], [g2[ik, :npwk[ik]].copy() for ik in range(nks)])
+
+
+def pw_transform(lat0, latvec, ecutwfc, kvec_d, ik, inp, inverse, add=False, factor=1.0, out=None, ecutrho=None,
+                 grid=None):
+    """The reference's own PW_Basis_K::recip2real (inverse) / real2recip <double> of k-point ik on the basis
+    pw_basis_k() builds, its FFT lines evaluated by the oracle build's direct-DFT stand-in for FFTW.  inp / out
+    are complex128 arrays (npwk coefficients or the nx ny nz box in r order); out is updated in place (add)."""
+    lib = _load()
+    pd = C.POINTER(C.c_double)
+    if not hasattr(lib, "_pwt_ready"):
+        lib.ref_pw_transform.argtypes = [C.c_double, pd, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, C.c_int,
+                                         pd, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_double]
+        lib.ref_pw_transform.restype = C.c_int
+        lib._pwt_ready = True
+    (nx, ny, nz), npwk, _, _ = pw_basis_k(lat0, latvec, ecutwfc, kvec_d, ecutrho=ecutrho, grid=grid)
+    kd = np.ascontiguousarray(np.atleast_2d(kvec_d), dtype=np.float64)
+    lv = np.ascontiguousarray(np.asarray(latvec, dtype=np.float64).reshape(9))
+    src = np.ascontiguousarray(inp, dtype=np.complex128)
+    n_out = nx * ny * nz if inverse else int(npwk[ik])
+    dst = np.zeros(n_out, dtype=np.complex128) if out is None else out
+    assert dst.dtype == np.complex128 and dst.flags.c_contiguous and dst.size == n_out
+    gx, gy, gz = grid if grid is not None else (0, 0, 0)
+    rc = lib.ref_pw_transform(lat0, lv.ctypes.data_as(pd), ecutwfc, 4.0 * ecutwfc if ecutrho is None else ecutrho,
+                              gx, gy, gz, len(kd), kd.ctypes.data_as(pd), ik, int(bool(inverse)), src.ctypes.data,
+                              dst.ctypes.data, int(bool(add)), float(factor))
+    if rc != 0:
+        raise RuntimeError("reference PW_Basis_K transform failed: " + lib.ref_pw_basis_last_error().decode())
+    return dst
