@@ -22,10 +22,13 @@ Compiled from the reference (unchanged, from where they lie):
   source/module_basis/module_pw/{pw_basis,pw_basis_k,pw_init,pw_distributeg*,pw_distributer,fft,
   pw_transform_k}.cpp, module_base/matrix3.cpp, module_base/mymath.cpp
                                                    the plane-wave basis and its transforms
+  source/module_hamilt_pw/hamilt_pwdft/{operator_pw/{operator_pw,ekinetic_pw,veff_pw},kernels/{ekinetic_op,
+  veff_op}}.cpp                                    the kinetic and local operators of H|psi>
 plus this directory's ref/shim.cpp (process-level services: WARNING_QUIT throws, TITLE is silent, the CPU
 device tag, a one-process reduce_pool, NPROC_IN_POOL = 1, diagH_LAPACK on the reference's dngvd_op) and
 ref/david_capi.cpp, ref/dav_subspace_capi.cpp, ref/bpcg_capi.cpp (C entry points with a callback H|psi>),
-ref/occupy_capi.cpp (the occupation functions), ref/pw_basis_capi.cpp (the basis set-up).
+ref/occupy_capi.cpp (the occupation functions), ref/pw_basis_capi.cpp (the basis set-up, its transforms
+and the local H|psi> operators).
 ref/include/fftw3.h declares the FFTW API names those sources use and ref/fftw_stub.cpp stands in for them
 (FFTW is absent): plans record a batch of 1-D complex transforms that executing evaluates as direct DFTs.
 
@@ -84,6 +87,12 @@ SOURCES = [
     "module_basis/module_pw/pw_distributer.cpp",
     "module_basis/module_pw/fft.cpp",
     "module_basis/module_pw/pw_transform_k.cpp",
+    # the kinetic and local operators of H|psi> and their CPU kernels
+    "module_hamilt_pw/hamilt_pwdft/operator_pw/operator_pw.cpp",
+    "module_hamilt_pw/hamilt_pwdft/operator_pw/ekinetic_pw.cpp",
+    "module_hamilt_pw/hamilt_pwdft/operator_pw/veff_pw.cpp",
+    "module_hamilt_pw/hamilt_pwdft/kernels/ekinetic_op.cpp",
+    "module_hamilt_pw/hamilt_pwdft/kernels/veff_op.cpp",
     "module_base/matrix3.cpp",
     "module_base/mymath.cpp",
 ]

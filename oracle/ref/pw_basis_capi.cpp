@@ -8,6 +8,7 @@
 // ecutrho), the 2,3,5-smooth rule) unless an explicit grid is given, then the wavefunction basis on that grid
 // (initgrids(lat0, latvec, nx, ny, nz)), initparameters(gamma_only = false, ecutwfc, nks, kvec_d),
 // setuptransform, collect_local_pw and get_ig2ixyz_k.
+#include <algorithm>
 #include <complex>
 #include <exception>
 #include <memory>
@@ -18,6 +19,8 @@
 #include "module_base/vector3.h"
 #include "module_basis/module_pw/pw_basis.h"
 #include "module_basis/module_pw/pw_basis_k.h"
+#include "module_hamilt_pw/hamilt_pwdft/operator_pw/ekinetic_pw.h"
+#include "module_hamilt_pw/hamilt_pwdft/operator_pw/veff_pw.h"
 
 namespace {
 std::string g_err_pw;
@@ -92,6 +95,34 @@ int ref_pw_transform(double lat0, const double* latvec, double ecutwfc, double e
             b->recip2real<double>(static_cast<const C*>(in), static_cast<C*>(out), ik, add != 0, factor);
         else
             b->real2recip<double>(static_cast<const C*>(in), static_cast<C*>(out), ik, add != 0, factor);
+        g_err_pw.clear();
+        return 0;
+    } catch (const std::exception& e) {
+        g_err_pw = e.what();
+        return 1;
+    }
+}
+
+// The kinetic and local parts of H|psi> for k-point ik by the reference's own operators, Ekinetic then Veff
+// (operator_pw/ekinetic_pw.cpp, veff_pw.cpp with kernels/ekinetic_op.cpp, veff_op.cpp), chained as
+// Operator::hPsi does for them (hpsi zeroed first, operator.cpp:39-88): psi and hpsi are nbands vectors at
+// stride npwk_max; veff: the nx ny nz box in r order (one spin).
+int ref_hpsi_local(double lat0, const double* latvec, double ecutwfc, double ecutrho, int nx, int ny, int nz, int nks,
+                   const double* kvec_d, int ik, const double* veff, int nbands, const void* psi, void* hpsi) {
+    try {
+        using T = std::complex<double>;
+        using Cpu = base_device::DEVICE_CPU;
+        auto b = make_basis(lat0, latvec, ecutwfc, ecutrho, nx, ny, nz, nks, kvec_d);
+        hamilt::Ekinetic<hamilt::OperatorPW<T, Cpu>> ek(b->tpiba2, b->gk2, b->nks, b->npwk_max);
+        std::vector<int> isk(nks, 0);
+        hamilt::Veff<hamilt::OperatorPW<T, Cpu>> ve(isk.data(), veff, 1, b->nrxx, b.get());
+        ek.init(ik);
+        ve.init(ik);
+        const int ld = b->npwk_max;
+        T* out = static_cast<T*>(hpsi);
+        std::fill(out, out + static_cast<size_t>(nbands) * ld, T(0.0, 0.0));
+        ek.act(nbands, ld, 1, static_cast<const T*>(psi), out, b->npwk[ik]);
+        ve.act(nbands, ld, 1, static_cast<const T*>(psi), out, b->npwk[ik]);
         g_err_pw.clear();
         return 0;
     } catch (const std::exception& e) {

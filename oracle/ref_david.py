@@ -199,3 +199,27 @@ def pw_transform(lat0, latvec, ecutwfc, kvec_d, ik, inp, inverse, add=False, fac
     if rc != 0:
         raise RuntimeError("reference PW_Basis_K transform failed: " + lib.ref_pw_basis_last_error().decode())
     return dst
+
+
+def hpsi_local(lat0, latvec, ecutwfc, kvec_d, ik, veff, psi, nbands, ecutrho=None, grid=None):
+    """The kinetic + local part of H|psi> of k-point ik by the reference's own Ekinetic and Veff operators on
+    the basis pw_basis_k() builds: psi (nbands x npwk_max complex) -> hpsi of the same shape."""
+    lib = _load()
+    pd = C.POINTER(C.c_double)
+    if not hasattr(lib, "_hl_ready"):
+        lib.ref_hpsi_local.argtypes = [C.c_double, pd, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, C.c_int, pd,
+                                       C.c_int, pd, C.c_int, C.c_void_p, C.c_void_p]
+        lib.ref_hpsi_local.restype = C.c_int
+        lib._hl_ready = True
+    kd = np.ascontiguousarray(np.atleast_2d(kvec_d), dtype=np.float64)
+    lv = np.ascontiguousarray(np.asarray(latvec, dtype=np.float64).reshape(9))
+    v = np.ascontiguousarray(veff, dtype=np.float64)
+    x = np.ascontiguousarray(psi, dtype=np.complex128)
+    out = np.zeros_like(x)
+    gx, gy, gz = grid if grid is not None else (0, 0, 0)
+    rc = lib.ref_hpsi_local(lat0, lv.ctypes.data_as(pd), ecutwfc, 4.0 * ecutwfc if ecutrho is None else ecutrho,
+                            gx, gy, gz, len(kd), kd.ctypes.data_as(pd), ik, v.ctypes.data_as(pd), nbands, x.ctypes.data,
+                            out.ctypes.data)
+    if rc != 0:
+        raise RuntimeError("reference local H|psi> failed: " + lib.ref_pw_basis_last_error().decode())
+    return out
