@@ -30,7 +30,7 @@ ref/david_capi.cpp, ref/dav_subspace_capi.cpp, ref/bpcg_capi.cpp (C entry points
 ref/occupy_capi.cpp (the occupation functions), ref/pw_basis_capi.cpp (the basis set-up, its transforms
 and the local H|psi> operators).
 ref/include/fftw3.h declares the FFTW API names those sources use and ref/fftw_stub.cpp stands in for them
-(FFTW is absent): plans record a batch of 1-D complex transforms that executing evaluates as direct DFTs.
+(FFTW is absent): plans record a batch of 1-D complex transforms that executing runs as mixed-radix FFTs.
 
 The reference calls Fortran BLAS/LAPACK (zgemm_, zheevx_, ...); scipy's OpenBLAS exports the same routines
 under a scipy_ prefix, so the object files' references are renamed with objcopy before linking.

@@ -3,7 +3,7 @@
  * module_basis/module_pw/fft.h, and the reference's PW_Basis_K set-up and transforms (pw_basis*.cpp, fft.cpp,
  * pw_transform_k.cpp) are compiled to compare their maps and transforms with this repository's.
  * oracle/ref/fftw_stub.cpp defines these routines: plans record a batch of one-dimensional complex lines,
- * executing one evaluates each line's DFT directly (slow, exact enough for the small parity grids). */
+ * executing one runs a mixed-radix (2, 3, 5) FFT on each line. */
 #pragma once
 #include <stddef.h>
 

@@ -176,7 +176,7 @@ def pw_basis_k(lat0, latvec, ecutwfc, kvec_d, ecutrho=None, grid=None):
 def pw_transform(lat0, latvec, ecutwfc, kvec_d, ik, inp, inverse, add=False, factor=1.0, out=None, ecutrho=None,
                  grid=None):
     """The reference's own PW_Basis_K::recip2real (inverse) / real2recip <double> of k-point ik on the basis
-    pw_basis_k() builds, its FFT lines evaluated by the oracle build's direct-DFT stand-in for FFTW.  inp / out
+    pw_basis_k() builds, its FFT lines evaluated by the oracle build's mixed-radix stand-in for FFTW.  inp / out
     are complex128 arrays (npwk coefficients or the nx ny nz box in r order); out is updated in place (add)."""
     lib = _load()
     pd = C.POINTER(C.c_double)

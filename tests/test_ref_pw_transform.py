@@ -1,7 +1,7 @@
 """The oracle's plane-wave transforms (oracle/hamilt_ref.py: sphere <-> box with a 3-D FFT) against the
 reference's own PW_Basis_K::recip2real / real2recip <double> (pw_transform_k.cpp: stick scatter, z FFTs,
 stick-to-plane transposition, x and y FFTs over the occupied columns, gather), compiled from its sources with
-its FFT class; FFTW's lines evaluated by the oracle build's direct-DFT stand-in.  Skipped where oracle/_ref
+its FFT class; FFTW's lines evaluated by the oracle build's mixed-radix stand-in.  Skipped where oracle/_ref
 was not built."""
 from __future__ import annotations
 
