@@ -20,7 +20,7 @@ f32 = C.c_float
 pi32 = C.POINTER(C.c_int)
 pf64 = C.POINTER(C.c_double)
 
-HPSI_CB = C.CFUNCTYPE(None, vp, vp, vp, i32, i32, i32, i32)
+HPSI_CB = C.CFUNCTYPE(i32, vp, vp, vp, i32, i32, i32, i32)
 
 _SIGS = {
     "b200_last_error": ([], C.c_char_p),
@@ -95,6 +95,7 @@ _SIGS = {
                             i32, i32, i32, pi32], i32),
     "b200_tc_cgemm": ([C.c_char, C.c_char, i32, i32, i32, f32, f32, vp, i32, vp, i32, f32, f32, vp, i32, vp], i32),
     "b200_tc_cgemm_error": ([pi32], i32),
+    "b200_tc_set_wait_limit_ns": ([C.c_ulonglong], i32),
     "b200_gemm_op_f64": ([C.c_char, C.c_char, i32, i32, i32, pf64, vp, i32, vp, i32, pf64, vp, i32, vp], i32),
     "b200_gemv_op_f64": ([C.c_char, i32, i32, pf64, vp, i32, vp, i32, pf64, vp, i32, vp], i32),
     "b200_dot_real_op_f64": ([i32, vp, vp, i32, pf64, vp], i32),
@@ -160,6 +161,38 @@ def call(name: str, *args) -> None:
     rc = getattr(lib, name)(*args)
     if rc != 0:
         raise B200Error(name, rc, lib.b200_last_error().decode())
+
+
+class HostCallback:
+    """A Python H|psi> function as a b200_hpsi_cb.  ctypes cannot carry an exception out of a callback (it
+    prints it and returns to C as if nothing happened), so the exception is kept here, the callback returns
+    1 and the solver abandons the solve with B200_STATUS_CALLBACK_ERROR; call_with() then raises the kept
+    exception.  After a successful call the current torch stream is synchronised, so the block's writes are
+    complete when the solver reads them, whichever stream the function used."""
+
+    def __init__(self, fn):
+        self.exc = None
+
+        def cb(user, x, hx, nvec, dim, i0, i1):
+            try:
+                fn(x, hx, nvec, dim, i0, i1)
+                import torch
+                torch.cuda.current_stream().synchronize()
+                return 0
+            except BaseException as exc:  # noqa: BLE001 -- re-raised by call_with on the Python side
+                if self.exc is None:
+                    self.exc = exc
+                return 1
+
+        self.cfn = HPSI_CB(cb)
+
+    def call_with(self, name: str, *args) -> None:
+        try:
+            call(name, *args)
+        except B200Error:
+            if self.exc is not None:
+                raise self.exc
+            raise
 
 
 def ptr(t) -> int:

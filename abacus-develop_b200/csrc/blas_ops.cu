@@ -12,16 +12,22 @@ namespace {
 
 using b200::guarded;
 
-// one cuBLAS handle per host thread, made at first use (the reference keeps one static handle)
+// one cuBLAS handle per host thread and device, made at first use on that device (the reference keeps one
+// static handle on its one device); a thread that moves between devices gets the current device's handle
 struct ThreadBlas {
-    cublasHandle_t h = nullptr;
+    static constexpr int kMaxDev = 64;
+    cublasHandle_t h[kMaxDev] = {};
     ~ThreadBlas() {
-        if (h) cublasDestroy(h);
+        for (int d = 0; d < kMaxDev; ++d)
+            if (h[d]) cublasDestroy(h[d]);
     }
     cublasHandle_t get(cudaStream_t s) {
-        if (!h) B200_CUBLAS(cublasCreate(&h));
-        B200_CUBLAS(cublasSetStream(h, s));
-        return h;
+        int dev = 0;
+        B200_CUDA(cudaGetDevice(&dev));
+        B200_CHECK(dev >= 0 && dev < kMaxDev, b200::kInvalidArgument, "device ordinal out of range");
+        if (!h[dev]) B200_CUBLAS(cublasCreate(&h[dev]));
+        B200_CUBLAS(cublasSetStream(h[dev], s));
+        return h[dev];
     }
 };
 thread_local ThreadBlas g_blas;
@@ -70,23 +76,31 @@ __global__ void k_dot_final(int nparts, const double* __restrict__ part, double*
     }
 }
 
+// kDotBlocks partial sums and the result, per host thread and device (as the cuBLAS handles)
 struct DotScratch {
-    b200::DeviceArray<double> part;  // kDotBlocks partial sums and the result
+    b200::DeviceArray<double> part[ThreadBlas::kMaxDev];
+    b200::DeviceArray<double>& on_current_device() {
+        int dev = 0;
+        B200_CUDA(cudaGetDevice(&dev));
+        B200_CHECK(dev >= 0 && dev < ThreadBlas::kMaxDev, b200::kInvalidArgument, "device ordinal out of range");
+        return part[dev];
+    }
 };
-thread_local DotScratch g_dot;
+thread_local DotScratch g_dot_scratch;
 
 template <typename T> double dot_real(int dim, const void* l, const void* r, cudaStream_t s) {
-    g_dot.part.resize(kDotBlocks + 1);
+    b200::DeviceArray<double>& part = g_dot_scratch.on_current_device();
+    part.resize(kDotBlocks + 1);
     const long n = dim;
     k_dot_partial<T><<<kDotBlocks, kDotThreads, 0, s>>>(n, static_cast<const T*>(l), static_cast<const T*>(r),
-                                                        g_dot.part.ptr);
+                                                        part.ptr);
     b200::note_launch();
     B200_CUDA(cudaGetLastError());
-    k_dot_final<<<1, kDotThreads, 0, s>>>(kDotBlocks, g_dot.part.ptr, g_dot.part.ptr + kDotBlocks);
+    k_dot_final<<<1, kDotThreads, 0, s>>>(kDotBlocks, part.ptr, part.ptr + kDotBlocks);
     b200::note_launch();
     B200_CUDA(cudaGetLastError());
     double out = 0.0;
-    B200_CUDA(cudaMemcpyAsync(&out, g_dot.part.ptr + kDotBlocks, sizeof(double), cudaMemcpyDeviceToHost, s));
+    B200_CUDA(cudaMemcpyAsync(&out, part.ptr + kDotBlocks, sizeof(double), cudaMemcpyDeviceToHost, s));
     B200_CUDA(cudaStreamSynchronize(s));
     return out;
 }

@@ -31,6 +31,26 @@ unsigned long long launches() { return g_launches.load(std::memory_order_relaxed
 namespace {
 using b200::guarded;
 inline cudaStream_t S(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+// A user H|psi> callback as the solvers' HPsiDevice.  The solver's stream is drained first, so the callback
+// may read X from any stream or the host; afterwards the solver's stream waits for the legacy default stream,
+// where a callback that does not synchronise leaves its writes (torch's default stream is that stream).  A
+// nonzero return abandons the solve with B200_STATUS_CALLBACK_ERROR instead of reading an unwritten HX.
+b200::HPsiDevice host_callback(b200_hpsi_cb hpsi, void* user) {
+    return [hpsi, user](const void* x, void* hx, int nvec, int dim, int i0, int i1, cudaStream_t s) {
+        B200_CUDA(cudaStreamSynchronize(s));
+        const int rc = hpsi(user, x, hx, nvec, dim, i0, i1);
+        B200_CHECK(rc == 0, b200::kCallbackError, "H|psi> callback returned status " + std::to_string(rc));
+        if (s != nullptr && s != cudaStreamLegacy) {
+            cudaEvent_t ev;
+            B200_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+            cudaError_t e = cudaEventRecord(ev, cudaStreamLegacy);
+            if (e == cudaSuccess) e = cudaStreamWaitEvent(s, ev, 0);
+            cudaEventDestroy(ev);
+            B200_CUDA(e);
+        }
+    };
+}
 }  // namespace
 
 namespace {
@@ -323,9 +343,7 @@ int b200_david_diag(b200_david* d, b200_hpsi_cb hpsi, void* user, int ldpsi, voi
                     int maxiter, int ntry_max, int notconv_max, int* iters) {
     return guarded([&] {
         B200_CHECK(d && hpsi && psi && eig, b200::kInvalidArgument, "NULL argument");
-        b200::HPsiDevice f = [hpsi, user](const void* x, void* hx, int nvec, int dim, int i0, int i1, cudaStream_t) {
-            hpsi(user, x, hx, nvec, dim, i0, i1);
-        };
+        b200::HPsiDevice f = host_callback(hpsi, user);
         const int it = d->d->diag(f, ldpsi, psi, eig, thr, maxiter, ntry_max, notconv_max);
         if (iters) *iters = it;
     });
@@ -347,6 +365,9 @@ int b200_tc_cgemm_error(int* code) {
         B200_CHECK(code != nullptr, b200::kInvalidArgument, "NULL argument");
         *code = g_tc_ws.read_error();
     });
+}
+int b200_tc_set_wait_limit_ns(unsigned long long ns) {
+    return guarded([&] { b200::set_tc_wait_limit_ns(ns); });
 }
 int b200_david_set_stream(b200_david* d, void* stream) {
     return guarded([&] {
@@ -440,9 +461,7 @@ int b200_dav_subspace_diag(b200_dav_subspace* d, b200_hpsi_cb hpsi, void* user, 
                            const int* is_occupied, int scf_type, int* iters) {
     return guarded([&] {
         B200_CHECK(d && hpsi && psi && eig, b200::kInvalidArgument, "NULL argument");
-        b200::HPsiDevice f = [hpsi, user](const void* x, void* hx, int nvec, int dim, int i0, int i1, cudaStream_t) {
-            hpsi(user, x, hx, nvec, dim, i0, i1);
-        };
+        b200::HPsiDevice f = host_callback(hpsi, user);
         const int it = d->d->diag(f, psi, psi_in_dmax, eig, is_occupied, scf_type != 0);
         if (iters) *iters = it;
     });
@@ -497,9 +516,7 @@ int b200_bpcg_destroy(b200_bpcg* d) {
 int b200_bpcg_diag(b200_bpcg* d, b200_hpsi_cb hpsi, void* user, void* psi, double* eig, int scf_iter, int* iters) {
     return guarded([&] {
         B200_CHECK(d && hpsi && psi && eig, b200::kInvalidArgument, "NULL argument");
-        b200::HPsiDevice f = [hpsi, user](const void* x, void* hx, int nvec, int dim, int i0, int i1, cudaStream_t) {
-            hpsi(user, x, hx, nvec, dim, i0, i1);
-        };
+        b200::HPsiDevice f = host_callback(hpsi, user);
         const int it = d->d->diag(f, psi, eig, scf_iter);
         if (iters) *iters = it;
     });

@@ -18,6 +18,7 @@ enum Status : int {
     kNumericalError = 5,
     kCapacityError = 6,
     kNotConverged = 7,
+    kCallbackError = 8,
 };
 
 // A failure raised inside the library; the C-ABI turns it into a status code

@@ -113,6 +113,28 @@ template <typename A, typename B> __global__ void k_convert(long n, const A* __r
         b[i] = cmake<B>(a[i].x, a[i].y);
 }
 
+// subspace matrix -> FP64 eigensolver input (columns of ld, the leading nbase rows used); a non-finite entry
+// there sets *flag
+template <typename A>
+__global__ void k_to_eig_input(int nbase, int ld, const A* __restrict__ a, double2* __restrict__ b, int* flag) {
+    const long n = long(ld) * nbase;
+    int bad = 0;
+    for (long i = blockIdx.x * long(blockDim.x) + threadIdx.x; i < n; i += long(gridDim.x) * blockDim.x) {
+        const double re = double(a[i].x), im = double(a[i].y);
+        b[i] = make_double2(re, im);
+        if (int(i % ld) < nbase && !(isfinite(re) && isfinite(im))) bad = 1;
+    }
+    if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(flag, 1);
+}
+// after k_to_eig_input flagged a non-finite entry: the eigensolver gets I instead (the solve is reported as a
+// numerical error afterwards; the eigensolver never iterates on NaN/Inf)
+__global__ void k_eig_input_guard(int nbase, int ld, const int* __restrict__ flag, double2* __restrict__ b) {
+    if (*flag == 0) return;
+    const long n = long(ld) * nbase;
+    for (long i = blockIdx.x * long(blockDim.x) + threadIdx.x; i < n; i += long(gridDim.x) * blockDim.x)
+        b[i] = make_double2(long(i % ld) == i / ld ? 1.0 : 0.0, 0.0);
+}
+
 template <typename R> __global__ void k_convert_real(long n, const double* __restrict__ a, R* __restrict__ b) {
     for (long i = blockIdx.x * long(blockDim.x) + threadIdx.x; i < n; i += long(gridDim.x) * blockDim.x) b[i] = R(a[i]);
 }
@@ -419,13 +441,10 @@ template <typename T> struct Engine {
     void eigsolve(int nbase) {
         tick();
         const long n = long(nbase_x) * nbase;
-        if constexpr (std::is_same<T, double2>::value) {
-            B200_CUDA(cudaMemcpyAsync(A64.ptr, hcc.ptr, n * sizeof(double2), cudaMemcpyDeviceToDevice, s));
-        } else {
-            k_convert<T, double2><<<grid_of(n), kT, 0, s>>>(n, hcc.ptr, A64.ptr);
-            note_launch();
-            B200_CUDA(cudaGetLastError());
-        }
+        k_to_eig_input<T><<<grid_of(n), kT, 0, s>>>(nbase, nbase_x, hcc.ptr, A64.ptr, info.ptr + 3);
+        k_eig_input_guard<<<grid_of(n), kT, 0, s>>>(nbase, nbase_x, info.ptr + 3, A64.ptr);
+        note_launch(2);
+        B200_CUDA(cudaGetLastError());
         // lowest nband eigenpairs only (the reference's zheevx range 'I', dngvd_op.cpp:142-235): divide and
         // conquer on the tridiagonal form, back-transforming nband vectors instead of nbase
         if (nbase > nband) {
@@ -450,6 +469,8 @@ template <typename T> struct Engine {
         B200_CUDA(cudaMemcpyAsync(eig_h.data(), w.ptr, nband * sizeof(double), cudaMemcpyDeviceToHost, s));
         B200_CUDA(cudaMemcpyAsync(hinfo, info.ptr, 4 * sizeof(int), cudaMemcpyDeviceToHost, s));
         B200_CUDA(cudaStreamSynchronize(s));
+        B200_CHECK(hinfo[3] == 0, kNumericalError,
+                   "non-finite entries in the subspace matrix (NaN/Inf in psi, V_eff, D or H|psi>)");
         B200_CHECK(hinfo[1] == 0, kNumericalError,
                    "Cholesky of the new block failed (linearly dependent search directions), info " + std::to_string(hinfo[1]));
         B200_CHECK(hinfo[0] == 0, kNumericalError, "subspace eigensolver failed, info " + std::to_string(hinfo[0]));

@@ -29,6 +29,7 @@
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
+#include <atomic>
 #include <mutex>
 
 #include "common.h"
@@ -42,7 +43,7 @@ constexpr int kBK = 32;      // real K per stage (one 128-byte swizzle row of fp
 constexpr int kStages = 4;
 constexpr int kAcc = 2;      // K stages accumulated in one TMEM buffer before it is drained
 constexpr int kThreads = 320;   // warp 0 TMA, warp 1 MMA, warps 2-9 split / drain / store
-constexpr unsigned long long kWaitNs = 2000000000ull;  // 2 s bound on any single wait
+constexpr unsigned long long kWaitNs = 2000000000ull;  // default bound on any single wait: 2 s
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) {
     return static_cast<unsigned>(__cvta_generic_to_shared(p));
@@ -72,13 +73,13 @@ __device__ __forceinline__ bool mbar_try(unsigned bar, unsigned parity) {
         : "memory");
     return ok != 0;
 }
-// bounded wait: true on success, false after kWaitNs
-__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity) {
+// bounded wait: true on success, false after limit_ns
+__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity, unsigned long long limit_ns) {
     if (mbar_try(bar, parity)) return true;
     const unsigned long long t0 = gtimer();
     while (true) {
         if (mbar_try(bar, parity)) return true;
-        if (gtimer() - t0 > kWaitNs) return false;
+        if (gtimer() - t0 > limit_ns) return false;
     }
 }
 __device__ __forceinline__ void tma_load_2d(unsigned dst, const CUtensorMap* map, int x, int y, unsigned bar) {
@@ -176,8 +177,12 @@ template <int BN, int OPA, int PRE>
 __global__ void __launch_bounds__(kThreads, 1)
     k_tc_cgemm(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
                const __grid_constant__ CUtensorMap mapBl, int M2, int N, int K2, int kstages_per_split, float2 alpha,
-               float2 beta, float* __restrict__ C, long ldc2, float* __restrict__ ws, int* __restrict__ err) {
+               float2 beta, float* __restrict__ C, long ldc2, float* __restrict__ ws, int* __restrict__ err,
+               unsigned long long wait_ns) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
+    // pipeline waits use wait_ns; the waits for this CTA's own copies and MMAs in flight after an abort use
+    // at least the default, as they always end (plain loads of valid memory, MMAs on resident operands)
+    const unsigned long long drain_ns = wait_ns > kWaitNs ? wait_ns : kWaitNs;
     using TB = TileBytes<BN>;
     // 1024-byte alignment of the tile area (the swizzle pattern depends on address bits 7..9)
     unsigned char* base = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
@@ -234,7 +239,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             int issued = 0;
             for (int i = 0; i < nk && !*abort_flag; ++i) {
                 const int s = i % kStages;
-                if (i >= kStages && !mbar_wait(smem_u32(&empty[s]), ((i / kStages) - 1) & 1)) {
+                if (i >= kStages && !mbar_wait(smem_u32(&empty[s]), ((i / kStages) - 1) & 1, wait_ns)) {
                     fail(1);
                     break;
                 }
@@ -255,7 +260,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             // drain: every load this thread issued must land before the CTA exits
             for (int i = max(0, issued - kStages); i < issued; ++i) {
                 const int s = i % kStages;
-                if (!mbar_wait(smem_u32(&full[s]), (i / kStages) & 1)) atomicOr(err, 8);
+                if (!mbar_wait(smem_u32(&full[s]), (i / kStages) & 1, drain_ns)) atomicOr(err, 8);
             }
         }
     } else if (warp == 1) {
@@ -264,17 +269,18 @@ __global__ void __launch_bounds__(kThreads, 1)
             // TMEM buffer (i / kAcc) & 1; A from TMEM, B from shared memory
             const unsigned idesc =
                 (1u << 4) | (2u << 7) | (2u << 10) | (unsigned(BN >> 3) << 17) | (unsigned(kBM >> 4) << 24);
+            int issued = 0;
             for (int i = 0; i < nk && !*abort_flag; ++i) {
                 const int s = i % kStages;
                 const int grp = i / kAcc;
                 const int bf = grp & 1;
                 const bool first = (i % kAcc) == 0;
                 const bool last = (i % kAcc) == kAcc - 1 || i == nk - 1;
-                if (first && grp >= 2 && !mbar_wait(smem_u32(&acc_empty[bf]), ((grp >> 1) - 1) & 1)) {
+                if (first && grp >= 2 && !mbar_wait(smem_u32(&acc_empty[bf]), ((grp >> 1) - 1) & 1, wait_ns)) {
                     fail(32);
                     break;
                 }
-                if (!mbar_wait(smem_u32(&ready[s]), (i / kStages) & 1)) {
+                if (!mbar_wait(smem_u32(&ready[s]), (i / kStages) & 1, wait_ns)) {
                     fail(2);
                     break;
                 }
@@ -296,6 +302,13 @@ __global__ void __launch_bounds__(kThreads, 1)
                 }
                 mma_commit(smem_u32(&empty[s]));
                 if (last) mma_commit(smem_u32(&acc_full[bf]));
+                ++issued;
+            }
+            // after an abort: the MMAs issued so far complete (the commit of the last issued stage tracks all
+            // of them) before TMEM is freed below
+            if (*abort_flag && issued > 0) {
+                const int il = issued - 1;
+                if (!mbar_wait(smem_u32(&empty[il % kStages]), (il / kStages) & 1, drain_ns)) atomicOr(err, 64);
             }
         }
     } else {
@@ -317,7 +330,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         bool ok = true;
         auto drain = [&](int grp) {  // the accumulator of stage group grp
             const int bf = grp & 1;
-            ok = ok && mbar_wait(smem_u32(&acc_full[bf]), (grp >> 1) & 1);
+            ok = ok && mbar_wait(smem_u32(&acc_full[bf]), (grp >> 1) & 1, wait_ns);
             if (!ok) {
                 fail(16);
                 return;
@@ -336,7 +349,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         };
         for (int i = 0; i < nk && !*abort_flag; ++i) {
             const int s = i % kStages;
-            if (!mbar_wait(smem_u32(&full[s]), (i / kStages) & 1)) {
+            if (!mbar_wait(smem_u32(&full[s]), (i / kStages) & 1, wait_ns)) {
                 fail(4);
                 break;
             }
@@ -511,6 +524,9 @@ CUtensorMap make_map(const void* base, long inner, long outer, long pitch_floats
     return m;
 }
 
+std::atomic<unsigned long long> g_wait_ns{kWaitNs};
+unsigned long long wait_limit_ns() { return g_wait_ns.load(std::memory_order_relaxed); }
+
 template <int BN, int OPA, int PRE> void set_attr_once() {
     static std::once_flag once;
     std::call_once(once, [] {
@@ -581,11 +597,11 @@ void launch(int M, int N, int K, float2 alpha, const float2* A, int lda, const f
     if (pre) {
         set_attr_once<BN, OPA, 1>();
         k_tc_cgemm<BN, OPA, 1><<<grid, kThreads, TileBytes<BN>::total, s>>>(
-            mA, mB, mBl, M2, N, K2, per, alpha, beta, reinterpret_cast<float*>(C), 2L * ldc, ws, w.err.ptr);
+            mA, mB, mBl, M2, N, K2, per, alpha, beta, reinterpret_cast<float*>(C), 2L * ldc, ws, w.err.ptr, wait_limit_ns());
     } else {
         set_attr_once<BN, OPA, 0>();
         k_tc_cgemm<BN, OPA, 0><<<grid, kThreads, TileBytes<BN>::total, s>>>(
-            mA, mB, mBl, M2, N, K2, per, alpha, beta, reinterpret_cast<float*>(C), 2L * ldc, ws, w.err.ptr);
+            mA, mB, mBl, M2, N, K2, per, alpha, beta, reinterpret_cast<float*>(C), 2L * ldc, ws, w.err.ptr, wait_limit_ns());
     }
     note_launch();
     B200_CUDA(cudaGetLastError());
@@ -620,9 +636,12 @@ int TcGemmWorkspace::read_error(cudaStream_t s) {
     if (err.ptr) {
         B200_CUDA(cudaMemcpyAsync(&h, err.ptr, sizeof(int), cudaMemcpyDeviceToHost, s));
         B200_CUDA(cudaStreamSynchronize(s));
+        if (h) B200_CUDA(cudaMemsetAsync(err.ptr, 0, sizeof(int), s));  // reported once, then cleared
     }
     return h;
 }
+
+void set_tc_wait_limit_ns(unsigned long long ns) { g_wait_ns.store(ns ? ns : kWaitNs, std::memory_order_relaxed); }
 
 void tc_cgemm(char opa, int M, int N, int K, float2 alpha, const float2* A, int lda, const float2* B, int ldb,
               float2 beta, float2* C, int ldc, TcGemmWorkspace& w, cudaStream_t s) {

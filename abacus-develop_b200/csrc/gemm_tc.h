@@ -15,7 +15,7 @@ struct TcGemmWorkspace {
     // allocate up front (no allocation inside later calls whose workspace fits): split-K partial tiles of
     // at most ws_floats (also the cap), and a pre-split B of up to bsplit_elems complex values
     void reserve(size_t ws_floats, size_t bsplit_elems);
-    int read_error(cudaStream_t s = 0);  // read of the error word after the work queued on s
+    int read_error(cudaStream_t s = 0);  // read (and clear) of the error word after the work queued on s
     size_t device_bytes() const { return ws.n * sizeof(float) + bsplit.n * sizeof(float2) + err.n * sizeof(int); }
 };
 
@@ -23,5 +23,9 @@ struct TcGemmWorkspace {
 // lda and ldb must be even and A, B 16-byte aligned (TMA row pitch).
 void tc_cgemm(char opa, int M, int N, int K, float2 alpha, const float2* A, int lda, const float2* B, int ldb,
               float2 beta, float2* C, int ldc, TcGemmWorkspace& w, cudaStream_t s);
+
+// Time limit of every pipeline wait inside the tensor-core GEMM kernels launched from now on, all threads
+// (0 restores the default of 2 s).  A wait that runs out sets the workspace's error word.
+void set_tc_wait_limit_ns(unsigned long long ns);
 
 }  // namespace b200

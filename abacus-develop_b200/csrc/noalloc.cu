@@ -28,6 +28,7 @@
 // Bands are processed in chunks that fit the array; a grid whose single-band
 // stick buffer (nst * nz complex values) exceeds the array is rejected with
 // B200_STATUS_CAPACITY_ERROR.
+#include <algorithm>
 #include <mutex>
 
 #include "../../include/abacus_b200.h"
@@ -73,7 +74,8 @@ void hpsi_local_noalloc(b200::Hamilt& H, int ik, int nb, int ld, const T* psi, T
                    std::to_string(kNoAllocScratchBytes) + "-byte no-alloc scratch");
     if (nb == 0) return;
     T* sb = static_cast<T*>(noalloc_scratch_on_current_device());
-    const int chunk = int(kNoAllocScratchBytes / per_band);
+    // bands per launch: what the scratch holds, and at most 65535 (the launches put bands on gridDim.y)
+    const int chunk = int(std::min<size_t>(kNoAllocScratchBytes / per_band, 65535));
     const R* veff = H.veff_of<R>();
     const R* veffp = H.veff_perm_of<R>();
     for (int b0 = 0; b0 < nb; b0 += chunk) {

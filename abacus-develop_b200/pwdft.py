@@ -98,9 +98,15 @@ def tc_cgemm(transa, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, stream=None):
 
 
 def tc_cgemm_error():
+    """Error word of this thread's tensor-core GEMMs (nonzero: a bounded wait ran out); the read clears it."""
     code = C.c_int()
     call("b200_tc_cgemm_error", C.byref(code))
     return code.value
+
+
+def tc_set_wait_limit_ns(ns):
+    """Limit of each pipeline wait inside the tensor-core GEMMs launched afterwards (0: the default, 2 s)."""
+    call("b200_tc_set_wait_limit_ns", int(ns))
 
 
 def _ints(v):
@@ -470,15 +476,12 @@ class DiagoDavid:
         """hpsi_func(x_ptr, hx_ptr, nvec, dim, id_start, id_end) with raw device pointers (HPsiFunc contract).
         eigenvalue: numpy float64 array of nband, filled on return. Returns the iteration count."""
 
-        def cb(user, x, hx, nvec, dim, i0, i1):
-            hpsi_func(x, hx, nvec, dim, i0, i1)
-
         _check_block(psi, True, self.nband, ld_psi, "psi")
         if len(eigenvalue) < self.nband or eigenvalue.dtype != np.float64:
             raise ValueError("eigenvalue: need a float64 array of nband entries")
-        cfn = _lib.HPSI_CB(cb)
+        cb = _lib.HostCallback(hpsi_func)
         it = C.c_int()
-        call("b200_david_diag", self._h, cfn, None, ld_psi, ptr(psi), eigenvalue.ctypes.data_as(_lib.pf64), thr, maxiter,
+        cb.call_with("b200_david_diag", self._h, cb.cfn, None, ld_psi, ptr(psi), eigenvalue.ctypes.data_as(_lib.pf64), thr, maxiter,
              ntry_max, notconv_max, C.byref(it))
         return it.value
 
@@ -569,13 +572,10 @@ class DiagoDavSubspace:
         eigenvalue: numpy float64 array of nband (in: ignored; out: the eigenvalues).  Returns the total
         iteration count."""
 
-        def cb(user, x, hx, nvec, dim, i0, i1):
-            hpsi_func(x, hx, nvec, dim, i0, i1)
-
         occ, occ_p = self._args(psi, psi_in_dmax, eigenvalue, is_occupied)
-        cfn = _lib.HPSI_CB(cb)
+        cb = _lib.HostCallback(hpsi_func)
         it = C.c_int()
-        call("b200_dav_subspace_diag", self._h, cfn, None, ptr(psi), psi_in_dmax,
+        cb.call_with("b200_dav_subspace_diag", self._h, cb.cfn, None, ptr(psi), psi_in_dmax,
              eigenvalue.ctypes.data_as(_lib.pf64), occ_p, int(bool(scf_type)), C.byref(it))
         return it.value
 
@@ -630,13 +630,10 @@ class DiagoBPCG:
         """hpsi_func(x_ptr, hx_ptr, nvec, dim, id_start, id_end) with raw device pointers (HPsiFunc contract),
         called for all bands.  scf_iter: DiagoIterAssist::SCF_ITER.  Returns the CG iterations."""
 
-        def cb(user, x, hx, nvec, dim, i0, i1):
-            hpsi_func(x, hx, nvec, dim, i0, i1)
-
         self._check(psi, eigenvalue)
-        cfn = _lib.HPSI_CB(cb)
+        cb = _lib.HostCallback(hpsi_func)
         it = C.c_int()
-        call("b200_bpcg_diag", self._h, cfn, None, ptr(psi), eigenvalue.ctypes.data_as(_lib.pf64), int(scf_iter),
+        cb.call_with("b200_bpcg_diag", self._h, cb.cfn, None, ptr(psi), eigenvalue.ctypes.data_as(_lib.pf64), int(scf_iter),
              C.byref(it))
         return it.value
 

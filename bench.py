@@ -198,71 +198,118 @@ def local_bytes_per_band(basis, b, r):
     return b * (3 * npw + 4 * S) + r * basis.nxyz
 
 
-def cpu_port_bands_per_s(wl, budget_s=10.0, sample_bands=8, workers=1):
-    """The oracle's H|psi> on the host cores over a bounded sample of bands."""
+# ---- the CPU arm: the oracle's H|psi> (numpy/scipy restatement of the reference CPU functors and
+# PW_Basis_K transforms) on the host cores, band-parallel: one single-threaded process per core, each
+# holding the cell's Hamiltonian; a step hands every process its share of the bands ----
+_CPU_HAM = None
+
+
+def _cpu_worker_init(cfg):
+    global _CPU_HAM
+    from threadpoolctl import threadpool_limits
+    threadpool_limits(1)  # one BLAS thread per process; the oracle's FFTs run with one worker
     sys.path.insert(0, str(ROOT))
     from oracle import hamilt_ref as H
     from oracle.pw_basis_ref import PWBasisKRef
-    H.FFT_WORKERS = workers
-    spec = wl.spec
-    ref_b = PWBasisKRef(spec.a, wl.cell.latvec, spec.ecut, np.zeros((1, 3)), grid=spec.grid)
-    ld = wl.basis.npwk_max
-    ref = H.HamiltPWRef(ref_b, 0, wl.veff_h, wl.vkb_h[0][:, :ld], wl.deeq_h, [8], [wl.cell.nat])
-    psi = wl.psi0_h[0][:sample_bands].reshape(-1)
-    done = 0
-    t0 = time.perf_counter()
-    while True:
-        ref.hpsi(psi, sample_bands, ld)
-        done += sample_bands
-        el = time.perf_counter() - t0
-        if el >= budget_s:
-            break
-    return done / el, done, el
+    spec_s = importlib.util.spec_from_file_location("_bench_synth", ROOT / "abacus-develop_b200" / "synth.py")
+    synth = importlib.util.module_from_spec(spec_s)
+    spec_s.loader.exec_module(synth)
+    H.FFT_WORKERS = 1
+    spec = synth.config(cfg)
+    cell = synth.make_cell(spec)
+    b = PWBasisKRef(spec.a, cell.latvec, spec.ecut, np.zeros((1, 3)), grid=spec.grid)
+    ld = int(b.npwk_max)
+    ham = H.HamiltPWRef(b, 0, cell.veff(b.nx, b.ny, b.nz), cell.vkb(b.gplusk_cart(0), ld, b.omega), cell.deeq(),
+                        [8], [cell.nat])
+    psi = cell.psi0(b.gplusk_cart(0), spec.nbands, ld).reshape(-1)
+    _CPU_HAM = (ham, psi, ld)
+
+
+def _cpu_worker_hpsi(b0, nb):
+    ham, psi, ld = _CPU_HAM
+    ham.hpsi(psi[b0 * ld:(b0 + nb) * ld], nb, ld)
+    return nb
+
+
+class CpuArm:
+    """The oracle's H|psi> of the 64-atom cell on `procs` host processes (spawned, so that a pool started
+    after GPU work is safe).  step(nb) applies H to nb bands, split evenly over the processes."""
+
+    def __init__(self, procs, cfg=1):
+        import multiprocessing as mp
+        self.procs = procs
+        self.pool = mp.get_context("spawn").Pool(procs, initializer=_cpu_worker_init, initargs=(cfg,))
+        self.pool.starmap(_cpu_worker_hpsi, [(0, 1)] * procs)  # every process set up and warm
+
+    def step(self, nb):
+        share = [nb // self.procs + (1 if i < nb % self.procs else 0) for i in range(self.procs)]
+        tasks, b0 = [], 0
+        for n in share:
+            if n:
+                tasks.append((b0, n))
+                b0 += n
+        t0 = time.perf_counter()
+        done = sum(self.pool.starmap(_cpu_worker_hpsi, tasks))
+        return done, time.perf_counter() - t0
+
+    def close(self):
+        self.pool.close()
+        self.pool.join()
+
+
+def host_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def cpu_bands_per_s(procs, budget_s=10.0, nb_step=None):
+    """Bands/s of the CPU arm over steps of nb_step bands (default 2 per process, at least 16) until
+    budget_s has passed; returns (bands/s, bands done, seconds, per-step seconds)."""
+    arm = CpuArm(procs)
+    try:
+        nb = nb_step or max(16, 2 * procs)
+        done, el, steps = 0, 0.0, []
+        while el < budget_s:
+            d, t = arm.step(nb)
+            done += d
+            el += t
+            steps.append(t)
+        return done / el, done, el, steps
+    finally:
+        arm.close()
 
 
 def run_reference(args, ws, rank):
-    """CPU reference arm: the reference's algorithm for this path on the host cores."""
+    """CPU reference arm: the reference's algorithm for this path on all the host cores (band-parallel)."""
     if rank != 0:
         return
-    load_package()
-    sys.path.insert(0, str(ROOT))
-    from oracle import hamilt_ref as H
-    from oracle.pw_basis_ref import PWBasisKRef
-    from importlib import import_module
-    synth = import_module("abacus_develop_b200.synth")
-    spec = synth.config(1)
-    cell = synth.make_cell(spec)
-    b = PWBasisKRef(spec.a, cell.latvec, spec.ecut, np.zeros((1, 3)))
-    ld = int(b.npwk_max)
-    veff = cell.veff(b.nx, b.ny, b.nz)
-    vkb = cell.vkb(b.gplusk_cart(0), ld, b.omega)
-    psi = cell.psi0(b.gplusk_cart(0), 8, ld).reshape(-1)
-    cores = os.cpu_count() or 1
-    H.FFT_WORKERS = cores
-    ref = H.HamiltPWRef(b, 0, veff, vkb, cell.deeq(), [8], [cell.nat])
-    sample = 4
-    for _ in range(args.warmup):
-        ref.hpsi(psi[:sample * ld], sample, ld)
-    times = []
-    for _ in range(args.steps):
-        t0 = time.perf_counter()
-        ref.hpsi(psi[:sample * ld], sample, ld)
-        times.append(time.perf_counter() - t0)
-    per_step = float(np.mean(times))
-    val = sample / per_step
+    cores = host_cores()
+    nb = max(16, 2 * cores)
+    arm = CpuArm(cores)
+    try:
+        for _ in range(args.warmup):
+            arm.step(nb)
+        times = [arm.step(nb)[1] for _ in range(args.steps)]
+    finally:
+        arm.close()
+    per_step = float(np.median(times))
+    val = nb / per_step
     line = {
         "impl": "reference", "metric": METRIC, "value": val, "unit": "bands/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": per_step * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD_NAME, "sample": f"{sample} of 160 bands per step"},
+        "config": {"workload": WORKLOAD_NAME, "sample": f"{nb} of 160 bands per step"},
         "cpu_baseline": {"value": val, "unit": "bands/s", "cores": cores, "kind": "port",
-                         "sample": f"{sample} bands of the 160-band block per step, numpy/scipy restatement of the "
-                                   f"reference CPU functors and PW_Basis_K transforms, {cores} FFT/BLAS threads"},
+                         "sample": f"{nb} bands of the 160-band block per step (median of {args.steps} steps), "
+                                   f"numpy/scipy restatement of the reference CPU functors and PW_Basis_K "
+                                   f"transforms, {cores} single-threaded processes, bands split evenly"},
         "e2e": {"value": val, "unit": "bands/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
-    ref = cpu_reference_davidson_8atom(load_package())
-    if ref is not None:
-        ref.pop("eig")
+    ref = guarded_section(cpu_reference_davidson_8atom, load_package())
+    if isinstance(ref, dict):
+        ref.pop("eig", None)
         line["davidson_8atom"] = ref
     print(json.dumps(line), flush=True)
 
@@ -389,12 +436,51 @@ def run_ours(args, ws, rank, local):
 
     if rank == 0 and ws == 1 and not args.skip_cpu:
         line["davidson_8atom"] = guarded_section(davidson_8atom, pkg)
-        bps, done, el = cpu_port_bands_per_s(wl, budget_s=args.cpu_budget)
-        line["cpu_baseline"] = {"value": bps, "unit": "bands/s", "cores": 1, "kind": "port",
-                                "sample": f"{done} bands of the 160-band block in {el:.1f} s, numpy restatement "
-                                          f"of the reference CPU functors + PW_Basis_K transforms, 1 thread"}
+        cores = host_cores()
+        bps, done, el, _ = cpu_bands_per_s(cores, budget_s=args.cpu_budget)
+        bps1, done1, el1, _ = cpu_bands_per_s(1, budget_s=args.cpu_budget / 2, nb_step=4)
+        line["cpu_baseline"] = {"value": bps, "unit": "bands/s", "cores": cores, "kind": "port",
+                                "sample": f"{done} bands of the 160-band block in {el:.1f} s on {cores} single-threaded "
+                                          f"processes (bands split evenly), numpy restatement of the reference CPU "
+                                          f"functors + PW_Basis_K transforms",
+                                "one_core": {"value": bps1, "sample": f"{done1} bands in {el1:.1f} s, 1 process"}}
+    line["summary"] = summary_of(line)
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def _r(x, nd=3):
+    """A number rounded for the compact summary (None stays None)."""
+    if x is None:
+        return None
+    return float(f"{x:.{nd}g}")
+
+
+def summary_of(line):
+    """The figures the headline metric names, compact, as the line's last key (a reader that keeps only the
+    end of the output still sees them): FP64 / mixed H|psi>, the roofline fraction, the Davidson solves
+    (median times, speed-ups, errors against the oracle), serving latency."""
+    out = {"hpsi_fp64_bands_s": _r(line.get("value"), 4), "hpsi_mixed_bands_s": _r(line.get("mixed", {}).get("value"), 4),
+           "e2e_bands_s": _r(line.get("e2e", {}).get("value"), 4),
+           "local_frac": _r(line.get("roofline", {}).get("frac")),
+           "local_frac_mixed": _r(line.get("roofline", {}).get("mixed", {}).get("frac"))}
+    for key in ("davidson", "davidson_216"):
+        d = line.get(key)
+        if isinstance(d, dict) and "fp64_s" in d:
+            out[key] = {k: _r(d.get(k)) for k in ("fp64_s", "mixed_s", "speedup", "fp64_to_1e-8_s", "mixed_to_1e-8_s",
+                                                   "speedup_to_1e-8", "fp64_err_ry", "mixed_err_ry")}
+            out[key]["err_vs"] = d.get("err_vs")
+    sv = line.get("serving")
+    if isinstance(sv, dict):
+        def lat(x):
+            return {"rps": _r(x.get("throughput_rps")), "p50_ms": _r(x.get("p50_ms")), "p99_ms": _r(x.get("p99_ms")),
+                    "p99_over_p50": _r(x.get("p99_ms") / x["p50_ms"]) if x.get("p50_ms") else None}
+        out["serving"] = {k: lat(v) for k, v in sv.items() if isinstance(v, dict) and "p50_ms" in v}
+    cb = line.get("cpu_baseline")
+    if isinstance(cb, dict):
+        out["cpu_bands_s"] = _r(cb.get("value"))
+        out["cpu_cores"] = cb.get("cores")
+    return out
 
 
 def guarded_section(fn, *args):
@@ -463,8 +549,8 @@ def davidson_8atom(pkg):
     pc = P.precondition_d(wl.basis, 0)
     out = {"workload": "8-atom diamond a=10.26 bohr, ecut 30 Ry, 36^3 grid, npw 2945, 32 bands, Gamma, thr 1e-9"}
     for name, prec in (("gpu_fp64", P.PREC_FP64), ("gpu_mixed", P.PREC_MIXED)):
-        best = None
-        for _ in range(3):
+        runs = []
+        for _ in range(4):  # the first run warms the kernels and handles; the median of the other three
             dav = P.DiagoDavid(pc, nb, ld, 4, prec)
             x = torch.from_numpy(wl.psi0_h[0].reshape(-1).copy()).cuda()
             e = np.zeros(nb)
@@ -472,9 +558,9 @@ def davidson_8atom(pkg):
             t0 = time.perf_counter()
             it = dav.diag_hamilt(h, 0, ld, x, e, 1e-9, 200)
             torch.cuda.synchronize()
-            dt = time.perf_counter() - t0
-            best = dt if best is None else min(best, dt)
-        out[name + "_s"] = best
+            runs.append(time.perf_counter() - t0)
+        out[name + "_s"] = float(np.median(runs[1:]))
+        out[name + "_runs_s"] = runs[1:]
         out[name + "_iters"] = it
         out[name + "_eig"] = e
     ref = cpu_reference_davidson_8atom(pkg)
@@ -505,12 +591,29 @@ def settle_time(trace, ref, tol=1e-8):
     return float(t[i])
 
 
-def solve_pair(P, h, pc, nb, ld, psi0_h, thr_ref=1e-11, thr=1e-9, repeats=2):
-    """FP64 reference solve to thr_ref, then FP64 and mixed solves to thr with eigenvalue traces: wall time
-    of each solve and time until every eigenvalue is within 1e-8 Ry of the reference."""
+def residual_norms(P, h, x, e, nb, ld):
+    """|H x_m - e_m x_m| of returned vectors through the FP64 H|psi> (which the tests pin to the oracle at
+    1e-12 on this cell): for orthonormal x_m each e_m is within that norm of an eigenvalue of H."""
+    import torch
+    hx = torch.zeros_like(x)
+    h.hpsi(0, x, hx, nb, ld)
+    X = x.view(nb, ld)
+    r = hx.view(nb, ld) - torch.from_numpy(e).to(x.device)[:, None] * X
+    norms = torch.linalg.vector_norm(r, dim=1).cpu().numpy()
+    ortho = (X.conj() @ X.T - torch.eye(nb, dtype=x.dtype, device=x.device)).abs().max().item()
+    del hx, r
+    return float(norms.max()), ortho
+
+
+def solve_pair(P, h, pc, nb, ld, psi0_h, thr_ref=1e-11, thr=1e-9, repeats=3, e_oracle=None, oracle_what=None):
+    """FP64 and mixed solves to thr, alternating, `repeats` each, with per-iteration eigenvalue traces.
+    The reference eigenvalues are the oracle's (e_oracle, a fixture) when given, else an FP64 device solve
+    to thr_ref; each arm reports the median wall time and time to 1e-8 Ry over its repeats (with min / max),
+    its largest eigenvalue error against the reference, and the residual norms of its returned vectors
+    through the pinned FP64 H|psi>."""
     import torch
 
-    def solve(prec, t_thr):
+    def solve(prec, t_thr, keep=False):
         dav = P.DiagoDavid(pc, nb, ld, 4, prec)
         dav.set_trace(True)
         x = torch.from_numpy(psi0_h.copy()).cuda()
@@ -520,39 +623,63 @@ def solve_pair(P, h, pc, nb, ld, psi0_h, thr_ref=1e-11, thr=1e-9, repeats=2):
         dav.diag_hamilt(h, 0, ld, x, e, t_thr, 300)
         torch.cuda.synchronize()
         wall = time.perf_counter() - t0
-        out = (wall, e, dav.stats(), dav.trace())
+        res = residual_norms(P, h, x, e, nb, ld) if keep else None
+        out = (wall, e, dav.stats(), dav.trace(), res)
         del dav, x
         torch.cuda.empty_cache()
         return out
 
     solve(P.PREC_MIXED, 1e-6)  # warm-up: first use of every kernel, handle and workspace shape
-    _, e_ref, st_ref, _ = solve(P.PREC_FP64, thr_ref)
+    if e_oracle is not None:
+        e_ref, st_ref = np.asarray(e_oracle, dtype=np.float64), None
+        err_vs = oracle_what
+    else:
+        _, e_ref, st_ref, _, _ = solve(P.PREC_FP64, thr_ref)
+        err_vs = f"FP64 device solve to thr {thr_ref}"
     runs64, runsmx = [], []
-    for _ in range(repeats):  # alternating, the faster of each arm is reported
-        runs64.append(solve(P.PREC_FP64, thr))
-        runsmx.append(solve(P.PREC_MIXED, thr))
-    w64, e64, st64, tr64 = min(runs64, key=lambda r: r[0])
-    wmx, emx, stmx, trmx = min(runsmx, key=lambda r: r[0])
-    s64, smx = settle_time(tr64, e_ref), settle_time(trmx, e_ref)
-    return {"fp64_s": w64, "mixed_s": wmx, "speedup": w64 / wmx,
-            "fp64_runs_s": [r[0] for r in runs64], "mixed_runs_s": [r[0] for r in runsmx],
-            "fp64_to_1e-8_s": s64, "mixed_to_1e-8_s": smx,
-            "speedup_to_1e-8": (s64 / smx) if (s64 and smx) else None,
-            "fp64_iters": st64[1], "mixed_iters_fp32": stmx[0], "mixed_iters_fp64": stmx[1],
-            "fp64_hpsi_bands": st64[2], "mixed_hpsi_bands": stmx[2], "ref_iters": st_ref[1],
-            "fp64_max_err_ry": float(np.max(np.abs(e64 - e_ref))),
-            "mixed_max_err_ry": float(np.max(np.abs(emx - e_ref))),
-            "reference_solve": f"FP64 Davidson to thr {thr_ref} on the same device (the oracle pins it at the "
-                               "8-atom size)", "thr": thr,
-            "to_1e-8": "time after which every Ritz value stays within 1e-8 Ry of the reference, from the "
-                       "per-iteration trace"}
+    for i in range(repeats):
+        runs64.append(solve(P.PREC_FP64, thr, keep=(i == 0)))
+        runsmx.append(solve(P.PREC_MIXED, thr, keep=(i == 0)))
+
+    def arm(runs):
+        walls = [r[0] for r in runs]
+        settles = [settle_time(r[3], e_ref) for r in runs]
+        ok = [t for t in settles if t is not None]
+        return {"median_s": float(np.median(walls)), "runs_s": walls,
+                "to_1e-8_s": float(np.median(ok)) if len(ok) == len(runs) else None, "to_1e-8_runs_s": settles,
+                "err_ry": float(max(np.max(np.abs(r[1] - e_ref)) for r in runs)),
+                "max_residual": runs[0][4][0], "orthonormality": runs[0][4][1], "stats": runs[0][2]}
+
+    a64, amx = arm(runs64), arm(runsmx)
+    out = {"fp64_s": a64["median_s"], "mixed_s": amx["median_s"], "speedup": a64["median_s"] / amx["median_s"],
+           "fp64_runs_s": a64["runs_s"], "mixed_runs_s": amx["runs_s"],
+           "fp64_to_1e-8_s": a64["to_1e-8_s"], "mixed_to_1e-8_s": amx["to_1e-8_s"],
+           "fp64_to_1e-8_runs_s": a64["to_1e-8_runs_s"], "mixed_to_1e-8_runs_s": amx["to_1e-8_runs_s"],
+           "speedup_to_1e-8": (a64["to_1e-8_s"] / amx["to_1e-8_s"]) if (a64["to_1e-8_s"] and amx["to_1e-8_s"]) else None,
+           "fp64_err_ry": a64["err_ry"], "mixed_err_ry": amx["err_ry"], "err_vs": err_vs,
+           "fp64_max_residual": a64["max_residual"], "mixed_max_residual": amx["max_residual"],
+           "fp64_orthonormality": a64["orthonormality"], "mixed_orthonormality": amx["orthonormality"],
+           "fp64_iters": a64["stats"][1], "mixed_iters_fp32": amx["stats"][0], "mixed_iters_fp64": amx["stats"][1],
+           "fp64_hpsi_bands": a64["stats"][2], "mixed_hpsi_bands": amx["stats"][2],
+           "ref_iters": st_ref[1] if st_ref else None, "thr": thr, "repeats": repeats,
+           "timing": "medians over alternating repeats (runs listed); to_1e-8: time after which every Ritz value "
+                     "stays within 1e-8 Ry of the reference eigenvalues, from the per-iteration trace; residuals "
+                     "|Hx - ex| of the first repeat's vectors through the FP64 H|psi>"}
+    return out
+
+
+EIG_FIXTURE_64 = ROOT / "tests" / "golden" / "eig_diamond64.npz"
 
 
 def davidson_bench(P, wl, h64):
+    """64-atom cell: errors and time to 1e-8 Ry against the oracle's eigenvalues (tests/golden/eig_diamond64.npz:
+    the reference's DiagoDavid on the oracle's H|psi> to thr 1e-11)."""
     nb = wl.spec.nbands
     ld = wl.basis.npwk_max
     pc = P.precondition_d(wl.basis, 0)
-    out = solve_pair(P, h64, pc, nb, ld, wl.psi0_h[0][:nb].reshape(-1))
+    fx = np.load(EIG_FIXTURE_64)
+    out = solve_pair(P, h64, pc, nb, ld, wl.psi0_h[0][:nb].reshape(-1), e_oracle=fx["eig"],
+                     oracle_what=f"oracle fixture eig_diamond64.npz ({fx['solver']}, thr {float(fx['thr'])})")
     out["workload"] = WORKLOAD_NAME
     return out
 
@@ -591,11 +718,13 @@ def dav_subspace_bench(pkg, P, wl, h64, with_cpu):
         return time.perf_counter() - t0, it, e, dav.stats()
 
     run_ds()  # warm-up
-    ds_runs = [run_ds() for _ in range(2)]
-    dav_runs = [run_dav() for _ in range(2)]
-    ds, dv = min(ds_runs, key=lambda r: r[0]), min(dav_runs, key=lambda r: r[0])
-    out = {"workload": WORKLOAD_NAME + ", thr 1e-9", "dav_subspace_s": ds[0], "dav_subspace_iters": ds[1],
-           "dav_subspace_hpsi_bands": ds[3][1], "david_fp64_s": dv[0], "david_fp64_iters": dv[1],
+    ds_runs = [run_ds() for _ in range(3)]
+    dav_runs = [run_dav() for _ in range(3)]
+    ds, dv = ds_runs[0], dav_runs[0]
+    out = {"workload": WORKLOAD_NAME + ", thr 1e-9", "dav_subspace_s": float(np.median([r[0] for r in ds_runs])),
+           "dav_subspace_runs_s": [r[0] for r in ds_runs], "dav_subspace_iters": ds[1],
+           "dav_subspace_hpsi_bands": ds[3][1], "david_fp64_s": float(np.median([r[0] for r in dav_runs])),
+           "david_fp64_runs_s": [r[0] for r in dav_runs], "david_fp64_iters": dv[1],
            "david_fp64_hpsi_bands": dv[3][2], "max_abs_diff_vs_david_ry": float(np.max(np.abs(ds[2] - dv[2])))}
     if with_cpu:
         out["8atom"] = guarded_section(dav_subspace_8atom, pkg)
@@ -620,8 +749,8 @@ def dav_subspace_8atom(pkg):
     psi0 = np.zeros((nb, ld), complex)
     psi0[:, :npw] = q.T
     pc = P.precondition_dav_subspace_d(wl.basis, 0)
-    best = None
-    for _ in range(3):
+    runs = []
+    for _ in range(4):  # the first run warms the kernels and handles; the median of the other three
         ds = P.DiagoDavSubspace(pc, nb, npw, 4, 1e-9, 200)
         x = torch.from_numpy(psi0.reshape(-1).copy()).cuda()
         e = np.zeros(nb)
@@ -629,9 +758,9 @@ def dav_subspace_8atom(pkg):
         t0 = time.perf_counter()
         it = ds.diag_hamilt(h, 0, x, ld, e)
         torch.cuda.synchronize()
-        dt = time.perf_counter() - t0
-        best = dt if best is None else min(best, dt)
-    out = {"gpu_s": best, "gpu_iters": it}
+        runs.append(time.perf_counter() - t0)
+    best = float(np.median(runs[1:]))
+    out = {"gpu_s": best, "gpu_runs_s": runs[1:], "gpu_iters": it}
     if not ref_david.available():
         return out
     H.FFT_WORKERS = os.cpu_count() or 1
@@ -677,19 +806,21 @@ def bpcg_bench(pkg, P, wl, h64, with_cpu):
         torch.cuda.synchronize()
         return time.perf_counter() - t0, it, e, bp.stats()
 
-    best = None
-    for _ in range(3):  # the first repeat warms every kernel and handle
+    pairs = []
+    for _ in range(4):  # the first repeat warms every kernel and handle; medians of the other three
         bp = P.DiagoBPCG(pc, nb, ld)
         x = torch.from_numpy(psi0.reshape(-1).copy()).cuda()
         first = run(x, 1, bp)
         later = run(x, 2, bp)
-        if best is None or first[0] + later[0] < best[0][0] + best[1][0]:
-            best = (first, later)
-    first, later = best
-    out = {"workload": WORKLOAD_NAME, "first_step_s": first[0], "first_step_iters": first[1],
-           "first_step_max_residual": first[3][0], "first_step_hpsi_bands": first[3][1],
-           "later_step_s": later[0], "later_step_iters": later[1], "later_step_max_residual": later[3][0],
-           "ms_per_iteration_later_step": 1e3 * later[0] / max(1, later[1])}
+        pairs.append((first, later))
+    pairs = pairs[1:]
+    first, later = pairs[0]
+    t_first = float(np.median([p[0][0] for p in pairs]))
+    t_later = float(np.median([p[1][0] for p in pairs]))
+    out = {"workload": WORKLOAD_NAME, "first_step_s": t_first, "first_step_runs_s": [p[0][0] for p in pairs],
+           "first_step_iters": first[1], "first_step_max_residual": first[3][0], "first_step_hpsi_bands": first[3][1],
+           "later_step_s": t_later, "later_step_runs_s": [p[1][0] for p in pairs], "later_step_iters": later[1],
+           "later_step_max_residual": later[3][0], "ms_per_iteration_later_step": 1e3 * t_later / max(1, later[1])}
     if with_cpu:
         out["8atom"] = guarded_section(bpcg_8atom, pkg)
     return out
@@ -713,8 +844,8 @@ def bpcg_8atom(pkg):
     q, _ = np.linalg.qr(wl.psi0_h[0][:nb, :npw].T)
     psi0 = np.ascontiguousarray(q.T)
     pc = P.precondition_d(wl.basis, 0)
-    best = None
-    for _ in range(3):
+    runs = []
+    for _ in range(4):  # the first run warms the kernels and handles; the median of the other three
         bp = P.DiagoBPCG(pc, nb, npw)
         x = torch.from_numpy(psi0.reshape(-1).copy()).cuda()
         e = np.zeros(nb)
@@ -722,9 +853,9 @@ def bpcg_8atom(pkg):
         t0 = time.perf_counter()
         it = bp.diag_hamilt(h, 0, x, e, 2)
         torch.cuda.synchronize()
-        dt = time.perf_counter() - t0
-        best = dt if best is None else min(best, dt)
-    out = {"gpu_s": best, "gpu_iters": it}
+        runs.append(time.perf_counter() - t0)
+    best = float(np.median(runs[1:]))
+    out = {"gpu_s": best, "gpu_runs_s": runs[1:], "gpu_iters": it}
     if not ref_david.available() or ld != npw:
         return out
     H.FFT_WORKERS = os.cpu_count() or 1
@@ -776,9 +907,10 @@ def davidson_216(pkg):
     psi0 = cell.psi0(basis.gplusk_cart(0), spec.nbands, ld).reshape(-1)
     setup = time.perf_counter() - t0
     pc = P.precondition_d(basis, 0)
-    # five alternating repeats (the faster of each arm is reported): a solve synchronises with the host
-    # every iteration, and a stall of the shared host cores shows up in single repeats (the mixed arm's
-    # repeats spread by up to 0.6 s in one run)
+    # five alternating repeats, medians reported with every run listed: a solve synchronises with the host
+    # every iteration, and a stall of the shared host cores shows up in single repeats.  The errors are
+    # against an FP64 solve to 1e-10; the residual norms through the FP64 H|psi> (pinned to the oracle at
+    # 1e-12 on this cell by the tests) bound every returned eigenvalue's distance to the spectrum
     out = solve_pair(P, h, pc, spec.nbands, ld, psi0, thr_ref=1e-10, repeats=5)
     out["workload"] = (f"216-atom diamond supercell a=30.78 bohr, ecut 40 Ry, 128^3 grid, npw {int(basis.npwk[0])}, "
                        f"480 bands, 1728 projectors (device getvnl), Gamma")
@@ -862,17 +994,17 @@ def kbatch_bench(pkg, steps):
     h = P.device_hamilt(wl, P.PREC_FP64)
     pcs = [P.precondition_d(wl.basis, ik) for ik in iks]
     for name, prec in (("fp64", P.PREC_FP64), ("mixed", P.PREC_MIXED)):
-        # two calls, the faster reported: each call builds its 8 workers' solvers (handles, buffers) and drives
-        # 8 host threads that synchronise every iteration, so single calls vary with the shared host cores
+        # three calls, the median reported (all listed): each call builds its 8 workers' solvers (handles,
+        # buffers) and drives 8 host threads that synchronise every iteration, so calls vary with the host cores
         runs = []
-        for _ in range(2):
+        for _ in range(3):
             psis = [torch.from_numpy(wl.psi0_h[ik].reshape(-1).copy()).cuda() for ik in iks]
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             eig, its = h.solve_kpoints(iks, pcs, psis, ld, nb, 1e-9, 200, precision=prec, nworkers=8)
             torch.cuda.synchronize()
             runs.append(time.perf_counter() - t0)
-        res[name]["solve_all_k_s"] = min(runs)
+        res[name]["solve_all_k_s"] = float(np.median(runs))
         res[name]["solve_all_k_runs_s"] = runs
         res[name]["solve_iters_mean"] = float(np.mean(its))
         if name == "fp64":

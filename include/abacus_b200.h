@@ -30,6 +30,7 @@ extern "C" {
 #define B200_STATUS_NUMERICAL_ERROR 5
 #define B200_STATUS_CAPACITY_ERROR 6
 #define B200_STATUS_NOT_CONVERGED 7
+#define B200_STATUS_CALLBACK_ERROR 8 /* a user H|psi> callback returned nonzero; the solve was abandoned */
 
 /* precision of a handle: plain FP64, or mixed (FP32 FFTs / split-precision GEMMs) */
 #define B200_PREC_FP64 0
@@ -274,9 +275,15 @@ int b200_hamilt_copy_vkb(const b200_hamilt* h, int ik, void* vkb_d, void* stream
  * B200_STATUS_INVALID_ARGUMENT. */
 int b200_tc_cgemm(char transa, char transb, int m, int n, int k, float alpha_re, float alpha_im, const void* a_d,
                   int lda, const void* b_d, int ldb, float beta_re, float beta_im, void* c_d, int ldc, void* stream);
-/* Error word of the calling thread's tensor-core GEMMs (synchronous read): nonzero if a bounded
- * wait inside a kernel ran out (the kernel then returned without finishing its tile). */
+/* Error word of the calling thread's tensor-core GEMMs (synchronous read, cleared by the read):
+ * nonzero if a bounded wait inside a kernel ran out (the kernel then drained its own copies and
+ * MMAs in flight, freed its tensor memory and returned without finishing its tile). */
 int b200_tc_cgemm_error(int* code);
+/* Time limit of each pipeline wait inside the tensor-core GEMMs launched after this call, in
+ * nanoseconds (process-wide; 0 restores the default, 2 s).  No counterpart in the reference, whose
+ * cuBLAS calls have no bounded waits: a test sets a limit that cannot be met and checks that
+ * b200_tc_cgemm_error reports it and that the next GEMM with the default limit is correct. */
+int b200_tc_set_wait_limit_ns(unsigned long long ns);
 
 /* ---- FP64 BLAS functors of the Davidson / nonlocal path (module_hsolver/kernels/math_kernel_op.h) ----
  * gemm_op<std::complex<double>, DEVICE_GPU> (math_kernel_op.h:240-265, cuda/math_kernel_op.cu:815-874):
@@ -304,8 +311,14 @@ int b200_david_create(int nband, int dim, int david_ndim, int precision, const d
                       b200_david** out);
 int b200_david_destroy(b200_david* d);
 /* HPsiFunc (diago_david.h:57): hpsi(X, HX, nvec, dim, id_start, id_end) with X the base pointer of
- * the block (vectors of length dim at X + m*dim) and HX already offset to vector id_start. */
-typedef void (*b200_hpsi_cb)(void* user, const void* x_d, void* hx_d, int nvec, int dim, int id_start, int id_end);
+ * the block (vectors of length dim at X + m*dim) and HX already offset to vector id_start.
+ * Returns 0 on success; any other value abandons the solve, which then returns
+ * B200_STATUS_CALLBACK_ERROR (the reference's HPsiFunc returns void and has no failure path).
+ * Ordering: the solver's stream is synchronised before the call, so X may be read on any stream or
+ * from the host.  The callback's writes to HX must be complete when it returns, or queued on the
+ * legacy default stream (the solver's stream waits for that stream before it reads HX); work left on
+ * another stream is not waited for. */
+typedef int (*b200_hpsi_cb)(void* user, const void* x_d, void* hx_d, int nvec, int dim, int id_start, int id_end);
 /* psi_d: nband vectors at psi_d + m*ldpsi (complex128 for FP64, complex128 for mixed: the solver
  * demotes internally); eigenvalue: host array of nband doubles; returns iterations in *iters. */
 int b200_david_diag(b200_david* d, b200_hpsi_cb hpsi, void* user, int ldpsi, void* psi_d, double* eigenvalue,

@@ -1,7 +1,7 @@
 """Build oracle/_ref/libref_david.so: the reference's own CPU DiagoDavid, compiled from its sources.
 
 Test infrastructure: only the tests and bench.py's CPU reference arm load the library.  Run in a container
-where the reference tree is mounted (default /root/reference, override with ABACUS_REF); the result is a
+where the reference tree is mounted, given by the ABACUS_REF environment variable or build(ref=...); the result is a
 shared library under oracle/_ref/ (git-ignored) that needs only scipy's bundled OpenBLAS at run time.
 
 Compiled from the reference (unchanged, from where they lie):
@@ -47,7 +47,10 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 OUT = HERE / "_ref"
-REF = Path(os.environ.get("ABACUS_REF", "/root/reference")) / "source"
+def _ref_source(ref: str | os.PathLike | None) -> Path | None:
+    """The reference's source/ tree: the argument, else $ABACUS_REF; None when neither is given."""
+    root = ref if ref is not None else os.environ.get("ABACUS_REF")
+    return Path(root) / "source" if root else None
 SOURCES = [
     "module_hsolver/diago_david.cpp",
     "module_hsolver/diago_dav_subspace.cpp",
@@ -116,10 +119,14 @@ def run(cmd):
     return r.stdout
 
 
-def build(quiet: bool = False) -> Path | None:
-    if not REF.exists():
+def build(quiet: bool = False, ref: str | os.PathLike | None = None) -> Path | None:
+    """Compile the library from the reference checkout at `ref` (or $ABACUS_REF); without either, or when the
+    tree is absent, nothing is built and None is returned."""
+    REF = _ref_source(ref)
+    if REF is None or not REF.exists():
         if not quiet:
-            print("reference tree not present: oracle/_ref not rebuilt", file=sys.stderr)
+            print("reference tree not given (ABACUS_REF unset) or not present: oracle/_ref not rebuilt",
+                  file=sys.stderr)
         return None
     OUT.mkdir(exist_ok=True)
     tmp = OUT / "obj"
@@ -146,4 +153,4 @@ def build(quiet: bool = False) -> Path | None:
 
 
 if __name__ == "__main__":
-    print(build())
+    print(build(ref=sys.argv[1] if len(sys.argv) > 1 else None))

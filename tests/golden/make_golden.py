@@ -1,7 +1,7 @@
 """Extract the reference's own golden vectors into small numpy fixtures.
 
-Run in a container where the reference source tree is mounted (default
-/root/reference, override with ABACUS_REF).  Reads the literal arrays of the
+Run in a container where the reference source tree is mounted, with its path in
+ABACUS_REF or as the first argument.  Reads the literal arrays of the
 reference's unit tests as text and writes ``tests/golden/*.npz``:
 
   ekinetic_op.npz  <- source/module_hamilt_pw/hamilt_pwdft/kernels/test/ekinetic_op_test.cpp
@@ -31,7 +31,7 @@ from pathlib import Path
 
 import numpy as np
 
-REF = Path(os.environ.get("ABACUS_REF", "/root/reference"))
+REF = Path(os.environ["ABACUS_REF"]) if os.environ.get("ABACUS_REF") else None
 OUT = Path(__file__).resolve().parent
 
 _num = r"[-+]?(?:\d+\.?\d*|\.\d+)(?:[eE][-+]?\d+)?"
@@ -199,4 +199,8 @@ def io_fixtures():
 
 
 if __name__ == "__main__":
+    if len(sys.argv) > 1:
+        REF = Path(sys.argv[1])
+    if REF is None or not REF.exists():
+        sys.exit("give the reference checkout: ABACUS_REF=<path> or make_golden.py <path>")
     main()

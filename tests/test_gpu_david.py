@@ -53,6 +53,97 @@ def test_david_pyabacus_si2_callback(pkg):
     np.testing.assert_allclose(e, ref, atol=1e-8)
 
 
+def _si2(pkg):
+    import os
+    d = np.load(os.path.join(os.path.dirname(__file__), "golden", "pyabacus_si2.npz"))
+    A = scipy.sparse.csc_matrix((d["data"], d["indices"], d["indptr"]), shape=tuple(d["shape"]))
+    diag = np.abs(A.diagonal())
+    return A, np.where(diag < 1e-8, 1e-8, diag)
+
+
+def test_david_callback_on_side_stream(pkg):
+    """The solver on a non-blocking stream of its own, the callback on torch's default stream: the C-ABI drains
+    the solver's stream before the callback reads X and orders the solver after the callback's writes."""
+    A, diag = _si2(pkg)
+    n, nband = A.shape[0], 16
+    Ad = torch.from_numpy(A.toarray().astype(np.complex128)).cuda()
+    pc = torch.from_numpy(diag).cuda()
+    rng = np.random.default_rng(12)
+    psi = torch.from_numpy(rng.random(n * nband).astype(np.complex128)).cuda()
+
+    def hpsi(x, hx, nvec, dim, i0, i1):
+        m = i1 - i0 + 1
+        X = torch.as_tensor(DevPtr(x, nvec * dim), device="cuda").view(nvec, dim)[i0:i1 + 1]
+        HX = torch.as_tensor(DevPtr(hx, m * dim), device="cuda").view(m, dim)
+        HX.copy_((Ad @ X.T).T)
+
+    side = torch.cuda.Stream()
+    dav = pkg.pwdft.DiagoDavid(pc, nband, n, david_ndim=8)
+    dav.set_stream(side)
+    e = np.zeros(nband)
+    dav.diag(hpsi, n, psi, e, 1e-12, 5000)
+    torch.cuda.synchronize()
+    ref = np.sort(scipy.sparse.linalg.eigsh(A.tocsc(), k=nband, which="SA", tol=1e-12, maxiter=5000)[0])
+    np.testing.assert_allclose(e, ref, atol=1e-8)
+
+
+@pytest.mark.parametrize("solver", ["david", "dav_subspace", "bpcg"])
+def test_callback_exception_reaches_caller(pkg, solver):
+    """An exception raised inside a user H|psi> callback abandons the solve and is raised to the caller
+    (the C-ABI returns B200_STATUS_CALLBACK_ERROR), instead of the solve going on with HX unwritten."""
+    A, diag = _si2(pkg)
+    n, nband = A.shape[0], 8
+    pc = torch.from_numpy(diag).cuda()
+    psi = torch.from_numpy(np.random.default_rng(3).random(n * nband).astype(np.complex128)).cuda()
+    calls = []
+
+    class Boom(Exception):
+        pass
+
+    def hpsi(x, hx, nvec, dim, i0, i1):
+        calls.append(i1 - i0 + 1)
+        if len(calls) == 2:
+            raise Boom("H|psi> failed")
+        m = i1 - i0 + 1
+        HX = torch.as_tensor(DevPtr(hx, m * dim), device="cuda").view(m, dim)
+        HX.zero_()
+
+    P = pkg.pwdft
+    e = np.zeros(nband)
+    with pytest.raises(Boom):
+        if solver == "david":
+            P.DiagoDavid(pc, nband, n, david_ndim=4).diag(hpsi, n, psi, e, 1e-10, 50)
+        elif solver == "dav_subspace":
+            P.DiagoDavSubspace(pc, nband, n, 4, 1e-10, 50, False).diag(hpsi, psi, n, e)
+        else:
+            P.DiagoBPCG(pc, nband, n).diag(hpsi, psi, e, scf_iter=1)
+    assert len(calls) == 2
+    # the library stays usable: the same solver type solves the next problem
+    if solver == "david":
+        Ad = torch.from_numpy(A.toarray().astype(np.complex128)).cuda()
+
+        def good(x, hx, nvec, dim, i0, i1):
+            m = i1 - i0 + 1
+            X = torch.as_tensor(DevPtr(x, nvec * dim), device="cuda").view(nvec, dim)[i0:i1 + 1]
+            torch.as_tensor(DevPtr(hx, m * dim), device="cuda").view(m, dim).copy_((Ad @ X.T).T)
+
+        P.DiagoDavid(pc, nband, n, david_ndim=8).diag(good, n, psi, e, 1e-12, 5000)
+        ref = np.sort(scipy.sparse.linalg.eigsh(A.tocsc(), k=nband, which="SA", tol=1e-12, maxiter=5000)[0])
+        np.testing.assert_allclose(e, ref, atol=1e-8)
+
+
+def test_hsolver_mvv_op_wrong_shape_raises(pkg):
+    """pyabacus-style misuse (mvv_op returning the wrong shape) raises ValueError from davidson()."""
+    A, diag = _si2(pkg)
+    n, nband = A.shape[0], 4
+    v0 = np.random.default_rng(5).random((n, nband))
+    with pytest.raises(ValueError, match="mvv_op returned shape"):
+        pkg.hsolver.davidson(lambda x: A.dot(x)[:-1], v0, n, nband, 1.0 / diag, dav_ndim=4, tol=1e-8, max_iter=50)
+    with pytest.raises(ValueError, match="mvv_op returned shape"):
+        pkg.hsolver.dav_subspace(lambda x: A.dot(x)[:-1], v0, n, nband, 1.0 / diag, dav_ndim=4, tol=1e-8,
+                                 max_iter=50)
+
+
 @pytest.fixture(scope="module")
 def diamond8(pkg):
     spec = pkg.synth.config(0)
@@ -150,3 +241,28 @@ def test_david_136_bands_match_dense_spectrum(pkg, diamond8_dense, prec):
     assert np.max(np.abs(e - w[:nband])) < 1e-8, np.max(np.abs(e - w[:nband]))
     it_low, it64, _ = dav.stats()
     assert (it_low > 0) == (prec == "mixed")
+
+
+@pytest.fixture(scope="module")
+def diamond64(pkg):
+    P = pkg.pwdft
+    wl = P.build_workload(pkg.synth.config(1))
+    return wl, P.device_hamilt(wl, P.PREC_FP64)
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_david_diamond64_matches_oracle_fixture(pkg, golden, diamond64, prec):
+    """The 64-atom cell at full size (npw 51 627, 160 bands, 512 projectors, 96^3): the device FP64 and mixed
+    Davidson solves to thr 1e-9 reach the oracle's eigenvalues (the reference's DiagoDavid driven by the
+    oracle's H|psi> to thr 1e-11, tests/golden/eig_diamond64.npz) within 1e-8 Ry."""
+    P = pkg.pwdft
+    wl, h = diamond64
+    fx = golden("eig_diamond64")
+    nb, ld = wl.spec.nbands, wl.basis.npwk_max
+    pc = P.precondition_d(wl.basis, 0)
+    dav = P.DiagoDavid(pc, nb, ld, 4, P.PREC_FP64 if prec == "fp64" else P.PREC_MIXED)
+    x = torch.from_numpy(wl.psi0_h[0][:nb].reshape(-1).copy()).cuda()
+    e = np.zeros(nb)
+    dav.diag_hamilt(h, 0, ld, x, e, 1e-9, 300)
+    torch.cuda.synchronize()
+    assert np.max(np.abs(e - fx["eig"])) < 1e-8

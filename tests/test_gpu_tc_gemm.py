@@ -88,3 +88,33 @@ def test_tc_cgemm_integer_inputs_exact(pkg, ta, M, N, K):
                        0.0, cd, M)
     torch.cuda.synchronize()
     assert np.array_equal(cd.cpu().numpy().T.astype(np.complex128), ref)
+
+
+def test_tc_cgemm_wait_runout_reports_and_recovers(pkg):
+    """The kernel's bounded waits: with a limit no pipeline can meet (1 ns) a GEMM gives up, drains its own
+    copies and MMAs, frees its tensor memory and sets the error word, which the host reads (and which the read
+    clears); the context stays usable and the next GEMM with the default limit is correct."""
+    P = pkg.pwdft
+    rng = np.random.default_rng(7)
+    M, N, K = 512, 160, 6000
+    A = cplx(rng, M, K)  # column-major K x M (op 'C')
+    B = cplx(rng, N, K)
+    ad, bd = torch.from_numpy(A).cuda(), torch.from_numpy(B).cuda()
+    cd = torch.zeros((N, M), dtype=torch.complex64, device="cuda")
+    assert P.tc_cgemm_error() == 0
+    try:
+        P.tc_set_wait_limit_ns(1)
+        P.tc_cgemm("C", M, N, K, 1.0, ad, K, bd, K, 0.0, cd, M)
+        torch.cuda.synchronize()
+    finally:
+        P.tc_set_wait_limit_ns(0)
+    code = P.tc_cgemm_error()
+    assert code != 0, "a 1 ns wait limit should have run out"
+    assert P.tc_cgemm_error() == 0, "the read clears the error word"
+    P.tc_cgemm("C", M, N, K, 1.0, ad, K, bd, K, 0.0, cd, M)
+    torch.cuda.synchronize()
+    assert P.tc_cgemm_error() == 0
+    ref = A.astype(np.complex128).conj() @ B.astype(np.complex128).T  # (M, N)
+    out = cd.cpu().numpy().T
+    err = np.linalg.norm(out - ref) / np.linalg.norm(ref)
+    assert err < 1e-6, err
