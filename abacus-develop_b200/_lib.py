@@ -67,7 +67,8 @@ _SIGS = {
                                         C.POINTER(vp)], i32),
     "b200_graph_launch": ([vp, vp], i32),
     "b200_graph_destroy": ([vp], i32),
-    "b200_hamilt_autotune": ([vp, i32, i32, i32, vp, vp, vp, pi32], i32),
+    "b200_hamilt_autotune": ([vp, i32, i32, i32, vp, vp, vp, pi32, pi32], i32),
+    "b200_hamilt_set_plane_variant": ([vp, i32], i32),
     "b200_elecstate_pw_op_f64": ([i32, i32, f64, C.POINTER(vp), vp, vp], i32),
     "b200_elecstate_pw_op_f32": ([i32, i32, f32, C.POINTER(vp), vp, vp], i32),
     "b200_elecstate_pw_op_nc_f64": ([i32, i32, i32, f64, C.POINTER(vp), vp, vp, vp], i32),
@@ -96,6 +97,7 @@ _SIGS = {
     "b200_tc_cgemm": ([C.c_char, C.c_char, i32, i32, i32, f32, f32, vp, i32, vp, i32, f32, f32, vp, i32, vp], i32),
     "b200_tc_cgemm_error": ([pi32], i32),
     "b200_tc_set_wait_limit_ns": ([C.c_ulonglong], i32),
+    "b200_measure_peaks": ([pf64, pf64, pf64], i32),
     "b200_gemm_op_f64": ([C.c_char, C.c_char, i32, i32, i32, pf64, vp, i32, vp, i32, pf64, vp, i32, vp], i32),
     "b200_gemv_op_f64": ([C.c_char, i32, i32, pf64, vp, i32, vp, i32, pf64, vp, i32, vp], i32),
     "b200_dot_real_op_f64": ([i32, vp, vp, i32, pf64, vp], i32),

@@ -5,6 +5,7 @@
 // compile-time radices (fft_warp.cuh), so a CTA needs only a handful of block
 // barriers.  Other sizes use the generic kernels.
 #include "fft_warp.cuh"
+#include "plane_t.cuh"
 #include "pw_grid.h"
 
 namespace b200 {
@@ -727,24 +728,57 @@ bool plane_launch(const PWGrid& g, int nb, const R* veff, T* sb, cudaStream_t s)
     return true;
 }
 
-template <typename T, typename R, int N>
-bool plane_launch_r(const PWGrid& g, int nb, const R* vperm, T* sb, cudaStream_t s) {
-    const size_t smem = size_t(g.nxc) * (N | 1) * sizeof(T) + size_t(N) * sizeof(int);
+// Plane pass with the two-pass register transforms (plane_t.cuh): N = R1 * R2, NT threads, RB rows per
+// x batch, at least MINB CTAs per SM.  vt: V_eff arranged for it (launch_arrange_veff).
+template <typename T, typename R, int N, int R1, int R2, int NT, int RB, int MINB>
+bool plane_launch_t(const PWGrid& g, int nb, const R* vt, T* sb, cudaStream_t s) {
+    const size_t smem = plane_t::smem_bytes<T>(R1, R2, RB, N, g.nxc);
     if (smem > 227 * 1024) return false;
-    // FP64: two CTAs of 8 warps per SM (up to 128 registers a thread, 2 x 73 KB of shared memory on the
-    // 96^3 grid); FP32: four of 8 warps (64 registers).  Independent CTAs overlap one CTA's loads and
-    // barriers with another's transforms.
-    constexpr int P = plane_lanes<T, N>();
-    if constexpr (std::is_same<T, double2>::value) {
-        smem_attr(k_plane_p<T, R, N, P, 8, 2>, smem);
-        k_plane_p<T, R, N, P, 8, 2><<<dim3(nb, g.nz), 8 * 32, smem, s>>>(g.plane_view(), g.nz, rtp<T>(g.ax), vperm, sb);
-    } else {
-        smem_attr(k_plane_p<T, R, N, P, 8, 4>, smem);
-        k_plane_p<T, R, N, P, 8, 4><<<dim3(nb, g.nz), 8 * 32, smem, s>>>(g.plane_view(), g.nz, rtp<T>(g.ax), vperm, sb);
-    }
+    auto kern = plane_t::k_plane_t<T, R, N, R1, R2, NT, RB, MINB>;
+    smem_attr(kern, smem);
+    kern<<<dim3(nb, g.nz), NT, smem, s>>>(g.plane_view(), g.nz, rtp<T>(g.ax), vt, sb);
     note_launch();
     B200_CUDA(cudaGetLastError());
     return true;
+}
+
+// the register-transform plane pass of variant `var` (1: one warp per line with warp-shuffle lane stages;
+// 2-5: two-pass transforms in four launch shapes; 0: the default shape)
+template <typename T, typename R, int N>
+bool plane_launch_var(const PWGrid& g, int var, int nb, const R* vperm, T* sb, cudaStream_t s) {
+    constexpr bool f64 = std::is_same<T, double2>::value;
+    const R* vt = vperm + g.nxyz();
+    if (var == 1) {
+        const size_t smem = size_t(g.nxc) * (N | 1) * sizeof(T) + size_t(N) * sizeof(int);
+        if (smem > 227 * 1024) return false;
+        // FP64: two CTAs of 8 warps per SM (up to 128 registers a thread); FP32: four of 8 warps
+        constexpr int P = plane_lanes<T, N>();
+        if constexpr (f64) {
+            smem_attr(k_plane_p<T, R, N, P, 8, 2>, smem);
+            k_plane_p<T, R, N, P, 8, 2><<<dim3(nb, g.nz), 8 * 32, smem, s>>>(g.plane_view(), g.nz, rtp<T>(g.ax), vperm, sb);
+        } else {
+            smem_attr(k_plane_p<T, R, N, P, 8, 4>, smem);
+            k_plane_p<T, R, N, P, 8, 4><<<dim3(nb, g.nz), 8 * 32, smem, s>>>(g.plane_view(), g.nz, rtp<T>(g.ax), vperm, sb);
+        }
+        note_launch();
+        B200_CUDA(cudaGetLastError());
+        return true;
+    }
+    constexpr int R2 = 8, R1 = N / 8;
+    constexpr int M2 = f64 ? 1 : 2;  // FP32 planes take half the shared memory: twice the CTAs per SM
+    switch (var) {
+        case 3: return plane_launch_t<T, R, N, R1, R2, 256, 32, 1 * M2>(g, nb, vt, sb, s);
+        case 4: return plane_launch_t<T, R, N, R1, R2, 384, 32, 1>(g, nb, vt, sb, s);
+        case 5: return plane_launch_t<T, R, N, R1, R2, 256, 16, 2>(g, nb, vt, sb, s);
+        default: return plane_launch_t<T, R, N, R1, R2, 192, 16, 2 * M2>(g, nb, vt, sb, s);
+    }
+}
+
+template <typename T, typename R, int N>
+bool plane_launch_r(const PWGrid& g, int nb, const R* vperm, T* sb, cudaStream_t s) {
+    const int var = std::is_same<T, double2>::value ? g.plane_variant64 : g.plane_variant32;
+    if (plane_launch_var<T, R, N>(g, var, nb, vperm, sb, s)) return true;
+    return var != 1 && plane_launch_var<T, R, N>(g, 1, nb, vperm, sb, s);  // shapes whose plane does not fit
 }
 
 template <typename T, typename R>
@@ -800,6 +834,25 @@ bool zbatch_dispatch(bool inv, const PWGrid& g, const KBatchArgs& args, int nk, 
 template <typename T, typename R, int NZ, typename Src>
 void zpass_r(bool inv, const PWGrid& g, const Src& src, int nk, int b0, int nbc, T* sb, double tpiba2, int accumulate,
              cudaStream_t s) {
+    const int var = std::is_same<T, double2>::value ? g.plane_variant64 : g.plane_variant32;
+    if (var != 1) {
+        // two-pass register transforms: 32 sticks per CTA, 4 warps
+        constexpr int R2 = 8, R1 = NZ / 8, TS = 32, NT = 128;
+        const dim3 grid(ceil_div(g.nst, TS), nbc, nk);
+        constexpr size_t smem = plane_t::zpass_smem_bytes<T>(R1, R2, TS);
+        if (inv) {
+            auto kern = plane_t::k_zinv_t<T, NZ, R1, R2, TS, NT, Src>;
+            smem_attr(kern, smem);
+            kern<<<grid, NT, smem, s>>>(src, b0, nbc, rtp<T>(g.az), sb);
+        } else {
+            auto kern = plane_t::k_zfwd_t<T, R, NZ, R1, R2, TS, NT, Src>;
+            smem_attr(kern, smem);
+            kern<<<grid, NT, smem, s>>>(src, b0, nbc, rtp<T>(g.az), sb, R(tpiba2), R(1.0 / double(g.nxyz())), accumulate);
+        }
+        note_launch();
+        B200_CUDA(cudaGetLastError());
+        return;
+    }
     const dim3 grid(ceil_div(g.nst, kStickTile), nbc, nk);
     if (inv)
         k_zinv_r<T, NZ, Src><<<grid, kZWarps * 32, 0, s>>>(src, b0, nbc, rtp<T>(g.az), sb);
@@ -836,7 +889,7 @@ template <typename T, typename R, typename Src>
 bool local_r(const PWGrid& g, const Src& src, int nk, int b0, int nbc, const R* vperm, T* sb, double tpiba2,
              int accumulate, cudaStream_t s) {
     const size_t smem = size_t(g.nxc) * (g.nx | 1) * sizeof(T) + size_t(g.nx) * sizeof(int);
-    if (smem > 227 * 1024) return false;
+    if (smem > 227 * 1024) return false;  // neither plane pass fits (the two-pass one needs more)
     zpass_r_dispatch<T, R>(true, g, src, nk, b0, nbc, sb, tpiba2, accumulate, s);
     plane_r_dispatch<T, R>(g, nk * nbc, vperm, sb, s);
     zpass_r_dispatch<T, R>(false, g, src, nk, b0, nbc, sb, tpiba2, accumulate, s);
@@ -928,6 +981,17 @@ bool launch_permute_veff(const PWGrid& g, const R* veff_zyx, R* out, cudaStream_
 }
 template bool launch_permute_veff<double>(const PWGrid&, const double*, double*, cudaStream_t);
 template bool launch_permute_veff<float>(const PWGrid&, const float*, float*, cudaStream_t);
+
+template <typename R>
+bool launch_arrange_veff(const PWGrid& g, const R* veff_zyx, R* out, cudaStream_t s) {
+    if (!plane_perm_supported(g)) return false;
+    plane_t::k_arrange_veff<R><<<1184, 256, 0, s>>>(g.nz, g.nx, g.nx / 8, 8, veff_zyx, out);
+    note_launch();
+    B200_CUDA(cudaGetLastError());
+    return true;
+}
+template bool launch_arrange_veff<double>(const PWGrid&, const double*, double*, cudaStream_t);
+template bool launch_arrange_veff<float>(const PWGrid&, const float*, float*, cudaStream_t);
 
 bool rho_r_supported(const PWGrid& g) {
     const size_t smem = size_t(g.nxc) * (g.nx | 1) * sizeof(double2) + size_t(g.nx) * sizeof(int);

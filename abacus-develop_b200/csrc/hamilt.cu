@@ -5,9 +5,6 @@
 
 namespace b200 {
 
-__global__ void k_d2f(long n, const double* __restrict__ a, float* __restrict__ b) {
-    for (long i = blockIdx.x * long(blockDim.x) + threadIdx.x; i < n; i += long(gridDim.x) * blockDim.x) b[i] = float(a[i]);
-}
 // rows x cols (row pitch lda) complex128 -> complex64 with row pitch ldb (the extra column zeroed)
 __global__ void k_z2c_pitch(int rows, int cols, int lda, int ldb, const double2* __restrict__ a, float2* __restrict__ b) {
     const long n = long(rows) * ldb;
@@ -18,22 +15,40 @@ __global__ void k_z2c_pitch(int rows, int cols, int lda, int ldb, const double2*
     }
 }
 
-// ps in the K-major (becp) layout, ps[b*nkb + j] = sum_x D[x, k] becp[b*nkb + x] over the atom block of j:
-// the same contraction as nonlocal_pw_op (nonlocal_op.cpp:8-41) with the output transposed for the GEMM that follows
-template <typename T, typename R>
-__global__ void k_nonlocal_kmajor(int l1, int nb, int l3, int sum, int iat, int spin, int nkb, int dx, int dy, int dz,
-                                  const R* __restrict__ deeq, T* __restrict__ ps, const T* __restrict__ becp) {
-    const long total = long(l1) * l3 * nb;
+// The atom types of D as the folding kernel sees them (by value)
+struct FoldTypes {
+    int ntype;
+    int sum0[kVnlMaxTypes + 1];  // first projector row of each type
+    int iat0[kVnlMaxTypes];      // first atom of each type
+    int nh[kVnlMaxTypes];
+};
+
+// out[sum + ia*nh + x][g] = sum_k D(spin, iat + ia, x, k) vkb[sum + ia*nh + k][g], in FP64, stored in To with
+// row pitch ldo (the order of add_nonlocal_pp's ps = D becp, nonlocal_pw.cpp:64-110, moved onto the projectors)
+template <typename To>
+__global__ void k_fold_deeq(int nkb, int npwx, int ldo, FoldTypes ft, int spin, int dx, int dy, int dz,
+                            const double* __restrict__ deeq, const double2* __restrict__ vkb, To* __restrict__ out) {
+    const long total = long(nkb) * npwx;
     for (long t = blockIdx.x * long(blockDim.x) + threadIdx.x; t < total; t += long(gridDim.x) * blockDim.x) {
-        const int kk = int(t % l3);
-        const long r = t / l3;
-        const int ii = int(r % l1);
-        const int b = int(r / l1);
-        const R* d = deeq + (long(spin * dx + iat + ii) * dy) * dz + kk;
-        const T* bp = becp + long(b) * nkb + sum + ii * l3;
-        T acc = cmake<T>(0, 0);
-        for (int xx = 0; xx < l3; ++xx) acc = cadd(acc, cscale(bp[xx], d[long(xx) * dz]));
-        ps[long(b) * nkb + sum + ii * l3 + kk] = acc;
+        const int g = int(t % npwx);
+        const int j = int(t / npwx);
+        int it = 0;
+        while (it + 1 < ft.ntype && j >= ft.sum0[it + 1]) ++it;
+        const int nh = ft.nh[it];
+        const int ia = (j - ft.sum0[it]) / nh;
+        const int x = (j - ft.sum0[it]) - ia * nh;
+        const int row0 = ft.sum0[it] + ia * nh;
+        const double* d = deeq + (long(spin * dx + ft.iat0[it] + ia) * dy + x) * dz;
+        double re = 0.0, im = 0.0;
+        for (int k = 0; k < nh; ++k) {
+            const double2 v = vkb[long(row0 + k) * npwx + g];
+            re = fma(d[k], v.x, re);
+            im = fma(d[k], v.y, im);
+        }
+        To o;
+        o.x = re;
+        o.y = im;
+        out[long(j) * ldo + g] = o;
     }
 }
 
@@ -63,10 +78,13 @@ void Hamilt::set_veff(const double* veff_d) {
     launch_transpose_veff<float>(*grid, veff_d, veff_zyxf.ptr, 0);
     has_perm = plane_perm_supported(*grid);
     if (has_perm) {
-        veff_perm.resize(N);
-        veff_permf.resize(N);
+        // two layouts back to back: the warp-shuffle plane pass's, then the two-pass plane pass's
+        veff_perm.resize(2 * N);
+        veff_permf.resize(2 * N);
         launch_permute_veff<double>(*grid, veff_zyx.ptr, veff_perm.ptr, 0);
         launch_permute_veff<float>(*grid, veff_zyxf.ptr, veff_permf.ptr, 0);
+        launch_arrange_veff<double>(*grid, veff_zyx.ptr, veff_perm.ptr + N, 0);
+        launch_arrange_veff<float>(*grid, veff_zyxf.ptr, veff_permf.ptr + N, 0);
     }
     B200_CUDA(cudaStreamSynchronize(0));
     has_veff = true;
@@ -92,6 +110,7 @@ void Hamilt::set_vkb(int ik, int nkb, int npwx, const double2* vkb_d) {
     k_z2c_pitch<<<592, 256>>>(nkb, npwx, npwx, k.ldf, vkb_d, k.vkbf.ptr);
     note_launch();
     B200_CUDA(cudaGetLastError());
+    fold_projectors(ik, 0);
     B200_CUDA(cudaStreamSynchronize(0));
 }
 
@@ -108,11 +127,44 @@ void Hamilt::set_deeq(int ntype_, const int* na_, const int* nh_, int nspin_, in
     const long n = long(nspin) * dx * dy * dz;
     deeq.resize(n);
     B200_CUDA(cudaMemcpyAsync(deeq.ptr, deeq_d, n * sizeof(double), cudaMemcpyDeviceToDevice, 0));
-    deeqf.resize(n);
-    k_d2f<<<592, 256>>>(n, deeq_d, deeqf.ptr);
-    note_launch();
-    B200_CUDA(cudaGetLastError());
+    for (int ik = 0; ik < int(nl.size()); ++ik) fold_projectors(ik, 0);
     B200_CUDA(cudaStreamSynchronize(0));
+}
+
+void Hamilt::fold_projectors(int ik, cudaStream_t s) {
+    NonlocalK& k = nl[ik];
+    k.folded = false;
+    if (k.nkb <= 0 || !deeq.ptr || k.vkb.ptr == nullptr) return;
+    B200_CHECK(ntype >= 1 && ntype <= kVnlMaxTypes, kInvalidArgument, "1..8 atom types supported by the projector fold");
+    FoldTypes ft{};
+    ft.ntype = ntype;
+    int sum = 0, iat = 0;
+    for (int it = 0; it < ntype; ++it) {
+        ft.sum0[it] = sum;
+        ft.iat0[it] = iat;
+        ft.nh[it] = nh[it];
+        B200_CHECK(nh[it] >= 1 && nh[it] <= dy && nh[it] <= dz, kInvalidArgument, "nh larger than deeq's nhm");
+        sum += na[it] * nh[it];
+        iat += na[it];
+    }
+    ft.sum0[ntype] = sum;
+    B200_CHECK(sum == k.nkb, kInvalidArgument, "sum of na*nh over types differs from nkb");
+    B200_CHECK(iat <= dx, kInvalidArgument, "more atoms than deeq's first dimension");
+    const long total = long(k.nkb) * k.npwx;
+    int blocks = int((total + 255) / 256);
+    if (blocks > 148 * 8) blocks = 148 * 8;
+    k.vkbd.resize(size_t(nspin) * total);
+    k.vkbdf.resize(size_t(nspin) * k.nkb * k.ldf);
+    if (k.ldf != k.npwx) B200_CUDA(cudaMemsetAsync(k.vkbdf.ptr, 0, k.vkbdf.n * sizeof(float2), s));
+    for (int sp = 0; sp < nspin; ++sp) {
+        k_fold_deeq<double2><<<blocks, 256, 0, s>>>(k.nkb, k.npwx, k.npwx, ft, sp, dx, dy, dz, deeq.ptr, k.vkb.ptr,
+                                                    k.vkbd.ptr + size_t(sp) * total);
+        k_fold_deeq<float2><<<blocks, 256, 0, s>>>(k.nkb, k.npwx, k.ldf, ft, sp, dx, dy, dz, deeq.ptr, k.vkb.ptr,
+                                                   k.vkbdf.ptr + size_t(sp) * k.nkb * k.ldf);
+        note_launch(2);
+        B200_CUDA(cudaGetLastError());
+    }
+    k.folded = true;
 }
 
 int Hamilt::band_chunk(size_t elem) const {
@@ -156,9 +208,7 @@ void Hamilt::hpsi(int ik, int spin, int nb, int ld, const T* psi, T* hpsi, int m
     auto& sb64 = W.sb64;
     auto& sb32 = W.sb32;
     auto& becp64 = W.becp64;
-    auto& ps64 = W.ps64;
     auto& becp32 = W.becp32;
-    auto& ps32 = W.ps32;
     auto& psi_pad32 = W.psi_pad32;
     auto& tcw = W.tcw;
     cublasHandle_t cublas = W.cublas;
@@ -194,47 +244,31 @@ void Hamilt::hpsi(int ik, int spin, int nb, int ld, const T* psi, T* hpsi, int m
         return;
     }
     const int nkb = k.nkb;
-    T* becp;
-    T* ps;
-    if constexpr (f64) {
-        becp64.resize(size_t(nkb) * nb);
-        ps64.resize(size_t(nkb) * nb);
-        becp = becp64.ptr;
-        ps = ps64.ptr;
-    } else {
-        becp32.resize(size_t(nkb) * nb);
-        ps32.resize(size_t(nkb) * nb);
-        becp = becp32.ptr;
-        ps = ps32.ptr;
-    }
-    const T one = cmake<T>(1, 0), zero = cmake<T>(0, 0);
-    const R* d = f64 ? (const R*)deeq.ptr : (const R*)deeqf.ptr;
-    B200_CHECK(d != nullptr, kInvalidArgument, "deeq not set");
+    B200_CHECK(deeq.ptr != nullptr, kInvalidArgument, "deeq not set");
     B200_CHECK(spin >= 0 && spin < nspin, kInvalidArgument, "spin out of range");
-    const int ldps = f64 ? nkb : nkb + (nkb & 1);
-    if constexpr (!f64) {
-        if (ldps != nkb) {
-            becp32.resize(size_t(ldps) * nb);
-            ps32.resize(size_t(ldps) * nb);
-            becp = becp32.ptr;
-            ps = ps32.ptr;
-        }
+    const T one = cmake<T>(1, 0), zero = cmake<T>(0, 0);
+    // becp with an even leading dimension in FP32 (TMA row pitch of the second product)
+    const int ldb_p = f64 ? nkb : nkb + (nkb & 1);
+    T* becp;
+    if constexpr (f64) {
+        becp64.resize(size_t(ldb_p) * nb);
+        becp = becp64.ptr;
+    } else {
+        becp32.resize(size_t(ldb_p) * nb);
+        becp = becp32.ptr;
     }
-    // first half of Nonlocal::act, which reads only psi: becp = vkb^H psi (nonlocal_pw.cpp:261-276) and
-    // ps = D becp per atom type (add_nonlocal_pp, nonlocal_pw.cpp:64-110)
+    // Nonlocal::act (nonlocal_pw.cpp:211-304): becp = vkb^H psi, then H psi += vkb (D becp), here with D folded
+    // into the projectors once per k-point and spin: H psi += vkbd becp (vkbd = D vkb per atom block)
+    B200_CHECK(k.folded, kInvalidArgument, "projectors and D not both set for this k-point");
+    const T* vkbd = f64 ? reinterpret_cast<const T*>(k.vkbd.ptr + size_t(spin) * nkb * k.npwx)
+                        : reinterpret_cast<const T*>(k.vkbdf.ptr + size_t(spin) * nkb * k.ldf);
     auto projections = [&](cudaStream_t st) {
         if constexpr (f64) {
-            const T* vkb = (const T*)k.vkb.ptr;
             B200_CUBLAS(cublasSetStream(cublas, st));
-            B200_CUBLAS(Blas<T>::gemm(cublas, CUBLAS_OP_C, CUBLAS_OP_N, nkb, nb, npw, &one, vkb, k.npwx, psi, ld, &zero,
-                                      becp, nkb));
-            B200_CUDA(cudaMemsetAsync(ps, 0, size_t(nkb) * nb * sizeof(T), st));
-            int sum = 0, iat = 0;
-            for (int it = 0; it < ntype; ++it)
-                nonlocal_pw<T, R>(na[it], nb, nh[it], sum, iat, spin, nkb, dx, dy, dz, d, ps, becp, st);
-            B200_CHECK(sum == nkb, kInvalidArgument, "sum of na*nh over types differs from nkb");
+            B200_CUBLAS(Blas<T>::gemm(cublas, CUBLAS_OP_C, CUBLAS_OP_N, nkb, nb, npw, &one, (const T*)k.vkb.ptr, k.npwx,
+                                      psi, ld, &zero, becp, nkb));
         } else {
-            // mixed precision: both projector products on the tensor cores (3xTF32), ps kept in becp's layout
+            // mixed precision: both projector products on the tensor cores (3xTF32)
             const float2* psi_b = psi;
             int ldb = ld;
             if (ld & 1) {  // the TMA row pitch must be a multiple of 16 bytes: stage psi with an even pitch
@@ -244,28 +278,13 @@ void Hamilt::hpsi(int ik, int spin, int nb, int ld, const T* psi, T* hpsi, int m
                                             size_t(npw) * sizeof(float2), nb, cudaMemcpyDeviceToDevice, st));
                 psi_b = psi_pad32.ptr;
             }
-            tc_cgemm('C', nkb, nb, npw, one, k.vkbf.ptr, k.ldf, psi_b, ldb, zero, becp, ldps, tcw, st);
-            int sum = 0, iat = 0;
-            for (int it = 0; it < ntype; ++it) {
-                const long total = long(na[it]) * nh[it] * nb;
-                if (total > 0) {
-                    int blocks = int((total + 255) / 256);
-                    if (blocks > 148 * 8) blocks = 148 * 8;
-                    k_nonlocal_kmajor<T, R><<<blocks, 256, 0, st>>>(na[it], nb, nh[it], sum, iat, spin, ldps, dx, dy, dz,
-                                                                   d, ps, becp);
-                    note_launch();
-                    B200_CUDA(cudaGetLastError());
-                }
-                sum += na[it] * nh[it];
-                iat += na[it];
-            }
-            B200_CHECK(sum == nkb, kInvalidArgument, "sum of na*nh over types differs from nkb");
+            tc_cgemm('C', nkb, nb, npw, one, k.vkbf.ptr, k.ldf, psi_b, ldb, zero, becp, ldb_p, tcw, st);
         }
     };
     if (mode == 2) {
         projections(s);
     } else {
-        // the projections run on a second stream beside the local pass (they read psi only); hpsi += vkb ps
+        // the projection runs on a second stream beside the local pass (it reads psi only); H psi += vkbd becp
         // waits for both
         W.ensure_side();
         B200_CUDA(cudaEventRecord(W.ev_fork, s));
@@ -275,13 +294,12 @@ void Hamilt::hpsi(int ik, int spin, int nb, int ld, const T* psi, T* hpsi, int m
         local_pass(s);
         B200_CUDA(cudaStreamWaitEvent(s, W.ev_join, 0));
     }
-    // hpsi += vkb ps^T (nonlocal_pw.cpp:190-205)
     if constexpr (f64) {
         B200_CUBLAS(cublasSetStream(cublas, s));
-        B200_CUBLAS(Blas<T>::gemm(cublas, CUBLAS_OP_N, CUBLAS_OP_T, npw, nb, nkb, &one, (const T*)k.vkb.ptr, k.npwx, ps,
-                                  nb, &one, hpsi, ld));
+        B200_CUBLAS(Blas<T>::gemm(cublas, CUBLAS_OP_N, CUBLAS_OP_N, npw, nb, nkb, &one, vkbd, k.npwx, becp, nkb, &one,
+                                  hpsi, ld));
     } else {
-        tc_cgemm('N', npw, nb, nkb, one, k.vkbf.ptr, k.ldf, ps, ldps, one, hpsi, ld, tcw, s);
+        tc_cgemm('N', npw, nb, nkb, one, vkbd, k.ldf, becp, ldb_p, one, hpsi, ld, tcw, s);
     }
 }
 

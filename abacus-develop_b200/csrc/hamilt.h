@@ -16,14 +16,21 @@ struct NonlocalK {
     DeviceArray<double2> vkb;   // nkb x npwx row-major (column-major npwx x nkb)
     DeviceArray<float2> vkbf;   // FP32 copy, leading dimension ldf = npwx rounded up to even (TMA row pitch)
     int ldf = 0;
+    // D folded into the projectors for the second product of Nonlocal::act: row x of atom a is
+    // sum_k D(spin, a, x, k) vkb_k, so that H psi += vkbd becp needs no ps = D becp step.  One block of
+    // nkb rows per spin; rebuilt whenever the projectors or D change (set-up calls only, so H|psi> itself
+    // only reads them and concurrent callers need no lock).
+    DeviceArray<double2> vkbd;  // nspin x nkb x npwx
+    DeviceArray<float2> vkbdf;  // nspin x nkb x ldf
+    bool folded = false;
 };
 
-// Scratch of one H|psi> caller: stick buffer, becp / ps, the padded-psi stage, a cuBLAS handle and the
+// Scratch of one H|psi> caller: stick buffer, becp, the padded-psi stage, a cuBLAS handle and the
 // tensor-core GEMM workspace.  Callers that run H|psi> concurrently (different streams or threads) each
 // own one; the Hamiltonian itself is read-only after set-up.
 struct HpsiWork {
-    DeviceArray<double2> sb64, becp64, ps64;
-    DeviceArray<float2> sb32, becp32, ps32, psi_pad32;
+    DeviceArray<double2> sb64, becp64;
+    DeviceArray<float2> sb32, becp32, psi_pad32;
     cublasHandle_t cublas = nullptr;
     TcGemmWorkspace tcw;
     // second stream of an H|psi>: the projections (becp, D becp) run on it beside the local pass
@@ -60,7 +67,9 @@ struct Hamilt {
     int precision = 0;  // 0 = FP64, 1 = mixed
     DeviceArray<double> veff_zyx;
     DeviceArray<float> veff_zyxf;
-    DeviceArray<double> veff_perm;  // (z, y, x) in the register-transform order (grids with 32*m square planes)
+    // grids with 32*m square planes: (z, y, x) in the warp-shuffle register-transform order, then (N more
+    // values) the arrangement of the two-pass plane transforms
+    DeviceArray<double> veff_perm;
     DeviceArray<float> veff_permf;
     bool has_perm = false;
     template <typename R> const R* veff_of() const;
@@ -70,7 +79,6 @@ struct Hamilt {
     int ntype = 0, nspin = 1, dx = 0, dy = 0, dz = 0;
     std::vector<int> na, nh;
     DeviceArray<double> deeq;
-    DeviceArray<float> deeqf;
     HpsiWork work;  // default scratch for callers that do not bring their own
     int chunk_override = 0;  // bands per stick-buffer chunk chosen by the autotuner (0 = 48 MB rule)
     VnlTables vnl;           // projector tables for on-device getvnl
@@ -87,6 +95,8 @@ struct Hamilt {
     void set_vkb(int ik, int nkb, int npwx, const double2* vkb_d);
     void set_deeq(int ntype, const int* na, const int* nh, int nspin, int dx, int dy, int dz, const double* deeq_d);
     int band_chunk(size_t elem) const;
+    // fold D into the projectors of k-point ik (all spins), on stream s; nothing if either is not set
+    void fold_projectors(int ik, cudaStream_t s);
     // mode 0 = full H, 1 = kinetic + local only (overwrites hpsi), 2 = nonlocal only (accumulates)
     template <typename T>
     void hpsi(int ik, int spin, int nb, int ld, const T* psi, T* hpsi, int mode, cudaStream_t s, HpsiWork* w = nullptr);

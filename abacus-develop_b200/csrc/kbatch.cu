@@ -88,47 +88,78 @@ int b200_graph_destroy(b200_graph* g) {
 }
 
 int b200_hamilt_autotune(b200_hamilt* h, int ik, int nbands, int ld, const void* psi_d, void* hpsi_d, void* stream,
-                         int* best_chunk) {
+                         int* best_chunk, int* best_variant) {
     return guarded([&] {
         B200_CHECK(h && psi_d && hpsi_d, b200::kInvalidArgument, "NULL argument");
         cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
         b200::Hamilt& H = *h->h;
+        b200::PWGrid& G = *H.grid;
         const bool f64 = H.precision == B200_PREC_FP64;
+        int& variant = f64 ? G.plane_variant64 : G.plane_variant32;
         std::vector<int> cand = {1, 2, 4, 8, 16, 32, 64, 128};
         cand.push_back(nbands);
         std::sort(cand.begin(), cand.end());
         cand.erase(std::unique(cand.begin(), cand.end()), cand.end());
+        // plane-pass variants: only grids with the register transforms have a choice
+        std::vector<int> vars = {variant};
+        if (b200::plane_perm_supported(G)) {
+            vars.clear();
+            for (int v = 1; v <= b200::kPlaneVariants; ++v) vars.push_back(v);
+        }
         cudaEvent_t e0, e1;
         B200_CUDA(cudaEventCreate(&e0));
         B200_CUDA(cudaEventCreate(&e1));
         float best = 1e30f;
-        int best_c = 0;
-        const int saved = H.chunk_override;
-        for (int c : cand) {
-            if (c > nbands) continue;
-            H.chunk_override = c;
-            auto run = [&] {
-                if (f64)
-                    H.hpsi<double2>(ik, 0, nbands, ld, (const double2*)psi_d, (double2*)hpsi_d, 1, s);
-                else
-                    H.hpsi<float2>(ik, 0, nbands, ld, (const float2*)psi_d, (float2*)hpsi_d, 1, s);
-            };
-            run();  // warm-up (allocates the stick buffer for this chunk size)
-            B200_CUDA(cudaEventRecord(e0, s));
-            for (int r = 0; r < 3; ++r) run();
-            B200_CUDA(cudaEventRecord(e1, s));
-            B200_CUDA(cudaEventSynchronize(e1));
-            float ms = 0.f;
-            B200_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-            if (ms < best) {
-                best = ms;
-                best_c = c;
+        int best_c = 0, best_v = variant;
+        const int saved_c = H.chunk_override, saved_v = variant;
+        try {
+            for (int v : vars) {
+                variant = v;
+                for (int c : cand) {
+                    if (c > nbands) continue;
+                    H.chunk_override = c;
+                    auto run = [&] {
+                        if (f64)
+                            H.hpsi<double2>(ik, 0, nbands, ld, (const double2*)psi_d, (double2*)hpsi_d, 1, s);
+                        else
+                            H.hpsi<float2>(ik, 0, nbands, ld, (const float2*)psi_d, (float2*)hpsi_d, 1, s);
+                    };
+                    run();  // warm-up (allocates the stick buffer for this chunk size)
+                    B200_CUDA(cudaEventRecord(e0, s));
+                    for (int r = 0; r < 3; ++r) run();
+                    B200_CUDA(cudaEventRecord(e1, s));
+                    B200_CUDA(cudaEventSynchronize(e1));
+                    float ms = 0.f;
+                    B200_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+                    if (ms < best) {
+                        best = ms;
+                        best_c = c;
+                        best_v = v;
+                    }
+                }
             }
+        } catch (...) {
+            H.chunk_override = saved_c;
+            variant = saved_v;
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            throw;
         }
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
-        H.chunk_override = best_c > 0 ? best_c : saved;
+        H.chunk_override = best_c > 0 ? best_c : saved_c;
+        variant = best_v;
         if (best_chunk) *best_chunk = H.chunk_override;
+        if (best_variant) *best_variant = variant;
+    });
+}
+
+int b200_hamilt_set_plane_variant(b200_hamilt* h, int variant) {
+    return guarded([&] {
+        B200_CHECK(h != nullptr, b200::kInvalidArgument, "NULL argument");
+        B200_CHECK(variant >= 0 && variant <= b200::kPlaneVariants, b200::kInvalidArgument, "plane variant out of range");
+        b200::PWGrid& G = *h->h->grid;
+        (h->h->precision == B200_PREC_FP64 ? G.plane_variant64 : G.plane_variant32) = variant;
     });
 }
 

@@ -70,6 +70,8 @@ struct PWGrid {
     std::vector<int> h_xpos, h_xc, h_sy, h_sixy;
     std::vector<KMap> kmaps;
     bool on_device = false;
+    // plane pass of the register transforms, per precision (0: default shape; see plane_launch_var)
+    int plane_variant64 = 0, plane_variant32 = 0;
 
     void build(const PWBasisK& b);  // host-side plans and maps only (no GPU needed)
     void ensure_device();           // uploads plans and maps on first device use
@@ -141,5 +143,11 @@ template <typename R>
 void launch_rho_reduce_r(const PWGrid& g, int nsplit, const R* ws, R* rho, cudaStream_t s);
 template <typename R>
 bool launch_permute_veff(const PWGrid& g, const R* veff_zyx, R* out, cudaStream_t s);
+// The same grids: V_eff arranged for the two-pass plane transforms, out[z slot][p][k1][k2] =
+// veff_zyx[z][y(p)][k1 + R1 k2] with N = 8 R1, y(p) = p/8 + R1 (p mod 8) (plane_t.cuh)
+template <typename R>
+bool launch_arrange_veff(const PWGrid& g, const R* veff_zyx, R* out, cudaStream_t s);
+// Number of plane-pass variants the autotuner may choose from (1 .. kPlaneVariants)
+constexpr int kPlaneVariants = 5;
 
 }  // namespace b200

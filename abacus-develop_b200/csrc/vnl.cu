@@ -279,6 +279,7 @@ void Hamilt::build_vkb(int ik, cudaStream_t s) {
                                                                 k.vkb.ptr, k.npwx, k.vkbf.ptr, k.ldf);
     note_launch();
     B200_CUDA(cudaGetLastError());
+    fold_projectors(ik, s);
 }
 
 }  // namespace b200

@@ -104,6 +104,13 @@ def tc_cgemm_error():
     return code.value
 
 
+def measure_peaks():
+    """Measured FP64 / FP32 CUDA-core FMA and FP64 tensor-core MMA peaks of the current device, TFLOP/s."""
+    a, b, c = C.c_double(), C.c_double(), C.c_double()
+    call("b200_measure_peaks", C.byref(a), C.byref(b), C.byref(c))
+    return {"fp64_tflops": a.value, "fp32_tflops": b.value, "dmma_fp64_tflops": c.value}
+
+
 def tc_set_wait_limit_ns(ns):
     """Limit of each pipeline wait inside the tensor-core GEMMs launched afterwards (0: the default, 2 s)."""
     call("b200_tc_set_wait_limit_ns", int(ns))
@@ -407,12 +414,19 @@ class HamiltPW:
              C.byref(g))
         return HpsiGraph(g, keep=(self, list(psis), list(hpsis)))
 
-    def autotune(self, ik, psi, hpsi, nbands, ld, stream=None):
-        """Pick the band-chunk size of the local pass by timing candidates; returns the chosen size."""
+    def autotune(self, ik, psi, hpsi, nbands, ld, stream=None, with_variant=False):
+        """Pick the band-chunk size and plane-pass variant of the local pass by timing candidates; returns the
+        chosen chunk size (and the variant with with_variant=True)."""
         self._chk(psi, hpsi, nbands, ld)
-        best = C.c_int()
-        call("b200_hamilt_autotune", self._h, ik, nbands, ld, ptr(psi), ptr(hpsi), stream_ptr(stream), C.byref(best))
-        return best.value
+        best, var = C.c_int(), C.c_int()
+        call("b200_hamilt_autotune", self._h, ik, nbands, ld, ptr(psi), ptr(hpsi), stream_ptr(stream), C.byref(best),
+             C.byref(var))
+        return (best.value, var.value) if with_variant else best.value
+
+    def set_plane_variant(self, variant):
+        """Plane pass of the register transforms (1: warp-shuffle lanes; 2-5: two-pass transforms; 0: default)
+        for every handle of this basis in this handle's precision."""
+        call("b200_hamilt_set_plane_variant", self._h, int(variant))
 
     def solve_kpoints(self, iks, precond_ds, psis, ld_psi, nband, thr, maxiter, david_ndim=4, precision=PREC_FP64,
                       nworkers=4, ntry_max=5, notconv_max=0, spin=0):

@@ -213,6 +213,7 @@ def _cpu_worker_init(cfg):
     from oracle.pw_basis_ref import PWBasisKRef
     spec_s = importlib.util.spec_from_file_location("_bench_synth", ROOT / "abacus-develop_b200" / "synth.py")
     synth = importlib.util.module_from_spec(spec_s)
+    sys.modules["_bench_synth"] = synth  # dataclasses look their module up there
     spec_s.loader.exec_module(synth)
     H.FFT_WORKERS = 1
     spec = synth.config(cfg)
@@ -235,11 +236,19 @@ class CpuArm:
     """The oracle's H|psi> of the 64-atom cell on `procs` host processes (spawned, so that a pool started
     after GPU work is safe).  step(nb) applies H to nb bands, split evenly over the processes."""
 
+    TIMEOUT_S = 600  # a step that takes longer than this means a broken pool: fail instead of waiting
+
     def __init__(self, procs, cfg=1):
         import multiprocessing as mp
         self.procs = procs
+        # maxtasksperchild=None and a bounded wait: a worker whose set-up fails would otherwise be respawned
+        # forever while the parent waits
         self.pool = mp.get_context("spawn").Pool(procs, initializer=_cpu_worker_init, initargs=(cfg,))
-        self.pool.starmap(_cpu_worker_hpsi, [(0, 1)] * procs)  # every process set up and warm
+        try:
+            self.pool.starmap_async(_cpu_worker_hpsi, [(0, 1)] * procs).get(self.TIMEOUT_S)  # all set up and warm
+        except BaseException:
+            self.pool.terminate()
+            raise
 
     def step(self, nb):
         share = [nb // self.procs + (1 if i < nb % self.procs else 0) for i in range(self.procs)]
@@ -249,11 +258,11 @@ class CpuArm:
                 tasks.append((b0, n))
                 b0 += n
         t0 = time.perf_counter()
-        done = sum(self.pool.starmap(_cpu_worker_hpsi, tasks))
+        done = sum(self.pool.starmap_async(_cpu_worker_hpsi, tasks).get(self.TIMEOUT_S))
         return done, time.perf_counter() - t0
 
     def close(self):
-        self.pool.close()
+        self.pool.terminate()
         self.pool.join()
 
 

@@ -202,10 +202,17 @@ int b200_graph_capture_hpsi_kbatch(b200_hamilt* h, int nk, const int* iks, int s
 int b200_graph_launch(b200_graph* g, void* stream);
 int b200_graph_destroy(b200_graph* g);
 /* Times the kinetic + local pass of k-point ik over candidate band-chunk sizes (1, 2, 4 ... 128 and
- * nbands; three timed repetitions each after one warm-up) and keeps the fastest for this handle.
- * Overwrites hpsi_d.  No counterpart in the reference. */
+ * nbands) and, on grids with square planes of 64, 96 or 128 points, over the plane-pass variants
+ * (three timed repetitions each after one warm-up), and keeps the fastest pair: the chunk for this
+ * handle, the plane variant for every handle of this basis in the handle's precision.  Overwrites
+ * hpsi_d.  best_chunk / best_variant may be NULL.  No counterpart in the reference. */
 int b200_hamilt_autotune(b200_hamilt* h, int ik, int nbands, int ld, const void* psi_d, void* hpsi_d, void* stream,
-                         int* best_chunk);
+                         int* best_chunk, int* best_variant);
+/* Plane pass of the local H|psi> on grids with square planes of 64, 96 or 128 points, for every
+ * handle of this basis in this handle's precision: 1 = one warp per line, five warp-shuffle lane
+ * stages; 2-5 = two-pass register transforms through shared memory (four launch shapes); 0 = the
+ * default.  All variants give the same results within rounding.  No counterpart in the reference. */
+int b200_hamilt_set_plane_variant(b200_hamilt* h, int variant);
 
 /* ---- psi -> rho (ElecStatePW::psiToRho, module_elecstate/elecstate_pw.cpp:78-216) ---- */
 /* elecstate::elecstate_pw_op<FP, DEVICE_GPU> (module_elecstate/kernels/elecstate_op.h):
@@ -284,6 +291,12 @@ int b200_tc_cgemm_error(int* code);
  * cuBLAS calls have no bounded waits: a test sets a limit that cannot be met and checks that
  * b200_tc_cgemm_error reports it and that the next GEMM with the default limit is correct. */
 int b200_tc_set_wait_limit_ns(unsigned long long ns);
+
+/* Measured arithmetic peaks of the current device in TFLOP/s (CUDA events on the legacy default
+ * stream; one warm-up launch each): FP64 and FP32 fused multiply-add chains on the CUDA cores, and
+ * FP64 tensor-core MMAs (mma.sync m8n8k4 f64).  The compute denominators of the rooflines.  No
+ * counterpart in the reference. */
+int b200_measure_peaks(double* fp64_tflops, double* fp32_tflops, double* dmma_tflops);
 
 /* ---- FP64 BLAS functors of the Davidson / nonlocal path (module_hsolver/kernels/math_kernel_op.h) ----
  * gemm_op<std::complex<double>, DEVICE_GPU> (math_kernel_op.h:240-265, cuda/math_kernel_op.cu:815-874):

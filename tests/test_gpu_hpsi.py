@@ -204,3 +204,27 @@ def test_headline_cells_match_oracle(pkg, cfg):
             assert rel(hd.cpu().numpy().astype(np.complex128), href) < 2e-5
         del h
         torch.cuda.empty_cache()
+
+
+@pytest.mark.parametrize("n", [64, 96, 128])
+@pytest.mark.parametrize("variant", [1, 2, 3, 4, 5])
+def test_plane_variants_match_oracle(pkg, n, variant):
+    """Every plane-pass variant of the register transforms (1: warp-shuffle lane stages; 2-5: two-pass
+    transforms through shared memory in four launch shapes) gives the oracle's local H|psi> (kinetic +
+    V_eff) on square planes of 64, 96 and 128 points, at k != 0: FP64 within 1e-12, mixed within 2e-5."""
+    import dataclasses
+    spec = dataclasses.replace(pkg.synth.config(0), grid=(n, n, n))
+    wl, ref, psi, nb, ld = _setup(pkg, spec, np.array([0.25, -0.125, 0.375]), 6)
+    href = ref.hpsi_local(psi, nb, ld)
+    P = pkg.pwdft
+    for prec in (P.PREC_FP64, P.PREC_MIXED):
+        h = P.device_hamilt(wl, prec)
+        h.set_plane_variant(variant)
+        ct = torch.complex128 if prec == P.PREC_FP64 else torch.complex64
+        pd = torch.from_numpy(psi).to(ct).cuda()
+        hd = torch.full_like(pd, complex(7.0, -3.0))
+        h.hpsi_part(0, pd, hd, nb, ld, mode=1)
+        torch.cuda.synchronize()
+        err = rel(hd.cpu().numpy().astype(np.complex128), href)
+        assert err < (1e-12 if prec == P.PREC_FP64 else 2e-5), (prec, err)
+        h.set_plane_variant(0)
