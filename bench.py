@@ -189,6 +189,16 @@ def time_steps(fn, steps, stream):
     return e0.elapsed_time(e1) / steps
 
 
+def local_flops_per_band(basis):
+    """Algorithmic flops of the local part of H|psi> per band: two pruned 3-D transforms,
+    2*[5*S*log2(nz) + 5*nx_act*nz*ny*log2(ny) + 5*N*log2(nx)] with S = nst*nz sticks x z and nx_act the
+    occupied x-columns (the reference's own pruning, fft.cpp:583-591)."""
+    import math
+    S = basis.nst * basis.nz
+    return 2.0 * (5 * S * math.log2(basis.nz) + 5 * basis.nxc * basis.nz * basis.ny * math.log2(basis.ny)
+                  + 5 * basis.nxyz * math.log2(basis.nx))
+
+
 def local_bytes_per_band(basis, b, r):
     """Algorithmic HBM bytes of the local part of H|psi> per band:
     b*(3*npw + 4*nst*nz) + r*N (psi read, hpsi write + psi re-read for the kinetic term,
@@ -384,10 +394,16 @@ def run_ours(args, ws, rank, local):
     ms_e2e = max_over_ranks(time_steps(e2e_step, args.steps, stream), ws)
 
     hbm_peak, _, peak_kind = peaks()
+    fp_peaks = P.measure_peaks()
     b_local64 = local_bytes_per_band(basis, 16, 8) * nb
     b_local32 = local_bytes_per_band(basis, 8, 4) * nb
+    f_local = local_flops_per_band(basis) * nb
     ach64 = b_local64 / (ms_loc64 * 1e-3) / 1e9
     ach32 = b_local32 / (ms_loc32 * 1e-3) / 1e9
+    # the roofline time of the pass: the slower of its bytes at the HBM peak and its flops at the CUDA-core
+    # peak of its precision (both measured); frac = that time / the measured time
+    t_roof64 = max(b_local64 / (hbm_peak * 1e9), f_local / (fp_peaks["fp64_tflops"] * 1e12))
+    t_roof32 = max(b_local32 / (hbm_peak * 1e9), f_local / (fp_peaks["fp32_tflops"] * 1e12))
     nkb = wl.nkb
     nl_flops = 16.0 * npw * nkb * nb
 
@@ -408,15 +424,18 @@ def run_ours(args, ws, rank, local):
                    "l2": "inputs larger than L2 (psi+hpsi+projectors ~690 MB), no flush"},
         "mixed": {"value": ws * nb / (ms32 * 1e-3), "unit": "bands/s", "ms_per_step": ms32,
                   "dtype": "f32 FFT + f32 projector GEMM"},
-        "roofline": {"kernel": "fused local H|psi> FP64 (k_zinv_r + k_plane_p + k_zfwd_r, 9 band chunks)",
+        "roofline": {"kernel": "fused local H|psi> FP64 (z pass, plane pass, z pass per band chunk)",
                      "bound": "hbm", "achieved": ach64, "peak": hbm_peak, "unit": "GB/s",
                      "frac": ach64 / hbm_peak, "peak_kind": peak_kind,
                      "traffic": NCU_TRAFFIC_LOCAL_FP64,
-                     "traffic_note": "DRAM bytes of one 160-band local pass (27 launches), ncu without cache flush; "
+                     "traffic_note": "DRAM bytes of one 160-band local pass, ncu without cache flush; "
                                      "achieved and algorithmic_bytes are per the same pass",
-                     "algorithmic_bytes": b_local64, "ms": ms_loc64,
+                     "algorithmic_bytes": b_local64, "algorithmic_flops": f_local, "ms": ms_loc64,
+                     "t_roof_ms": t_roof64 * 1e3, "frac_of_t_roof": t_roof64 / (ms_loc64 * 1e-3),
+                     "compute_peaks_measured": fp_peaks,
                      "mixed": {"achieved": ach32, "frac": ach32 / hbm_peak, "ms": ms_loc32,
-                               "algorithmic_bytes": b_local32}},
+                               "algorithmic_bytes": b_local32, "t_roof_ms": t_roof32 * 1e3,
+                               "frac_of_t_roof": t_roof32 / (ms_loc32 * 1e-3)}},
         "nonlocal": {"flops": nl_flops, "ms_fp64": ms64 - ms_loc64, "tflops_fp64": nl_flops / ((ms64 - ms_loc64) * 1e-3) / 1e12},
         "e2e": {"value": ws * nb / (ms_e2e * 1e-3), "unit": "bands/s",
                 "h2d_bytes_per_step": psi.numel() * 16, "d2h_bytes_per_step": hpsi.numel() * 16},
@@ -426,6 +445,7 @@ def run_ours(args, ws, rank, local):
 
     line["psi_to_rho"] = rho_bench(P, wl, psi, args.steps, stream)
     line["tc_gemm"] = gemm_bench(P)
+    line["fp64_gemm"] = guarded_section(gemm64_bench, pkg, fp_peaks)
     if not args.skip_david:
         line["davidson"] = davidson_bench(P, wl, h64)
         line["dav_subspace"] = dav_subspace_bench(pkg, P, wl, h64, rank == 0 and ws == 1 and not args.skip_cpu)
@@ -960,6 +980,52 @@ def gemm_bench(P, reps=5):
         del a, b, c
         torch.cuda.empty_cache()
     assert P.tc_cgemm_error() == 0
+    return out
+
+
+# FP64 complex GEMM shapes of the plain path: the 64-atom projector products and the 216-atom subspace
+# products (transa, transb, M, N, K)
+GEMM64_SHAPES = [("C", "N", 512, 160, 51627), ("N", "N", 51627, 160, 512), ("N", "N", 124289, 480, 480),
+                 ("C", "N", 480, 1920, 124289)]
+
+
+def gemm64_bench(pkg, peaks_tf, reps=5):
+    """The FP64 complex GEMM the plain path calls (gemm_op<complex<double>, GPU>: cuBLAS ZGEMM through
+    b200_gemm_op_f64) on the shapes above, against the measured FP64 tensor-core peak: a complex product
+    is four real products on the FP64 tensor pipe, so 8 M N K flop at the DMMA rate is its ceiling."""
+    import ctypes as C
+    import torch
+    lib = pkg._lib.load()
+    one = (C.c_double * 2)(1.0, 0.0)
+    zero = (C.c_double * 2)(0.0, 0.0)
+    out = []
+    for ta, tb, M, N, K in GEMM64_SHAPES:
+        rows_a = M if ta == "N" else K
+        cols_a = K if ta == "N" else M
+        a = torch.randn(cols_a, rows_a, dtype=torch.complex128, device="cuda")
+        b = torch.randn(N, K, dtype=torch.complex128, device="cuda")
+        c = torch.zeros(N, M, dtype=torch.complex128, device="cuda")
+
+        def call():
+            rc = lib.b200_gemm_op_f64(ta.encode(), tb.encode(), M, N, K, one, a.data_ptr(), rows_a, b.data_ptr(), K, zero,
+                                      c.data_ptr(), M, None)
+            assert rc == 0
+
+        for _ in range(2):
+            call()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            call()
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        tf = 8.0 * M * N * K / (ms * 1e-3) / 1e12
+        out.append({"op": ta + tb, "M": M, "N": N, "K": K, "ms": ms, "tflops": tf,
+                    "frac_of_dmma_peak": tf / peaks_tf["dmma_fp64_tflops"]})
+        del a, b, c
+        torch.cuda.empty_cache()
     return out
 
 
