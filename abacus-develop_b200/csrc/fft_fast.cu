@@ -765,12 +765,19 @@ bool plane_launch_var(const PWGrid& g, int var, int nb, const R* vperm, T* sb, c
         return true;
     }
     constexpr int R2 = 8, R1 = N / 8;
+    // thread counts that are multiples of R1 and R2 (each thread keeps its twiddles in registers): 24 | NT for
+    // N = 96, 16 | NT for 128, 8 | NT for 64.  An FP64 plane of 128 takes ~146 KB of shared memory (one CTA
+    // per SM) and its 16-point transforms ~230 registers a thread, so its CTAs stay at 256 threads.
+    constexpr bool big64 = f64 && N == 128;
+    constexpr int NTL = N == 96 ? 384 : (big64 ? 256 : 512);  // large CTA, one per SM
+    constexpr int NTS = N == 96 ? 192 : 256;                   // small CTA, two (FP32: more) per SM
     constexpr int M2 = f64 ? 1 : 2;  // FP32 planes take half the shared memory: twice the CTAs per SM
+    constexpr int MS = big64 ? 1 : 2 * M2;
     switch (var) {
-        case 3: return plane_launch_t<T, R, N, R1, R2, 256, 32, 1 * M2>(g, nb, vt, sb, s);
-        case 4: return plane_launch_t<T, R, N, R1, R2, 384, 32, 1>(g, nb, vt, sb, s);
-        case 5: return plane_launch_t<T, R, N, R1, R2, 256, 16, 2>(g, nb, vt, sb, s);
-        default: return plane_launch_t<T, R, N, R1, R2, 192, 16, 2 * M2>(g, nb, vt, sb, s);
+        case 3: return plane_launch_t<T, R, N, R1, R2, NTL, 32, 1>(g, nb, vt, sb, s);
+        case 4: return plane_launch_t<T, R, N, R1, R2, NTS, 32, big64 ? 1 : M2>(g, nb, vt, sb, s);
+        case 5: return plane_launch_t<T, R, N, R1, R2, NTL, 16, 1>(g, nb, vt, sb, s);
+        default: return plane_launch_t<T, R, N, R1, R2, NTS, 16, MS>(g, nb, vt, sb, s);
     }
 }
 
@@ -836,8 +843,9 @@ void zpass_r(bool inv, const PWGrid& g, const Src& src, int nk, int b0, int nbc,
              cudaStream_t s) {
     const int var = std::is_same<T, double2>::value ? g.plane_variant64 : g.plane_variant32;
     if (var != 1) {
-        // two-pass register transforms: 32 sticks per CTA, 4 warps
-        constexpr int R2 = 8, R1 = NZ / 8, TS = 32, NT = 128;
+        // two-pass register transforms: 32 sticks per CTA; 12 warps (nz = 96: a multiple of R1 = 12 and R2 = 8,
+        // so each thread keeps its twiddles) or 8
+        constexpr int R2 = 8, R1 = NZ / 8, TS = 32, NT = NZ == 96 ? 384 : 256;
         const dim3 grid(ceil_div(g.nst, TS), nbc, nk);
         constexpr size_t smem = plane_t::zpass_smem_bytes<T>(R1, R2, TS);
         if (inv) {

@@ -146,6 +146,32 @@ __global__ void k_arrange_veff(int nz, int n, int r1, int r2, const R* __restric
     }
 }
 
+// The twiddles W_N^(t*k1) of one thread: with NT a multiple of R1 and R2, a thread keeps the same t in every
+// pass-A item and the same k1 in every pass-B item, so it loads its R1-1 (pass A) and R2-1 (pass B) twiddles
+// once; otherwise they are read per item from the (L1-resident) root table.
+template <typename T, int N, int R1, int R2, int NT> struct Twiddles {
+    static constexpr bool kFixed = NT % R1 == 0 && NT % R2 == 0;
+    T a[kFixed ? R1 : 1], b[kFixed ? R2 : 1];
+    __device__ __forceinline__ void load(const T* __restrict__ roots, int tid) {
+        if constexpr (kFixed) {
+            const int t = tid % R2, k1 = tid % R1;
+#pragma unroll
+            for (int j = 1; j < R1; ++j) a[j] = __ldg(roots + (t * j) % N);
+#pragma unroll
+            for (int j = 1; j < R2; ++j) b[j] = __ldg(roots + (j * k1) % N);
+        }
+    }
+    // W_N^(t*j) for pass A (thread's t, j = k1) and pass B (j = t, thread's k1)
+    __device__ __forceinline__ T wa(const T* __restrict__ roots, int t, int j) const {
+        if constexpr (kFixed) return a[j];
+        else return __ldg(roots + (t * j) % N);
+    }
+    __device__ __forceinline__ T wb(const T* __restrict__ roots, int k1, int j) const {
+        if constexpr (kFixed) return b[j];
+        else return __ldg(roots + (j * k1) % N);
+    }
+};
+
 // One CTA per (band, z slot): inverse y and x transforms, x V_eff(r), forward x and y transforms.
 template <typename T, typename R, int N, int R1, int R2, int NT, int RB, int MINB>
 __global__ void __launch_bounds__(NT, MINB) k_plane_t(PlaneMapView pm, int nz, const T* __restrict__ roots,
@@ -161,6 +187,8 @@ __global__ void __launch_bounds__(NT, MINB) k_plane_t(PlaneMapView pm, int nz, c
     const int tid = threadIdx.x;
     const int band = blockIdx.x, zs = blockIdx.y;
     const T zero = cmake<T>(0, 0);
+    Twiddles<T, N, R1, R2, NT> tw;
+    tw.load(roots, tid);
 
     for (int i = tid; i < nxc * LDC; i += NT) A[i] = zero;
     for (int i = tid; i < N; i += NT) cmap[i] = -1;
@@ -179,7 +207,7 @@ __global__ void __launch_bounds__(NT, MINB) k_plane_t(PlaneMapView pm, int nz, c
         for (int n1 = 0; n1 < R1; ++n1) u[n1] = col[n1 * RS];
         dft<T, +1, R1>(u);
 #pragma unroll
-        for (int k1 = 1; k1 < R1; ++k1) u[k1] = cmulc(u[k1], __ldg(roots + (t * k1) % N));
+        for (int k1 = 1; k1 < R1; ++k1) u[k1] = cmulc(u[k1], tw.wa(roots, t, k1));
 #pragma unroll
         for (int k1 = 0; k1 < R1; ++k1) col[k1 * RS] = u[k1];
     }
@@ -210,7 +238,7 @@ __global__ void __launch_bounds__(NT, MINB) k_plane_t(PlaneMapView pm, int nz, c
             }
             dft<T, +1, R1>(u);
 #pragma unroll
-            for (int k1 = 1; k1 < R1; ++k1) u[k1] = cmulc(u[k1], __ldg(roots + (t * k1) % N));
+            for (int k1 = 1; k1 < R1; ++k1) u[k1] = cmulc(u[k1], tw.wa(roots, t, k1));
             T* b = buf + r * R1 * RS + t;
 #pragma unroll
             for (int k1 = 0; k1 < R1; ++k1) b[k1 * RS] = u[k1];
@@ -218,17 +246,21 @@ __global__ void __launch_bounds__(NT, MINB) k_plane_t(PlaneMapView pm, int nz, c
         __syncthreads();
         for (int i = tid; i < RB * R1; i += NT) {
             const int r = i / R1, k1 = i % R1;
+            // V_eff of the item first: its loads are in flight during the inverse transform
+            const R* vv = vz + (size_t(p0 + r) * R1 + k1) * R2;
+            R vr[R2];
+#pragma unroll
+            for (int k2 = 0; k2 < R2; ++k2) vr[k2] = __ldg(vv + k2);
             T* b = buf + (r * R1 + k1) * RS;
             T v[R2];
 #pragma unroll
             for (int t = 0; t < R2; ++t) v[t] = b[t];
             dft<T, +1, R2>(v);
-            const R* vv = vz + (size_t(p0 + r) * R1 + k1) * R2;
 #pragma unroll
-            for (int k2 = 0; k2 < R2; ++k2) v[k2] = cscale(v[k2], __ldg(vv + k2));
+            for (int k2 = 0; k2 < R2; ++k2) v[k2] = cscale(v[k2], vr[k2]);
             dft<T, -1, R2>(v);
 #pragma unroll
-            for (int t = 1; t < R2; ++t) v[t] = cmul(v[t], __ldg(roots + (t * k1) % N));
+            for (int t = 1; t < R2; ++t) v[t] = cmul(v[t], tw.wb(roots, k1, t));
 #pragma unroll
             for (int t = 0; t < R2; ++t) b[t] = v[t];
         }
@@ -259,7 +291,7 @@ __global__ void __launch_bounds__(NT, MINB) k_plane_t(PlaneMapView pm, int nz, c
         for (int k2 = 0; k2 < R2; ++k2) v[k2] = blk[k2];
         dft<T, -1, R2>(v);
 #pragma unroll
-        for (int t = 1; t < R2; ++t) v[t] = cmul(v[t], __ldg(roots + (t * k1) % N));
+        for (int t = 1; t < R2; ++t) v[t] = cmul(v[t], tw.wb(roots, k1, t));
 #pragma unroll
         for (int t = 0; t < R2; ++t) blk[t] = v[t];
     }
@@ -307,6 +339,8 @@ __global__ void __launch_bounds__(NT) k_zinv_t(Src src, int b0, int nbc, const T
     const int ns = min(TS, sm.nst - s0);
     const int band = blockIdx.y;
     const T zero = cmake<T>(0, 0);
+    Twiddles<T, NZ, R1, R2, NT> tw;
+    tw.load(roots, tid);
     for (int i = tid; i < ns * LDZ; i += NT) A[i] = zero;
     __syncthreads();
     const T* p = reinterpret_cast<const T*>(e.psi) + size_t(b0 + band) * e.ld;
@@ -324,7 +358,7 @@ __global__ void __launch_bounds__(NT) k_zinv_t(Src src, int b0, int nbc, const T
         for (int n1 = 0; n1 < R1; ++n1) u[n1] = st[n1 * RS];
         dft<T, +1, R1>(u);
 #pragma unroll
-        for (int k1 = 1; k1 < R1; ++k1) u[k1] = cmulc(u[k1], __ldg(roots + (t * k1) % NZ));
+        for (int k1 = 1; k1 < R1; ++k1) u[k1] = cmulc(u[k1], tw.wa(roots, t, k1));
 #pragma unroll
         for (int k1 = 0; k1 < R1; ++k1) st[k1 * RS] = u[k1];
     }
@@ -362,6 +396,8 @@ __global__ void __launch_bounds__(NT) k_zfwd_t(Src src, int b0, int nbc, const T
     if (s0 >= sm.nst) return;
     const int ns = min(TS, sm.nst - s0);
     const int band = blockIdx.y;
+    Twiddles<T, NZ, R1, R2, NT> tw;
+    tw.load(roots, tid);
     const T* in = sb + (size_t(blockIdx.z) * nbc + band) * NZ * sm.nst;
     for (int i = tid; i < ns * NZ; i += NT) {
         const int sz = i / ns;
@@ -377,7 +413,7 @@ __global__ void __launch_bounds__(NT) k_zfwd_t(Src src, int b0, int nbc, const T
         for (int k2 = 0; k2 < R2; ++k2) v[k2] = blk[k2];
         dft<T, -1, R2>(v);
 #pragma unroll
-        for (int t = 1; t < R2; ++t) v[t] = cmul(v[t], __ldg(roots + (t * k1) % NZ));
+        for (int t = 1; t < R2; ++t) v[t] = cmul(v[t], tw.wb(roots, k1, t));
 #pragma unroll
         for (int t = 0; t < R2; ++t) blk[t] = v[t];
     }

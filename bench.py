@@ -353,6 +353,9 @@ def run_ours(args, ws, rank, local):
     psi32 = psi.to(torch.complex64)
     hpsi32 = torch.zeros_like(psi32)
 
+    # set-up: the autotuner picks the band chunk and the plane-pass variant of each precision on this workload
+    tuned64 = h64.autotune(0, psi, hpsi, nb, ld, with_variant=True)
+    tuned32 = h32.autotune(0, psi32, hpsi32, nb, ld, with_variant=True)
     step64 = lambda: h64.hpsi(0, psi, hpsi, nb, ld)  # noqa: E731
     step32 = lambda: h32.hpsi(0, psi32, hpsi32, nb, ld)  # noqa: E731
     local64 = lambda: h64.hpsi_part(0, psi, hpsi, nb, ld, 1)  # noqa: E731
@@ -421,7 +424,8 @@ def run_ours(args, ws, rank, local):
         "dtype": "f64",
         "data": "synthetic",
         "config": {"workload": WORKLOAD_NAME, "parallelism": f"replicas{ws}",
-                   "l2": "inputs larger than L2 (psi+hpsi+projectors ~690 MB), no flush"},
+                   "l2": "inputs larger than L2 (psi+hpsi+projectors ~690 MB), no flush",
+                   "autotuned_chunk_variant": {"fp64": list(tuned64), "mixed": list(tuned32)}},
         "mixed": {"value": ws * nb / (ms32 * 1e-3), "unit": "bands/s", "ms_per_step": ms32,
                   "dtype": "f32 FFT + f32 projector GEMM"},
         "roofline": {"kernel": "fused local H|psi> FP64 (z pass, plane pass, z pass per band chunk)",
