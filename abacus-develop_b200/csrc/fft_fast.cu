@@ -781,9 +781,18 @@ bool plane_launch_var(const PWGrid& g, int var, int nb, const R* vperm, T* sb, c
     }
 }
 
+// the default plane variant of a precision and plane size, from CUDA-event timings of the local pass on B200
+// (64-atom cell at 96^2, 216-atom cell at 128^2, band chunks of 18 and 160): FP64 the two-pass transforms
+// (96: 2.14 ms against 2.22 for the warp-shuffle pass per 160 bands; 128: 3.21 against 3.57 per 96 bands);
+// FP32 the warp-shuffle pass (1.12 against 1.19 ms; 1.57 against 1.64 ms)
+template <typename T> constexpr int default_plane_variant(int n) {
+    return std::is_same<T, double2>::value ? (n == 128 ? 4 : 2) : 1;
+}
+
 template <typename T, typename R, int N>
 bool plane_launch_r(const PWGrid& g, int nb, const R* vperm, T* sb, cudaStream_t s) {
-    const int var = std::is_same<T, double2>::value ? g.plane_variant64 : g.plane_variant32;
+    int var = std::is_same<T, double2>::value ? g.plane_variant64 : g.plane_variant32;
+    if (var == 0) var = default_plane_variant<T>(N);
     if (plane_launch_var<T, R, N>(g, var, nb, vperm, sb, s)) return true;
     return var != 1 && plane_launch_var<T, R, N>(g, 1, nb, vperm, sb, s);  // shapes whose plane does not fit
 }
@@ -841,7 +850,8 @@ bool zbatch_dispatch(bool inv, const PWGrid& g, const KBatchArgs& args, int nk, 
 template <typename T, typename R, int NZ, typename Src>
 void zpass_r(bool inv, const PWGrid& g, const Src& src, int nk, int b0, int nbc, T* sb, double tpiba2, int accumulate,
              cudaStream_t s) {
-    const int var = std::is_same<T, double2>::value ? g.plane_variant64 : g.plane_variant32;
+    int var = std::is_same<T, double2>::value ? g.plane_variant64 : g.plane_variant32;
+    if (var == 0) var = default_plane_variant<T>(g.nx);
     if (var != 1) {
         // two-pass register transforms: 32 sticks per CTA; 12 warps (nz = 96: a multiple of R1 = 12 and R2 = 8,
         // so each thread keeps its twiddles) or 8

@@ -154,6 +154,14 @@ int b200_hamilt_autotune(b200_hamilt* h, int ik, int nbands, int ld, const void*
     });
 }
 
+int b200_hamilt_set_band_chunk(b200_hamilt* h, int chunk) {
+    return guarded([&] {
+        B200_CHECK(h != nullptr, b200::kInvalidArgument, "NULL argument");
+        B200_CHECK(chunk >= 0, b200::kInvalidArgument, "band chunk must be >= 0");
+        h->h->chunk_override = chunk;
+    });
+}
+
 int b200_hamilt_set_plane_variant(b200_hamilt* h, int variant) {
     return guarded([&] {
         B200_CHECK(h != nullptr, b200::kInvalidArgument, "NULL argument");

@@ -423,6 +423,10 @@ class HamiltPW:
              C.byref(var))
         return (best.value, var.value) if with_variant else best.value
 
+    def set_chunk(self, chunk):
+        """Bands per stick-buffer chunk of the local pass (0: the 48 MB default rule)."""
+        call("b200_hamilt_set_band_chunk", self._h, int(chunk))
+
     def set_plane_variant(self, variant):
         """Plane pass of the register transforms (1: warp-shuffle lanes; 2-5: two-pass transforms; 0: default)
         for every handle of this basis in this handle's precision."""

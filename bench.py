@@ -354,8 +354,17 @@ def run_ours(args, ws, rank, local):
     hpsi32 = torch.zeros_like(psi32)
 
     # set-up: the autotuner picks the band chunk and the plane-pass variant of each precision on this workload
-    tuned64 = h64.autotune(0, psi, hpsi, nb, ld, with_variant=True)
-    tuned32 = h32.autotune(0, psi32, hpsi32, nb, ld, with_variant=True)
+    # (--tune C64:V64,C32:V32 sets them instead, e.g. to profile exactly what an earlier run chose)
+    if args.tune == "auto":
+        tuned64 = h64.autotune(0, psi, hpsi, nb, ld, with_variant=True)
+        tuned32 = h32.autotune(0, psi32, hpsi32, nb, ld, with_variant=True)
+    else:
+        (c64, v64), (c32, v32) = [tuple(int(x) for x in part.split(":")) for part in args.tune.split(",")]
+        h64.set_chunk(c64)
+        h64.set_plane_variant(v64)
+        h32.set_chunk(c32)
+        h32.set_plane_variant(v32)
+        tuned64, tuned32 = (c64, v64), (c32, v32)
     step64 = lambda: h64.hpsi(0, psi, hpsi, nb, ld)  # noqa: E731
     step32 = lambda: h32.hpsi(0, psi32, hpsi32, nb, ld)  # noqa: E731
     local64 = lambda: h64.hpsi_part(0, psi, hpsi, nb, ld, 1)  # noqa: E731
@@ -1135,6 +1144,8 @@ def main():
     ap.add_argument("--skip-serve", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=10.0)
+    ap.add_argument("--tune", default="auto",
+                    help="'auto' (autotune at set-up) or C64:V64,C32:V32 band chunk and plane variant per precision")
     ap.add_argument("--gemm-only", action="store_true", help="only the tensor-core GEMM shapes (for profiling)")
     ap.add_argument("--solvers-only", action="store_true",
                     help="only the Diago_DavSubspace and DiagoBPCG sections on the 64-atom cell (for profiling)")

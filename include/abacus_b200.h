@@ -213,6 +213,9 @@ int b200_hamilt_autotune(b200_hamilt* h, int ik, int nbands, int ld, const void*
  * stages; 2-5 = two-pass register transforms through shared memory (four launch shapes); 0 = the
  * default.  All variants give the same results within rounding.  No counterpart in the reference. */
 int b200_hamilt_set_plane_variant(b200_hamilt* h, int variant);
+/* Bands per stick-buffer chunk of this handle's local pass (0 = the default: the largest chunk whose
+ * stick buffer stays within 48 MB).  What b200_hamilt_autotune sets.  No counterpart in the reference. */
+int b200_hamilt_set_band_chunk(b200_hamilt* h, int chunk);
 
 /* ---- psi -> rho (ElecStatePW::psiToRho, module_elecstate/elecstate_pw.cpp:78-216) ---- */
 /* elecstate::elecstate_pw_op<FP, DEVICE_GPU> (module_elecstate/kernels/elecstate_op.h):
