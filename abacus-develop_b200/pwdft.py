@@ -449,6 +449,24 @@ class HamiltPW:
              notconv_max, nworkers, its.ctypes.data_as(_lib.pi32))
         return eig, its
 
+    def solve_kpoints_batched(self, iks, precond_ds, psis, ld_psi, nband, thr, maxiter, david_ndim=4, spin=0,
+                              stream=None):
+        """Davidson of the k-points iks in lock-step (one batched call per phase for all k, FP64).  psis[q]
+        (complex128, nband x ld_psi, ld_psi >= the largest npw of the batch) is overwritten with the
+        eigenvectors.  Returns (eigenvalues nk x nband, iteration after which each k-point had converged)."""
+        nk = len(iks)
+        for p in psis:
+            _check_block(p, True, nband, ld_psi, "psi")
+        ik_a = (C.c_int * nk)(*[int(i) for i in iks])
+        pc_a = (_lib.vp * nk)(*[ptr(p) for p in precond_ds])
+        ps_a = (_lib.vp * nk)(*[ptr(p) for p in psis])
+        eig = np.zeros((nk, nband))
+        its = np.zeros(nk, dtype=np.int32)
+        call("b200_solve_kpoints_batched", self._h, nk, ik_a, spin, nband, david_ndim, C.cast(pc_a, C.POINTER(_lib.vp)),
+             C.cast(ps_a, C.POINTER(_lib.vp)), ld_psi, eig.ctypes.data_as(_lib.pf64), thr, maxiter,
+             its.ctypes.data_as(_lib.pi32), stream_ptr(stream))
+        return eig, its
+
     def __del__(self):
         try:
             if getattr(self, "_h", None):

@@ -57,10 +57,10 @@ METRIC = "H|psi> bands/s (FP64) + Davidson time-to-1e-8 Ry, mixed vs FP64"
 # halves the first and last piece; 32 bands are about two 48 MB band chunks of the local pass); 4, 5, 7, 8,
 # 9 or 11 pieces measured 9-25 % slower on B200
 E2E_PIECES = 6
-# dram__bytes_read.sum + dram__bytes_write.sum of the fused local H|psi> kernels (27 launches: 9 band
-# chunks x 3 passes) for one 160-band FP64 application, from an ncu capture without cache flush (the
-# local-pass traffic summary under profiles/)
-NCU_TRAFFIC_LOCAL_FP64 = 591453440
+# dram__bytes_read.sum + dram__bytes_write.sum of the fused local H|psi> kernels (3 launches: one band chunk
+# of all 160 bands, the autotuner's choice, x 3 passes) for one 160-band FP64 application, from an ncu
+# capture without cache flush (the local-pass traffic summary under profiles/)
+NCU_TRAFFIC_LOCAL_FP64 = 2029709824
 
 
 def load_package():
