@@ -95,8 +95,8 @@ _SIGS = {
     "b200_hamilt_copy_vkb": ([vp, i32, vp, vp], i32),
     "b200_solve_kpoints": ([vp, i32, pi32, i32, i32, i32, i32, C.POINTER(vp), C.POINTER(vp), i32, pf64, f64, i32,
                             i32, i32, i32, pi32], i32),
-    "b200_solve_kpoints_batched": ([vp, i32, pi32, i32, i32, i32, C.POINTER(vp), C.POINTER(vp), i32, pf64, f64, i32,
-                                    pi32, vp], i32),
+    "b200_solve_kpoints_batched": ([vp, i32, pi32, i32, i32, i32, i32, C.POINTER(vp), C.POINTER(vp), i32, pf64, f64,
+                                    i32, pi32, vp], i32),
     "b200_tc_cgemm": ([C.c_char, C.c_char, i32, i32, i32, f32, f32, vp, i32, vp, i32, f32, f32, vp, i32, vp], i32),
     "b200_tc_cgemm_error": ([pi32], i32),
     "b200_tc_set_wait_limit_ns": ([C.c_ulonglong], i32),

@@ -450,8 +450,9 @@ class HamiltPW:
         return eig, its
 
     def solve_kpoints_batched(self, iks, precond_ds, psis, ld_psi, nband, thr, maxiter, david_ndim=4, spin=0,
-                              stream=None):
-        """Davidson of the k-points iks in lock-step (one batched call per phase for all k, FP64).  psis[q]
+                              precision=PREC_FP64, stream=None):
+        """Davidson of the k-points iks in lock-step (one batched call per phase for all k; FP64, or mixed: an FP32
+        stage to 1e-7 refined in FP64).  psis[q]
         (complex128, nband x ld_psi, ld_psi >= the largest npw of the batch) is overwritten with the
         eigenvectors.  Returns (eigenvalues nk x nband, iteration after which each k-point had converged)."""
         nk = len(iks)
@@ -462,7 +463,8 @@ class HamiltPW:
         ps_a = (_lib.vp * nk)(*[ptr(p) for p in psis])
         eig = np.zeros((nk, nband))
         its = np.zeros(nk, dtype=np.int32)
-        call("b200_solve_kpoints_batched", self._h, nk, ik_a, spin, nband, david_ndim, C.cast(pc_a, C.POINTER(_lib.vp)),
+        call("b200_solve_kpoints_batched", self._h, nk, ik_a, spin, nband, david_ndim, precision,
+             C.cast(pc_a, C.POINTER(_lib.vp)),
              C.cast(ps_a, C.POINTER(_lib.vp)), ld_psi, eig.ctypes.data_as(_lib.pf64), thr, maxiter,
              its.ctypes.data_as(_lib.pi32), stream_ptr(stream))
         return eig, its

@@ -425,10 +425,12 @@ int b200_solve_kpoints(b200_hamilt* h, int nk, const int* iks, int spin, int nba
                        const double* const* precond_d, void* const* psi_d, int ldpsi, double* eigenvalues, double thr,
                        int maxiter, int ntry_max, int notconv_max, int nworkers, int* iters);
 /* The same Davidson for nk k-points of one pool advanced in lock-step (HSolverPW::solve's k loop,
- * hsolver_pw.cpp:240-270, around DiagoDavid, diago_david.cpp:151-341), FP64: every phase of an
- * iteration is one batched call for all k (H|psi> of every k's new vectors through one local pass
- * per FFT pass, strided-batched subspace products, batched Cholesky-QR, one batched subspace
+ * hsolver_pw.cpp:240-270, around DiagoDavid, diago_david.cpp:151-341): every phase of an iteration
+ * is one batched call for all k (H|psi> of every k's new vectors through one local pass per FFT
+ * pass, strided-batched subspace products, batched FP64 Cholesky-QR, one batched FP64 subspace
  * eigensolver call) and the convergence test runs on the device (one small read per iteration).
+ * precision: B200_PREC_FP64, or B200_PREC_MIXED (an FP32 stage to 1e-7, then the FP64 iteration
+ * from its vectors).
  * k-points with fewer unconverged bands pad their new block with zero columns kept out of the
  * subspace problem; all k-points restart together when the common basis would exceed
  * david_ndim*nband.  precond_d / psi_d: host arrays of nk device pointers; psi_d[q] holds nband
@@ -436,8 +438,8 @@ int b200_solve_kpoints(b200_hamilt* h, int nk, const int* iks, int spin, int nba
  * eigenvalues: host nk x nband; iters: host nk, the iteration after which each k-point had
  * converged (may be NULL).  1 <= nk <= 128.  Runs on stream (NULL = legacy default). */
 int b200_solve_kpoints_batched(b200_hamilt* h, int nk, const int* iks, int spin, int nband, int david_ndim,
-                               const double* const* precond_d, void* const* psi_d, int ldpsi, double* eigenvalues,
-                               double thr, int maxiter, int* iters, void* stream);
+                               int precision, const double* const* precond_d, void* const* psi_d, int ldpsi,
+                               double* eigenvalues, double thr, int maxiter, int* iters, void* stream);
 
 /* ---- serving: non-self-consistent band solves with continuous admission (no counterpart in the
  * reference, whose NSCF driver solves its k-points one after another, hsolver_pw.cpp:212-299) ----

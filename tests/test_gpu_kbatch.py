@@ -184,10 +184,12 @@ def test_concurrent_solves_equal_alone(pkg, mp444, prec):
         assert np.max(np.linalg.norm(HX - eig[q][:, None] * X, axis=1)) < 1e-3
 
 
-def test_batched_solve_equals_per_k_and_oracle(pkg, mp444):
-    """The lock-step batched Davidson of 8 k-points (uneven npw) gives each k-point's eigenvalues of its own
-    solve within 1e-8 Ry, and, at two k-points, the dense spectrum of the oracle's Hamiltonian within 1e-8 Ry;
-    the returned vectors are orthonormal eigenvectors (small residuals)."""
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_batched_solve_equals_per_k_and_oracle(pkg, mp444, prec):
+    """The lock-step batched Davidson of 8 k-points (uneven npw), FP64 and mixed (FP32 stage + FP64 refinement),
+    gives each k-point's eigenvalues of its own FP64 solve within 1e-8 Ry, and, at two k-points, the dense
+    spectrum of the oracle's Hamiltonian within 1e-8 Ry; the returned vectors are orthonormal eigenvectors (small
+    residuals)."""
     spec, wl = mp444
     P = pkg.pwdft
     h = P.device_hamilt(wl, P.PREC_FP64)
@@ -195,7 +197,8 @@ def test_batched_solve_equals_per_k_and_oracle(pkg, mp444):
     iks = list(range(wl.basis.nks))
     pcs = [P.precondition_d(wl.basis, ik) for ik in iks]
     psis = [torch.from_numpy(wl.psi0_h[ik].reshape(-1).copy()).cuda() for ik in iks]
-    eig, its = h.solve_kpoints_batched(iks, pcs, psis, ld, nband, 1e-10, 200)
+    p = P.PREC_FP64 if prec == "fp64" else P.PREC_MIXED
+    eig, its = h.solve_kpoints_batched(iks, pcs, psis, ld, nband, 1e-10, 200, precision=p)
     assert np.all(its > 0)
     for q, ik in enumerate(iks):
         npw = int(wl.basis.npwk[ik])
