@@ -6,6 +6,7 @@
 #include "bpcg.h"
 #include "dav_subspace.h"
 #include "david.h"
+#include "david_batch.h"
 #include "hamilt.h"
 #include "pw_grid.h"
 
@@ -30,9 +31,18 @@ struct HostPipe {
         if (down) cudaStreamDestroy(down);
     }
 };
+// the lock-step k-point solver of b200_solve_kpoints_batched, kept with the handle between calls of the same
+// shape (k-point capacity, bands, subspace, plane-wave capacity, precision, stream) so repeated solves allocate
+// nothing
+struct KBatchSolverCache {
+    std::unique_ptr<b200::DavidBatchSolver, void (*)(b200::DavidBatchSolver*)> solver{nullptr, nullptr};
+    int cap = 0, nband = 0, ndim = 0, dim_cap = 0, precision = -1;
+    cudaStream_t stream = nullptr;
+};
 struct b200_hamilt {
     std::unique_ptr<b200::Hamilt> h;
     std::unique_ptr<HostPipe> pipe;
+    KBatchSolverCache kbatch;
 };
 struct b200_david {
     std::unique_ptr<b200::DavidBase> d;

@@ -696,7 +696,18 @@ extern "C" int b200_solve_kpoints_batched(b200_hamilt* h, int nk, const int* iks
                        "k-point index out of range");
             dim_cap = std::max(dim_cap, h->h->grid->kmaps[iks[q]].npw);
         }
-        b200::DavidBatchSolver d(h->h.get(), nk, nband, david_ndim, dim_cap, precision, s);
-        d.solve(nk, iks, spin, precond_d, psi_d, ldpsi, eigenvalues, thr, maxiter, iters);
+        KBatchSolverCache& c = h->kbatch;
+        if (!c.solver || c.cap < nk || c.nband != nband || c.ndim != david_ndim || c.dim_cap < dim_cap ||
+            c.precision != precision || c.stream != s) {
+            c.solver.reset();  // the old solver's buffers go before the new ones are made
+            c.solver = b200::make_david_batch(h->h.get(), nk, nband, david_ndim, dim_cap, precision, s);
+            c.cap = nk;
+            c.nband = nband;
+            c.ndim = david_ndim;
+            c.dim_cap = dim_cap;
+            c.precision = precision;
+            c.stream = s;
+        }
+        b200::david_batch_solve(*c.solver, nk, iks, spin, precond_d, psi_d, ldpsi, eigenvalues, thr, maxiter, iters);
     });
 }
