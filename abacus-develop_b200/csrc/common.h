@@ -19,6 +19,7 @@ enum Status : int {
     kCapacityError = 6,
     kNotConverged = 7,
     kCallbackError = 8,
+    kShed = 9,
 };
 
 // A failure raised inside the library; the C-ABI turns it into a status code

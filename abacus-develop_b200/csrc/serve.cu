@@ -147,6 +147,7 @@ class Server {
         }
         std::lock_guard<std::mutex> lk(mu_);
         cells_.push_back(c);
+        svc_mean_.push_back(0.0);
         return int(cells_.size()) - 1;
     }
 
@@ -216,6 +217,18 @@ class Server {
         cv_done_.wait(lk, [&] { return queue_.empty() && inflight_ == 0; });
     }
 
+    void set_policy(int policy, double shed_factor) {
+        B200_CHECK(policy == 0 || policy == 1, kInvalidArgument, "policy must be 0 (oldest first) or 1 (response ratio)");
+        B200_CHECK(shed_factor >= 0, kInvalidArgument, "shed_factor must be >= 0");
+        std::lock_guard<std::mutex> lk(mu_);
+        policy_ = policy;
+        shed_factor_ = shed_factor;
+    }
+    long long shed_count() {
+        std::lock_guard<std::mutex> lk(mu_);
+        return shed_count_;
+    }
+
     void stats(double* out) {
         std::lock_guard<std::mutex> lk(mu_);
         out[0] = double(pool_bytes_);
@@ -250,17 +263,49 @@ class Server {
         return b;
     }
 
-    // the oldest queued request whose cell is below its cap and whose slot can be had; for each cell only
-    // its oldest request is considered (first come, first served within a cell)
+    // The next request to run.  For each cell only its oldest queued request is considered (first come, first
+    // served within a cell); among those whose cell is below its cap and whose slot can be had: policy 0 the
+    // oldest, policy 1 the highest response ratio (wait + S_c) / S_c (S_c: running mean service time of the
+    // cell; a cell not yet timed counts as the shortest).  With shedding on, requests that waited past
+    // shed_factor * S_c are completed as shed first.
     std::deque<Request*>::iterator next_admissible_locked() {
+        const double now = now_s(t0_);
+        if (shed_factor_ > 0) {
+            bool shed = false;
+            for (auto it = queue_.begin(); it != queue_.end();) {
+                Request* r = *it;
+                const double sc = svc_mean_[r->cell];
+                if (sc > 0 && now - r->t_submit > shed_factor_ * sc) {
+                    r->status = kShed;
+                    r->err = "waited past the cell's admission bound";
+                    r->t_admit = r->t_done = now;
+                    done_.push_back(r);
+                    ++shed_count_;
+                    it = queue_.erase(it);
+                    shed = true;
+                } else {
+                    ++it;
+                }
+            }
+            if (shed) cv_done_.notify_all();
+        }
         std::vector<char> seen(cells_.size(), 0);
+        auto best = queue_.end();
+        double best_key = -1e300;
         for (auto it = queue_.begin(); it != queue_.end(); ++it) {
             const int c = (*it)->cell;
             if (seen[c]) continue;
             seen[c] = 1;
-            if (cells_[c].inflight < cells_[c].max_inflight && can_admit_locked(**it)) return it;
+            if (!(cells_[c].inflight < cells_[c].max_inflight && can_admit_locked(**it))) continue;
+            if (policy_ == 0) return it;  // the queue is in arrival order: the first admissible one is the oldest
+            const double sc = svc_mean_[c];
+            const double key = sc > 0 ? (now - (*it)->t_submit + sc) / sc : 1e300;
+            if (key > best_key) {
+                best_key = key;
+                best = it;
+            }
         }
-        return queue_.end();
+        return best;
     }
 
     bool can_admit_locked(const Request& r) const {
@@ -404,6 +449,11 @@ class Server {
             }
             r->t_done = now_s(t0_);
             lk.lock();
+            if (r->status == 0) {  // running mean of the cell's service time (the last 16 requests' weight)
+                double& m = svc_mean_[r->cell];
+                const double svc = r->t_done - r->t_admit;
+                m = m > 0 ? m + (svc - m) / 16.0 : svc;
+            }
             if (slot) {
                 slot->last_used = ++use_clock_;
                 free_.emplace(SlotKey{slot->cell, slot->nbands, slot->precision}, std::move(slot));
@@ -421,6 +471,10 @@ class Server {
 
     size_t budget_;
     int ndim_;
+    int policy_ = 0;
+    double shed_factor_ = 0;
+    long long shed_count_ = 0;
+    std::vector<double> svc_mean_;  // per cell
     int dev_ = 0;
     std::chrono::steady_clock::time_point t0_;
     std::mutex mu_;
@@ -496,6 +550,13 @@ int b200_server_drain(b200_server* s) {
     return guarded([&] {
         B200_CHECK(s != nullptr, b200::kInvalidArgument, "NULL argument");
         s->s->drain();
+    });
+}
+
+int b200_server_set_policy(b200_server* s, int policy, double shed_factor) {
+    return guarded([&] {
+        B200_CHECK(s != nullptr, b200::kInvalidArgument, "NULL argument");
+        s->s->set_policy(policy, shed_factor);
     });
 }
 

@@ -24,6 +24,7 @@ from ._lib import call
 from .pwdft import PREC_FP64, PREC_MIXED, HamiltPW, PWBasisK, _torch  # noqa: F401
 
 STATUS_OK = 0
+STATUS_SHED = 9  # waited past the cell's admission bound (server policy with shedding)
 
 
 @dataclass
@@ -52,6 +53,11 @@ class Server:
         self._cells = []
         self._pending = {}
         self._mu = threading.Lock()
+
+    def set_policy(self, policy: int = 0, shed_factor: float = 0.0):
+        """Admission: policy 0 oldest first, 1 highest response ratio (wait + S_c) / S_c first; shed_factor > 0
+        completes requests that waited past shed_factor * S_c with STATUS_SHED (S_c: the cell's mean service)."""
+        call("b200_server_set_policy", self._h, int(policy), float(shed_factor))
 
     def add_cell(self, hamilt: HamiltPW, max_inflight: int = 2) -> int:
         """Register a resident cell; at most max_inflight of its requests run at once."""
@@ -183,7 +189,8 @@ def summarize(results, cells) -> dict:
         per_cell[cells[c].spec.name] = {
             "n": len(lc), "p50_ms": 1e3 * percentile(lc, 50), "p99_ms": 1e3 * percentile(lc, 99),
             "service_p50_ms": 1e3 * percentile([r.t_done - r.t_admit for r in rc], 50)}
-    return {"n": len(results), "n_ok": len(ok), "throughput_rps": len(ok) / (last - first),
+    shed = sum(1 for r in results if r.status == STATUS_SHED)
+    return {"n": len(results), "n_ok": len(ok), "n_shed": shed, "throughput_rps": len(ok) / (last - first),
             "p50_ms": 1e3 * percentile(lat, 50), "p99_ms": 1e3 * percentile(lat, 99), "per_cell": per_cell}
 
 

@@ -515,8 +515,15 @@ def summary_of(line):
     sv = line.get("serving")
     if isinstance(sv, dict):
         def lat(x):
-            return {"rps": _r(x.get("throughput_rps")), "p50_ms": _r(x.get("p50_ms")), "p99_ms": _r(x.get("p99_ms")),
-                    "p99_over_p50": _r(x.get("p99_ms") / x["p50_ms"]) if x.get("p50_ms") else None}
+            out = {"rps": _r(x.get("throughput_rps")), "p50_ms": _r(x.get("p50_ms")), "p99_ms": _r(x.get("p99_ms")),
+                   "p99_over_p50": _r(x.get("p99_ms") / x["p50_ms"]) if x.get("p50_ms") else None}
+            if x.get("n_shed"):
+                out["shed"] = x["n_shed"]
+            pc = x.get("per_cell") or {}
+            ratios = [c["p99_ms"] / c["p50_ms"] for c in pc.values() if c.get("p50_ms")]
+            if ratios:
+                out["worst_cell_p99_over_p50"] = _r(max(ratios))
+            return out
         out["serving"] = {k: lat(v) for k, v in sv.items() if isinstance(v, dict) and "p50_ms" in v}
     cb = line.get("cpu_baseline")
     if isinstance(cb, dict):
@@ -1140,12 +1147,24 @@ def serving_bench(pkg, npath=8, nreq=200, rate=200.0):
     cap = full["throughput_rps"]
     sustained = S.poisson_load(srv, ids, cells, 0.7 * cap, max(20, int(0.7 * cap * 8)), seed=12)
     sustained.pop("results")
+    # at the measured capacity (offered = capacity): the highest response ratio first, without and with
+    # shedding of requests that waited past their cell's mean service time
+    srv.set_policy(1, 0.0)
+    at_cap_rr = S.poisson_load(srv, ids, cells, cap, max(40, int(cap * 10)), seed=13)
+    at_cap_rr.pop("results")
+    srv.set_policy(1, 1.0)
+    at_cap_shed = S.poisson_load(srv, ids, cells, cap, max(40, int(cap * 10)), seed=13)
+    at_cap_shed.pop("results")
+    srv.set_policy(0, 0.0)
     st = srv.stats()
     srv.close()
-    return {"offered": full, "at_70pct_capacity": sustained, "alone_service_ms": alone,
+    return {"offered": full, "at_70pct_capacity": sustained, "at_capacity_response_ratio": at_cap_rr,
+            "at_capacity_response_ratio_shed1": at_cap_shed, "alone_service_ms": alone,
             "pool": {"peak_bytes": st["peak_pool_bytes"], "peak_in_flight": st["peak_in_flight"],
                      "slots": st["slots_created"], "budget_bytes": 64 << 30},
-            "workers": 8, "workload": "4 resident cells, 8 k-points each, mixed precision, thr 1e-9"}
+            "workers": 8, "workload": "4 resident cells, 8 k-points each, mixed precision, thr 1e-9",
+            "policies": "offered / at_70pct_capacity: oldest first; at_capacity_*: offered = the measured capacity, "
+                        "highest response ratio first, without / with shedding past 1x the cell's mean service"}
 
 
 def main():

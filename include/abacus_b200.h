@@ -31,6 +31,7 @@ extern "C" {
 #define B200_STATUS_CAPACITY_ERROR 6
 #define B200_STATUS_NOT_CONVERGED 7
 #define B200_STATUS_CALLBACK_ERROR 8 /* a user H|psi> callback returned nonzero; the solve was abandoned */
+#define B200_STATUS_SHED 9           /* a served request waited past its cell's admission bound and was not run */
 
 /* precision of a handle: plain FP64, or mixed (FP32 FFTs / split-precision GEMMs) */
 #define B200_PREC_FP64 0
@@ -464,6 +465,13 @@ int b200_server_poll(b200_server* s, int max_out, int wait, long long* ids, int*
                      double* t_admit, double* t_done, int* iters, int* iters_low, int* n_out);
 /* Blocks until every submitted request has completed. */
 int b200_server_drain(b200_server* s);
+/* Admission policy of the server (no counterpart in the reference, which has no serving mode).
+ * policy 0: the oldest admissible request first (first come, first served); 1: highest response ratio
+ * first, (waiting time + S_c) / S_c over the oldest request of each cell c, with S_c a running mean of
+ * the cell's service time (short cells go first, a long wait raises any request).  shed_factor > 0:
+ * a queued request that has waited longer than shed_factor * S_c is completed with B200_STATUS_SHED
+ * instead of being run (bounded latency under overload); 0 never sheds.  Default: 0 and 0. */
+int b200_server_set_policy(b200_server* s, int policy, double shed_factor);
 /* out6: pooled slot bytes, peak pooled bytes, peak requests in flight, slots created, slots evicted,
  * seconds since creation. */
 int b200_server_stats(b200_server* s, double* out6);

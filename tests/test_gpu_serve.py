@@ -82,3 +82,42 @@ def test_budget_too_small_is_rejected(served):
     r = tiny.drain()
     assert len(r) == 1 and r[0].status == 6  # B200_STATUS_CAPACITY_ERROR
     tiny.close()
+
+
+def test_admission_policy_and_shedding(served):
+    """The response-ratio policy serves every request of a burst with the same eigenvalues as first come, first
+    served; with shedding on, requests that waited past the bound come back as STATUS_SHED, the others are
+    served correctly and the server keeps serving afterwards."""
+    S, srv, cells, ids = served
+    c = 1
+    probe = (ids[c], 2, cells[c].nbands)
+    srv.set_policy(0, 0.0)
+    srv.submit(*probe, thr=1e-9)
+    ref = srv.drain()[0]
+    assert ref.status == 0
+    try:
+        srv.set_policy(1, 0.0)
+        for i in range(10):
+            srv.submit(ids[i % 2], i % 4, cells[i % 2].nbands, thr=1e-9, tag=("rr", i))
+        srv.submit(*probe, thr=1e-9, tag="probe")
+        res = srv.drain()
+        assert len(res) == 11 and all(r.status == 0 for r in res)
+        got = [r for r in res if r.tag == "probe"][0]
+        assert np.max(np.abs(got.eig - ref.eig)) <= 1e-10
+        # a bound of 1 % of the mean service time: a burst larger than the workers' slots must shed some
+        srv.set_policy(1, 0.01)
+        for i in range(24):
+            srv.submit(ids[c], i % 4, cells[c].nbands, thr=1e-9, tag=("shed", i))
+        res = srv.drain()
+        assert len(res) == 24
+        st = [r.status for r in res]
+        assert S.STATUS_SHED in st and 0 in st
+        assert set(st) <= {0, S.STATUS_SHED}
+        for r in res:
+            if r.status == 0 and r.tag[1] % 4 == 2:
+                assert np.max(np.abs(r.eig - ref.eig)) <= 1e-10
+    finally:
+        srv.set_policy(0, 0.0)
+    srv.submit(*probe, thr=1e-9)
+    after = srv.drain()
+    assert after[0].status == 0 and np.max(np.abs(after[0].eig - ref.eig)) <= 1e-10
