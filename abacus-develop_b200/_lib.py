@@ -103,6 +103,10 @@ _SIGS = {
     "b200_tc_set_wait_limit_ns": ([C.c_ulonglong], i32),
     "b200_measure_peaks": ([pf64, pf64, pf64], i32),
     "b200_gemm_op_f64": ([C.c_char, C.c_char, i32, i32, i32, pf64, vp, i32, vp, i32, pf64, vp, i32, vp], i32),
+    "b200_zgemm_i8": ([C.c_char, C.c_char, i32, i32, i32, pf64, vp, i32, vp, i32, pf64, vp, i32, i32, vp], i32),
+    "b200_zgemm_i8_error": ([pi32], i32),
+    "b200_hamilt_set_fp64_gemm": ([vp, i32, i32], i32),
+    "b200_zgemm_i8_constants": ([i32, C.c_longlong, pi32, pf64, pf64, pf64, pi32], i32),
     "b200_gemv_op_f64": ([C.c_char, i32, i32, pf64, vp, i32, vp, i32, pf64, vp, i32, vp], i32),
     "b200_dot_real_op_f64": ([i32, vp, vp, i32, pf64, vp], i32),
     "b200_dot_real_op_f32": ([i32, vp, vp, i32, C.POINTER(C.c_float), vp], i32),

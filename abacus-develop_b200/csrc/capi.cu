@@ -13,6 +13,7 @@
 #include "pw_grid.h"
 
 #include "capi_handles.h"
+#include "gemm_oz.h"
 #include "gemm_tc.h"
 
 #include <atomic>
@@ -368,6 +369,41 @@ int b200_tc_cgemm_error(int* code) {
 }
 int b200_tc_set_wait_limit_ns(unsigned long long ns) {
     return guarded([&] { b200::set_tc_wait_limit_ns(ns); });
+}
+static thread_local b200::OzWorkspace g_oz_ws;
+int b200_zgemm_i8(char transa, char transb, int m, int n, int k, const double* alpha, const void* a, int lda,
+                  const void* b, int ldb, const double* beta, void* c, int ldc, int nmods, void* stream) {
+    b200::OzWorkspace& ws = g_oz_ws;
+    return guarded([&] {
+        B200_CHECK(transb == 'N' || transb == 'n', b200::kInvalidArgument, "transb must be 'N'");
+        const char opa = (transa == 'n' || transa == 'N') ? 'N' : ((transa == 'c' || transa == 'C') ? 'C' : '?');
+        B200_CHECK(opa != '?', b200::kInvalidArgument, "transa must be 'N' or 'C'");
+        B200_CHECK(alpha && beta, b200::kInvalidArgument, "NULL alpha or beta");
+        B200_CHECK(m >= 0 && n >= 0 && k >= 0, b200::kInvalidArgument, "negative dimension");
+        if (m == 0 || n == 0) return;
+        B200_CHECK(a && b && c, b200::kInvalidArgument, "NULL matrix");
+        const double2 al = make_double2(alpha[0], alpha[1]), be = make_double2(beta[0], beta[1]);
+        if (k == 0) {  // C = beta C
+            b200::scale_matrix_z(m, n, be, static_cast<double2*>(c), ldc, S(stream));
+            return;
+        }
+        b200::oz_prepare_a(opa, m, k, static_cast<const double2*>(a), lda, nmods, ws.a, ws, S(stream));
+        b200::oz_zgemm(opa, m, n, k, al, ws.a, static_cast<const double2*>(b), ldb, be, static_cast<double2*>(c), ldc,
+                       ws, nullptr, S(stream));
+    });
+}
+int b200_zgemm_i8_error(int* code) {
+    return guarded([&] {
+        B200_CHECK(code != nullptr, b200::kInvalidArgument, "NULL argument");
+        *code = g_oz_ws.read_error(0);
+    });
+}
+int b200_zgemm_i8_constants(int nmods, long long kr, int* mods, double* wa, double* wb, double* mprod, int* q) {
+    return guarded([&] {
+        B200_CHECK(mods && wa && wb && mprod && q, b200::kInvalidArgument, "NULL argument");
+        B200_CHECK(kr >= 1, b200::kInvalidArgument, "kr < 1");
+        b200::oz_constants(nmods, long(kr), mods, wa, wb, mprod, q);
+    });
 }
 int b200_david_set_stream(b200_david* d, void* stream) {
     return guarded([&] {

@@ -34,75 +34,19 @@
 
 #include "common.h"
 #include "gemm_tc.h"
+#include "tcgen05_util.cuh"
 
 namespace b200 {
 namespace {
+
+using namespace tcu;
 
 constexpr int kBM = 128;     // real rows of C per tile
 constexpr int kBK = 32;      // real K per stage (one 128-byte swizzle row of fp32)
 constexpr int kStages = 4;
 constexpr int kAcc = 2;      // K stages accumulated in one TMEM buffer before it is drained
 constexpr int kThreads = 320;   // warp 0 TMA, warp 1 MMA, warps 2-9 split / drain / store
-constexpr unsigned long long kWaitNs = 2000000000ull;  // default bound on any single wait: 2 s
 
-__device__ __forceinline__ unsigned smem_u32(const void* p) {
-    return static_cast<unsigned>(__cvta_generic_to_shared(p));
-}
-__device__ __forceinline__ unsigned long long gtimer() {
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
-__device__ __forceinline__ void mbar_init(unsigned bar, unsigned count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count));
-}
-__device__ __forceinline__ void mbar_expect_tx(unsigned bar, unsigned bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ void mbar_arrive(unsigned bar) {
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
-}
-__device__ __forceinline__ bool mbar_try(unsigned bar, unsigned parity) {
-    unsigned ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(bar), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-// bounded wait: true on success, false after limit_ns
-__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity, unsigned long long limit_ns) {
-    if (mbar_try(bar, parity)) return true;
-    const unsigned long long t0 = gtimer();
-    while (true) {
-        if (mbar_try(bar, parity)) return true;
-        if (gtimer() - t0 > limit_ns) return false;
-    }
-}
-__device__ __forceinline__ void tma_load_2d(unsigned dst, const CUtensorMap* map, int x, int y, unsigned bar) {
-    asm volatile(
-        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(dst),
-        "l"(reinterpret_cast<unsigned long long>(map)), "r"(x), "r"(y), "r"(bar)
-        : "memory");
-}
-__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
-__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
-
-// Shared-memory matrix descriptor (Blackwell version 1).  layout 2 = SWIZZLE_128B (16-byte chunks XOR the
-// row within 8-row / 1024-byte atoms).
-__device__ __forceinline__ unsigned long long sdesc(unsigned addr, unsigned lbo, unsigned sbo, unsigned layout) {
-    unsigned long long d = 0;
-    d |= (unsigned long long)((addr >> 4) & 0x3FFF);
-    d |= (unsigned long long)((lbo >> 4) & 0x3FFF) << 16;
-    d |= (unsigned long long)((sbo >> 4) & 0x3FFF) << 32;
-    d |= 1ull << 46;                       // version
-    d |= (unsigned long long)(layout & 7) << 61;
-    return d;
-}
 // D (TMEM) (+)= A (TMEM: M = 128 rows in lanes 0..127, one column per K element) * B (shared-memory descriptor)
 __device__ __forceinline__ void mma_tf32_ta(unsigned tmem_d, unsigned tmem_a, unsigned long long b, unsigned idesc,
                                             unsigned accumulate) {
@@ -111,9 +55,6 @@ __device__ __forceinline__ void mma_tf32_ta(unsigned tmem_d, unsigned tmem_a, un
         "setp.ne.b32 p, %4, 0;\n\t"
         "tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(tmem_d),
         "r"(tmem_a), "l"(b), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
-}
-__device__ __forceinline__ void mma_commit(unsigned bar) {
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
 }
 __device__ __forceinline__ void tmem_ld16(unsigned taddr, float* v) {
     unsigned r[16];
@@ -496,20 +437,6 @@ __global__ void k_splitk_reduce(int M2, int N, int splits, const float* __restri
     }
 }
 
-PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
-    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-    static std::once_flag once;
-    std::call_once(once, [] {
-        void* p = nullptr;
-        cudaDriverEntryPointQueryResult q;
-        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
-            q == cudaDriverEntryPointSuccess)
-            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
-    });
-    B200_CHECK(fn != nullptr, kCudaError, "cuTensorMapEncodeTiled entry point not available");
-    return fn;
-}
-
 // 2-D fp32 tensor map: inner extent `inner` floats, `outer` rows of pitch `pitch_floats`
 CUtensorMap make_map(const void* base, long inner, long outer, long pitch_floats, unsigned box_inner, unsigned box_outer) {
     CUtensorMap m;
@@ -642,6 +569,7 @@ int TcGemmWorkspace::read_error(cudaStream_t s) {
 }
 
 void set_tc_wait_limit_ns(unsigned long long ns) { g_wait_ns.store(ns ? ns : kWaitNs, std::memory_order_relaxed); }
+unsigned long long tc_wait_limit_ns() { return wait_limit_ns(); }
 
 void tc_cgemm(char opa, int M, int N, int K, float2 alpha, const float2* A, int lda, const float2* B, int ldb,
               float2 beta, float2* C, int ldc, TcGemmWorkspace& w, cudaStream_t s) {

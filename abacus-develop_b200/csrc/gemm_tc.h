@@ -27,5 +27,7 @@ void tc_cgemm(char opa, int M, int N, int K, float2 alpha, const float2* A, int 
 // Time limit of every pipeline wait inside the tensor-core GEMM kernels launched from now on, all threads
 // (0 restores the default of 2 s).  A wait that runs out sets the workspace's error word.
 void set_tc_wait_limit_ns(unsigned long long ns);
+// the current limit (the tensor-core GEMMs of gemm_tc.cu and gemm_oz.cu both use it)
+unsigned long long tc_wait_limit_ns();
 
 }  // namespace b200

@@ -164,7 +164,28 @@ void Hamilt::fold_projectors(int ik, cudaStream_t s) {
         note_launch(2);
         B200_CUDA(cudaGetLastError());
     }
+    k.oz_ready = false;
+    if (fp64_gemm == 1) {
+        const int npw = grid->kmaps[ik].npw;
+        oz_prepare_a('C', k.nkb, npw, k.vkb.ptr, k.npwx, oz_mods, k.vkb_oz, oz_setup, s);
+        k.vkbd_oz.resize(size_t(nspin));
+        for (int sp = 0; sp < nspin; ++sp)
+            oz_prepare_a('N', npw, k.nkb, k.vkbd.ptr + size_t(sp) * total, k.npwx, oz_mods, k.vkbd_oz[sp], oz_setup, s);
+        k.oz_ready = true;
+    } else {
+        k.vkb_oz = OzOperand();
+        k.vkbd_oz.clear();
+    }
     k.folded = true;
+}
+
+void Hamilt::set_fp64_gemm(int mode, int nmods) {
+    B200_CHECK(mode == 0 || mode == 1, kInvalidArgument, "FP64 GEMM mode must be 0 (cuBLAS) or 1 (int8 tensor cores)");
+    B200_CHECK(nmods >= kOzMinMods && nmods <= kOzMaxMods, kInvalidArgument, "number of moduli must be 12..16");
+    fp64_gemm = mode;
+    oz_mods = nmods;
+    for (int ik = 0; ik < int(nl.size()); ++ik) fold_projectors(ik, 0);
+    B200_CUDA(cudaStreamSynchronize(0));
 }
 
 int Hamilt::band_chunk(size_t elem) const {
@@ -262,8 +283,14 @@ void Hamilt::hpsi(int ik, int spin, int nb, int ld, const T* psi, T* hpsi, int m
     B200_CHECK(k.folded, kInvalidArgument, "projectors and D not both set for this k-point");
     const T* vkbd = f64 ? reinterpret_cast<const T*>(k.vkbd.ptr + size_t(spin) * nkb * k.npwx)
                         : reinterpret_cast<const T*>(k.vkbdf.ptr + size_t(spin) * nkb * k.ldf);
+    const bool oz = f64 && fp64_gemm == 1 && k.oz_ready;
+    if (oz) W.tcw.ensure();  // the int8 GEMM reports a bounded wait that ran out in the same error word
     auto projections = [&](cudaStream_t st) {
         if constexpr (f64) {
+            if (oz) {
+                oz_zgemm('C', nkb, nb, npw, one, k.vkb_oz, psi, ld, zero, becp, nkb, W.ozw, W.tcw.err.ptr, st);
+                return;
+            }
             B200_CUBLAS(cublasSetStream(cublas, st));
             B200_CUBLAS(Blas<T>::gemm(cublas, CUBLAS_OP_C, CUBLAS_OP_N, nkb, nb, npw, &one, (const T*)k.vkb.ptr, k.npwx,
                                       psi, ld, &zero, becp, nkb));
@@ -295,9 +322,13 @@ void Hamilt::hpsi(int ik, int spin, int nb, int ld, const T* psi, T* hpsi, int m
         B200_CUDA(cudaStreamWaitEvent(s, W.ev_join, 0));
     }
     if constexpr (f64) {
-        B200_CUBLAS(cublasSetStream(cublas, s));
-        B200_CUBLAS(Blas<T>::gemm(cublas, CUBLAS_OP_N, CUBLAS_OP_N, npw, nb, nkb, &one, vkbd, k.npwx, becp, nkb, &one,
-                                  hpsi, ld));
+        if (oz) {
+            oz_zgemm('N', npw, nb, nkb, one, k.vkbd_oz[spin], becp, nkb, one, hpsi, ld, W.ozw, W.tcw.err.ptr, s);
+        } else {
+            B200_CUBLAS(cublasSetStream(cublas, s));
+            B200_CUBLAS(Blas<T>::gemm(cublas, CUBLAS_OP_N, CUBLAS_OP_N, npw, nb, nkb, &one, vkbd, k.npwx, becp, nkb,
+                                      &one, hpsi, ld));
+        }
     } else {
         tc_cgemm('N', npw, nb, nkb, one, vkbd, k.ldf, becp, ldb_p, one, hpsi, ld, tcw, s);
     }

@@ -5,6 +5,7 @@
 #include <vector>
 
 #include "common.h"
+#include "gemm_oz.h"
 #include "gemm_tc.h"
 #include "linalg_status.h"
 #include "pw_grid.h"
@@ -23,6 +24,12 @@ struct NonlocalK {
     DeviceArray<double2> vkbd;  // nspin x nkb x npwx
     DeviceArray<float2> vkbdf;  // nspin x nkb x ldf
     bool folded = false;
+    // the FP64 products' projector operands in int8 residue form (gemm_oz.h), built with the fold when the
+    // FP64 GEMMs run on the int8 tensor cores: vkb^H for becp (rows = projectors), vkbd per spin for
+    // H psi += vkbd becp (rows = plane waves)
+    OzOperand vkb_oz;
+    std::vector<OzOperand> vkbd_oz;
+    bool oz_ready = false;
 };
 
 // Scratch of one H|psi> caller: stick buffer, becp, the padded-psi stage, a cuBLAS handle and the
@@ -33,6 +40,7 @@ struct HpsiWork {
     DeviceArray<float2> sb32, becp32, psi_pad32;
     cublasHandle_t cublas = nullptr;
     TcGemmWorkspace tcw;
+    OzWorkspace ozw;  // the FP64 projector products on the int8 tensor cores (psi / becp residues, products)
     // second stream of an H|psi>: the projections (becp, D becp) run on it beside the local pass
     cudaStream_t side = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
@@ -81,6 +89,10 @@ struct Hamilt {
     DeviceArray<double> deeq;
     HpsiWork work;  // default scratch for callers that do not bring their own
     int chunk_override = 0;  // bands per stick-buffer chunk chosen by the autotuner (0 = 48 MB rule)
+    // FP64 projector products: 1 = int8 tensor cores (exact modular emulation, oz_mods moduli), 0 = cuBLAS
+    int fp64_gemm = 1;
+    int oz_mods = 16;
+    OzWorkspace oz_setup;  // scratch of the projector residues built at fold time
     VnlTables vnl;           // projector tables for on-device getvnl
 
     void set_projectors(int ntype, const int* na, const int* nbeta, const int* nh, int nhm, int lmax, const int* indv,
@@ -95,8 +107,11 @@ struct Hamilt {
     void set_vkb(int ik, int nkb, int npwx, const double2* vkb_d);
     void set_deeq(int ntype, const int* na, const int* nh, int nspin, int dx, int dy, int dz, const double* deeq_d);
     int band_chunk(size_t elem) const;
-    // fold D into the projectors of k-point ik (all spins), on stream s; nothing if either is not set
+    // fold D into the projectors of k-point ik (all spins), on stream s; nothing if either is not set.  With
+    // fp64_gemm = 1 also the int8 residue forms of vkb and vkbd.
     void fold_projectors(int ik, cudaStream_t s);
+    // choose the FP64 projector products (mode 1 int8 tensor cores with nmods moduli, 0 cuBLAS) and re-fold
+    void set_fp64_gemm(int mode, int nmods);
     // mode 0 = full H, 1 = kinetic + local only (overwrites hpsi), 2 = nonlocal only (accumulates)
     template <typename T>
     void hpsi(int ik, int spin, int nb, int ld, const T* psi, T* hpsi, int mode, cudaStream_t s, HpsiWork* w = nullptr);

@@ -171,6 +171,13 @@ int b200_hamilt_set_plane_variant(b200_hamilt* h, int variant) {
     });
 }
 
+int b200_hamilt_set_fp64_gemm(b200_hamilt* h, int mode, int nmods) {
+    return guarded([&] {
+        B200_CHECK(h != nullptr, b200::kInvalidArgument, "NULL argument");
+        h->h->set_fp64_gemm(mode, nmods);
+    });
+}
+
 int b200_solve_kpoints(b200_hamilt* h, int nk, const int* iks, int spin, int nband, int david_ndim, int precision,
                        const double* const* precond_d, void* const* psi_d, int ldpsi, double* eigenvalues,
                        double thr, int maxiter, int ntry_max, int notconv_max, int nworkers, int* iters) {

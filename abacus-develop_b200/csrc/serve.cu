@@ -260,6 +260,9 @@ class Server {
         const size_t per_band = size_t(g.nst) * g.nz * 16;
         b += std::max(per_band, std::min(per_band * nb, size_t(48) << 20)) + per_band;
         b += size_t(c.nkb + 1) * nb * 16 * 4 + (size_t(16) << 20);
+        // FP64 projector products on the int8 tensor cores: psi residues (2 real rows per band, one byte per
+        // modulus and real entry) and the per-modulus product residues of H psi
+        if (c.h->h->fp64_gemm == 1) b += size_t(c.h->h->oz_mods) * nb * (size_t(4) * c.npwx + 2 * size_t(c.npwx + 16));
         return b;
     }
 

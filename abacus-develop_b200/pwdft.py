@@ -97,6 +97,34 @@ def tc_cgemm(transa, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, stream=None):
          beta.real, beta.imag, ptr(c), ldc, stream_ptr(stream))
 
 
+def zgemm_i8(transa, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, nmods=16, stream=None):
+    """gemm_op<complex<double>, DEVICE_GPU> on the int8 tensor cores (exact modular emulation of the FP64
+    product): C = alpha*op(A)*B + beta*C, column-major complex128, transa 'N' or 'C', transb 'N'."""
+    al = (C.c_double * 2)(complex(alpha).real, complex(alpha).imag)
+    be = (C.c_double * 2)(complex(beta).real, complex(beta).imag)
+    call("b200_zgemm_i8", transa.encode(), b"N", m, n, k, al, ptr(a), lda, ptr(b), ldb, be, ptr(c), ldc, int(nmods),
+         stream_ptr(stream))
+
+
+def zgemm_i8_error():
+    """Error word of this thread's int8 GEMMs (nonzero: a bounded wait ran out); the read clears it."""
+    code = C.c_int()
+    call("b200_zgemm_i8_error", C.byref(code))
+    return code.value
+
+
+def zgemm_i8_constants(nmods, kr):
+    """Recombination constants of the int8 GEMM for nmods moduli and real rows of length kr: the moduli,
+    the weights w_l / M as (wa, wb), M as a double and the scale exponent q.  No GPU needed."""
+    mods = (C.c_int * nmods)()
+    wa = (C.c_double * nmods)()
+    wb = (C.c_double * nmods)()
+    mp = C.c_double()
+    q = C.c_int()
+    call("b200_zgemm_i8_constants", int(nmods), int(kr), mods, wa, wb, C.byref(mp), C.byref(q))
+    return list(mods), list(wa), list(wb), mp.value, q.value
+
+
 def tc_cgemm_error():
     """Error word of this thread's tensor-core GEMMs (nonzero: a bounded wait ran out); the read clears it."""
     code = C.c_int()
@@ -431,6 +459,11 @@ class HamiltPW:
         """Plane pass of the register transforms (1: warp-shuffle lanes; 2-5: two-pass transforms; 0: default)
         for every handle of this basis in this handle's precision."""
         call("b200_hamilt_set_plane_variant", self._h, int(variant))
+
+    def set_fp64_gemm(self, mode, nmods=16):
+        """FP64 projector products: mode 1 on the int8 tensor cores (exact modular emulation with nmods
+        moduli, the default), 0 on cuBLAS ZGEMM.  Rebuilds the projector residue forms."""
+        call("b200_hamilt_set_fp64_gemm", self._h, int(mode), int(nmods))
 
     def solve_kpoints(self, iks, precond_ds, psis, ld_psi, nband, thr, maxiter, david_ndim=4, precision=PREC_FP64,
                       nworkers=4, ntry_max=5, notconv_max=0, spin=0):

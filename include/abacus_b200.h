@@ -214,6 +214,13 @@ int b200_hamilt_autotune(b200_hamilt* h, int ik, int nbands, int ld, const void*
  * stages; 2-5 = two-pass register transforms through shared memory (four launch shapes); 0 = the
  * default.  All variants give the same results within rounding.  No counterpart in the reference. */
 int b200_hamilt_set_plane_variant(b200_hamilt* h, int variant);
+/* The FP64 projector products of Nonlocal::act (nonlocal_pw.cpp:255-276, becp = vkb^H psi and
+ * H psi += vkb (D becp), here with D folded into the projectors) for this handle: mode 1 (the default) on
+ * the int8 tensor cores, exact modular emulation of the FP64 product with nmods (12..16, default 16)
+ * moduli, as b200_zgemm_i8; mode 0 cuBLAS ZGEMM.  Mode 1 keeps the projectors also in residue form
+ * (2 x nmods bytes per projector entry and spin) and each H|psi> caller about 6 x nmods bytes per
+ * psi entry of scratch.  Rebuilds the projector forms of every k-point (synchronous). */
+int b200_hamilt_set_fp64_gemm(b200_hamilt* h, int mode, int nmods);
 /* Bands per stick-buffer chunk of this handle's local pass (0 = the default: the largest chunk whose
  * stick buffer stays within 48 MB).  What b200_hamilt_autotune sets.  No counterpart in the reference. */
 int b200_hamilt_set_band_chunk(b200_hamilt* h, int chunk);
@@ -295,6 +302,24 @@ int b200_tc_cgemm_error(int* code);
  * cuBLAS calls have no bounded waits: a test sets a limit that cannot be met and checks that
  * b200_tc_cgemm_error reports it and that the next GEMM with the default limit is correct. */
 int b200_tc_set_wait_limit_ns(unsigned long long ns);
+
+/* gemm_op<std::complex<double>, DEVICE_GPU> (math_kernel_op.h:240-265, cuda/math_kernel_op.cu:815-874) on
+ * the int8 tensor cores: C = alpha op(A) B + beta C, complex128 column-major, transa 'N' or 'C', transb
+ * 'N'; alpha, beta: host complex (2 doubles each).  Exact modular emulation of the FP64 product: every
+ * row of op(A) and column of B is scaled by a power of two to integers, reduced modulo nmods (12..16)
+ * coprime moduli <= 256, one int8 tcgen05 GEMM per modulus, and the product recombined by the Chinese
+ * remainder theorem.  With nmods = 16 the largest entry of each row and column keeps all 53 bits and the
+ * result is as accurate as an FP64 GEMM; NaN or infinite entries make the entries of C they reach NaN.
+ * Stream-ordered; its scratch (about 16 bytes per entry of A and B) is kept per calling thread. */
+int b200_zgemm_i8(char transa, char transb, int m, int n, int k, const double* alpha, const void* a_d, int lda,
+                  const void* b_d, int ldb, const double* beta, void* c_d, int ldc, int nmods, void* stream);
+/* Error word of the calling thread's int8 GEMMs (synchronous read of the legacy stream, cleared by the
+ * read): nonzero if a bounded wait inside the GEMM kernel ran out (its output is then not valid). */
+int b200_zgemm_i8_error(int* code);
+/* Host copies of the recombination constants of b200_zgemm_i8 for nmods moduli: the moduli, the weights
+ * w_l / M as wa + wb, M as a double, and the scale exponent q for real rows of length kr (every row is
+ * scaled so that its largest magnitude is below 2^q).  No GPU needed; for tests of the scheme. */
+int b200_zgemm_i8_constants(int nmods, long long kr, int* mods, double* wa, double* wb, double* mprod, int* q);
 
 /* Measured arithmetic peaks of the current device in TFLOP/s (CUDA events on the legacy default
  * stream; one warm-up launch each): FP64 and FP32 fused multiply-add chains on the CUDA cores, and
