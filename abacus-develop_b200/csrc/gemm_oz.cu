@@ -46,14 +46,15 @@ constexpr int kOzMods[kOzMaxMods] = {256, 255, 253, 251, 247, 241, 239, 233, 229
 constexpr int kOzNonFinite = -2147483647 - 1;  // row exponent marking a row with a NaN or infinite entry
 constexpr int kOzSeg = 4096;                   // complex entries per column segment of the norm / residue kernels
 constexpr int kOzMaxKbPerSplit = 1023;         // 128-byte K blocks per split: 1023 * 128 = 130944 reals
-constexpr int kOzThreads = 192;                // warp 0 TMA, warp 1 MMA, warps 2-5 epilogue
+constexpr int kOzThreads = 320;                // warp 0 TMA, warp 1 MMA, warps 2-9 epilogue
 constexpr int kOzATile = 128 * 128;            // bytes of one A stage: 128 rows x 128 K
-constexpr int kOzSmem = 110 * 1024;            // dynamic shared memory per CTA: two CTAs per SM, not three
+constexpr int kOzSmem = 227 * 1024;            // dynamic shared memory per CTA: one persistent CTA per SM
 
 struct OzConst {
     int n, q;  // q: set per call from K' (oz_scale_bits)
     unsigned m[kOzMaxMods], magic[kOzMaxMods];             // magic = ceil(2^32 / m)
     unsigned c21[kOzMaxMods], c42[kOzMaxMods], off62[kOzMaxMods], c31[kOzMaxMods];
+    unsigned h[kOzMaxMods];  // residues are kept shifted by h: 128 for m = 256, (m - 1) / 2 for odd m
     double wa[kOzMaxMods], wb[kOzMaxMods];
     double mprod, log2m;
 };
@@ -80,7 +81,8 @@ OzConst make_const(int n) {
         c.magic[l] = unsigned(((1ull << 32) + m - 1) / m);
         c.c21[l] = unsigned((1ull << 21) % m);
         c.c42[l] = unsigned((1ull << 42) % m);
-        c.off62[l] = unsigned((m - (1ull << 62) % m) % m);
+        c.h[l] = m == 256 ? 128u : (m - 1) / 2;
+        c.off62[l] = unsigned((m - (1ull << 62) % m + c.h[l]) % m);
         c.c31[l] = unsigned((1ull << 31) % m);
         const u128 Ml = M / m;
         const unsigned r = unsigned(Ml % m);
@@ -127,20 +129,29 @@ __device__ __forceinline__ unsigned oz_umod(unsigned x, unsigned m, unsigned mag
     const int r = int(x - q * m);
     return unsigned(r < 0 ? r + int(m) : r);
 }
-// (integer v) + 2^62 for |v| < 2^62, v an integral double
-__device__ __forceinline__ unsigned long long oz_offset(double v) {
-    return (unsigned long long)(__double2ll_rn(v) + (1ll << 62));
-}
-// residue in [0, m) of the integer u - 2^62 (u < 2^63): three 21-bit pieces
+// (u - 2^62 + h) mod m for u < 2^63: three 21-bit pieces
 __device__ __forceinline__ unsigned oz_res(unsigned long long u, const OzConst& c, int l) {
     const unsigned p0 = unsigned(u) & 0x1FFFFFu, p1 = unsigned(u >> 21) & 0x1FFFFFu, p2 = unsigned(u >> 42);
     return oz_umod(p2 * c.c42[l] + p1 * c.c21[l] + p0 + c.off62[l], c.m[l], c.magic[l]);
 }
-// symmetric representative of r in [0, m): [-128, 127] for m = 256, [-(m-1)/2, (m-1)/2] for odd m
-__device__ __forceinline__ unsigned oz_sym(unsigned r, unsigned m) {
-    return (r > (m - 1) / 2 ? r - m : r) & 0xFFu;
-}
-__device__ __forceinline__ unsigned oz_symneg(unsigned r, unsigned m) { return oz_sym(r == 0 ? 0 : m - r, m); }
+// x 2^e rounded to the nearest integer, offset by 2^62 (|x| 2^e < 2^62): two exact scalings by powers of two
+// (2^e itself may lie outside the double range), then one rounding conversion
+__device__ __forceinline__ double oz_pow2(int e) { return __longlong_as_double((long long)(e + 1023) << 52); }
+struct OzScale {
+    double s1, s2;
+    __device__ explicit OzScale(int e) {
+        const int e1 = e < 1000 ? e : 1000;  // e >= q - 1024 > -1022: both factors are normal doubles
+        s1 = oz_pow2(e1);
+        s2 = oz_pow2(e - e1);
+    }
+    __device__ unsigned long long operator()(double x) const {
+        return (unsigned long long)(__double2ll_rn((x * s1) * s2) + (1ll << 62));
+    }
+};
+// the symmetric representative (as a byte) of v, and of -v, from r = (v + h) mod m: r - h lies in
+// [-128, 127] for m = 256 and in [-(m-1)/2, (m-1)/2] for odd m; h - r is -v's (128 = -128 as a byte, m = 256)
+__device__ __forceinline__ unsigned oz_sym(unsigned r, unsigned h) { return (r - h) & 0xFFu; }
+__device__ __forceinline__ unsigned oz_symneg(unsigned r, unsigned h) { return (h - r) & 0xFFu; }
 
 // exponent e of a row whose largest magnitude is mx: mx 2^e < 2^q (kOzNonFinite for NaN / infinity)
 __device__ __forceinline__ int oz_exponent(double mx, int q) {
@@ -203,17 +214,18 @@ __global__ void __launch_bounds__(256) k_oz_res_cols(int K, const double2* __res
     const bool bad = e == kOzNonFinite;
     const double2* col = X + long(j) * ld;
     const long k0 = long(sg) * kOzSeg, k1 = min(long(K), k0 + kOzSeg);
+    const OzScale scale(bad ? 0 : e);
     for (long kb = k0 + 4L * threadIdx.x; kb < k1; kb += 4L * 256) {
         unsigned long long ur[4], ui[4];
 #pragma unroll
         for (int t = 0; t < 4; ++t) {
             const long k = kb + t;
             const double2 x = (k < k1 && !bad) ? col[k] : make_double2(0.0, 0.0);
-            ur[t] = oz_offset(rint(ldexp(x.x, e)));
-            ui[t] = oz_offset(rint(ldexp(x.y, e)));
+            ur[t] = scale(x.x);
+            ui[t] = scale(x.y);
         }
         for (int l = 0; l < c.n; ++l) {
-            const unsigned m = c.m[l];
+            const unsigned hs = c.h[l];
             unsigned rr[4], ri[4];
 #pragma unroll
             for (int t = 0; t < 4; ++t) {
@@ -223,21 +235,21 @@ __global__ void __launch_bounds__(256) k_oz_res_cols(int K, const double2* __res
             signed char* pl = res + long(l) * plane + 2 * kb;
             if (KIND == 0) {
                 uint2 v;
-                v.x = oz_sym(rr[0], m) | (oz_sym(ri[0], m) << 8) | (oz_sym(rr[1], m) << 16) | (oz_sym(ri[1], m) << 24);
-                v.y = oz_sym(rr[2], m) | (oz_sym(ri[2], m) << 8) | (oz_sym(rr[3], m) << 16) | (oz_sym(ri[3], m) << 24);
+                v.x = oz_sym(rr[0], hs) | (oz_sym(ri[0], hs) << 8) | (oz_sym(rr[1], hs) << 16) | (oz_sym(ri[1], hs) << 24);
+                v.y = oz_sym(rr[2], hs) | (oz_sym(ri[2], hs) << 8) | (oz_sym(rr[3], hs) << 16) | (oz_sym(ri[3], hs) << 24);
                 *reinterpret_cast<uint2*>(pl + long(j) * kp) = v;
             } else {
                 uint2 vre, vim;
                 if (KIND == 1) {  // re = [br, -bi], im = [bi, br]
-                    vre.x = oz_sym(rr[0], m) | (oz_symneg(ri[0], m) << 8) | (oz_sym(rr[1], m) << 16) | (oz_symneg(ri[1], m) << 24);
-                    vre.y = oz_sym(rr[2], m) | (oz_symneg(ri[2], m) << 8) | (oz_sym(rr[3], m) << 16) | (oz_symneg(ri[3], m) << 24);
-                    vim.x = oz_sym(ri[0], m) | (oz_sym(rr[0], m) << 8) | (oz_sym(ri[1], m) << 16) | (oz_sym(rr[1], m) << 24);
-                    vim.y = oz_sym(ri[2], m) | (oz_sym(rr[2], m) << 8) | (oz_sym(ri[3], m) << 16) | (oz_sym(rr[3], m) << 24);
+                    vre.x = oz_sym(rr[0], hs) | (oz_symneg(ri[0], hs) << 8) | (oz_sym(rr[1], hs) << 16) | (oz_symneg(ri[1], hs) << 24);
+                    vre.y = oz_sym(rr[2], hs) | (oz_symneg(ri[2], hs) << 8) | (oz_sym(rr[3], hs) << 16) | (oz_symneg(ri[3], hs) << 24);
+                    vim.x = oz_sym(ri[0], hs) | (oz_sym(rr[0], hs) << 8) | (oz_sym(ri[1], hs) << 16) | (oz_sym(rr[1], hs) << 24);
+                    vim.y = oz_sym(ri[2], hs) | (oz_sym(rr[2], hs) << 8) | (oz_sym(ri[3], hs) << 16) | (oz_sym(rr[3], hs) << 24);
                 } else {  // re = [br, bi], im = [bi, -br]
-                    vre.x = oz_sym(rr[0], m) | (oz_sym(ri[0], m) << 8) | (oz_sym(rr[1], m) << 16) | (oz_sym(ri[1], m) << 24);
-                    vre.y = oz_sym(rr[2], m) | (oz_sym(ri[2], m) << 8) | (oz_sym(rr[3], m) << 16) | (oz_sym(ri[3], m) << 24);
-                    vim.x = oz_sym(ri[0], m) | (oz_symneg(rr[0], m) << 8) | (oz_sym(ri[1], m) << 16) | (oz_symneg(rr[1], m) << 24);
-                    vim.y = oz_sym(ri[2], m) | (oz_symneg(rr[2], m) << 8) | (oz_sym(ri[3], m) << 16) | (oz_symneg(rr[3], m) << 24);
+                    vre.x = oz_sym(rr[0], hs) | (oz_sym(ri[0], hs) << 8) | (oz_sym(rr[1], hs) << 16) | (oz_sym(ri[1], hs) << 24);
+                    vre.y = oz_sym(rr[2], hs) | (oz_sym(ri[2], hs) << 8) | (oz_sym(rr[3], hs) << 16) | (oz_sym(ri[3], hs) << 24);
+                    vim.x = oz_sym(ri[0], hs) | (oz_symneg(rr[0], hs) << 8) | (oz_sym(ri[1], hs) << 16) | (oz_symneg(rr[1], hs) << 24);
+                    vim.y = oz_sym(ri[2], hs) | (oz_symneg(rr[2], hs) << 8) | (oz_sym(ri[3], hs) << 16) | (oz_symneg(rr[3], hs) << 24);
                 }
                 *reinterpret_cast<uint2*>(pl + long(2 * j) * kp) = vre;
                 *reinterpret_cast<uint2*>(pl + long(2 * j + 1) * kp) = vim;
@@ -268,13 +280,14 @@ __global__ void __launch_bounds__(256) k_oz_res_rows(int M, int K, const double2
     const int e = row < M ? oz_exponent(part[row], c.q) : 0;
     if (blockIdx.x == 0 && ty == 0 && row < M) exps[row] = e;
     const bool bad = e == kOzNonFinite;
+    const OzScale scale(bad ? 0 : e);
     for (int kk = ty; kk < 32; kk += 8) {
         const int k = k0 + kk;
         const double2 x = (row < M && k < K && !bad) ? X[row + long(k) * ld] : make_double2(0.0, 0.0);
-        const unsigned long long ur = oz_offset(rint(ldexp(x.x, e))), ui = oz_offset(rint(ldexp(x.y, e)));
+        const unsigned long long ur = scale(x.x), ui = scale(x.y);
         for (int l = 0; l < c.n; ++l) {
-            tile[l][tx][2 * kk] = (unsigned char)oz_sym(oz_res(ur, c, l), c.m[l]);
-            tile[l][tx][2 * kk + 1] = (unsigned char)oz_sym(oz_res(ui, c, l), c.m[l]);
+            tile[l][tx][2 * kk] = (unsigned char)oz_sym(oz_res(ur, c, l), c.h[l]);
+            tile[l][tx][2 * kk + 1] = (unsigned char)oz_sym(oz_res(ui, c, l), c.h[l]);
         }
     }
     __syncthreads();
@@ -315,133 +328,280 @@ struct OzMods {
     unsigned m[kOzMaxMods], magic[kOzMaxMods], c31[kOzMaxMods];
 };
 
-// One CTA: a 128-row x BN-column tile of the product for modulus l = blockIdx.z % n over the K blocks of
-// split blockIdx.z / n.  A: rows of op(A)'s residues, B: rows of B's residues (both K-major, 128-byte swizzle,
-// one TMA box of 128 K bytes per stage).  prod[((z * colsB) + col) * rows_pad + row] = (product mod m_l).
-// Every wait is bounded; a wait that runs out sets err, the CTA drains its copies and MMAs and returns.
+// The work of one GEMM launch: tiles of 128 msub rows (op(A)) x BN real columns (B') for every plane
+// z = split * n + l (modulus l, K split `split`).  Streaming schedule: tile t = blockIdx.x + i gridDim.x with
+// tile_n fastest, then tile_m, then z (the CTAs running together share their A and B tiles through L2).
+// Resident schedule (B' of one (z, tile_n) fits in shared memory): a fixed tile_n and a contiguous range of
+// (z, tile_m) per CTA, z major, so that a CTA loads B' once per plane z it meets.
+struct OzSched {
+    int tm, tn, nz, per_split, nk_total, msub, nbuf;
+    bool resident;
+};
+struct OzTile {
+    int tile_m, tile_n, z, pair, k_begin, nk;
+};
+struct OzIter {
+    long t, t_end, step;
+    int tile_n;  // resident schedule: this CTA's column tile
+    __device__ explicit OzIter(const OzSched& s) {
+        const long T = long(s.tm) * s.tn * s.nz;
+        if (s.resident) {
+            // CTA c takes column tile c % tn and chunk c / tn of the (z, tile_m) sequence: the tn CTAs of a
+            // group walk the same A tiles at the same pace, so A crosses HBM once
+            const long U = long(s.tm) * s.nz;
+            const int groups = gridDim.x / s.tn;
+            const int grp = blockIdx.x / s.tn;
+            tile_n = blockIdx.x % s.tn;
+            const long chunk = (U + groups - 1) / groups;
+            t = grp < groups ? long(grp) * chunk : U;
+            t_end = min(U, t + chunk);
+            step = 1;
+        } else {
+            t = blockIdx.x;
+            t_end = T;
+            step = gridDim.x;
+        }
+    }
+    // the next tile of this CTA with its K range (n moduli per split)
+    __device__ bool next(const OzSched& s, int n, OzTile& o) {
+        if (t >= t_end) return false;
+        if (s.resident) {
+            o.z = int(t / s.tm);
+            o.tile_m = int(t % s.tm);
+            o.tile_n = tile_n;
+            o.pair = o.z * s.tn + tile_n;
+        } else {
+            o.tile_n = int(t % s.tn);
+            const long r = t / s.tn;
+            o.tile_m = int(r % s.tm);
+            o.z = int(r / s.tm);
+            o.pair = o.z * s.tn + o.tile_n;
+        }
+        o.k_begin = (o.z / n) * s.per_split;
+        o.nk = max(0, min(s.nk_total, o.k_begin + s.per_split) - o.k_begin);
+        t += step;
+        return true;
+    }
+};
+
+constexpr int kOzEpiWarps = 8;  // warps 2..9: two per tensor-memory lane quarter
+
+// Persistent CTAs (one per SM): warp 0 issues the TMA loads, warp 1 allocates tensor memory and issues the
+// MMAs into msub accumulators of BN int32 columns per tile (two such sets 256 columns apart when they fit:
+// the next tile accumulates while the last one drains), warps 2-9 drain: residues of the products mod m_l,
+// stored 16 columns per thread and store in column groups, prod[((z * cgroups + cg) * rows_pad + row) * 16 + i]
+// (column 16 cg + i), so that both the stores here and the loads of the recombination are coalesced.
+// Every wait is bounded; a wait that runs out sets err and the CTA drains its copies and MMAs in flight and
+// returns.
 __global__ void __launch_bounds__(kOzThreads, 1)
-    k_oz_gemm(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB, int rowsA,
-              int colsB, int BN, int stages, int nk_total, int per_split, int n, const __grid_constant__ OzMods md,
-              unsigned char* __restrict__ prod, long rows_pad, int* __restrict__ err, unsigned long long wait_ns) {
+    k_oz_gemm(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB, int rowsA, int BN,
+              int stages, int n, const OzSched sc, const __grid_constant__ OzMods md, unsigned char* __restrict__ prod,
+              long rows_pad, int cgroups, int* __restrict__ err, unsigned long long wait_ns) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     const unsigned long long drain_ns = wait_ns > kWaitNs ? wait_ns : kWaitNs;
     unsigned char* base = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
-    const int stage_bytes = kOzATile + BN * 128;
-    unsigned long long* full = reinterpret_cast<unsigned long long*>(base + stages * stage_bytes);
+    const int a_stage = sc.msub * kOzATile;
+    const int b_box = BN * 128;  // one B' box: BN rows x 128 K bytes
+    const int a_area = stages * a_stage;
+    const int b_area = sc.resident ? sc.per_split * b_box : stages * b_box;
+    unsigned char* a_st = base;
+    unsigned char* b_st = base + a_area;
+    unsigned long long* full = reinterpret_cast<unsigned long long*>(base + a_area + b_area);
     unsigned long long* empty = full + stages;
-    unsigned long long* acc_full = empty + stages;
-    unsigned* tmem_slot = reinterpret_cast<unsigned*>(acc_full + 1);
+    unsigned long long* acc_full = empty + stages;  // [2]
+    unsigned long long* acc_empty = acc_full + 2;   // [2]
+    unsigned long long* bfull = acc_empty + 2;
+    unsigned long long* bempty = bfull + 1;
+    unsigned long long* drain = bempty + 1;
+    unsigned* tmem_slot = reinterpret_cast<unsigned*>(drain + 1);
     volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
-
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int tile_n = blockIdx.x, tile_m = blockIdx.y;
-    const int l = int(blockIdx.z) % n, split = int(blockIdx.z) / n;
-    const int k_begin = split * per_split;
-    const int k_end = min(nk_total, k_begin + per_split);
-    const int nk = max(0, k_end - k_begin);
+    const int nbuf = sc.nbuf;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < stages; ++s) {
             mbar_init(smem_u32(&full[s]), 1);
             mbar_init(smem_u32(&empty[s]), 1);
         }
-        mbar_init(smem_u32(acc_full), 1);
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(smem_u32(&acc_full[b]), 1);
+            mbar_init(smem_u32(&acc_empty[b]), 32 * kOzEpiWarps);
+        }
+        mbar_init(smem_u32(bfull), 1);
+        mbar_init(smem_u32(bempty), 1);
+        mbar_init(smem_u32(drain), 1);
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 1) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
-                     "r"(256u));
+                     "r"(512u));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
     const unsigned tmem = *tmem_slot;
+    auto fail = [&](int code) {
+        *abort_flag = 1;
+        atomicOr(err, code);
+    };
 
     if (warp == 0) {
         if (lane == 0) {
-            int issued = 0;
-            for (int i = 0; i < nk && !*abort_flag; ++i) {
-                const int s = i % stages;
-                if (i >= stages && !mbar_wait(smem_u32(&empty[s]), ((i / stages) - 1) & 1, wait_ns)) {
-                    *abort_flag = 1;
-                    atomicOr(err, 1);
-                    break;
+            long g = 0;  // A stages issued (all tiles)
+            int bp = 0, cur_pair = -1;
+            OzIter it(sc);
+            OzTile o;
+            bool ok = true;
+            while (ok && !*abort_flag && it.next(sc, n, o)) {
+                const int l = o.z % n;
+                if (sc.resident && o.pair != cur_pair) {
+                    // the MMAs that read the previous B' have completed before it is overwritten
+                    if (bp > 0 && !mbar_wait(smem_u32(bempty), (bp - 1) & 1, wait_ns)) {
+                        fail(1);
+                        break;
+                    }
+                    mbar_expect_tx(smem_u32(bfull), unsigned(o.nk * b_box));
+                    for (int kb = 0; kb < o.nk; ++kb)
+                        tma_load_3d(smem_u32(b_st + kb * b_box), &mapB, (o.k_begin + kb) * 128, o.tile_n * BN, l,
+                                    smem_u32(bfull));
+                    ++bp;
+                    cur_pair = o.pair;
                 }
-                unsigned char* st = base + s * stage_bytes;
-                const unsigned fb = smem_u32(&full[s]);
-                mbar_expect_tx(fb, unsigned(stage_bytes));
-                const int kx = (k_begin + i) * 128;
-                tma_load_3d(smem_u32(st), &mapA, kx, tile_m * 128, l, fb);
-                tma_load_3d(smem_u32(st + kOzATile), &mapB, kx, tile_n * BN, l, fb);
-                ++issued;
+                for (int i = 0; i < o.nk; ++i, ++g) {
+                    const int s = int(g % stages);
+                    if (g >= stages && !mbar_wait(smem_u32(&empty[s]), unsigned((g / stages) - 1) & 1u, wait_ns)) {
+                        fail(1);
+                        ok = false;
+                        break;
+                    }
+                    const unsigned fb = smem_u32(&full[s]);
+                    mbar_expect_tx(fb, unsigned(a_stage + (sc.resident ? 0 : b_box)));
+                    const int kx = (o.k_begin + i) * 128;
+                    for (int u = 0; u < sc.msub; ++u)
+                        tma_load_3d(smem_u32(a_st + s * a_stage + u * kOzATile), &mapA, kx,
+                                    (o.tile_m * sc.msub + u) * 128, l, fb);
+                    if (!sc.resident) tma_load_3d(smem_u32(b_st + s * b_box), &mapB, kx, o.tile_n * BN, l, fb);
+                }
             }
-            for (int i = max(0, issued - stages); i < issued; ++i)
-                if (!mbar_wait(smem_u32(&full[i % stages]), (i / stages) & 1, drain_ns)) atomicOr(err, 8);
+            // every copy this thread issued lands before the CTA exits
+            for (long i = g - stages > 0 ? g - stages : 0; i < g; ++i)
+                if (!mbar_wait(smem_u32(&full[i % stages]), unsigned(i / stages) & 1u, drain_ns)) atomicOr(err, 8);
+            if (bp > 0 && !mbar_wait(smem_u32(bfull), (bp - 1) & 1, drain_ns)) atomicOr(err, 8);
         }
     } else if (warp == 1) {
         if (lane == 0) {
             // D = S32, A and B signed 8-bit, both K-major, N = BN, M = 128
             const unsigned idesc = (2u << 4) | (1u << 7) | (1u << 10) | (unsigned(BN >> 3) << 17) | (8u << 24);
-            int issued = 0;
-            for (int i = 0; i < nk && !*abort_flag; ++i) {
-                const int s = i % stages;
-                if (!mbar_wait(smem_u32(&full[s]), (i / stages) & 1, wait_ns)) {
-                    *abort_flag = 1;
-                    atomicOr(err, 2);
+            long g = 0;
+            int j = 0, bp = 0, cur_pair = -1, issued = 0;
+            OzIter it(sc);
+            OzTile o;
+            bool ok = true;
+            while (ok && !*abort_flag && it.next(sc, n, o)) {
+                const int b = j % nbuf;
+                if (j >= nbuf && !mbar_wait(smem_u32(&acc_empty[b]), unsigned((j / nbuf) - 1) & 1u, wait_ns)) {
+                    fail(32);
                     break;
                 }
+                if (sc.resident && o.pair != cur_pair) {
+                    if (bp > 0) mma_commit(smem_u32(bempty));  // completes with every MMA on the previous B'
+                    if (!mbar_wait(smem_u32(bfull), bp & 1, wait_ns)) {
+                        fail(2);
+                        break;
+                    }
+                    ++bp;
+                    cur_pair = o.pair;
+                }
                 tc_fence_after();
-                const unsigned a = smem_u32(base + s * stage_bytes);
-                const unsigned b = a + kOzATile;
+                const unsigned d0 = tmem + unsigned(b * 256);
+                for (int i = 0; i < o.nk; ++i, ++g) {
+                    const int s = int(g % stages);
+                    if (!mbar_wait(smem_u32(&full[s]), unsigned(g / stages) & 1u, wait_ns)) {
+                        fail(2);
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const unsigned bs = smem_u32(b_st + (sc.resident ? i : s) * b_box);
+                    for (int u = 0; u < sc.msub; ++u) {
+                        const unsigned a = smem_u32(a_st + s * a_stage + u * kOzATile);
+                        const unsigned d = d0 + unsigned(u * BN);
 #pragma unroll
-                for (int kk = 0; kk < 4; ++kk)
-                    mma_i8(tmem, sdesc(a + kk * 32, 16, 1024, 2), sdesc(b + kk * 32, 16, 1024, 2), idesc,
-                           (i > 0 || kk > 0) ? 1u : 0u);
-                mma_commit(smem_u32(&empty[s]));
-                ++issued;
+                        for (int kk = 0; kk < 4; ++kk)
+                            mma_i8(d, sdesc(a + kk * 32, 16, 1024, 2), sdesc(bs + kk * 32, 16, 1024, 2), idesc,
+                                   (i > 0 || kk > 0) ? 1u : 0u);
+                    }
+                    mma_commit(smem_u32(&empty[s]));
+                    ++issued;
+                }
+                if (!ok) break;
+                if (o.nk > 0) mma_commit(smem_u32(&acc_full[b]));
+                else mbar_arrive(smem_u32(&acc_full[b]));
+                ++j;
             }
-            // the accumulator is complete (or, after an abort, every issued MMA has finished) when acc_full
-            // flips; with nothing issued a plain arrive releases the epilogue
-            if (issued > 0) mma_commit(smem_u32(acc_full));
-            else mbar_arrive(smem_u32(acc_full));
-            if (!mbar_wait(smem_u32(acc_full), 0, drain_ns)) atomicOr(err, 64);
+            // after an abort: every MMA issued so far completes before tensor memory is freed
+            if (*abort_flag && issued > 0) {
+                mma_commit(smem_u32(drain));
+                if (!mbar_wait(smem_u32(drain), 0, drain_ns)) atomicOr(err, 64);
+            }
         }
     } else {
-        const int q = warp & 3;
-        const int row = tile_m * 128 + 32 * q + lane;
-        bool ok = mbar_wait(smem_u32(acc_full), 0, wait_ns);
-        if (!ok) atomicOr(err, 16);
-        ok = __all_sync(0xffffffffu, ok && !*abort_flag);
-        if (ok) {
+        const int q = warp & 3;          // lane quarter this warp may access
+        const int grp = (warp - 2) >> 2;  // 0: warps 2-5, 1: warps 6-9 (alternate 16-column chunks)
+        const int rl = 32 * q + lane;
+        int j = 0;
+        OzIter it(sc);
+        OzTile o;
+        while (!*abort_flag && it.next(sc, n, o)) {
+            const int b = j % nbuf;
+            bool ok = mbar_wait(smem_u32(&acc_full[b]), unsigned(j / nbuf) & 1u, wait_ns);
+            if (!ok) fail(16);
+            ok = __all_sync(0xffffffffu, ok && !*abort_flag);
+            if (!ok) break;
             tc_fence_after();
+            const int l = o.z % n;
             const unsigned m = md.m[l], magic = md.magic[l], c31 = md.c31[l];
-            unsigned char* out = prod + (long(blockIdx.z) * colsB) * rows_pad;
-            for (int c0 = 0; c0 < BN; c0 += 16) {
-                int v[16];
-                if (nk > 0) {
-                    tmem_ld16i(tmem + (unsigned(32 * q) << 16) + unsigned(c0), v);
-                } else {
+            for (int u = 0; u < sc.msub; ++u) {
+                const int row = (o.tile_m * sc.msub + u) * 128 + rl;
+                for (int c0 = 16 * grp; c0 < BN; c0 += 32) {
+                    int v[16];
+                    if (o.nk > 0) {
+                        tmem_ld16i(tmem + (unsigned(32 * q) << 16) + unsigned(b * 256 + u * BN + c0), v);
+                    } else {
 #pragma unroll
-                    for (int j = 0; j < 16; ++j) v[j] = 0;
-                }
+                        for (int t = 0; t < 16; ++t) v[t] = 0;
+                    }
+                    unsigned w[4];
 #pragma unroll
-                for (int j = 0; j < 16; ++j) {
-                    const int col = tile_n * BN + c0 + j;
-                    // (v + 2^31) mod m, then minus 2^31 mod m
-                    const unsigned r = oz_umod(unsigned(v[j]) + 0x80000000u, m, magic);
-                    const int t = int(r) - int(c31);
-                    if (row < rowsA && col < colsB) out[long(col) * rows_pad + row] = (unsigned char)(t < 0 ? t + int(m) : t);
+                    for (int t4 = 0; t4 < 4; ++t4) {
+                        unsigned word = 0;
+#pragma unroll
+                        for (int t = 0; t < 4; ++t) {
+                            // (v + 2^31) mod m, then minus 2^31 mod m
+                            const unsigned r = oz_umod(unsigned(v[4 * t4 + t]) + 0x80000000u, m, magic);
+                            const int x = int(r) - int(c31);
+                            word |= unsigned(x < 0 ? x + int(m) : x) << (8 * t);
+                        }
+                        w[t4] = word;
+                    }
+                    const int cg = (o.tile_n * BN + c0) >> 4;
+                    if (row < rowsA && cg < cgroups)
+                        *reinterpret_cast<uint4*>(prod + ((long(o.z) * cgroups + cg) * rows_pad + row) * 16) =
+                            make_uint4(w[0], w[1], w[2], w[3]);
                 }
             }
+            tc_fence_before();
+            mbar_arrive(smem_u32(&acc_empty[b]));
+            ++j;
         }
     }
     tc_fence_before();
     __syncthreads();
     if (warp == 1) {
         tc_fence_after();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(256u));
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512u));
     }
 }
 
@@ -451,49 +611,60 @@ __device__ __forceinline__ double oz_frac(double s, double t) {
     return x - rint(x);
 }
 
-// C (row, col) = alpha (C_re + i C_im) + beta C: four rows per thread, column blockIdx.y
-__global__ void __launch_bounds__(128) k_oz_recombine(int M, int N, int splits, const unsigned char* __restrict__ prod,
-                                                      long rows_pad, const int* __restrict__ eA,
-                                                      const int* __restrict__ eB, const __grid_constant__ OzConst c, double2 alpha,
-                                                      double2 beta, double2* __restrict__ C, long ldc) {
-    const int col = blockIdx.y;
-    const int r0 = (blockIdx.x * 128 + threadIdx.x) * 4;
-    if (r0 >= M) return;
-    const long colsB = 2L * N;
-    double sr[4] = {0, 0, 0, 0}, tr[4] = {0, 0, 0, 0}, si[4] = {0, 0, 0, 0}, ti[4] = {0, 0, 0, 0};
-    for (int l = 0; l < c.n; ++l) {
-        unsigned ar[4] = {0, 0, 0, 0}, ai[4] = {0, 0, 0, 0};
-        for (int sp = 0; sp < splits; ++sp) {
+// C (row, col) = alpha (C_re + i C_im) + beta C: thread (row, h) with row = blockIdx.y * 128 + threadIdx.x / 2
+// takes the 4 complex columns 8 blockIdx.x + 4 h .. + 3 (8 bytes of column group blockIdx.x per modulus and
+// split: a warp reads 256 contiguous bytes per load)
+__global__ void __launch_bounds__(256) k_oz_recombine(int M, int N, int splits, const unsigned char* __restrict__ prod,
+                                                      long rows_pad, int cgroups, const int* __restrict__ eA,
+                                                      const int* __restrict__ eB, const __grid_constant__ OzConst c,
+                                                      double2 alpha, double2 beta, double2* __restrict__ C, long ldc) {
+    const int row = blockIdx.y * 128 + (threadIdx.x >> 1);
+    const int h = threadIdx.x & 1;
+    if (row >= M) return;
+    const int cg = blockIdx.x, col0 = 8 * cg + 4 * h;
+    if (col0 >= N) return;
+    uint2 v[kOzMaxMods];
+    // every load of the first split first (independent), then the other splits' residues added byte-wise
+#pragma unroll
+    for (int l = 0; l < kOzMaxMods; ++l)
+        if (l < c.n)
+            v[l] = *reinterpret_cast<const uint2*>(prod + ((long(l) * cgroups + cg) * rows_pad + row) * 16 + 8 * h);
+    double s[8], t[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) s[i] = t[i] = 0.0;
+#pragma unroll
+    for (int l = 0; l < kOzMaxMods; ++l) {
+        if (l >= c.n) break;
+        unsigned acc[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) acc[i] = ((i < 4 ? v[l].x : v[l].y) >> (8 * (i & 3))) & 0xFFu;
+        for (int sp = 1; sp < splits; ++sp) {
             const long z = long(sp) * c.n + l;
-            const uchar4 a = *reinterpret_cast<const uchar4*>(prod + (z * colsB + 2 * col) * rows_pad + r0);
-            const uchar4 b = *reinterpret_cast<const uchar4*>(prod + (z * colsB + 2 * col + 1) * rows_pad + r0);
-            ar[0] += a.x; ar[1] += a.y; ar[2] += a.z; ar[3] += a.w;
-            ai[0] += b.x; ai[1] += b.y; ai[2] += b.z; ai[3] += b.w;
+            const uint2 x = *reinterpret_cast<const uint2*>(prod + ((z * cgroups + cg) * rows_pad + row) * 16 + 8 * h);
+#pragma unroll
+            for (int i = 0; i < 8; ++i) acc[i] += ((i < 4 ? x.x : x.y) >> (8 * (i & 3))) & 0xFFu;
         }
 #pragma unroll
-        for (int t = 0; t < 4; ++t) {
-            const double cr = double(splits > 1 ? oz_umod(ar[t], c.m[l], c.magic[l]) : ar[t]);
-            const double ci = double(splits > 1 ? oz_umod(ai[t], c.m[l], c.magic[l]) : ai[t]);
-            sr[t] = fma(cr, c.wa[l], sr[t]);
-            tr[t] = fma(cr, c.wb[l], tr[t]);
-            si[t] = fma(ci, c.wa[l], si[t]);
-            ti[t] = fma(ci, c.wb[l], ti[t]);
+        for (int i = 0; i < 8; ++i) {
+            const double cv = double(splits > 1 ? oz_umod(acc[i], c.m[l], c.magic[l]) : acc[i]);
+            s[i] = fma(cv, c.wa[l], s[i]);
+            t[i] = fma(cv, c.wb[l], t[i]);
         }
     }
-    const int eb = eB[col];
+    const int ea = eA[row];
     const bool use_beta = beta.x != 0.0 || beta.y != 0.0;
 #pragma unroll
-    for (int t = 0; t < 4; ++t) {
-        const int row = r0 + t;
-        if (row >= M) break;
-        const int ea = eA[row];
+    for (int jj = 0; jj < 4; ++jj) {
+        const int col = col0 + jj;
+        if (col >= N) break;
+        const int eb = eB[col];
         double re, im;
         if (ea == kOzNonFinite || eb == kOzNonFinite) {
             re = im = __longlong_as_double(0x7ff8000000000000ll);
         } else {
             const int e = ea + eb;
-            re = ldexp(oz_frac(sr[t], tr[t]) * c.mprod, -e);
-            im = ldexp(oz_frac(si[t], ti[t]) * c.mprod, -e);
+            re = ldexp(oz_frac(s[2 * jj], t[2 * jj]) * c.mprod, -e);
+            im = ldexp(oz_frac(s[2 * jj + 1], t[2 * jj + 1]) * c.mprod, -e);
         }
         double2* cp = C + long(col) * ldc + row;
         double2 o = make_double2(alpha.x * re - alpha.y * im, alpha.x * im + alpha.y * re);
@@ -640,24 +811,61 @@ void oz_zgemm(char opa, int M, int N, int K, double2 alpha, const OzOperand& a, 
     if (opa == 'N') residues_of_columns<1>(K, N, B, ldb, c, w.b, w.part, s);
     else residues_of_columns<2>(K, N, B, ldb, c, w.b, w.part, s);
 
-    // tiles: 128 rows of op(A) x BN real columns (BN <= 256, a multiple of 16)
+    // tiles: 128 msub rows of op(A) x BN real columns (BN <= 256, a multiple of 16)
     const int colsB = 2 * N;
     const int tn = (colsB + 255) / 256;
     const int BN = int(round_up((colsB + tn - 1) / tn, 16));
-    const int tm = (M + 127) / 128;
+    const int tm128 = (M + 127) / 128;
     const int nk = (a.kr + 127) / 128;
-    // K splits: within the exact int32 range, and enough CTAs (two per SM) to fill the GPU a few times over
-    const long tiles = long(tm) * tn * a.n;
+    int sms = 148, dev = 0;
+    B200_CUDA(cudaGetDevice(&dev));
+    B200_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    // K splits: within the exact int32 range; among those, the fewest waves of tiles times K blocks per tile
+    // (plus a few blocks' worth per tile for its epilogue and pipeline fill) over the SMs
+    const long tiles128 = long(tm128) * tn * a.n;
+    const int msub = (tm128 >= 2 && nk >= 64) ? 2 : 1;  // 256-row tiles for long K (streamed B' read half as often)
+    const long tiles_sp = (long(tm128 + msub - 1) / msub) * tn * a.n;
     int splits = (nk + kOzMaxKbPerSplit - 1) / kOzMaxKbPerSplit;
-    while (tiles * splits < 4L * 296 && (nk + splits) / (splits + 1) >= 8) ++splits;
+    {
+        double best = 1e300;
+        int bs = splits;
+        for (int sp = splits; sp <= 64 && sp <= nk; ++sp) {
+            const long per_sp = (nk + sp - 1) / sp;
+            if (sp > splits && per_sp < 16) break;
+            const long waves = (tiles_sp * sp + sms - 1) / sms;
+            const double cost = double(waves) * double(per_sp + 4) + 0.02 * sp;
+            if (cost < best - 1e-9) {
+                best = cost;
+                bs = sp;
+            }
+        }
+        splits = bs;
+    }
+    (void)tiles128;
     const int per = (nk + splits - 1) / splits;
     splits = (nk + per - 1) / per;
-    B200_CHECK(tm <= 65535 && long(a.n) * splits <= 65535, kInvalidArgument, "int8 GEMM: grid too large");
-    const long rows_pad = round_up(M, 16);
-    w.prod.resize(size_t(splits) * a.n * colsB * rows_pad);
-    const int stage_bytes = kOzATile + BN * 128;
-    int stages = (kOzSmem - 2048) / stage_bytes;
+    // B' of one (plane, column tile) resident in shared memory when it leaves room for 3 stages of A; else
+    // streamed with A, and long K ranges take 256-row tiles (two accumulators: half the re-reads of B')
+    const int b_box = BN * 128;
+    const int fixed = 1024 + 256;  // alignment slack, barriers
+    OzSched sc{tm128, tn, a.n * splits, per, nk, 1, 2, false};
+    int stages;
+    if (tn <= sms && long(per) * b_box + 3L * kOzATile + fixed <= kOzSmem) {
+        sc.resident = true;
+        stages = int((kOzSmem - fixed - long(per) * b_box) / kOzATile);
+    } else {
+        sc.msub = msub;
+        sc.tm = (tm128 + msub - 1) / msub;
+        stages = (kOzSmem - fixed) / (sc.msub * kOzATile + b_box);
+    }
     if (stages > 8) stages = 8;
+    sc.nbuf = sc.msub * BN <= 256 ? 2 : 1;
+    const long T = long(sc.tm) * tn * sc.nz;
+    int grid = int(T < sms ? T : sms);
+    if (sc.resident) grid = int(std::min<long>(long(sms / tn) * tn, long(sc.tm) * sc.nz * tn));
+    const long rows_pad = M;
+    const int cgroups = int(round_up(colsB, 16) / 16);
+    w.prod.resize(size_t(sc.nz) * cgroups * rows_pad * 16);
     const CUtensorMap mA = make_map_u8(a.res.ptr, a.kr, M, a.n, a.kp, 128);
     const CUtensorMap mB = make_map_u8(w.b.res.ptr, w.b.kr, colsB, a.n, w.b.kp, unsigned(BN));
     OzMods md{};
@@ -670,11 +878,12 @@ void oz_zgemm(char opa, int M, int N, int K, double2 alpha, const OzOperand& a, 
     std::call_once(once, [] {
         B200_CUDA(cudaFuncSetAttribute(k_oz_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, kOzSmem));
     });
-    k_oz_gemm<<<dim3(tn, tm, a.n * splits), kOzThreads, kOzSmem, s>>>(mA, mB, M, colsB, BN, stages, nk, per, a.n, md,
-                                                                      w.prod.ptr, rows_pad, err, tc_wait_limit_ns());
+    k_oz_gemm<<<grid, kOzThreads, kOzSmem, s>>>(mA, mB, M, BN, stages, a.n, sc, md, w.prod.ptr, rows_pad, cgroups,
+                                                err, tc_wait_limit_ns());
     launch_check();
-    k_oz_recombine<<<dim3((M + 511) / 512, N), 128, 0, s>>>(M, N, splits, w.prod.ptr, rows_pad, a.exps.ptr,
-                                                            w.b.exps.ptr, c, alpha, beta, C, ldc);
+    B200_CHECK((M + 127) / 128 <= 65535, kInvalidArgument, "int8 GEMM: too many rows");
+    k_oz_recombine<<<dim3(cgroups, (M + 127) / 128), 256, 0, s>>>(M, N, splits, w.prod.ptr, rows_pad, cgroups,
+                                                                  a.exps.ptr, w.b.exps.ptr, c, alpha, beta, C, ldc);
     launch_check();
 }
 

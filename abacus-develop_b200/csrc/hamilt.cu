@@ -165,7 +165,7 @@ void Hamilt::fold_projectors(int ik, cudaStream_t s) {
         B200_CUDA(cudaGetLastError());
     }
     k.oz_ready = false;
-    if (fp64_gemm == 1) {
+    if (fp64_gemm != 0) {
         const int npw = grid->kmaps[ik].npw;
         oz_prepare_a('C', k.nkb, npw, k.vkb.ptr, k.npwx, oz_mods, k.vkb_oz, oz_setup, s);
         k.vkbd_oz.resize(size_t(nspin));
@@ -180,7 +180,8 @@ void Hamilt::fold_projectors(int ik, cudaStream_t s) {
 }
 
 void Hamilt::set_fp64_gemm(int mode, int nmods) {
-    B200_CHECK(mode == 0 || mode == 1, kInvalidArgument, "FP64 GEMM mode must be 0 (cuBLAS) or 1 (int8 tensor cores)");
+    B200_CHECK(mode >= 0 && mode <= 2, kInvalidArgument,
+               "FP64 GEMM mode must be 0 (cuBLAS), 1 (int8 tensor cores from 48 bands) or 2 (int8 always)");
     B200_CHECK(nmods >= kOzMinMods && nmods <= kOzMaxMods, kInvalidArgument, "number of moduli must be 12..16");
     fp64_gemm = mode;
     oz_mods = nmods;
@@ -283,7 +284,7 @@ void Hamilt::hpsi(int ik, int spin, int nb, int ld, const T* psi, T* hpsi, int m
     B200_CHECK(k.folded, kInvalidArgument, "projectors and D not both set for this k-point");
     const T* vkbd = f64 ? reinterpret_cast<const T*>(k.vkbd.ptr + size_t(spin) * nkb * k.npwx)
                         : reinterpret_cast<const T*>(k.vkbdf.ptr + size_t(spin) * nkb * k.ldf);
-    const bool oz = f64 && fp64_gemm == 1 && k.oz_ready;
+    const bool oz = f64 && k.oz_ready && (fp64_gemm == 2 || (fp64_gemm == 1 && nb >= kOzMinBands));
     if (oz) W.tcw.ensure();  // the int8 GEMM reports a bounded wait that ran out in the same error word
     auto projections = [&](cudaStream_t st) {
         if constexpr (f64) {

@@ -89,8 +89,11 @@ struct Hamilt {
     DeviceArray<double> deeq;
     HpsiWork work;  // default scratch for callers that do not bring their own
     int chunk_override = 0;  // bands per stick-buffer chunk chosen by the autotuner (0 = 48 MB rule)
-    // FP64 projector products: 1 = int8 tensor cores (exact modular emulation, oz_mods moduli), 0 = cuBLAS
+    // FP64 projector products: 0 = cuBLAS ZGEMM; int8 tensor cores (exact modular emulation, oz_mods moduli)
+    // 1 = for calls of at least kOzMinBands bands (each call reads the projectors' whole residue form, twice the
+    // bytes of the FP64 projectors, so narrow calls go to cuBLAS, whose cost scales with the bands), 2 = always
     int fp64_gemm = 1;
+    static constexpr int kOzMinBands = 48;
     int oz_mods = 16;
     OzWorkspace oz_setup;  // scratch of the projector residues built at fold time
     VnlTables vnl;           // projector tables for on-device getvnl
@@ -110,7 +113,8 @@ struct Hamilt {
     // fold D into the projectors of k-point ik (all spins), on stream s; nothing if either is not set.  With
     // fp64_gemm = 1 also the int8 residue forms of vkb and vkbd.
     void fold_projectors(int ik, cudaStream_t s);
-    // choose the FP64 projector products (mode 1 int8 tensor cores with nmods moduli, 0 cuBLAS) and re-fold
+    // choose the FP64 projector products (0 cuBLAS, 1 int8 tensor cores from kOzMinBands bands, 2 int8 always;
+    // nmods moduli) and re-fold
     void set_fp64_gemm(int mode, int nmods);
     // mode 0 = full H, 1 = kinetic + local only (overwrites hpsi), 2 = nonlocal only (accumulates)
     template <typename T>

@@ -262,7 +262,7 @@ class Server {
         b += size_t(c.nkb + 1) * nb * 16 * 4 + (size_t(16) << 20);
         // FP64 projector products on the int8 tensor cores: psi residues (2 real rows per band, one byte per
         // modulus and real entry) and the per-modulus product residues of H psi
-        if (c.h->h->fp64_gemm == 1) b += size_t(c.h->h->oz_mods) * nb * (size_t(4) * c.npwx + 2 * size_t(c.npwx + 16));
+        if (c.h->h->fp64_gemm != 0) b += size_t(c.h->h->oz_mods) * nb * (size_t(4) * c.npwx + 2 * size_t(c.npwx + 16));
         return b;
     }
 

@@ -461,8 +461,8 @@ class HamiltPW:
         call("b200_hamilt_set_plane_variant", self._h, int(variant))
 
     def set_fp64_gemm(self, mode, nmods=16):
-        """FP64 projector products: mode 1 on the int8 tensor cores (exact modular emulation with nmods
-        moduli, the default), 0 on cuBLAS ZGEMM.  Rebuilds the projector residue forms."""
+        """FP64 projector products: 0 cuBLAS ZGEMM; int8 tensor cores (exact modular emulation with nmods
+        moduli) for calls of at least 48 bands (1, the default) or always (2).  Rebuilds the residue forms."""
         call("b200_hamilt_set_fp64_gemm", self._h, int(mode), int(nmods))
 
     def solve_kpoints(self, iks, precond_ds, psis, ld_psi, nband, thr, maxiter, david_ndim=4, precision=PREC_FP64,

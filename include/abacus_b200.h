@@ -215,11 +215,13 @@ int b200_hamilt_autotune(b200_hamilt* h, int ik, int nbands, int ld, const void*
  * default.  All variants give the same results within rounding.  No counterpart in the reference. */
 int b200_hamilt_set_plane_variant(b200_hamilt* h, int variant);
 /* The FP64 projector products of Nonlocal::act (nonlocal_pw.cpp:255-276, becp = vkb^H psi and
- * H psi += vkb (D becp), here with D folded into the projectors) for this handle: mode 1 (the default) on
- * the int8 tensor cores, exact modular emulation of the FP64 product with nmods (12..16, default 16)
- * moduli, as b200_zgemm_i8; mode 0 cuBLAS ZGEMM.  Mode 1 keeps the projectors also in residue form
- * (2 x nmods bytes per projector entry and spin) and each H|psi> caller about 6 x nmods bytes per
- * psi entry of scratch.  Rebuilds the projector forms of every k-point (synchronous). */
+ * H psi += vkb (D becp), here with D folded into the projectors) for this handle: on the int8 tensor
+ * cores (exact modular emulation of the FP64 product with nmods (12..16, default 16) moduli, as
+ * b200_zgemm_i8) for H|psi> calls of at least 48 bands (mode 1, the default) or for every call (mode 2),
+ * else cuBLAS ZGEMM (mode 0, and narrower calls in mode 1: the int8 path reads the projectors' whole
+ * residue form per call).  Modes 1 and 2 keep the projectors also in residue form (2 x nmods bytes per
+ * projector entry and spin) and each H|psi> caller about 6 x nmods bytes per psi entry of scratch.
+ * Rebuilds the projector forms of every k-point (synchronous). */
 int b200_hamilt_set_fp64_gemm(b200_hamilt* h, int mode, int nmods);
 /* Bands per stick-buffer chunk of this handle's local pass (0 = the default: the largest chunk whose
  * stick buffer stays within 48 MB).  What b200_hamilt_autotune sets.  No counterpart in the reference. */

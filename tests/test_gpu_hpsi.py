@@ -32,9 +32,10 @@ def _setup(pkg, spec, kpt=None, nb=None):
     return wl, ref, psi, nb, npwx
 
 
+@pytest.mark.parametrize("gemm", [0, 2])  # FP64 projector products: cuBLAS ZGEMM / int8 tensor cores
 @pytest.mark.parametrize("cfg", ["si2", "diamond8", "diamond8_k", "diamond16", "diamond8_grid40", "diamond8_grid96_k",
                                  "diamond8_grid128"])
-def test_hpsi_fp64_matches_oracle(pkg, cfg):
+def test_hpsi_fp64_matches_oracle(pkg, cfg, gemm):
     S = pkg.synth
     if cfg == "si2":
         spec, kpt, nb = S.serving_cells()[0], None, 8
@@ -55,6 +56,7 @@ def test_hpsi_fp64_matches_oracle(pkg, cfg):
     wl, ref, psi, nb, ld = _setup(pkg, spec, kpt, nb)
     href = ref.hpsi(psi, nb, ld)
     h = pkg.pwdft.device_hamilt(wl, pkg.pwdft.PREC_FP64)
+    h.set_fp64_gemm(gemm)
     pd = torch.from_numpy(psi).cuda()
     hd = torch.full_like(pd, complex(7.0, -3.0))  # garbage: hPsi must overwrite, padding included
     h.hpsi(0, pd, hd, nb, ld)
