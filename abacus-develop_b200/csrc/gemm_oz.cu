@@ -42,6 +42,7 @@ namespace {
 
 using namespace tcu;
 
+// pairwise coprime; the first modulus is 256 (oz_res relies on it)
 constexpr int kOzMods[kOzMaxMods] = {256, 255, 253, 251, 247, 241, 239, 233, 229, 227, 223, 217, 211, 199, 197, 193};
 constexpr int kOzNonFinite = -2147483647 - 1;  // row exponent marking a row with a NaN or infinite entry
 constexpr int kOzSeg = 4096;                   // complex entries per column segment of the norm / residue kernels
@@ -131,6 +132,7 @@ __device__ __forceinline__ unsigned oz_umod(unsigned x, unsigned m, unsigned mag
 }
 // (u - 2^62 + h) mod m for u < 2^63: three 21-bit pieces
 __device__ __forceinline__ unsigned oz_res(unsigned long long u, const OzConst& c, int l) {
+    if (l == 0) return (unsigned(u) + 128u) & 0xFFu;  // m_0 = 256 (h = 128): 2^62 = 0 mod 256
     const unsigned p0 = unsigned(u) & 0x1FFFFFu, p1 = unsigned(u >> 21) & 0x1FFFFFu, p2 = unsigned(u >> 42);
     return oz_umod(p2 * c.c42[l] + p1 * c.c21[l] + p0 + c.off62[l], c.m[l], c.magic[l]);
 }
@@ -224,7 +226,9 @@ __global__ void __launch_bounds__(256) k_oz_res_cols(int K, const double2* __res
             ur[t] = scale(x.x);
             ui[t] = scale(x.y);
         }
-        for (int l = 0; l < c.n; ++l) {
+#pragma unroll
+        for (int l = 0; l < kOzMaxMods; ++l) {
+            if (l >= c.n) break;
             const unsigned hs = c.h[l];
             unsigned rr[4], ri[4];
 #pragma unroll
@@ -285,7 +289,9 @@ __global__ void __launch_bounds__(256) k_oz_res_rows(int M, int K, const double2
         const int k = k0 + kk;
         const double2 x = (row < M && k < K && !bad) ? X[row + long(k) * ld] : make_double2(0.0, 0.0);
         const unsigned long long ur = scale(x.x), ui = scale(x.y);
-        for (int l = 0; l < c.n; ++l) {
+#pragma unroll
+        for (int l = 0; l < kOzMaxMods; ++l) {
+            if (l >= c.n) break;
             tile[l][tx][2 * kk] = (unsigned char)oz_sym(oz_res(ur, c, l), c.h[l]);
             tile[l][tx][2 * kk + 1] = (unsigned char)oz_sym(oz_res(ui, c, l), c.h[l]);
         }
