@@ -5,7 +5,8 @@ Workload (default): 64-atom diamond supercell, a = 20.52 bohr, ecut 50 Ry,
 Gamma point, seeded synthetic V_eff / projectors / D / psi (no dataset).
 
 One step = one H|psi> (kinetic + local V_eff via the stick/plane FFT +
-nonlocal projectors) on the whole 160-band block, inputs resident in HBM.
+nonlocal projectors, whose FP64 products run on the int8 tensor cores as an
+exact modular emulation) on the whole 160-band block, inputs resident in HBM.
 psi + hpsi + projectors (about 690 MB) exceed the 126 MB L2, so no flush is
 needed between steps.
 
@@ -17,8 +18,11 @@ Besides the headline line, the same JSON line carries:
   e2e           the same H|psi> from pinned host psi to pinned host hpsi through b200_hamilt_hpsi_host
                 (uploads, H|psi> pieces and downloads overlapped);
   psi_to_rho    rho(r) += w|psi(r)|^2 over the 160 bands (ElecStatePW::psiToRho);
+  nonlocal      the projector part of the FP64 step, with the int8 tensor-core products and with cuBLAS;
   tc_gemm       the 3xTF32 tensor-core complex GEMM on the 216-atom subspace shapes and the projector
                 shapes (--gemm-only runs only this, for profiling);
+  fp64_gemm     FP64 complex GEMM (gemm_op) on the projector and 216-atom subspace shapes: cuBLAS ZGEMM
+                against the FP64 tensor peak, and the int8 tensor-core emulation (b200_zgemm_i8);
   davidson      FP64 vs mixed Davidson on the 64-atom cell: wall time to thr 1e-9 and the time after which
                 every eigenvalue stays within 1e-8 Ry of an FP64 solve to 1e-11 (per-iteration traces);
   davidson_216  the same on the 216-atom cell (128^3 grid, 480 bands, 1728 projectors);
@@ -390,6 +394,14 @@ def run_ours(args, ws, rank, local):
     ms64 = max_over_ranks(ms64, ws)
     ms32 = max_over_ranks(time_steps(step32, args.steps, stream), ws)
     ms_loc64 = time_steps(local64, args.steps, stream)
+    # the same FP64 step with the projector products on cuBLAS ZGEMM instead of the int8 tensor cores
+    h64.set_fp64_gemm(0)
+    for _ in range(2):
+        step64()
+    ms64_cublas = time_steps(step64, args.steps, stream)
+    h64.set_fp64_gemm(1)
+    for _ in range(2):
+        step64()
     ms_loc32 = time_steps(local32, args.steps, stream)
 
     # end to end through the public API: pinned host psi -> H|psi> -> pinned host hpsi, every step; the
@@ -449,7 +461,11 @@ def run_ours(args, ws, rank, local):
                      "mixed": {"achieved": ach32, "frac": ach32 / hbm_peak, "ms": ms_loc32,
                                "algorithmic_bytes": b_local32, "t_roof_ms": t_roof32 * 1e3,
                                "frac_of_t_roof": t_roof32 / (ms_loc32 * 1e-3)}},
-        "nonlocal": {"flops": nl_flops, "ms_fp64": ms64 - ms_loc64, "tflops_fp64": nl_flops / ((ms64 - ms_loc64) * 1e-3) / 1e12},
+        "nonlocal": {"flops": nl_flops, "ms_fp64": ms64 - ms_loc64,
+                     "tflops_fp64": nl_flops / ((ms64 - ms_loc64) * 1e-3) / 1e12,
+                     "path": "int8 tensor cores, exact modular emulation of the FP64 products (16 moduli)",
+                     "ms_fp64_cublas": ms64_cublas - ms_loc64,
+                     "bands_s_with_cublas": ws * nb / (ms64_cublas * 1e-3)},
         "e2e": {"value": ws * nb / (ms_e2e * 1e-3), "unit": "bands/s",
                 "h2d_bytes_per_step": psi.numel() * 16, "d2h_bytes_per_step": hpsi.numel() * 16},
         "gpu_launches": launches,
@@ -506,6 +522,9 @@ def summary_of(line):
            "e2e_bands_s": _r(line.get("e2e", {}).get("value"), 4),
            "local_frac": _r(line.get("roofline", {}).get("frac")),
            "local_frac_mixed": _r(line.get("roofline", {}).get("mixed", {}).get("frac"))}
+    nl = line.get("nonlocal") or {}
+    if "ms_fp64_cublas" in nl:
+        out["nonlocal_ms_int8_vs_cublas"] = [_r(nl.get("ms_fp64")), _r(nl.get("ms_fp64_cublas"))]
     for key in ("davidson", "davidson_216"):
         d = line.get(key)
         if isinstance(d, dict) and "fp64_s" in d:
@@ -1010,9 +1029,10 @@ GEMM64_SHAPES = [("C", "N", 512, 160, 51627), ("N", "N", 51627, 160, 512), ("N",
 
 
 def gemm64_bench(pkg, peaks_tf, reps=5):
-    """The FP64 complex GEMM the plain path calls (gemm_op<complex<double>, GPU>: cuBLAS ZGEMM through
-    b200_gemm_op_f64) on the shapes above, against the measured FP64 tensor-core peak: a complex product
-    is four real products on the FP64 tensor pipe, so 8 M N K flop at the DMMA rate is its ceiling."""
+    """The FP64 complex GEMM of gemm_op<complex<double>, GPU> on the shapes above: cuBLAS ZGEMM through
+    b200_gemm_op_f64 against the measured FP64 tensor-core peak (a complex product is four real products on
+    the FP64 tensor pipe, so 8 M N K flop at the DMMA rate is its ceiling), and the int8 tensor-core
+    emulation b200_zgemm_i8 (with both operands' residues built in every call)."""
     import ctypes as C
     import torch
     lib = pkg._lib.load()
@@ -1042,8 +1062,25 @@ def gemm64_bench(pkg, peaks_tf, reps=5):
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1) / reps
         tf = 8.0 * M * N * K / (ms * 1e-3) / 1e12
+
+        # the same product on the int8 tensor cores (b200_zgemm_i8: residues of both operands every call)
+        def call_i8():
+            rc = lib.b200_zgemm_i8(ta.encode(), tb.encode(), M, N, K, one, a.data_ptr(), rows_a, b.data_ptr(), K, zero,
+                                   c.data_ptr(), M, 16, None)
+            assert rc == 0
+
+        for _ in range(2):
+            call_i8()
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(reps):
+            call_i8()
+        e1.record()
+        torch.cuda.synchronize()
+        ms8 = e0.elapsed_time(e1) / reps
         out.append({"op": ta + tb, "M": M, "N": N, "K": K, "ms": ms, "tflops": tf,
-                    "frac_of_dmma_peak": tf / peaks_tf["dmma_fp64_tflops"]})
+                    "frac_of_dmma_peak": tf / peaks_tf["dmma_fp64_tflops"], "int8_ms": ms8,
+                    "int8_equiv_tflops": 8.0 * M * N * K / (ms8 * 1e-3) / 1e12})
         del a, b, c
         torch.cuda.empty_cache()
     return out
