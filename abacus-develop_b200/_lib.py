@@ -106,6 +106,9 @@ _SIGS = {
     "b200_zgemm_i8": ([C.c_char, C.c_char, i32, i32, i32, pf64, vp, i32, vp, i32, pf64, vp, i32, i32, vp], i32),
     "b200_zgemm_i8_error": ([pi32], i32),
     "b200_hamilt_set_fp64_gemm": ([vp, i32, i32], i32),
+    "b200_hamilt_set_veff_nc": ([vp, vp], i32),
+    "b200_hamilt_set_deeq_nc": ([vp, i32, pi32, pi32, i32, i32, i32, vp], i32),
+    "b200_hamilt_hpsi_nc": ([vp, i32, i32, i32, vp, vp, vp], i32),
     "b200_zgemm_i8_constants": ([i32, C.c_longlong, pi32, pf64, pf64, pf64, pi32], i32),
     "b200_gemv_op_f64": ([C.c_char, i32, i32, pf64, vp, i32, vp, i32, pf64, vp, i32, vp], i32),
     "b200_dot_real_op_f64": ([i32, vp, vp, i32, pf64, vp], i32),

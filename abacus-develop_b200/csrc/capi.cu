@@ -306,6 +306,28 @@ int b200_hamilt_set_deeq(b200_hamilt* h, int ntype, const int* na, const int* nh
         h->h->set_deeq(ntype, na, nh, nspin, dx, dy, dz, deeq);
     });
 }
+int b200_hamilt_set_veff_nc(b200_hamilt* h, const double* veff4) {
+    return guarded([&] {
+        B200_CHECK(h && veff4, b200::kInvalidArgument, "NULL argument");
+        h->h->set_veff_nc(veff4);
+    });
+}
+int b200_hamilt_set_deeq_nc(b200_hamilt* h, int ntype, const int* na, const int* nh, int dx, int dy, int dz,
+                            const void* deeq_nc) {
+    return guarded([&] {
+        B200_CHECK(h && na && nh && deeq_nc, b200::kInvalidArgument, "NULL argument");
+        h->h->set_deeq_nc(ntype, na, nh, dx, dy, dz, (const double2*)deeq_nc);
+    });
+}
+int b200_hamilt_hpsi_nc(b200_hamilt* h, int ik, int nbands, int ld, const void* psi, void* hpsi, void* stream) {
+    return guarded([&] {
+        B200_CHECK(h && psi && hpsi, b200::kInvalidArgument, "NULL argument");
+        if (h->h->precision == B200_PREC_FP64)
+            h->h->hpsi_nc<double2>(ik, nbands, ld, (const double2*)psi, (double2*)hpsi, S(stream));
+        else
+            h->h->hpsi_nc<float2>(ik, nbands, ld, (const float2*)psi, (float2*)hpsi, S(stream));
+    });
+}
 static int hpsi_impl(b200_hamilt* h, int ik, int spin, int nb, int ld, const void* psi, void* hpsi, int mode, void* st) {
     return guarded([&] {
         B200_CHECK(h && psi && hpsi, b200::kInvalidArgument, "NULL argument");

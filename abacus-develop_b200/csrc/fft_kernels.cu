@@ -253,6 +253,102 @@ __global__ void __launch_bounds__(512) k_plane(PlaneMapView pm, int nx, int ny, 
     for (int s = tid; s < pm.nst; s += nthr) plane[s] = A[pm.xc[s] * ldy + pm.sy[s]];
 }
 
+// ---- non-collinear (npol = 2) local pass: the plane pass split at the real-space product ----
+// (2a) inverse y and x transforms of spinor column blockIdx.x at plane z = blockIdx.y; the real-space plane
+// goes to r[col][z][y][x] (rows of nx)
+template <typename T>
+__global__ void __launch_bounds__(512) k_plane_inv_r(PlaneMapView pm, int nx, int ny, int nz, FftPlan1D px, FftPlan1D py,
+                                                     const T* __restrict__ twx, const T* __restrict__ twy,
+                                                     const T* __restrict__ sb, T* __restrict__ r) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int ldy = ny | 1, ldx = nx | 1;
+    T* A = reinterpret_cast<T*>(smem_raw);
+    T* C = A + pm.nxc * ldy;
+    T* R1 = C + kPlaneCols * ldy;
+    T* R2 = R1 + kPlaneRows * ldx;
+    const int tid = threadIdx.x, nthr = blockDim.x;
+    const int col = blockIdx.x, z = blockIdx.y;
+    for (int i = tid; i < pm.nxc * ldy; i += nthr) A[i] = czero<T>();
+    __syncthreads();
+    const T* plane = sb + (size_t(col) * nz + z) * pm.nst;
+    for (int st = tid; st < pm.nst; st += nthr) A[pm.xc[st] * ldy + pm.sy[st]] = plane[st];
+    __syncthreads();
+    for (int c = 0; c < pm.nxc; c += kPlaneCols)
+        fft_batch<T, +1>(A + c * ldy, C, min(kPlaneCols, pm.nxc - c), 1, ldy, py, twy, tid, nthr);
+    T* out = r + (size_t(col) * nz + z) * size_t(ny) * nx;
+    for (int y0 = 0; y0 < ny; y0 += kPlaneRows) {
+        const int nr = min(kPlaneRows, ny - y0);
+        for (int i = tid; i < nr * ldx; i += nthr) R1[i] = czero<T>();
+        __syncthreads();
+        for (int e = tid; e < nr * pm.nxc; e += nthr) {
+            const int rr = e / pm.nxc;
+            const int c = e - rr * pm.nxc;
+            R1[rr * ldx + pm.xpos[c]] = A[c * ldy + y0 + rr];
+        }
+        __syncthreads();
+        fft_batch<T, +1>(R1, R2, nr, 1, ldx, px, twx, tid, nthr);
+        for (int e = tid; e < nr * nx; e += nthr) {
+            const int rr = e / nx;
+            const int x = e - rr * nx;
+            out[size_t(y0 + rr) * nx + x] = R1[rr * ldx + x];
+        }
+        __syncthreads();
+    }
+}
+
+// (2b) the 2x2 spin potential of veff_pw_op's npol = 2 form (veff_op.cpp:20-37) on spinor column
+// blockIdx.x (component c = column & 1, partner column ^ 1) at plane z = blockIdx.y:
+//   up' = up (V0 + V3) + dn (V1 - i V2),   dn' = dn (V0 - V3) + up (V1 + i V2),
+// then the forward x and y transforms back into the column's sticks.  v4: the four components, (z, y, x).
+template <typename T, typename R>
+__global__ void __launch_bounds__(512) k_plane_fwd_nc(PlaneMapView pm, int nx, int ny, int nz, FftPlan1D px,
+                                                      FftPlan1D py, const T* __restrict__ twx,
+                                                      const T* __restrict__ twy, const R* __restrict__ v4,
+                                                      const T* __restrict__ r, T* __restrict__ sb) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int ldy = ny | 1, ldx = nx | 1;
+    T* A = reinterpret_cast<T*>(smem_raw);
+    T* C = A + pm.nxc * ldy;
+    T* R1 = C + kPlaneCols * ldy;
+    T* R2 = R1 + kPlaneRows * ldx;
+    const int tid = threadIdx.x, nthr = blockDim.x;
+    const int col = blockIdx.x, z = blockIdx.y;
+    const bool up = (col & 1) == 0;
+    const size_t N = size_t(nx) * ny * nz, P = size_t(ny) * nx;
+    const T* own = r + (size_t(col) * nz + z) * P;
+    const T* oth = r + (size_t(col ^ 1) * nz + z) * P;
+    const R* v0 = v4 + size_t(z) * P;
+    for (int y0 = 0; y0 < ny; y0 += kPlaneRows) {
+        const int nr = min(kPlaneRows, ny - y0);
+        for (int e = tid; e < nr * nx; e += nthr) {
+            const int rr = e / nx;
+            const int x = e - rr * nx;
+            const size_t i = size_t(y0 + rr) * nx + x;
+            const T a = own[i], b = oth[i];
+            const R va = v0[i], vb = v0[i + N], vc = v0[i + 2 * N], vd = v0[i + 3 * N];
+            // own component: (V0 +- V3) a + (V1 -+ i V2) b
+            const R d = up ? va + vd : va - vd;
+            const R sg = up ? R(-1) : R(1);
+            T o;
+            o.x = d * a.x + vb * b.x - sg * vc * b.y;
+            o.y = d * a.y + vb * b.y + sg * vc * b.x;
+            R1[rr * ldx + x] = o;
+        }
+        __syncthreads();
+        fft_batch<T, -1>(R1, R2, nr, 1, ldx, px, twx, tid, nthr);
+        for (int e = tid; e < nr * pm.nxc; e += nthr) {
+            const int rr = e / pm.nxc;
+            const int c = e - rr * pm.nxc;
+            A[c * ldy + y0 + rr] = R1[rr * ldx + pm.xpos[c]];
+        }
+        __syncthreads();
+    }
+    for (int c = 0; c < pm.nxc; c += kPlaneCols)
+        fft_batch<T, -1>(A + c * ldy, C, min(kPlaneCols, pm.nxc - c), 1, ldy, py, twy, tid, nthr);
+    T* plane = sb + (size_t(col) * nz + z) * pm.nst;
+    for (int st = tid; st < pm.nst; st += nthr) plane[st] = A[pm.xc[st] * ldy + pm.sy[st]];
+}
+
 // (3) sticks -> sphere (forward z FFT), + kinetic term, store/accumulate hpsi
 template <typename T, typename R>
 __global__ void __launch_bounds__(256) k_zpass_fwd(StickMapView sm, FftPlan1D pz, const T* __restrict__ twz,
@@ -456,6 +552,39 @@ void launch_hpsi_local(const PWGrid& g, int ik, const R* veff_zyx, const R* veff
     B200_CUDA(cudaGetLastError());
 }
 
+template <typename T, typename R>
+void launch_hpsi_local_nc(const PWGrid& g, int ik, const R* veff4_zyx, int ncols, int ld, const T* psi, T* hpsi,
+                          T* stickbuf, T* rbuf, double tpiba2, cudaStream_t s) {
+    if (ncols <= 0) return;
+    B200_CHECK(ncols <= 65535 && ncols % 2 == 0, kInvalidArgument, "npol = 2: an even number of spinor columns, at most 65535");
+    const size_t zs = zpass_smem(g, sizeof(T));
+    const size_t ps = plane_smem(g, sizeof(T));
+    B200_CHECK(ps <= 227 * 1024, kCapacityError, "plane pass does not fit in shared memory for this grid");
+    const StickMapView sm = g.stick_view(ik);
+    const dim3 gz(ceil_div(g.nst, kStickTile), ncols);
+    set_smem(k_zpass_inv<T>, zs);
+    k_zpass_inv<T><<<gz, 256, zs, s>>>(sm, g.az.plan, tw_of<T>(g.az), psi, ld, stickbuf);
+    note_launch();
+    B200_CUDA(cudaGetLastError());
+    set_smem(k_plane_inv_r<T>, ps);
+    k_plane_inv_r<T><<<dim3(ncols, g.nz), 512, ps, s>>>(g.plane_view(), g.nx, g.ny, g.nz, g.ax.plan, g.ay.plan,
+                                                       tw_of<T>(g.ax), tw_of<T>(g.ay), stickbuf, rbuf);
+    note_launch();
+    B200_CUDA(cudaGetLastError());
+    set_smem(k_plane_fwd_nc<T, R>, ps);
+    k_plane_fwd_nc<T, R><<<dim3(ncols, g.nz), 512, ps, s>>>(g.plane_view(), g.nx, g.ny, g.nz, g.ax.plan, g.ay.plan,
+                                                           tw_of<T>(g.ax), tw_of<T>(g.ay), veff4_zyx, rbuf, stickbuf);
+    note_launch();
+    B200_CUDA(cudaGetLastError());
+    const KMap& km = g.kmaps[ik];
+    const R* gk2 = std::is_same<R, double>::value ? (const R*)km.gk2.ptr : (const R*)km.gk2f.ptr;
+    set_smem(k_zpass_fwd<T, R>, zs);
+    k_zpass_fwd<T, R><<<gz, 256, zs, s>>>(sm, g.az.plan, tw_of<T>(g.az), stickbuf, psi, hpsi, ld, km.npw, gk2, R(tpiba2),
+                                          R(1.0 / double(g.nxyz())), 0);
+    note_launch();
+    B200_CUDA(cudaGetLastError());
+}
+
 template <typename T>
 void launch_recip_to_real(const PWGrid& g, int ik, const T* in, T* out, T* aux, int add, double factor, cudaStream_t s) {
     using R = typename RealOf<T>::type;
@@ -519,6 +648,10 @@ template void launch_hpsi_local<double2, double>(const PWGrid&, int, const doubl
 template void launch_hpsi_local<float2, float>(const PWGrid&, int, const float*, const float*, int, int, const float2*,
                                                float2*, float2*,
                                                double, int, cudaStream_t);
+template void launch_hpsi_local_nc<double2, double>(const PWGrid&, int, const double*, int, int, const double2*,
+                                                    double2*, double2*, double2*, double, cudaStream_t);
+template void launch_hpsi_local_nc<float2, float>(const PWGrid&, int, const float*, int, int, const float2*, float2*,
+                                                  float2*, float2*, double, cudaStream_t);
 template void launch_recip_to_real<double2>(const PWGrid&, int, const double2*, double2*, double2*, int, double, cudaStream_t);
 template void launch_recip_to_real<float2>(const PWGrid&, int, const float2*, float2*, float2*, int, double, cudaStream_t);
 template void launch_real_to_recip<double2>(const PWGrid&, int, const double2*, double2*, double2*, int, double, cudaStream_t);

@@ -1,5 +1,7 @@
 // Device Hamiltonian: the Ekinetic -> Veff -> Nonlocal chain of HamiltPW
 // (hamilt_pw.cpp:21-114) as one fused local pass plus the projector GEMMs.
+#include <algorithm>
+
 #include "functors.h"
 #include "hamilt.h"
 
@@ -49,6 +51,39 @@ __global__ void k_fold_deeq(int nkb, int npwx, int ldo, FoldTypes ft, int spin, 
         o.x = re;
         o.y = im;
         out[long(j) * ldo + g] = o;
+    }
+}
+
+// npol = 2: W_s[x][g] = sum_k D_s(iat, k, x) vkb[row0 + k][g] for the four spin blocks s (block s at rows
+// s * nkb, row pitch ldo): add_nonlocal_pp's spinor form (nonlocal_op.cpp:43-74: ps_up = D0 becp_up +
+// D1 becp_dn, ps_dn = D2 becp_up + D3 becp_dn, then H psi += vkb ps) moved onto the projectors
+template <typename To>
+__global__ void k_fold_deeq_nc(int nkb, int npwx, int ldo, FoldTypes ft, int dx, int dy, int dz,
+                               const double2* __restrict__ dnc, const double2* __restrict__ vkb, To* __restrict__ out) {
+    const long total = 4L * nkb * npwx;
+    for (long t = blockIdx.x * long(blockDim.x) + threadIdx.x; t < total; t += long(gridDim.x) * blockDim.x) {
+        const int g = int(t % npwx);
+        const long q = t / npwx;
+        const int sblk = int(q / nkb);
+        const int j = int(q - long(sblk) * nkb);
+        int it = 0;
+        while (it + 1 < ft.ntype && j >= ft.sum0[it + 1]) ++it;
+        const int nh = ft.nh[it];
+        const int ia = (j - ft.sum0[it]) / nh;
+        const int x = (j - ft.sum0[it]) - ia * nh;
+        const int row0 = ft.sum0[it] + ia * nh;
+        const double2* d = dnc + (long(sblk * dx + ft.iat0[it] + ia) * dy) * dz + x;  // D_s(iat, k, x) at d[k dz]
+        double re = 0.0, im = 0.0;
+        for (int k = 0; k < nh; ++k) {
+            const double2 c = d[long(k) * dz];
+            const double2 v = vkb[long(row0 + k) * npwx + g];
+            re = fma(c.x, v.x, fma(-c.y, v.y, re));
+            im = fma(c.x, v.y, fma(c.y, v.x, im));
+        }
+        To o;
+        o.x = re;
+        o.y = im;
+        out[q * ldo + g] = o;
     }
 }
 
@@ -131,10 +166,37 @@ void Hamilt::set_deeq(int ntype_, const int* na_, const int* nh_, int nspin_, in
     B200_CUDA(cudaStreamSynchronize(0));
 }
 
-void Hamilt::fold_projectors(int ik, cudaStream_t s) {
-    NonlocalK& k = nl[ik];
-    k.folded = false;
-    if (k.nkb <= 0 || !deeq.ptr || k.vkb.ptr == nullptr) return;
+void Hamilt::set_veff_nc(const double* veff4_d) {
+    const size_t N = size_t(grid->nxyz());
+    veff_nc_zyx.resize(4 * N);
+    veff_nc_zyxf.resize(4 * N);
+    for (int c = 0; c < 4; ++c) {
+        launch_transpose_veff<double>(*grid, veff4_d + c * N, veff_nc_zyx.ptr + c * N, 0);
+        launch_transpose_veff<float>(*grid, veff4_d + c * N, veff_nc_zyxf.ptr + c * N, 0);
+    }
+    B200_CUDA(cudaStreamSynchronize(0));
+    has_veff_nc = true;
+}
+
+void Hamilt::set_deeq_nc(int ntype_, const int* na_, const int* nh_, int dx_, int dy_, int dz_,
+                         const double2* deeq_nc_d) {
+    B200_CHECK(ntype_ >= 0 && dx_ >= 0 && dy_ >= 0 && dz_ >= 0, kInvalidArgument, "bad deeq_nc shape");
+    ntype = ntype_;
+    na.assign(na_, na_ + ntype);
+    nh.assign(nh_, nh_ + ntype);
+    nc_dx = dx_;
+    nc_dy = dy_;
+    nc_dz = dz_;
+    const long n = 4L * dx_ * dy_ * dz_;
+    deeq_nc.resize(size_t(n));
+    if (n) B200_CUDA(cudaMemcpyAsync(deeq_nc.ptr, deeq_nc_d, n * sizeof(double2), cudaMemcpyDeviceToDevice, 0));
+    for (int ik = 0; ik < int(nl.size()); ++ik) fold_projectors(ik, 0);
+    B200_CUDA(cudaStreamSynchronize(0));
+}
+
+// the atom types of D for the folding kernels (checked against the projector count)
+static FoldTypes fold_types(int ntype, const std::vector<int>& na, const std::vector<int>& nh, int nkb, int natoms_max,
+                            int nh_max) {
     B200_CHECK(ntype >= 1 && ntype <= kVnlMaxTypes, kInvalidArgument, "1..8 atom types supported by the projector fold");
     FoldTypes ft{};
     ft.ntype = ntype;
@@ -143,13 +205,56 @@ void Hamilt::fold_projectors(int ik, cudaStream_t s) {
         ft.sum0[it] = sum;
         ft.iat0[it] = iat;
         ft.nh[it] = nh[it];
-        B200_CHECK(nh[it] >= 1 && nh[it] <= dy && nh[it] <= dz, kInvalidArgument, "nh larger than deeq's nhm");
+        B200_CHECK(nh[it] >= 1 && nh[it] <= nh_max, kInvalidArgument, "nh larger than D's nhm");
         sum += na[it] * nh[it];
         iat += na[it];
     }
     ft.sum0[ntype] = sum;
-    B200_CHECK(sum == k.nkb, kInvalidArgument, "sum of na*nh over types differs from nkb");
-    B200_CHECK(iat <= dx, kInvalidArgument, "more atoms than deeq's first dimension");
+    B200_CHECK(sum == nkb, kInvalidArgument, "sum of na*nh over types differs from nkb");
+    B200_CHECK(iat <= natoms_max, kInvalidArgument, "more atoms than D's first dimension");
+    return ft;
+}
+
+// npol = 2: the spin blocks of D into the projectors of k-point ik (FP64, FP32, residue forms)
+static void fold_nc(Hamilt& H, NonlocalK& k, int ik, cudaStream_t s) {
+    k.nc_folded = false;
+    if (k.nkb <= 0 || !H.deeq_nc.ptr || k.vkb.ptr == nullptr) return;
+    const FoldTypes ft = fold_types(H.ntype, H.na, H.nh, k.nkb, H.nc_dx, std::min(H.nc_dy, H.nc_dz));
+    const long total = 4L * k.nkb * k.npwx;
+    const int blocks = int(std::min<long>((total + 255) / 256, 148L * 8));
+    k.wnc.resize(size_t(total));
+    k.wncf.resize(size_t(4) * k.nkb * k.ldf);
+    if (k.ldf != k.npwx) B200_CUDA(cudaMemsetAsync(k.wncf.ptr, 0, k.wncf.n * sizeof(float2), s));
+    k_fold_deeq_nc<double2><<<blocks, 256, 0, s>>>(k.nkb, k.npwx, k.npwx, ft, H.nc_dx, H.nc_dy, H.nc_dz, H.deeq_nc.ptr,
+                                                  k.vkb.ptr, k.wnc.ptr);
+    k_fold_deeq_nc<float2><<<blocks, 256, 0, s>>>(k.nkb, k.npwx, k.ldf, ft, H.nc_dx, H.nc_dy, H.nc_dz, H.deeq_nc.ptr,
+                                                 k.vkb.ptr, k.wncf.ptr);
+    note_launch(2);
+    B200_CUDA(cudaGetLastError());
+    if (H.fp64_gemm != 0) {
+        const int npw = H.grid->kmaps[ik].npw;
+        for (int half = 0; half < 2; ++half)
+            oz_prepare_a('N', npw, 2 * k.nkb, k.wnc.ptr + size_t(half) * 2 * k.nkb * k.npwx, k.npwx, H.oz_mods,
+                         k.wnc_oz[half], H.oz_setup, s);
+    } else {
+        k.wnc_oz[0] = OzOperand();
+        k.wnc_oz[1] = OzOperand();
+    }
+    k.nc_folded = true;
+}
+
+void Hamilt::fold_projectors(int ik, cudaStream_t s) {
+    NonlocalK& k = nl[ik];
+    // vkb^H in residue form (becp of both spin forms) when the FP64 products run on the int8 tensor cores
+    k.oz_ready = false;
+    if (fp64_gemm != 0 && k.nkb > 0 && k.vkb.ptr)
+        oz_prepare_a('C', k.nkb, grid->kmaps[ik].npw, k.vkb.ptr, k.npwx, oz_mods, k.vkb_oz, oz_setup, s);
+    else
+        k.vkb_oz = OzOperand();
+    fold_nc(*this, k, ik, s);
+    k.folded = false;
+    if (k.nkb <= 0 || !deeq.ptr || k.vkb.ptr == nullptr) return;
+    const FoldTypes ft = fold_types(ntype, na, nh, k.nkb, dx, std::min(dy, dz));
     const long total = long(k.nkb) * k.npwx;
     int blocks = int((total + 255) / 256);
     if (blocks > 148 * 8) blocks = 148 * 8;
@@ -164,16 +269,13 @@ void Hamilt::fold_projectors(int ik, cudaStream_t s) {
         note_launch(2);
         B200_CUDA(cudaGetLastError());
     }
-    k.oz_ready = false;
     if (fp64_gemm != 0) {
         const int npw = grid->kmaps[ik].npw;
-        oz_prepare_a('C', k.nkb, npw, k.vkb.ptr, k.npwx, oz_mods, k.vkb_oz, oz_setup, s);
         k.vkbd_oz.resize(size_t(nspin));
         for (int sp = 0; sp < nspin; ++sp)
             oz_prepare_a('N', npw, k.nkb, k.vkbd.ptr + size_t(sp) * total, k.npwx, oz_mods, k.vkbd_oz[sp], oz_setup, s);
         k.oz_ready = true;
     } else {
-        k.vkb_oz = OzOperand();
         k.vkbd_oz.clear();
     }
     k.folded = true;
@@ -210,15 +312,6 @@ template <> struct Blas<double2> {
         return cublasZgemm3m(h, ta, tb, m, n, k, reinterpret_cast<const cuDoubleComplex*>(alpha),
                            reinterpret_cast<const cuDoubleComplex*>(A), lda, reinterpret_cast<const cuDoubleComplex*>(B),
                            ldb, reinterpret_cast<const cuDoubleComplex*>(beta), reinterpret_cast<cuDoubleComplex*>(C), ldc);
-    }
-};
-template <> struct Blas<float2> {
-    static cublasStatus_t gemm(cublasHandle_t h, cublasOperation_t ta, cublasOperation_t tb, int m, int n, int k,
-                               const float2* alpha, const float2* A, int lda, const float2* B, int ldb,
-                               const float2* beta, float2* C, int ldc) {
-        return cublasCgemm(h, ta, tb, m, n, k, reinterpret_cast<const cuComplex*>(alpha),
-                           reinterpret_cast<const cuComplex*>(A), lda, reinterpret_cast<const cuComplex*>(B), ldb,
-                           reinterpret_cast<const cuComplex*>(beta), reinterpret_cast<cuComplex*>(C), ldc);
     }
 };
 }  // namespace
@@ -334,6 +427,96 @@ void Hamilt::hpsi(int ik, int spin, int nb, int ld, const T* psi, T* hpsi, int m
         tc_cgemm('N', npw, nb, nkb, one, vkbd, k.ldf, becp, ldb_p, one, hpsi, ld, tcw, s);
     }
 }
+
+template <typename T>
+void Hamilt::hpsi_nc(int ik, int nb, int ld, const T* psi, T* hpsi, cudaStream_t s, HpsiWork* wk) {
+    using R = typename RealOf<T>::type;
+    constexpr bool f64 = std::is_same<T, double2>::value;
+    HpsiWork& W = wk ? *wk : work;
+    B200_CHECK(ik >= 0 && ik < int(grid->kmaps.size()), kInvalidArgument, "k-point index out of range");
+    const int npw = grid->kmaps[ik].npw;
+    B200_CHECK(nb >= 0 && ld >= npw, kInvalidArgument, "ld smaller than npwk or negative band count");
+    B200_CHECK(has_veff_nc, kInvalidArgument, "npol = 2: V_eff's four components not set");
+    if (nb == 0) return;
+    // local part, in chunks of bands whose real-space planes (two boxes per band) stay within 512 MB
+    const size_t N = size_t(grid->nxyz());
+    const size_t per_col = N * sizeof(T);
+    int cb = int((size_t(512) << 20) / (2 * per_col));
+    if (cb < 1) cb = 1;
+    if (cb > nb) cb = nb;
+    if (cb > 32767) cb = 32767;
+    const R* v4 = f64 ? (const R*)veff_nc_zyx.ptr : (const R*)veff_nc_zyxf.ptr;
+    T *sb, *rb;
+    const size_t sbn = size_t(2) * cb * grid->nst * grid->nz, rbn = size_t(2) * cb * N;
+    if constexpr (f64) {
+        W.sb64.resize(sbn);
+        W.rb64.resize(rbn);
+        sb = W.sb64.ptr;
+        rb = W.rb64.ptr;
+    } else {
+        W.sb32.resize(sbn);
+        W.rb32.resize(rbn);
+        sb = W.sb32.ptr;
+        rb = W.rb32.ptr;
+    }
+    for (int b0 = 0; b0 < nb; b0 += cb) {
+        const int nbc = nb - b0 < cb ? nb - b0 : cb;
+        launch_hpsi_local_nc<T, R>(*grid, ik, v4, 2 * nbc, ld, psi + size_t(2) * b0 * ld, hpsi + size_t(2) * b0 * ld, sb,
+                                   rb, grid->basis.tpiba2, s);
+    }
+    // Nonlocal::act with npol = 2 (nonlocal_pw.cpp:211-283 with add_nonlocal_pp's spinor form): becp of the 2 nb
+    // spinor columns, read as [becp_up; becp_dn] (2 nkb x nb), then H psi_up += [W0 W1] becp, H psi_dn += [W2 W3] becp
+    const NonlocalK& k = nl[ik];
+    if (k.nkb <= 0) return;
+    B200_CHECK(k.nc_folded, kInvalidArgument, "npol = 2: projectors and deeq_nc not both set for this k-point");
+    const int nkb = k.nkb;
+    const T one = cmake<T>(1, 0), zero = cmake<T>(0, 0);
+    T* becp;
+    if constexpr (f64) {
+        W.becp64.resize(size_t(2) * nkb * nb);
+        becp = W.becp64.ptr;
+        const bool oz = k.vkb_oz.res.ptr && k.wnc_oz[0].res.ptr && (fp64_gemm == 2 || (fp64_gemm == 1 && nb >= kOzMinBands));
+        if (oz) {
+            W.tcw.ensure();
+            oz_zgemm('C', nkb, 2 * nb, npw, one, k.vkb_oz, psi, ld, zero, becp, nkb, W.ozw, W.tcw.err.ptr, s);
+            for (int half = 0; half < 2; ++half)
+                oz_zgemm('N', npw, nb, 2 * nkb, one, k.wnc_oz[half], becp, 2 * nkb, one, hpsi + size_t(half) * ld, 2 * ld,
+                         W.ozw, W.tcw.err.ptr, s);
+        } else {
+            B200_CUBLAS(cublasSetStream(W.cublas, s));
+            const cuDoubleComplex* o = reinterpret_cast<const cuDoubleComplex*>(&one);
+            const cuDoubleComplex* z0 = reinterpret_cast<const cuDoubleComplex*>(&zero);
+            B200_CUBLAS(cublasZgemm3m(W.cublas, CUBLAS_OP_C, CUBLAS_OP_N, nkb, 2 * nb, npw, o,
+                                      reinterpret_cast<const cuDoubleComplex*>(k.vkb.ptr), k.npwx,
+                                      reinterpret_cast<const cuDoubleComplex*>(psi), ld, z0,
+                                      reinterpret_cast<cuDoubleComplex*>(becp), nkb));
+            for (int half = 0; half < 2; ++half)
+                B200_CUBLAS(cublasZgemm3m(W.cublas, CUBLAS_OP_N, CUBLAS_OP_N, npw, nb, 2 * nkb, o,
+                                          reinterpret_cast<const cuDoubleComplex*>(k.wnc.ptr + size_t(half) * 2 * nkb * k.npwx),
+                                          k.npwx, reinterpret_cast<const cuDoubleComplex*>(becp), 2 * nkb, o,
+                                          reinterpret_cast<cuDoubleComplex*>(hpsi + size_t(half) * ld), 2 * ld));
+        }
+    } else {
+        W.becp32.resize(size_t(2) * nkb * nb);
+        becp = W.becp32.ptr;
+        const float2* psi_b = psi;
+        int ldb = ld;
+        if (ld & 1) {  // the TMA row pitch must be a multiple of 16 bytes: stage psi with an even pitch
+            ldb = ld + 1;
+            W.psi_pad32.resize(size_t(2) * nb * ldb);
+            B200_CUDA(cudaMemcpy2DAsync(W.psi_pad32.ptr, size_t(ldb) * sizeof(float2), psi, size_t(ld) * sizeof(float2),
+                                        size_t(npw) * sizeof(float2), 2 * nb, cudaMemcpyDeviceToDevice, s));
+            psi_b = W.psi_pad32.ptr;
+        }
+        tc_cgemm('C', nkb, 2 * nb, npw, one, k.vkbf.ptr, k.ldf, psi_b, ldb, zero, becp, nkb, W.tcw, s);
+        for (int half = 0; half < 2; ++half)
+            tc_cgemm('N', npw, nb, 2 * nkb, one, k.wncf.ptr + size_t(half) * 2 * nkb * k.ldf, k.ldf, becp, 2 * nkb, one,
+                     hpsi + size_t(half) * ld, 2 * ld, W.tcw, s);
+    }
+}
+
+template void Hamilt::hpsi_nc<double2>(int, int, int, const double2*, double2*, cudaStream_t, HpsiWork*);
+template void Hamilt::hpsi_nc<float2>(int, int, int, const float2*, float2*, cudaStream_t, HpsiWork*);
 
 template <typename T>
 void Hamilt::hpsi_kbatch(int nk, const int* iks, int spin, int nb, int ld, const T* const* psis, T* const* hpsis,

@@ -30,14 +30,20 @@ struct NonlocalK {
     OzOperand vkb_oz;
     std::vector<OzOperand> vkbd_oz;
     bool oz_ready = false;
+    // npol = 2: the four 2x2 spin blocks of D folded into the projectors, W_s = vkb D_s per atom block; rows
+    // [0, 2 nkb) = [W0; W1] (H psi_up += W0 becp_up + W1 becp_dn), rows [2 nkb, 4 nkb) = [W2; W3] (H psi_dn)
+    DeviceArray<double2> wnc;  // 4 x nkb x npwx
+    DeviceArray<float2> wncf;  // 4 x nkb x ldf
+    OzOperand wnc_oz[2];       // residue forms of the two halves (FP64 products on the int8 tensor cores)
+    bool nc_folded = false;
 };
 
 // Scratch of one H|psi> caller: stick buffer, becp, the padded-psi stage, a cuBLAS handle and the
 // tensor-core GEMM workspace.  Callers that run H|psi> concurrently (different streams or threads) each
 // own one; the Hamiltonian itself is read-only after set-up.
 struct HpsiWork {
-    DeviceArray<double2> sb64, becp64;
-    DeviceArray<float2> sb32, becp32, psi_pad32;
+    DeviceArray<double2> sb64, becp64, rb64;
+    DeviceArray<float2> sb32, becp32, psi_pad32, rb32;  // rb: real-space planes of the npol = 2 local pass
     cublasHandle_t cublas = nullptr;
     TcGemmWorkspace tcw;
     OzWorkspace ozw;  // the FP64 projector products on the int8 tensor cores (psi / becp residues, products)
@@ -87,6 +93,13 @@ struct Hamilt {
     int ntype = 0, nspin = 1, dx = 0, dy = 0, dz = 0;
     std::vector<int> na, nh;
     DeviceArray<double> deeq;
+    // npol = 2 (non-collinear): V_eff's four components in (z, y, x) order, and D's four complex spin blocks
+    // deeq_nc(4, dx, dy, dz) (nonlocal_op.cpp:43-74)
+    DeviceArray<double> veff_nc_zyx;
+    DeviceArray<float> veff_nc_zyxf;
+    bool has_veff_nc = false;
+    DeviceArray<double2> deeq_nc;
+    int nc_dx = 0, nc_dy = 0, nc_dz = 0;
     HpsiWork work;  // default scratch for callers that do not bring their own
     int chunk_override = 0;  // bands per stick-buffer chunk chosen by the autotuner (0 = 48 MB rule)
     // FP64 projector products: 0 = cuBLAS ZGEMM; int8 tensor cores (exact modular emulation, oz_mods moduli)
@@ -113,6 +126,13 @@ struct Hamilt {
     // fold D into the projectors of k-point ik (all spins), on stream s; nothing if either is not set.  With
     // fp64_gemm = 1 also the int8 residue forms of vkb and vkbd.
     void fold_projectors(int ik, cudaStream_t s);
+    // npol = 2 set-up: V_eff's four components (4 x nrxx, the reference's (x, y, z) order), D's spin blocks
+    void set_veff_nc(const double* veff4_d);
+    void set_deeq_nc(int ntype, const int* na, const int* nh, int dx, int dy, int dz, const double2* deeq_nc_d);
+    // H|psi> with npol = 2 (hPsi's spinor branches: Ekinetic and Veff on both components, Nonlocal with deeq_nc):
+    // band b's components at psi + (2 b + c) ld, c = 0, 1
+    template <typename T>
+    void hpsi_nc(int ik, int nb, int ld, const T* psi, T* hpsi, cudaStream_t s, HpsiWork* w = nullptr);
     // choose the FP64 projector products (0 cuBLAS, 1 int8 tensor cores from kOzMinBands bands, 2 int8 always;
     // nmods moduli) and re-fold
     void set_fp64_gemm(int mode, int nmods);

@@ -121,6 +121,12 @@ template <typename T, typename R>
 bool launch_hpsi_local_kbatch(const PWGrid& g, const KBatchArgs& args, int nk, int nb, const R* veff_zyx,
                               const R* veff_perm, T* stickbuf, int chunk, double tpiba2, cudaStream_t s);
 // Drop-in transforms (PW_Basis_K::recip_to_real / real_to_recip on the GPU), one band.
+// the local part of H|psi> for npol = 2 (Veff::act's spinor branch, veff_pw.cpp:73-104, with Ekinetic::act on both
+// components): ncols spinor columns (band b's components at columns 2b, 2b+1, pitch ld), the four V_eff
+// components in (z, y, x) order; stickbuf holds ncols stick sets, rbuf ncols real-space boxes
+template <typename T, typename R>
+void launch_hpsi_local_nc(const PWGrid& g, int ik, const R* veff4_zyx, int ncols, int ld, const T* psi, T* hpsi,
+                          T* stickbuf, T* rbuf, double tpiba2, cudaStream_t s);
 template <typename T>
 void launch_recip_to_real(const PWGrid& g, int ik, const T* in, T* out, T* aux, int add, double factor, cudaStream_t s);
 template <typename T>

@@ -368,6 +368,27 @@ class HamiltPW:
         ns, dx, dy, dz = (int(v) for v in deeq_d.shape)
         call("b200_hamilt_set_deeq", self._h, len(na), na_a, nh_a, ns, dx, dy, dz, ptr(deeq_d))
 
+    def set_veff_nc(self, veff4_d):
+        """npol = 2: V_eff's four components, a (4, nrxx) float64 device tensor in set_veff's order."""
+        torch = _torch()
+        if veff4_d.dtype != torch.float64 or veff4_d.numel() < 4 * self.basis.nxyz:
+            raise ValueError("veff4_d must be float64 with 4 x nrxx values")
+        call("b200_hamilt_set_veff_nc", self._h, ptr(veff4_d))
+
+    def set_deeq_nc(self, na, nh, deeq_nc_d):
+        """npol = 2: D's four complex spin blocks, a (4, dx, dy, dz) complex128 device tensor."""
+        na_a = (C.c_int * len(na))(*na)
+        nh_a = (C.c_int * len(nh))(*nh)
+        four, dx, dy, dz = (int(v) for v in deeq_nc_d.shape)
+        if four != 4:
+            raise ValueError("deeq_nc_d must have shape (4, dx, dy, dz)")
+        call("b200_hamilt_set_deeq_nc", self._h, len(na), na_a, nh_a, dx, dy, dz, ptr(deeq_nc_d))
+
+    def hpsi_nc(self, ik, psi, hpsi, nbands, ld, stream=None):
+        """Operator::hPsi with npol = 2: band b's spinor components at psi[(2b + c) ld : ...]."""
+        self._chk(psi, hpsi, 2 * nbands, ld)
+        call("b200_hamilt_hpsi_nc", self._h, ik, nbands, ld, ptr(psi), ptr(hpsi), stream_ptr(stream))
+
     def _chk(self, psi, hpsi, nbands, ld):
         f64 = self.precision == PREC_FP64
         _check_block(psi, f64, nbands, ld, "psi")

@@ -159,6 +159,23 @@ int b200_hamilt_set_deeq(b200_hamilt* h, int ntype, const int* na, const int* nh
  * spin selects the deeq spin channel (isk[ik]). */
 int b200_hamilt_hpsi(b200_hamilt* h, int ik, int spin, int nbands, int ld, const void* psi_d, void* hpsi_d,
                      void* stream);
+/* ---- npol = 2 (non-collinear) ----
+ * Veff's four components for the spinor branch of Veff::act (veff_pw.cpp:73-104, veff_pw_op's npol = 2
+ * form veff_op.cpp:20-37): veff4_d = 4 x nrxx doubles (V, then the three magnetic components), each in
+ * b200_hamilt_set_veff's order. */
+int b200_hamilt_set_veff_nc(b200_hamilt* h, const double* veff4_d);
+/* D's four complex spin blocks deeq_nc(4, dx, dy, dz) (nonlocal_pw_op's npol = 2 overload,
+ * nonlocal_op.h:82-113, CPU body nonlocal_op.cpp:43-74), folded into the projectors of every k-point:
+ * W_s = vkb D_s per atom block, so that H psi_up += W0 becp_up + W1 becp_dn, H psi_dn += W2 becp_up +
+ * W3 becp_dn. */
+int b200_hamilt_set_deeq_nc(b200_hamilt* h, int ntype, const int* na, const int* nh, int deeq_x, int deeq_y,
+                            int deeq_z, const void* deeq_nc_d);
+/* Operator::hPsi with npol = 2 (operator.cpp:39-88): band b's two spinor components at psi_d + (2b + c) ld
+ * (the reference's nbasis = 2 ld layout), hpsi_d overwritten (padding zeroed): the kinetic diagonal on
+ * both components, the 2x2 V_eff in real space, the projectors with deeq_nc.  The local part runs the stick
+ * passes on the 2 nbands spinor columns and splits the plane pass at the real-space product (a scratch of
+ * two real-space boxes per band, in chunks of 512 MB). */
+int b200_hamilt_hpsi_nc(b200_hamilt* h, int ik, int nbands, int ld, const void* psi_d, void* hpsi_d, void* stream);
 /* H|psi> between host buffers (psi_h in, hpsi_h out, band b at b*ld, the handle's element type), through
  * the caller's device buffers psi_d / hpsi_d (nbands*ld each): the bands go in npieces pieces through
  * three streams so that the upload of piece p+1, H|psi> of piece p and the download of piece p-1 overlap

@@ -14,6 +14,7 @@ Followed reference code (abacus-develop v3.8.0):
     exp(-iGr), the 1/N applied at the gather) -- scipy's pocketfft has the
     same convention (fftn = forward, ifftn * N = backward).
   * Veff::act ................. source/module_hamilt_pw/hamilt_pwdft/operator_pw/veff_pw.cpp:38-109
+                                (npol = 2 branch :73-104 in HamiltPWRefNC)
   * Ekinetic::act ............. source/module_hamilt_pw/hamilt_pwdft/operator_pw/ekinetic_pw.cpp:34-50
   * Nonlocal::act / add_nonlocal_pp
                                 source/module_hamilt_pw/hamilt_pwdft/operator_pw/nonlocal_pw.cpp:64-283
@@ -206,6 +207,57 @@ class HamiltPWRef:
             eye[i * npw + i] = 1.0
         h = self.hpsi(eye, npw, npw).reshape(npw, npw)  # row ib = H e_ib
         return h.T
+
+
+class HamiltPWRefNC:
+    """Ekinetic -> Veff -> Nonlocal chain with npol = 2 for one k-point: band b's spinor components are the
+    columns 2b and 2b + 1 (pitch nbasis).  Ekinetic::act on every column (ekinetic_pw.cpp:34-50 with
+    max_npw = nbasis), Veff::act's spinor branch (veff_pw.cpp:73-104: both components to real space,
+    veff_pw_op's npol = 2 form, both back), Nonlocal::act with add_nonlocal_pp's spinor branch
+    (nonlocal_pw.cpp:117-160, 211-283; nonlocal_pw_op's deeq_nc overload)."""
+
+    def __init__(self, basis, ik, veff4, vkb, deeq_nc, nh, natoms_per_type):
+        self.basis = basis
+        self.ik = ik
+        self.veff4 = [np.asarray(v, dtype=np.float64) for v in veff4]
+        self.vkb = np.asarray(vkb)  # (nkb, npwx) row-major
+        self.nkb = self.vkb.shape[0]
+        self.deeq_nc = np.asarray(deeq_nc)  # (4, dx, dy, dz) complex
+        self.nh = nh
+        self.na = natoms_per_type
+
+    def hpsi(self, psi, nbands, nbasis):
+        """hpsi of nbands spinor bands (2 nbands columns of nbasis)."""
+        ncol = 2 * nbands
+        npw = int(self.basis.npwk[self.ik])
+        N = self.basis.nxyz
+        psi = np.asarray(psi).reshape(-1)
+        hpsi = np.zeros(ncol * nbasis, dtype=np.complex128)
+        ekinetic_pw_op(ncol, npw, nbasis, self.basis.tpiba2, self.basis.gk2_k(self.ik), hpsi, psi)
+        for ib in range(nbands):
+            up, dn = (2 * ib) * nbasis, (2 * ib + 1) * nbasis
+            porter = recip_to_real(self.basis, psi[up: up + npw], self.ik)
+            porter1 = recip_to_real(self.basis, psi[dn: dn + npw], self.ik)
+            veff_pw_op_npol2(N, porter, porter1, self.veff4)
+            for off, buf in ((up, porter), (dn, porter1)):
+                seg = hpsi[off: off + npw]
+                real_to_recip(self.basis, buf, self.ik, out=seg, add=True)
+                hpsi[off: off + npw] = seg
+        nkb = self.nkb
+        if nkb:
+            V = self.vkb[:, :npw]
+            P = np.stack([psi[c * nbasis: c * nbasis + npw] for c in range(ncol)], 1)
+            becp = (V.conj() @ P).T.reshape(-1)  # becp[c*nkb + j]
+            ps = np.zeros(nkb * ncol, dtype=np.complex128)
+            sum_, iat = 0, 0
+            dx, dy, dz = self.deeq_nc.shape[1], self.deeq_nc.shape[2], self.deeq_nc.shape[3]
+            for it in range(len(self.na)):
+                sum_, iat = nonlocal_pw_op_nc(self.na[it], ncol, self.nh[it], sum_, iat, nkb, dx, dy, dz,
+                                              self.deeq_nc, ps, becp)
+            add = V.T @ ps.reshape(nkb, ncol)
+            for c in range(ncol):
+                hpsi[c * nbasis: c * nbasis + npw] += add[:, c]
+        return hpsi
 
 
 def precondition_dav_subspace(basis, ik):
