@@ -231,3 +231,23 @@ def test_zgemm_i8_repeated_calls_agree(pkg):
     o1 = _run(pkg, torch, "C", M, N, K, K, A_store, B_store, C_store, 1.0, 0.0, K, M)
     o2 = _run(pkg, torch, "C", M, N, K, K, A_store, B_store, C_store, 1.0, 0.0, K, M)
     assert np.array_equal(o1, o2)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("nmods", [12, 14])
+def test_zgemm_i8_fewer_moduli(pkg, nmods):
+    """Fewer moduli, smaller scale exponent q: the error stays within the rounding of op(A) and B to q bits."""
+    torch = pytest.importorskip("torch")
+    rng = np.random.default_rng(40 + nmods)
+    M, N, K = 200, 30, 3000
+    A_store = _cplx(rng, M, K)  # 'C': A is K x M
+    B_store = _cplx(rng, N, K)
+    C_store = np.zeros((N, M), dtype=np.complex128)
+    out = _run(pkg, torch, "C", M, N, K, K, A_store, B_store, C_store, 1.0, 0.0, K, M, nmods=nmods).T
+    ref = A_store.conj() @ B_store.T
+    q = pkg.pwdft.zgemm_i8_constants(nmods, 2 * K)[4]
+    amax = np.maximum(np.abs(A_store.real), np.abs(A_store.imag)).max(axis=1)[:, None]
+    bmax = np.maximum(np.abs(B_store.real), np.abs(B_store.imag)).max(axis=1)[None, :]
+    # each of the 2K products carries the two operands' roundings (half a unit of 2^-q of the row maximum)
+    bar = 2.0 * 2 * K * 2.0 ** -q * amax * bmax
+    assert np.all(np.abs(out - ref) <= bar)
