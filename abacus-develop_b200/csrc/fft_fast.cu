@@ -853,9 +853,10 @@ void zpass_r(bool inv, const PWGrid& g, const Src& src, int nk, int b0, int nbc,
     int var = std::is_same<T, double2>::value ? g.plane_variant64 : g.plane_variant32;
     if (var == 0) var = default_plane_variant<T>(g.nx);
     if (var != 1) {
-        // two-pass register transforms: 32 sticks per CTA; 12 warps (nz = 96: a multiple of R1 = 12 and R2 = 8,
-        // so each thread keeps its twiddles) or 8
-        constexpr int R2 = 8, R1 = NZ / 8, TS = 32, NT = NZ == 96 ? 384 : 256;
+        // two-pass register transforms: 32 sticks per CTA, 8 warps.  Twiddles come from the L1-resident roots
+        // table; at 64-84 registers three CTAs share an SM, which hides the latency of the sphere gathers and
+        // scatters better than one 12-warp CTA keeping its twiddles in registers (116 registers at nz = 96)
+        constexpr int R2 = 8, R1 = NZ / 8, TS = 32, NT = 256;
         const dim3 grid(ceil_div(g.nst, TS), nbc, nk);
         constexpr size_t smem = plane_t::zpass_smem_bytes<T>(R1, R2, TS);
         if (inv) {
