@@ -465,9 +465,9 @@ __global__ void __launch_bounds__(kPlaneWarps * 32) k_rho_plane_r(PlaneMapView p
     }
 }
 
-// ---- register z passes for nz = 32*M: the inverse transform leaves every stick in the permuted order, so
-// the planes of the stick buffer are stored by slot (plane slot sz holds z = sz/32 + M*bitrev5(sz mod 32));
-// V_eff is permuted along z as well, and the forward z transform takes the slots back to natural z.
+// ---- stick buffer of the register-transform grids (nz = 32*M): the planes are stored by slot (plane slot sz
+// holds z = sz/32 + M*bitrev5(sz mod 32)), V_eff is permuted along z as well, and the forward z pass takes
+// the slots back to natural z (the z passes: plane_t.cuh, k_zinv_t / k_zfwd_t).
 // Src gives the k-point entry of a block: one k-point (OneK) or a batch indexed by blockIdx.z (ManyK).
 struct OneK {
     KBatchEntry e;
@@ -477,98 +477,6 @@ struct ManyK {
     KBatchArgs a;
     __device__ __forceinline__ const KBatchEntry& get(int q) const { return a.e[q]; }
 };
-
-template <typename T, int NZ, typename Src>
-__global__ void __launch_bounds__(kZWarps * 32) k_zinv_r(Src src, int b0, int nbc, const T* __restrict__ roots,
-                                                        T* __restrict__ sb) {
-    constexpr int M = NZ / 32;
-    constexpr int LDZ = NZ | 1;
-    __shared__ T A[kStickTile * LDZ];
-    const KBatchEntry& e = src.get(blockIdx.z);
-    const StickMapView sm = e.sm;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int s0 = blockIdx.x * kStickTile;
-    if (s0 >= sm.nst) return;
-    const int ns = min(kStickTile, sm.nst - s0);
-    const int band = blockIdx.y;
-    for (int i = tid; i < kStickTile * LDZ; i += kZWarps * 32) A[i] = zero_c<T>();
-    T lk[M];
-    LaneTw<T> tw;
-    lane_twiddles<T, NZ>(roots, lane, lk, tw);
-    __syncthreads();
-    const T* p = reinterpret_cast<const T*>(e.psi) + size_t(b0 + band) * e.ld;
-    const int j0 = sm.gofs[s0], j1 = sm.gofs[s0 + ns];
-    for (int j = j0 + tid; j < j1; j += kZWarps * 32) {
-        const int pk = sm.gpk[j];
-        A[((pk >> 10) - s0) * LDZ + (pk & 1023)] = p[sm.glist[j]];
-    }
-    __syncthreads();
-    for (int sl = warp; sl < ns; sl += kZWarps) {
-        T u[M];
-        T* stick = A + sl * LDZ;
-#pragma unroll
-        for (int n1 = 0; n1 < M; ++n1) u[n1] = stick[32 * n1 + lane];
-        regfft_inv_dif<T, M>(u, lk, tw, lane);
-#pragma unroll
-        for (int k1 = 0; k1 < M; ++k1) stick[32 * k1 + lane] = u[k1];
-    }
-    __syncthreads();
-    T* out = sb + (size_t(blockIdx.z) * nbc + band) * NZ * sm.nst;
-    for (int i = tid; i < ns * NZ; i += kZWarps * 32) {
-        const int sz = i / ns;
-        const int sl = i - sz * ns;
-        out[size_t(sz) * sm.nst + s0 + sl] = A[sl * LDZ + sz];
-    }
-}
-
-template <typename T, typename R, int NZ, typename Src>
-__global__ void __launch_bounds__(kZWarps * 32) k_zfwd_r(Src src, int b0, int nbc, const T* __restrict__ roots,
-                                                        const T* __restrict__ sb, R tpiba2, R invn, int accumulate) {
-    constexpr int M = NZ / 32;
-    constexpr int LDZ = NZ | 1;
-    __shared__ T A[kStickTile * LDZ];
-    const KBatchEntry& e = src.get(blockIdx.z);
-    const StickMapView sm = e.sm;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int s0 = blockIdx.x * kStickTile;
-    if (s0 >= sm.nst) return;
-    const int ns = min(kStickTile, sm.nst - s0);
-    const int band = blockIdx.y;
-    const T* in = sb + (size_t(blockIdx.z) * nbc + band) * NZ * sm.nst;
-    for (int i = tid; i < ns * NZ; i += kZWarps * 32) {
-        const int sz = i / ns;
-        const int sl = i - sz * ns;
-        A[sl * LDZ + sz] = in[size_t(sz) * sm.nst + s0 + sl];
-    }
-    T lk[M];
-    LaneTw<T> tw;
-    lane_twiddles<T, NZ>(roots, lane, lk, tw);
-    __syncthreads();
-    for (int sl = warp; sl < ns; sl += kZWarps) {
-        T u[M];
-        T* stick = A + sl * LDZ;
-#pragma unroll
-        for (int k1 = 0; k1 < M; ++k1) u[k1] = stick[32 * k1 + lane];
-        regfft_fwd_dit<T, M>(u, lk, tw, lane);
-#pragma unroll
-        for (int n1 = 0; n1 < M; ++n1) stick[32 * n1 + lane] = u[n1];
-    }
-    __syncthreads();
-    const T* p = reinterpret_cast<const T*>(e.psi) + size_t(b0 + band) * e.ld;
-    T* h = reinterpret_cast<T*>(e.hpsi) + size_t(b0 + band) * e.ld;
-    const R* gk2 = reinterpret_cast<const R*>(e.gk2);
-    const int j0 = sm.gofs[s0], j1 = sm.gofs[s0 + ns];
-    for (int j = j0 + tid; j < j1; j += kZWarps * 32) {
-        const int pk = sm.gpk[j];
-        const int g = sm.glist[j];
-        T v = cscale(A[((pk >> 10) - s0) * LDZ + (pk & 1023)], invn);
-        v = cadd(v, cscale(p[g], gk2[g] * tpiba2));
-        if (accumulate) v = cadd(v, h[g]);
-        h[g] = v;
-    }
-    if (!accumulate && blockIdx.x == 0)
-        for (int g = e.npw + tid; g < e.ld; g += kZWarps * 32) h[g] = zero_c<T>();
-}
 
 __device__ __forceinline__ int perm_slot(int s, int m) { return (s >> 5) + m * int(__brev(unsigned(s & 31)) >> 27); }
 // the same for lines of P = 2^lp lanes and q values per lane: slot s holds index s/P + q * bitrev_lp(s mod P)
@@ -850,34 +758,22 @@ bool zbatch_dispatch(bool inv, const PWGrid& g, const KBatchArgs& args, int nk, 
 template <typename T, typename R, int NZ, typename Src>
 void zpass_r(bool inv, const PWGrid& g, const Src& src, int nk, int b0, int nbc, T* sb, double tpiba2, int accumulate,
              cudaStream_t s) {
-    int var = std::is_same<T, double2>::value ? g.plane_variant64 : g.plane_variant32;
-    if (var == 0) var = default_plane_variant<T>(g.nx);
-    if (var != 1) {
-        // two-pass register transforms: 32 sticks per CTA, 8 warps.  Twiddles come from the L1-resident roots
-        // table; at 64-84 registers three CTAs share an SM, which hides the latency of the sphere gathers and
-        // scatters better than one 12-warp CTA keeping its twiddles in registers (116 registers at nz = 96)
-        constexpr int R2 = 8, R1 = NZ / 8, TS = 32, NT = 256;
-        const dim3 grid(ceil_div(g.nst, TS), nbc, nk);
-        constexpr size_t smem = plane_t::zpass_smem_bytes<T>(R1, R2, TS);
-        if (inv) {
-            auto kern = plane_t::k_zinv_t<T, NZ, R1, R2, TS, NT, Src>;
-            smem_attr(kern, smem);
-            kern<<<grid, NT, smem, s>>>(src, b0, nbc, rtp<T>(g.az), sb);
-        } else {
-            auto kern = plane_t::k_zfwd_t<T, R, NZ, R1, R2, TS, NT, Src>;
-            smem_attr(kern, smem);
-            kern<<<grid, NT, smem, s>>>(src, b0, nbc, rtp<T>(g.az), sb, R(tpiba2), R(1.0 / double(g.nxyz())), accumulate);
-        }
-        note_launch();
-        B200_CUDA(cudaGetLastError());
-        return;
+    // two-pass register transforms (both plane-pass families read and write this stick layout): 32 sticks per
+    // CTA, 8 warps.  Twiddles come from the L1-resident roots table; at 41-84 registers three or more CTAs
+    // share an SM, which hides the latency of the sphere gathers and scatters better than one 12-warp CTA
+    // keeping its twiddles in registers (116 registers at nz = 96) or the one-warp-per-stick shuffle passes
+    constexpr int R2 = 8, R1 = NZ / 8, TS = 32, NT = 256;
+    const dim3 grid(ceil_div(g.nst, TS), nbc, nk);
+    constexpr size_t smem = plane_t::zpass_smem_bytes<T>(R1, R2, TS);
+    if (inv) {
+        auto kern = plane_t::k_zinv_t<T, NZ, R1, R2, TS, NT, Src>;
+        smem_attr(kern, smem);
+        kern<<<grid, NT, smem, s>>>(src, b0, nbc, rtp<T>(g.az), sb);
+    } else {
+        auto kern = plane_t::k_zfwd_t<T, R, NZ, R1, R2, TS, NT, Src>;
+        smem_attr(kern, smem);
+        kern<<<grid, NT, smem, s>>>(src, b0, nbc, rtp<T>(g.az), sb, R(tpiba2), R(1.0 / double(g.nxyz())), accumulate);
     }
-    const dim3 grid(ceil_div(g.nst, kStickTile), nbc, nk);
-    if (inv)
-        k_zinv_r<T, NZ, Src><<<grid, kZWarps * 32, 0, s>>>(src, b0, nbc, rtp<T>(g.az), sb);
-    else
-        k_zfwd_r<T, R, NZ, Src><<<grid, kZWarps * 32, 0, s>>>(src, b0, nbc, rtp<T>(g.az), sb, R(tpiba2),
-                                                             R(1.0 / double(g.nxyz())), accumulate);
     note_launch();
     B200_CUDA(cudaGetLastError());
 }
