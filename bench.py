@@ -64,7 +64,7 @@ E2E_PIECES = 6
 # dram__bytes_read.sum + dram__bytes_write.sum of the fused local H|psi> kernels (3 launches: one band chunk
 # of all 160 bands, the autotuner's choice, x 3 passes) for one 160-band FP64 application, from an ncu
 # capture without cache flush (the local-pass traffic summary under profiles/)
-NCU_TRAFFIC_LOCAL_FP64 = 2029709824
+NCU_TRAFFIC_LOCAL_FP64 = 2030089984
 
 
 def load_package():
