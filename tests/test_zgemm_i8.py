@@ -251,3 +251,37 @@ def test_zgemm_i8_fewer_moduli(pkg, nmods):
     # each of the 2K products carries the two operands' roundings (half a unit of 2^-q of the row maximum)
     bar = 2.0 * 2 * K * 2.0 ** -q * amax * bmax
     assert np.all(np.abs(out - ref) <= bar)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("shape", [("C", 512, 160, 6000), ("N", 3000, 160, 512)])
+def test_zgemm_i8_wait_runout_reports_and_recovers(pkg, shape):
+    """The GEMM kernel's bounded waits (streamed and shared-memory-resident B'): with a limit no pipeline can meet
+    (1 ns) the kernel gives up, drains its own copies and MMAs, frees its tensor memory and sets the error word,
+    which the host reads (and the read clears); the next product with the default limit is correct."""
+    torch = pytest.importorskip("torch")
+    P = pkg.pwdft
+    ta, M, N, K = shape
+    rng = np.random.default_rng(17)
+    A_store = _cplx(rng, M, K) if ta == "C" else _cplx(rng, K, M)
+    lda = K if ta == "C" else M
+    B_store = _cplx(rng, N, K)
+    ad, bd = torch.from_numpy(A_store).cuda(), torch.from_numpy(B_store).cuda()
+    cd = torch.zeros((N, M), dtype=torch.complex128, device="cuda")
+    assert P.zgemm_i8_error() == 0
+    try:
+        P.tc_set_wait_limit_ns(1)
+        P.zgemm_i8(ta, M, N, K, 1.0, ad, lda, bd, K, 0.0, cd, M)
+        torch.cuda.synchronize()
+    finally:
+        P.tc_set_wait_limit_ns(0)
+    assert P.zgemm_i8_error() != 0, "a 1 ns wait limit should have run out"
+    assert P.zgemm_i8_error() == 0, "the read clears the error word"
+    P.zgemm_i8(ta, M, N, K, 1.0, ad, lda, bd, K, 0.0, cd, M)
+    torch.cuda.synchronize()
+    assert P.zgemm_i8_error() == 0
+    A = A_store.T
+    opA = A if ta == "N" else A.conj().T
+    ref = opA @ B_store.T
+    bound = np.abs(opA) @ np.abs(B_store.T)
+    assert (np.abs(cd.cpu().numpy().T - ref) / bound).max() < 4e-16 * np.sqrt(K) + 4e-16
