@@ -330,6 +330,23 @@ __device__ __forceinline__ void tmem_ld16i(unsigned taddr, int* v) {
     for (int i = 0; i < 16; ++i) v[i] = int(r[i]);
 }
 
+// 32 consecutive TMEM columns of this thread's lane in one load (one wait for all of them)
+__device__ __forceinline__ void tmem_ld32i(unsigned taddr, int* v) {
+    unsigned r[32];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+        "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];\n\t"
+        "tcgen05.wait::ld.sync.aligned;"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+          "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]),
+          "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+          "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr)
+        : "memory");
+#pragma unroll
+    for (int i = 0; i < 32; ++i) v[i] = int(r[i]);
+}
+
 struct OzMods {
     unsigned m[kOzMaxMods], magic[kOzMaxMods], c31[kOzMaxMods];
 };
@@ -571,31 +588,41 @@ __global__ void __launch_bounds__(kOzThreads, 1)
             const unsigned m = md.m[l], magic = md.magic[l], c31 = md.c31[l];
             for (int u = 0; u < sc.msub; ++u) {
                 const int row = (o.tile_m * sc.msub + u) * 128 + rl;
-                for (int c0 = 16 * grp; c0 < BN; c0 += 32) {
-                    int v[16];
-                    if (o.nk > 0) {
-                        tmem_ld16i(tmem + (unsigned(32 * q) << 16) + unsigned(b * 256 + u * BN + c0), v);
+                // chunks of 32 columns (16 at the tail) dealt to the two warp groups in turn: one TMEM load
+                // and one wait per chunk
+                for (int c0 = 32 * grp; c0 < BN; c0 += 64) {
+                    const int w32 = BN - c0 >= 32 ? 32 : 16;
+                    int v[32];
+                    const unsigned ta = tmem + (unsigned(32 * q) << 16) + unsigned(b * 256 + u * BN + c0);
+                    if (o.nk == 0) {
+#pragma unroll
+                        for (int t = 0; t < 32; ++t) v[t] = 0;
+                    } else if (w32 == 32) {
+                        tmem_ld32i(ta, v);
                     } else {
-#pragma unroll
-                        for (int t = 0; t < 16; ++t) v[t] = 0;
+                        tmem_ld16i(ta, v);
                     }
-                    unsigned w[4];
 #pragma unroll
-                    for (int t4 = 0; t4 < 4; ++t4) {
-                        unsigned word = 0;
+                    for (int h = 0; h < 2; ++h) {
+                        if (h * 16 >= w32) break;
+                        unsigned w[4];
 #pragma unroll
-                        for (int t = 0; t < 4; ++t) {
-                            // (v + 2^31) mod m, then minus 2^31 mod m
-                            const unsigned r = oz_umod(unsigned(v[4 * t4 + t]) + 0x80000000u, m, magic);
-                            const int x = int(r) - int(c31);
-                            word |= unsigned(x < 0 ? x + int(m) : x) << (8 * t);
+                        for (int t4 = 0; t4 < 4; ++t4) {
+                            unsigned word = 0;
+#pragma unroll
+                            for (int t = 0; t < 4; ++t) {
+                                // (v + 2^31) mod m, then minus 2^31 mod m
+                                const unsigned r = oz_umod(unsigned(v[16 * h + 4 * t4 + t]) + 0x80000000u, m, magic);
+                                const int x = int(r) - int(c31);
+                                word |= unsigned(x < 0 ? x + int(m) : x) << (8 * t);
+                            }
+                            w[t4] = word;
                         }
-                        w[t4] = word;
+                        const int cg = (o.tile_n * BN + c0 + 16 * h) >> 4;
+                        if (row < rowsA && cg < cgroups)
+                            *reinterpret_cast<uint4*>(prod + ((long(o.z) * cgroups + cg) * rows_pad + row) * 16) =
+                                make_uint4(w[0], w[1], w[2], w[3]);
                     }
-                    const int cg = (o.tile_n * BN + c0) >> 4;
-                    if (row < rowsA && cg < cgroups)
-                        *reinterpret_cast<uint4*>(prod + ((long(o.z) * cgroups + cg) * rows_pad + row) * 16) =
-                            make_uint4(w[0], w[1], w[2], w[3]);
                 }
             }
             tc_fence_before();
