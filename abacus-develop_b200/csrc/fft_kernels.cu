@@ -97,6 +97,8 @@ void PWGrid::build(const PWBasisK& b) {
     nxc = int(h_xpos.size());
     h_xc.assign(nst, 0);
     for (int s = 0; s < nst; ++s) h_xc[s] = int(std::lower_bound(h_xpos.begin(), h_xpos.end(), sx[s]) - h_xpos.begin());
+    h_smap.assign(size_t(nxc) * ny, -1);
+    for (int s = 0; s < nst; ++s) h_smap[size_t(h_xc[s]) * ny + h_sy[s]] = s;
     kmaps.clear();
     kmaps.resize(b.nks);
     const size_t L = size_t(b.npwk_max);
@@ -140,6 +142,7 @@ void PWGrid::ensure_device() {
     st_y.upload(h_sy.data(), nst);
     st_ixy.upload(h_sixy.data(), nst);
     xpos.upload(h_xpos.data(), nxc);
+    smap.upload(h_smap.data(), h_smap.size());
     const size_t L = size_t(basis.npwk_max);
     for (int ik = 0; ik < basis.nks; ++ik) {
         KMap& km = kmaps[ik];

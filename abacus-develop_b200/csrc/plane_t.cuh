@@ -12,7 +12,10 @@
 //
 // Per (band, z slot) CTA: the occupied x-columns of the plane in shared memory, column-major, every
 // column in "block" order: position p = R2*k + t' of a column lives at k*(R2+1) + t' (a pad every R2
-// entries, so that pass B's threads, R2+1 entries apart, fall on different banks).  The y transforms run
+// entries, so that pass B's threads, R2+1 entries apart, fall on different banks).  The inverse y
+// transform's pass A reads the plane's sticks straight from the stick buffer through the (column, y) ->
+// stick map (zero where a column has no stick) and the forward y transform's pass A writes them back the
+// same way, so the plane enters and leaves shared memory only in transformed form.  The y transforms run
 // in place on the columns: after the inverse, position p of a column holds y = p/R2 + R1*(p mod R2).  The
 // x transforms take rows of RB positions at a time through a row buffer laid out [row][k1][t] with the
 // same padding; the forward x transform writes back the occupied columns only.  V_eff comes pre-arranged
@@ -190,24 +193,26 @@ __global__ void __launch_bounds__(NT, MINB) k_plane_t(PlaneMapView pm, int nz, c
     Twiddles<T, N, R1, R2, NT> tw;
     tw.load(roots, tid);
 
-    for (int i = tid; i < nxc * LDC; i += NT) A[i] = zero;
     for (int i = tid; i < N; i += NT) cmap[i] = -1;
     __syncthreads();
     for (int c = tid; c < nxc; c += NT) cmap[pm.xpos[c]] = c;
     T* plane = sb + (size_t(band) * nz + zs) * pm.nst;
-    for (int s = tid; s < pm.nst; s += NT) A[pm.xc[s] * LDC + G::pos(pm.sy[s])] = plane[s];
-    __syncthreads();
 
-    // ---- inverse y: pass A on (column, t), pass B on (column, k1) ----
+    // ---- inverse y: pass A on (column, t) straight from the plane's sticks (y without a stick is zero), pass B
+    // on (column, k1) ----
     for (int i = tid; i < nxc * R2; i += NT) {
         const int c = i / R2, t = i % R2;
-        T* col = A + c * LDC + t;
+        const int* sm = pm.smap + c * N + t;
+        int si[R1];
+#pragma unroll
+        for (int n1 = 0; n1 < R1; ++n1) si[n1] = __ldg(sm + n1 * R2);
         T u[R1];
 #pragma unroll
-        for (int n1 = 0; n1 < R1; ++n1) u[n1] = col[n1 * RS];
+        for (int n1 = 0; n1 < R1; ++n1) u[n1] = si[n1] >= 0 ? plane[si[n1]] : zero;
         dft<T, +1, R1>(u);
 #pragma unroll
         for (int k1 = 1; k1 < R1; ++k1) u[k1] = cmulc(u[k1], tw.wa(roots, t, k1));
+        T* col = A + c * LDC + t;
 #pragma unroll
         for (int k1 = 0; k1 < R1; ++k1) col[k1 * RS] = u[k1];
     }
@@ -298,16 +303,19 @@ __global__ void __launch_bounds__(NT, MINB) k_plane_t(PlaneMapView pm, int nz, c
     __syncthreads();
     for (int i = tid; i < nxc * R2; i += NT) {
         const int c = i / R2, t = i % R2;
-        T* col = A + c * LDC + t;
+        const T* col = A + c * LDC + t;
         T u[R1];
 #pragma unroll
         for (int k1 = 0; k1 < R1; ++k1) u[k1] = col[k1 * RS];
         dft<T, -1, R1>(u);
+        // straight back to the plane's sticks
+        const int* sm = pm.smap + c * N + t;
 #pragma unroll
-        for (int n1 = 0; n1 < R1; ++n1) col[n1 * RS] = u[n1];
+        for (int n1 = 0; n1 < R1; ++n1) {
+            const int si = __ldg(sm + n1 * R2);
+            if (si >= 0) plane[si] = u[n1];
+        }
     }
-    __syncthreads();
-    for (int s = tid; s < pm.nst; s += NT) plane[s] = A[pm.xc[s] * LDC + G::pos(pm.sy[s])];
 }
 
 }  // namespace plane_t

@@ -60,14 +60,15 @@ struct PlaneMapView {
     const int* xc;    // per stick: compact x-column index
     const int* sy;    // per stick: y
     const int* xpos;  // per compact column: x
+    const int* smap;  // per compact column c and y < ny: the stick at (xpos[c], y), or -1 (nxc x ny)
 };
 
 struct PWGrid {
     PWBasisK basis;
     int nx = 0, ny = 0, nz = 0, nst = 0, nxc = 0;
     FftAxis ax, ay, az;
-    DeviceArray<int> st_xc, st_y, xpos, st_ixy;
-    std::vector<int> h_xpos, h_xc, h_sy, h_sixy;
+    DeviceArray<int> st_xc, st_y, xpos, st_ixy, smap;
+    std::vector<int> h_xpos, h_xc, h_sy, h_sixy, h_smap;
     std::vector<KMap> kmaps;
     bool on_device = false;
     // plane pass of the register transforms, per precision (0: default shape; see plane_launch_var)
@@ -79,7 +80,7 @@ struct PWGrid {
         const KMap& k = kmaps[ik];
         return StickMapView{nst, nz, k.gofs.ptr, k.gpk.ptr, k.glist.ptr};
     }
-    PlaneMapView plane_view() const { return PlaneMapView{nst, nxc, st_xc.ptr, st_y.ptr, xpos.ptr}; }
+    PlaneMapView plane_view() const { return PlaneMapView{nst, nxc, st_xc.ptr, st_y.ptr, xpos.ptr, smap.ptr}; }
     long nxyz() const { return long(nx) * ny * nz; }
 };
 
