@@ -31,6 +31,7 @@
 #include "linalg_status.h"
 #include "david.h"
 #include "fft_core.cuh"
+#include "gemm_oz.h"
 #include "gemm_tc.h"
 
 namespace b200 {
@@ -204,6 +205,12 @@ template <typename T> struct Engine {
     DeviceArray<double> cn2;  // FP32 engine: squared column norms before the projection
     int reorth = 0;           // FP32 engine: second projection passes taken (counted per solve)
     TcGemmWorkspace tcw;
+    // FP64 engine: the subspace products on the int8 tensor cores (exact modular emulation of the FP64
+    // products, gemm_oz.h) instead of cuBLAS ZGEMM; op(A) residues and products are workspaces grown at
+    // first use.  0: cuBLAS; 1: the emulation for the products it is faster on; 2: for every product
+    int oz = 0;
+    OzOperand ozA;
+    OzWorkspace ozw;
     int lwork = 0;
     std::vector<double> eig_h;
     std::vector<int> unconv_h;
@@ -306,7 +313,7 @@ template <typename T> struct Engine {
     size_t device_bytes() const {
         return (basis.n + hp.n + newv.n + hcc.n + vcc.n + vc.n + vcl.n + lag.n + gram.n) * sizeof(T) +
                (A64.n + gram64.n + winv.n + work.n) * sizeof(double2) + (w.n + ein.n) * sizeof(double) +
-               pc.n * sizeof(R) + tcw.device_bytes();
+               pc.n * sizeof(R) + tcw.device_bytes() + ozA.device_bytes() + ozw.device_bytes();
     }
     ~Engine() {
         if (cb) cublasDestroy(cb);
@@ -352,6 +359,17 @@ template <typename T> struct Engine {
             if (k > 0 && b == CUBLAS_OP_N && (a == CUBLAS_OP_N || a == CUBLAS_OP_C) && lda % 2 == 0 && ldb % 2 == 0 &&
                 aligned) {
                 tc_cgemm(a == CUBLAS_OP_N ? 'N' : 'C', m, n, k, al, A, lda, B, ldb, be, C, ldc, tcw, s);
+                return;
+            }
+        } else {
+            // the emulation reduces both operands to residues in every call (work ~ (m + n) k) against m n k
+            // products: it pays from m n / (m + n) of about 256 on (B200: a 51 627 x 160 x 512 product is
+            // slower than cuBLAS, 124 289 x 480 x 480 1.4x and 480 x 1920 x 124 289 2x faster)
+            if (oz && k > 0 && b == CUBLAS_OP_N && (a == CUBLAS_OP_N || a == CUBLAS_OP_C) &&
+                (oz == 2 || (k >= 128 && double(m) * n / (double(m) + n) >= 256.0))) {
+                const char opa = a == CUBLAS_OP_N ? 'N' : 'C';
+                oz_prepare_a(opa, m, k, A, lda, kOzMaxMods, ozA, ozw, s);
+                oz_zgemm(opa, m, n, k, al, ozA, B, ldb, be, C, ldc, ozw, nullptr, s);
                 return;
             }
         }
@@ -480,6 +498,9 @@ template <typename T> struct Engine {
         if constexpr (kF32) {
             const int e = tcw.err.ptr ? tcw.read_error(s) : 0;
             B200_CHECK(e == 0, kCudaError, "tensor-core GEMM wait ran out (error word " + std::to_string(e) + ")");
+        } else if (oz) {
+            const int e = ozw.err.ptr ? ozw.read_error(s) : 0;
+            B200_CHECK(e == 0, kCudaError, "int8 tensor-core GEMM wait ran out (error word " + std::to_string(e) + ")");
         }
     }
 
@@ -610,6 +631,7 @@ class David : public DavidBase {
         trace_.reset();
         e64_->trace = &trace_;
         e64_->hpsi_bands = 0;
+        e64_->oz = fp64_gemm_ == 3 ? 2 : fp64_gemm_ == 2 ? 1 : 0;
         int nc = 0;
         const int it = e64_->diag(f64, ldpsi, (double2*)psi, eig, thr, maxiter, ntry_max, notconv_max, nc);
         stats_.iters_fp64 = it;
@@ -656,6 +678,7 @@ class David : public DavidBase {
             total += it32;
         }
         e64_->hpsi_bands = 0;
+        e64_->oz = fp64_gemm_ == 3 ? 2 : (fp64_gemm_ == 2 || (fp64_gemm_ == 1 && precision == 1)) ? 1 : 0;
         const int it64 = e64_->diag(f64, ldpsi, (double2*)psi, eig, thr, maxiter, ntry_max, notconv_max, nc);
         stats_.iters_fp64 = it64;
         stats_.hpsi_bands += e64_->hpsi_bands;
@@ -696,6 +719,10 @@ class David : public DavidBase {
     // the reference's refresh (stale off-diagonal vcc entries) for the FP64 iteration; the FP32 stage of a
     // mixed solve always restarts cleanly
     void set_reference_refresh(bool on) override { e64_->ref_refresh = on; }
+    void set_fp64_gemm(int mode) override {
+        B200_CHECK(mode >= 0 && mode <= 3, kInvalidArgument, "FP64 GEMM mode must be 0, 1, 2 or 3");
+        fp64_gemm_ = mode;
+    }
 
   private:
     int nband_, dim_, cap_, ndim_, precision_;
@@ -704,6 +731,7 @@ class David : public DavidBase {
     cudaStream_t stream_ = 0;
     double mixed_thr_ = 1e-7;
     int low_ndim_ = 0;
+    int fp64_gemm_ = 0;
     DeviceArray<double> pc_;
     DeviceArray<float2> psi32_;
     std::unique_ptr<Engine<double2>> e64_;

@@ -55,6 +55,10 @@ struct DavidBase {
     // solver's own david_ndim); a smaller FP32 subspace means smaller FP64 subspace eigensolves there
     virtual void set_low_ndim(int ndim) = 0;
     virtual void set_reference_refresh(bool on) = 0;
+    // FP64 subspace products: 0 = cuBLAS ZGEMM; 1 = the int8 tensor-core emulation in the FP64 refinement
+    // sweep of a mixed solve; 2 = the int8 emulation in every FP64 stage (1, 2: for the product shapes on
+    // which it is faster); 3 = the int8 emulation for every product of every FP64 stage
+    virtual void set_fp64_gemm(int mode) = 0;
     virtual int precision() const = 0;
     // 0 = quiet; 1 = one line per Davidson iteration on stderr (iteration, basis size, unconverged bands,
     // largest eigenvalue change), the role of DiagoDavid's test_david levels (diago_david.cpp:53-58)

@@ -5,6 +5,7 @@
 // host <-> device copies are the caller's (psi is kept on the device).  This is the entry point a host
 // program uses when psi lives in host memory.
 #include <algorithm>
+#include <vector>
 
 #include "capi_guard.h"
 #include "../../include/abacus_b200.h"
@@ -33,16 +34,19 @@ extern "C" int b200_hamilt_hpsi_host(b200_hamilt* h, int ik, int spin, int nband
         }
         const bool f64 = H->precision == B200_PREC_FP64;
         const size_t row = size_t(ld) * (f64 ? sizeof(double2) : sizeof(float2));  // bytes of one band
-        // piece boundaries: the first and the last piece are half as large as the others (the first upload
-        // and the last download are the two copies nothing overlaps), so the P pieces weigh 1, 2, ..., 2, 1
-        auto bound = [&](int p) -> int {
-            if (p <= 0) return 0;
-            if (p >= P) return nbands;
-            return int(long(nbands) * (2 * p - 1) / (2 * (P - 1)));
-        };
+        // piece boundaries: the first and the last piece are a quarter of the others (the first upload and
+        // the last download are the two copies nothing overlaps, and the H|psi> of a large middle piece runs
+        // at the full-block rate), so the P pieces weigh 1, 4, ..., 4, 1 (two pieces: 1, 1); every piece
+        // keeps at least one band (P <= nbands)
+        std::vector<int> bnd(P + 1, 0);
+        const long total = P == 2 ? 2 : 4L * (P - 2) + 2;  // sum of the weights
+        for (int p = 1; p < P; ++p) bnd[p] = int(long(nbands) * (1 + 4L * (p - 1)) / total);
+        bnd[P] = nbands;
+        for (int p = 1; p < P; ++p) bnd[p] = std::max(bnd[p], bnd[p - 1] + 1);
+        for (int p = P - 1; p >= 1; --p) bnd[p] = std::min(bnd[p], bnd[p + 1] - 1);
         auto piece = [&](int p, int& b0, int& b1) {
-            b0 = bound(p);
-            b1 = bound(p + 1);
+            b0 = bnd[p];
+            b1 = bnd[p + 1];
         };
         // the copies start after the work already queued on the caller's stream (which may still use the
         // device buffers)

@@ -598,6 +598,11 @@ class DiagoDavid:
     def set_mixed_threshold(self, thr):
         call("b200_david_set_mixed_threshold", self._h, float(thr))
 
+    def set_fp64_gemm(self, mode):
+        """FP64 subspace products: 0 cuBLAS ZGEMM, 1 int8 tensor-core emulation in a mixed solve's FP64
+        refinement, 2 in every FP64 iteration (1, 2: on the shapes where it is faster), 3 for every product."""
+        call("b200_david_set_fp64_gemm", self._h, int(mode))
+
     def set_low_ndim(self, ndim):
         """Mixed precision: david_ndim of the FP32 stage (smaller subspace, smaller FP64 eigensolves)."""
         call("b200_david_set_low_ndim", self._h, int(ndim))

@@ -179,7 +179,7 @@ int b200_hamilt_hpsi_nc(b200_hamilt* h, int ik, int nbands, int ld, const void* 
 /* H|psi> between host buffers (psi_h in, hpsi_h out, band b at b*ld, the handle's element type), through
  * the caller's device buffers psi_d / hpsi_d (nbands*ld each): the bands go in npieces pieces through
  * three streams so that the upload of piece p+1, H|psi> of piece p and the download of piece p-1 overlap
- * (the first and last piece are half as large as the others: their copies are not overlapped).
+ * (the first and last piece are a quarter of the others: their copies are not overlapped).
  * Asynchronous: hpsi_h is complete when `stream` is.  Pinned (page-locked) host buffers give the overlap;
  * pageable ones work with synchronous copies.  The handle's copy streams are shared: one call at a time
  * per handle.  No counterpart in the reference (its Operator::hPsi works on device memory,
@@ -398,6 +398,14 @@ int b200_david_set_verbosity(b200_david* d, int level);
 /* Mixed precision only: eigenvalue-change threshold at which the FP32 stage hands over to the
  * FP64 refinement (default 1e-7 Ry; never below the requested thr). */
 int b200_david_set_mixed_threshold(b200_david* d, double thr);
+/* FP64 subspace products of the solver (GEMMs of cal_grad, cal_elem, the orthogonalisation and refresh,
+ * the reference's gemm_op<complex<double>> calls in diago_david.cpp): 0 = cuBLAS ZGEMM (the default);
+ * 1 = the int8 tensor-core emulation of b200_zgemm_i8 in the FP64 refinement sweep of a mixed solve;
+ * 2 = the int8 emulation in every FP64 iteration; 1 and 2 take it for the products on which it is
+ * faster (m n / (m + n) >= 256 and k >= 128 for an m x n result over k terms), cuBLAS for the others;
+ * 3 = the int8 emulation for every product of every FP64 iteration.  The emulation's operand residues
+ * and products are device workspaces grown at their first use.  No counterpart in the reference. */
+int b200_david_set_fp64_gemm(b200_david* d, int mode);
 /* Statistics of the last solve: Davidson iterations in the FP32 stage (mixed only), in FP64,
  * and the number of single-band H applications (all stages). */
 int b200_david_stats(const b200_david* d, int* iters_low, int* iters_fp64, int* hpsi_bands);

@@ -250,17 +250,20 @@ def diamond64(pkg):
     return wl, P.device_hamilt(wl, P.PREC_FP64)
 
 
-@pytest.mark.parametrize("prec", ["fp64", "mixed"])
-def test_david_diamond64_matches_oracle_fixture(pkg, golden, diamond64, prec):
+@pytest.mark.parametrize("prec,gemm", [("fp64", 0), ("mixed", 0), ("fp64", 3), ("mixed", 3)])
+def test_david_diamond64_matches_oracle_fixture(pkg, golden, diamond64, prec, gemm):
     """The 64-atom cell at full size (npw 51 627, 160 bands, 512 projectors, 96^3): the device FP64 and mixed
     Davidson solves to thr 1e-9 reach the oracle's eigenvalues (the reference's DiagoDavid driven by the
-    oracle's H|psi> to thr 1e-11, tests/golden/eig_diamond64.npz) within 1e-8 Ry."""
+    oracle's H|psi> to thr 1e-11, tests/golden/eig_diamond64.npz) within 1e-8 Ry, with the FP64 subspace
+    products on cuBLAS (gemm 0) and on the int8 tensor-core emulation (gemm 3: every product of every FP64
+    iteration, the refinement sweep of the mixed solve included)."""
     P = pkg.pwdft
     wl, h = diamond64
     fx = golden("eig_diamond64")
     nb, ld = wl.spec.nbands, wl.basis.npwk_max
     pc = P.precondition_d(wl.basis, 0)
     dav = P.DiagoDavid(pc, nb, ld, 4, P.PREC_FP64 if prec == "fp64" else P.PREC_MIXED)
+    dav.set_fp64_gemm(gemm)
     x = torch.from_numpy(wl.psi0_h[0][:nb].reshape(-1).copy()).cuda()
     e = np.zeros(nb)
     dav.diag_hamilt(h, 0, ld, x, e, 1e-9, 300)

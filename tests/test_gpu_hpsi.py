@@ -107,7 +107,7 @@ def test_hpsi_is_hermitian_and_linear(pkg):
 
 
 @pytest.mark.parametrize("prec", ["fp64", "mixed"])
-@pytest.mark.parametrize("pieces,pinned", [(1, True), (3, True), (5, False)])
+@pytest.mark.parametrize("pieces,pinned", [(1, True), (3, True), (4, True), (5, False)])
 def test_hpsi_host_pipeline_equals_device_hpsi(pkg, prec, pieces, pinned):
     """b200_hamilt_hpsi_host (host buffers, uploads / H|psi> pieces / downloads overlapped on three streams)
     gives the device H|psi> of the same pieces bit for bit (the projector GEMM of a smaller piece may round
@@ -125,11 +125,19 @@ def test_hpsi_host_pipeline_equals_device_hpsi(pkg, prec, pieces, pinned):
     h.hpsi(0, pdev, whole, nb, ld)
     P_ = min(pieces, nb)
 
-    def bound(q):  # the pipeline's pieces weigh 1, 2, ..., 2, 1 (half-size first and last pieces)
-        return 0 if q <= 0 else nb if q >= P_ else nb * (2 * q - 1) // (2 * (P_ - 1))
+    # the pipeline's pieces weigh 1, 4, ..., 4, 1 (two pieces: 1, 1), at least one band each
+    bnd = [0] * (P_ + 1)
+    total = 2 if P_ == 2 else 4 * (P_ - 2) + 2
+    for q in range(1, P_):
+        bnd[q] = nb * (1 + 4 * (q - 1)) // total
+    bnd[P_] = nb
+    for q in range(1, P_):
+        bnd[q] = max(bnd[q], bnd[q - 1] + 1)
+    for q in range(P_ - 1, 0, -1):
+        bnd[q] = min(bnd[q], bnd[q + 1] - 1)
 
     for q in range(P_):
-        b0, b1 = bound(q), bound(q + 1)
+        b0, b1 = bnd[q], bnd[q + 1]
         h.hpsi(0, pdev[b0 * ld:], ref_d[b0 * ld:], b1 - b0, ld)
     if pinned:
         ph = ph.pin_memory()
