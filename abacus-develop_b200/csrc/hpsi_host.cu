@@ -34,13 +34,14 @@ extern "C" int b200_hamilt_hpsi_host(b200_hamilt* h, int ik, int spin, int nband
         }
         const bool f64 = H->precision == B200_PREC_FP64;
         const size_t row = size_t(ld) * (f64 ? sizeof(double2) : sizeof(float2));  // bytes of one band
-        // piece boundaries: the first and the last piece are a quarter of the others (the first upload and
-        // the last download are the two copies nothing overlaps, and the H|psi> of a large middle piece runs
-        // at the full-block rate), so the P pieces weigh 1, 4, ..., 4, 1 (two pieces: 1, 1); every piece
-        // keeps at least one band (P <= nbands)
+        // piece boundaries: the first and the last piece are half as large as the others (the first upload
+        // and the last download are the two copies nothing overlaps), so the P pieces weigh 1, 2, ..., 2, 1
+        // (two pieces: 1, 1).  Larger middle pieces lengthen the pipeline: the upload of piece 1 and the
+        // download of piece P-2 are on its critical path beside them (B200: 16, 64, 64, 16 bands took 5.1 ms
+        // where 16, 32, 32, 32, 32, 16 took 4.3).  Every piece keeps at least one band (P <= nbands).
         std::vector<int> bnd(P + 1, 0);
-        const long total = P == 2 ? 2 : 4L * (P - 2) + 2;  // sum of the weights
-        for (int p = 1; p < P; ++p) bnd[p] = int(long(nbands) * (1 + 4L * (p - 1)) / total);
+        const long total = 2L * (P - 1);  // sum of the weights
+        for (int p = 1; p < P; ++p) bnd[p] = int(long(nbands) * (2L * p - 1) / total);
         bnd[P] = nbands;
         for (int p = 1; p < P; ++p) bnd[p] = std::max(bnd[p], bnd[p - 1] + 1);
         for (int p = P - 1; p >= 1; --p) bnd[p] = std::min(bnd[p], bnd[p + 1] - 1);

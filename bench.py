@@ -57,9 +57,9 @@ ROOT = Path(__file__).resolve().parent
 WORKLOAD_NAME = ("64-atom diamond supercell a=20.52 bohr, ecut 50 Ry, 96^3 grid, npw 51627, "
                  "160 bands, 512 projectors, Gamma")
 METRIC = "H|psi> bands/s (FP64) + Davidson time-to-1e-8 Ry, mixed vs FP64"
-# band pieces of the end-to-end H|psi> pipeline, timed at set-up (the pipeline makes the first and last
-# piece a quarter of the others: 4 pieces of 160 bands are 16, 64, 64, 16)
-E2E_PIECES = (2, 3, 4, 5, 6)
+# band pieces of the end-to-end H|psi> pipeline, timed at set-up (the pipeline halves the first and last
+# piece: 6 pieces of 160 bands are 16, 32, 32, 32, 32, 16)
+E2E_PIECES = (4, 5, 6, 7, 8, 10)
 # dram__bytes_read.sum + dram__bytes_write.sum of the fused local H|psi> kernels (3 launches: one band chunk
 # of all 160 bands, the autotuner's choice, x 3 passes) for one 160-band FP64 application, from an ncu
 # capture without cache flush (the local-pass traffic summary under profiles/)

@@ -179,7 +179,7 @@ int b200_hamilt_hpsi_nc(b200_hamilt* h, int ik, int nbands, int ld, const void* 
 /* H|psi> between host buffers (psi_h in, hpsi_h out, band b at b*ld, the handle's element type), through
  * the caller's device buffers psi_d / hpsi_d (nbands*ld each): the bands go in npieces pieces through
  * three streams so that the upload of piece p+1, H|psi> of piece p and the download of piece p-1 overlap
- * (the first and last piece are a quarter of the others: their copies are not overlapped).
+ * (the first and last piece are half as large as the others: their copies are not overlapped).
  * Asynchronous: hpsi_h is complete when `stream` is.  Pinned (page-locked) host buffers give the overlap;
  * pageable ones work with synchronous copies.  The handle's copy streams are shared: one call at a time
  * per handle.  No counterpart in the reference (its Operator::hPsi works on device memory,

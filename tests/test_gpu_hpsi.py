@@ -125,11 +125,11 @@ def test_hpsi_host_pipeline_equals_device_hpsi(pkg, prec, pieces, pinned):
     h.hpsi(0, pdev, whole, nb, ld)
     P_ = min(pieces, nb)
 
-    # the pipeline's pieces weigh 1, 4, ..., 4, 1 (two pieces: 1, 1), at least one band each
+    # the pipeline's pieces weigh 1, 2, ..., 2, 1 (two pieces: 1, 1), at least one band each
     bnd = [0] * (P_ + 1)
-    total = 2 if P_ == 2 else 4 * (P_ - 2) + 2
+    total = 2 * (P_ - 1)
     for q in range(1, P_):
-        bnd[q] = nb * (1 + 4 * (q - 1)) // total
+        bnd[q] = nb * (2 * q - 1) // total
     bnd[P_] = nb
     for q in range(1, P_):
         bnd[q] = max(bnd[q], bnd[q - 1] + 1)
