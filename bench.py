@@ -562,6 +562,8 @@ def summary_of(line):
             out[key] = {k: _r(d.get(k)) for k in ("fp64_s", "mixed_s", "speedup", "fp64_to_1e-8_s", "mixed_to_1e-8_s",
                                                    "speedup_to_1e-8", "fp64_err_ry", "mixed_err_ry")}
             out[key]["err_vs"] = d.get("err_vs")
+            if "fp64_int8_s" in d:
+                out[key].update({k: _r(d.get(k)) for k in ("fp64_int8_to_1e-8_s", "speedup_to_1e-8_vs_fp64_int8")})
     sv = line.get("serving")
     if isinstance(sv, dict):
         def lat(x):
@@ -704,12 +706,15 @@ def residual_norms(P, h, x, e, nb, ld):
     return float(norms.max()), ortho
 
 
-def solve_pair(P, h, pc, nb, ld, psi0_h, thr_ref=1e-11, thr=1e-9, repeats=3, e_oracle=None, oracle_what=None):
+def solve_pair(P, h, pc, nb, ld, psi0_h, thr_ref=1e-11, thr=1e-9, repeats=3, e_oracle=None, oracle_what=None,
+               int8_repeats=0):
     """FP64 and mixed solves to thr, alternating, `repeats` each, with per-iteration eigenvalue traces.
     The reference eigenvalues are the oracle's (e_oracle, a fixture) when given, else an FP64 device solve
     to thr_ref; each arm reports the median wall time and time to 1e-8 Ry over its repeats (with min / max),
     its largest eigenvalue error against the reference, and the residual norms of its returned vectors
-    through the pinned FP64 H|psi>."""
+    through the pinned FP64 H|psi>.  int8_repeats > 0 adds an FP64 arm whose subspace products run on the
+    int8 tensor-core emulation where it is faster (b200_david_set_fp64_gemm mode 2; one solver reused, its
+    workspaces grown by an untimed solve first)."""
     import torch
 
     def solve(prec, t_thr, keep=False):
@@ -750,6 +755,31 @@ def solve_pair(P, h, pc, nb, ld, psi0_h, thr_ref=1e-11, thr=1e-9, repeats=3, e_o
                 "max_residual": runs[0][4][0], "orthonormality": runs[0][4][1], "stats": runs[0][2]}
 
     a64, amx = arm(runs64), arm(runsmx)
+    extra = {}
+    if int8_repeats > 0:
+        dav = P.DiagoDavid(pc, nb, ld, 4, P.PREC_FP64)
+        dav.set_fp64_gemm(2)
+        x = torch.from_numpy(psi0_h.copy()).cuda()
+        dav.diag_hamilt(h, 0, ld, x, np.zeros(nb), 1e-4, 300)
+        runs8 = []
+        for _ in range(int8_repeats):
+            dav.set_trace(True)
+            x.copy_(torch.from_numpy(psi0_h))
+            e = np.zeros(nb)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            dav.diag_hamilt(h, 0, ld, x, e, thr, 300)
+            torch.cuda.synchronize()
+            runs8.append((time.perf_counter() - t0, e, dav.stats(), dav.trace(), (None, None)))
+        del dav, x
+        torch.cuda.empty_cache()
+        a8 = arm(runs8)
+        extra = {"fp64_int8_s": a8["median_s"], "fp64_int8_runs_s": a8["runs_s"],
+                 "fp64_int8_to_1e-8_s": a8["to_1e-8_s"], "fp64_int8_err_ry": a8["err_ry"],
+                 "speedup_to_1e-8_vs_fp64_int8": (a8["to_1e-8_s"] / amx["to_1e-8_s"])
+                 if (a8["to_1e-8_s"] and amx["to_1e-8_s"]) else None,
+                 "fp64_int8": "the FP64 solve with its subspace products on the int8 tensor-core emulation of the "
+                              "FP64 products where that is faster (cuBLAS ZGEMM elsewhere)"}
     out = {"fp64_s": a64["median_s"], "mixed_s": amx["median_s"], "speedup": a64["median_s"] / amx["median_s"],
            "fp64_runs_s": a64["runs_s"], "mixed_runs_s": amx["runs_s"],
            "fp64_to_1e-8_s": a64["to_1e-8_s"], "mixed_to_1e-8_s": amx["to_1e-8_s"],
@@ -763,11 +793,12 @@ def solve_pair(P, h, pc, nb, ld, psi0_h, thr_ref=1e-11, thr=1e-9, repeats=3, e_o
            "ref_iters": st_ref[1] if st_ref else None, "thr": thr, "repeats": repeats,
            "timing": "medians over alternating repeats (runs listed); to_1e-8: time after which every Ritz value "
                      "stays within 1e-8 Ry of the reference eigenvalues, from the per-iteration trace; residuals "
-                     "|Hx - ex| of the first repeat's vectors through the FP64 H|psi>"}
+                     "|Hx - ex| of the first repeat's vectors through the FP64 H|psi>", **extra}
     return out
 
 
 EIG_FIXTURE_64 = ROOT / "tests" / "golden" / "eig_diamond64.npz"
+EIG_FIXTURE_216 = ROOT / "tests" / "golden" / "eig_diamond216.npz"
 
 
 def davidson_bench(P, wl, h64):
@@ -1008,9 +1039,15 @@ def davidson_216(pkg):
     pc = P.precondition_d(basis, 0)
     # five alternating repeats, medians reported with every run listed: a solve synchronises with the host
     # every iteration, and a stall of the shared host cores shows up in single repeats.  The errors are
-    # against an FP64 solve to 1e-10; the residual norms through the FP64 H|psi> (pinned to the oracle at
+    # against the oracle's eigenvalues (tests/golden/eig_diamond216.npz: the reference's DiagoDavid on the
+    # oracle's H|psi>) where that fixture exists, else against an FP64 device solve to 1e-10; the residual norms through the FP64 H|psi> (pinned to the oracle at
     # 1e-12 on this cell by the tests) bound every returned eigenvalue's distance to the spectrum
-    out = solve_pair(P, h, pc, spec.nbands, ld, psi0, thr_ref=1e-10, repeats=5)
+    if EIG_FIXTURE_216.exists():
+        fx = np.load(EIG_FIXTURE_216)
+        out = solve_pair(P, h, pc, spec.nbands, ld, psi0, repeats=5, e_oracle=fx["eig"], int8_repeats=3,
+                         oracle_what=f"oracle fixture eig_diamond216.npz ({fx['solver']}, thr {float(fx['thr'])})")
+    else:
+        out = solve_pair(P, h, pc, spec.nbands, ld, psi0, thr_ref=1e-10, repeats=5, int8_repeats=3)
     out["workload"] = (f"216-atom diamond supercell a=30.78 bohr, ecut 40 Ry, 128^3 grid, npw {int(basis.npwk[0])}, "
                        f"480 bands, 1728 projectors (device getvnl), Gamma")
     out["setup_s"] = setup

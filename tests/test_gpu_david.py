@@ -3,7 +3,9 @@
 * the pyabacus golden case (Si2.mat, 16 bands) through the callback HPsiFunc
   interface: eigenvalues within 1e-8 of scipy's eigsh (test_hsolver.py:52-59);
 * the 8-atom workload, FP64 and mixed precision, within 1e-8 Ry of the oracle's
-  Davidson (the restated reference algorithm) run to the same threshold.
+  Davidson (the restated reference algorithm) run to the same threshold;
+* the 64- and 216-atom cells at full size, FP64 and mixed precision, within 1e-8 Ry of
+  eigenvalue fixtures made by the reference's compiled DiagoDavid on the oracle's H|psi>.
 """
 from __future__ import annotations
 
@@ -269,3 +271,36 @@ def test_david_diamond64_matches_oracle_fixture(pkg, golden, diamond64, prec, ge
     dav.diag_hamilt(h, 0, ld, x, e, 1e-9, 300)
     torch.cuda.synchronize()
     assert np.max(np.abs(e - fx["eig"])) < 1e-8
+
+
+def test_david_diamond216_matches_oracle_fixture(pkg, golden):
+    """The 216-atom cell at full size (a = 30.78 bohr, ecut 40 Ry, 128^3 grid, npw 124 289, 480 bands, 1728
+    projectors built on the device by getvnl): the device FP64 and mixed Davidson solves to thr 1e-9 reach
+    the oracle's eigenvalues (the reference's DiagoDavid driven by the oracle's H|psi>, with the oracle's
+    getvnl projectors, to thr 1e-10: tests/golden/eig_diamond216.npz) within 1e-8 Ry."""
+    P = pkg.pwdft
+    S = pkg.synth
+    fx = golden("eig_diamond216")
+    spec = S.config(4)
+    cell = S.make_cell(spec)
+    basis = P.PWBasisK(spec.a, cell.latvec, spec.ecut, np.zeros((1, 3)), grid=spec.grid)
+    ld, nb = basis.npwk_max, spec.nbands
+    h = P.HamiltPW(basis, P.PREC_FP64)
+    veff = torch.from_numpy(cell.veff(basis.nx, basis.ny, basis.nz)).cuda()
+    deeq = torch.from_numpy(cell.deeq()).cuda()
+    h.set_veff(veff)
+    h.set_deeq([cell.nat], [S.NH], deeq)
+    h.set_projectors(cell.projector_tables(basis.omega, spec.ecut), cell.tau / spec.a)
+    h.build_vkb(0)
+    psi0 = cell.psi0(basis.gplusk_cart(0), nb, ld).reshape(-1)
+    pc = P.precondition_d(basis, 0)
+    for prec in (P.PREC_FP64, P.PREC_MIXED):
+        dav = P.DiagoDavid(pc, nb, ld, 4, prec)
+        x = torch.from_numpy(psi0.copy()).cuda()
+        e = np.zeros(nb)
+        dav.diag_hamilt(h, 0, ld, x, e, 1e-9, 300)
+        torch.cuda.synchronize()
+        err = np.max(np.abs(e - fx["eig"]))
+        assert err < 1e-8, (prec, err)
+        del dav, x
+        torch.cuda.empty_cache()
