@@ -209,6 +209,9 @@ template <typename T> struct Engine {
     // products, gemm_oz.h) instead of cuBLAS ZGEMM; op(A) residues and products are workspaces grown at
     // first use.  0: cuBLAS; 1: the emulation for the products it is faster on; 2: for every product
     int oz = 0;
+    // FP64 engine of a mixed solve: the start vectors are the FP32 stage's Ritz vectors (first try only)
+    bool handover = false;
+    int ntry_ = 0;
     OzOperand ozA;
     OzWorkspace ozw;
     int lwork = 0;
@@ -423,7 +426,9 @@ template <typename T> struct Engine {
     // column or its Cholesky failed.  The reference orthogonalises each new vector once
     // (diago_david.cpp, SchmidtOrth); the 216-atom FP32 stage runs the same iterations with one pass as with
     // two and 10 % faster.
-    void orth_block(T* X, int nc, int nprev) {
+    // one_pass: X is orthonormal to a few ulps of the lower precision already (the Ritz vectors the FP32 stage
+    // of a mixed solve hands over): one Cholesky-QR pass brings it to FP64 orthonormality
+    void orth_block(T* X, int nc, int nprev, bool one_pass = false) {
         const T one = cmake<T>(1, 0), zero = cmake<T>(0, 0), mone = cmake<T>(-1, 0);
         // small blocks always take both passes: their products are latency-bound, the second pass costs
         // little, and k-point solves of 32 bands took 15 % more iterations with one
@@ -440,6 +445,7 @@ template <typename T> struct Engine {
                 gemm(CUBLAS_OP_N, CUBLAS_OP_N, dim, nc, nprev, mone, basis.ptr, ld, lag.ptr, L, one, X, ld);
             }
             cholqr(X, nc, adaptive && pass == 0);
+            if (one_pass) break;
             if (adaptive && pass == 0) {
                 int fl[2] = {0, 0};  // Cholesky info, cancellation flag: either asks for the second pass
                 B200_CUDA(cudaMemcpyAsync(fl, info.ptr + 1, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -547,7 +553,7 @@ template <typename T> struct Engine {
         B200_CUDA(cudaMemsetAsync(info.ptr, 0, 4 * sizeof(int), s));
         B200_CUDA(cudaMemcpy2DAsync(basis.ptr, ld * sizeof(T), psi, size_t(ldpsi) * sizeof(T), dim * sizeof(T), nband,
                                     cudaMemcpyDeviceToDevice, s));
-        orth_block(basis.ptr, nband, 0);
+        orth_block(basis.ptr, nband, 0, handover && ntry_ == 0);
         f(basis.ptr, hp.ptr, nbase_x, ld, 0, nband - 1, s);
         hpsi_bands += nband;
         cal_elem(0, nband);
@@ -596,6 +602,7 @@ template <typename T> struct Engine {
              int& notconv) {
         int ntry = 0, total = 0;
         notconv = 0;
+        ntry_ = 0;
         reorth = 0;
         // a fresh subspace, as a newly constructed DiagoDavid has (diago_david.cpp:34-148): the refresh reads
         // columns of vcc that this solve may not have written, so a reused solver must start from zeros
@@ -604,6 +611,7 @@ template <typename T> struct Engine {
         do {
             total += diag_once(f, ldpsi, psi, eig, thr, maxiter, notconv);
             ++ntry;
+            ntry_ = ntry;
         } while (!(ntry > ntry_max || notconv <= notconv_max));
         return total;
     }
@@ -632,6 +640,7 @@ class David : public DavidBase {
         e64_->trace = &trace_;
         e64_->hpsi_bands = 0;
         e64_->oz = fp64_gemm_ == 3 ? 2 : fp64_gemm_ == 2 ? 1 : 0;
+        e64_->handover = false;
         int nc = 0;
         const int it = e64_->diag(f64, ldpsi, (double2*)psi, eig, thr, maxiter, ntry_max, notconv_max, nc);
         stats_.iters_fp64 = it;
@@ -679,6 +688,7 @@ class David : public DavidBase {
         }
         e64_->hpsi_bands = 0;
         e64_->oz = fp64_gemm_ == 3 ? 2 : (fp64_gemm_ == 2 || (fp64_gemm_ == 1 && precision == 1)) ? 1 : 0;
+        e64_->handover = precision == 1;
         const int it64 = e64_->diag(f64, ldpsi, (double2*)psi, eig, thr, maxiter, ntry_max, notconv_max, nc);
         stats_.iters_fp64 = it64;
         stats_.hpsi_bands += e64_->hpsi_bands;

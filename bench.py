@@ -1035,6 +1035,19 @@ def davidson_216(pkg):
     cell, basis, h = device_cell(pkg, spec)
     ld = basis.npwk_max
     psi0 = cell.psi0(basis.gplusk_cart(0), spec.nbands, ld).reshape(-1)
+    # the autotuner picks the local pass's band chunk and plane variant on this cell: the chunk of the FP64
+    # handle (used by both precisions of its solves) and the FP64 variant on it, the FP32 variant on an FP32
+    # handle of the same basis (plane variants are kept per basis and precision)
+    import torch
+    x = torch.from_numpy(psi0).cuda()
+    hx = torch.zeros_like(x)
+    tuned64 = h.autotune(0, x, hx, spec.nbands, ld, with_variant=True)
+    h32 = P.HamiltPW(basis, P.PREC_MIXED)
+    h32.set_veff(h._keep[-2])
+    x32, hx32 = x.to(torch.complex64), hx.to(torch.complex64)
+    tuned32 = h32.autotune(0, x32, hx32, spec.nbands, ld, with_variant=True)
+    del x, hx, x32, hx32, h32
+    torch.cuda.empty_cache()
     setup = time.perf_counter() - t0
     pc = P.precondition_d(basis, 0)
     # five alternating repeats, medians reported with every run listed: a solve synchronises with the host
@@ -1051,6 +1064,7 @@ def davidson_216(pkg):
     out["workload"] = (f"216-atom diamond supercell a=30.78 bohr, ecut 40 Ry, 128^3 grid, npw {int(basis.npwk[0])}, "
                        f"480 bands, 1728 projectors (device getvnl), Gamma")
     out["setup_s"] = setup
+    out["autotuned_chunk_variant"] = {"fp64": list(tuned64), "fp32_variant": tuned32[1]}
     return out
 
 
