@@ -125,7 +125,6 @@ _SIGS = {
     "b200_david_set_stream": ([vp, vp], i32),
     "b200_david_set_mixed_threshold": ([vp, f64], i32),
     "b200_david_set_fp64_gemm": ([vp, i32], i32),
-    "b200_david_set_fp32_refresh": ([vp, i32], i32),
     "b200_dav_subspace_create": ([i32, i32, i32, f64, i32, i32, vp, C.POINTER(vp)], i32),
     "b200_dav_subspace_destroy": ([vp], i32),
     "b200_dav_subspace_diag": ([vp, HPSI_CB, vp, vp, i32, pf64, pi32, i32, pi32], i32),

@@ -445,12 +445,6 @@ int b200_david_set_mixed_threshold(b200_david* d, double thr) {
         d->d->set_mixed_thr(thr);
     });
 }
-int b200_david_set_fp32_refresh(b200_david* d, int factor) {
-    return guarded([&] {
-        B200_CHECK(d != nullptr, b200::kInvalidArgument, "NULL argument");
-        d->d->set_fp32_refresh(factor);
-    });
-}
 int b200_david_set_fp64_gemm(b200_david* d, int mode) {
     return guarded([&] {
         B200_CHECK(d != nullptr, b200::kInvalidArgument, "NULL argument");

@@ -212,7 +212,6 @@ template <typename T> struct Engine {
     // FP64 engine of a mixed solve: the start vectors are the FP32 stage's Ritz vectors (first try only)
     bool handover = false;
     int ntry_ = 0;
-    int late_refresh = 0;  // FP32 engine: early restart factor (0: restart only when the basis is full)
     OzOperand ozA;
     OzWorkspace ozw;
     int lwork = 0;
@@ -587,12 +586,7 @@ template <typename T> struct Engine {
                              "[david %s] iter %3d nbase %4d notconv %4d max|dE| %.3e  t(hpsi/lin/eig) %.3f %.3f %.3f  "
                              "second passes %d\n",
                              kF32 ? "fp32" : "fp64", iter, nbase, notconv, dmax, t_hpsi, t_lin, t_eig, reorth);
-            // FP32 stage of a mixed solve with late_refresh = f > 0: also restart from the Ritz vectors once at
-            // most nband / f bands remain unconverged and the basis holds more than f times their number of
-            // extra vectors, so that the last iterations' subspace eigensolves stay small
-            const bool late = kF32 && late_refresh > 0 && long(notconv) * late_refresh <= nband &&
-                              nbase > nband + late_refresh * notconv;
-            if (notconv == 0 || nbase + notconv > nbase_x || iter == maxiter || late) {
+            if (notconv == 0 || nbase + notconv > nbase_x || iter == maxiter) {
                 B200_CUDA(cudaMemsetAsync(psi, 0, size_t(nband) * ldpsi * sizeof(T), s));
                 gemm(CUBLAS_OP_N, CUBLAS_OP_N, dim, nband, nbase, one, basis.ptr, ld, vcc.ptr, nbase_x, zero, psi, ldpsi);
                 if (notconv == 0 || iter == maxiter) break;
@@ -675,7 +669,6 @@ class David : public DavidBase {
             // mixed vectors (the 216-atom stage ran 20 % longer); smaller blocks keep the reference's refresh,
             // with which 32-band k-point solves took 25 iterations instead of 29
             e32_->ref_refresh = e64_->ref_refresh && nband_ < 128;
-            e32_->late_refresh = fp32_refresh_;
             e32_->trace = &trace_;
             e32_->verbosity = verbosity_;
             e32_->hpsi_bands = 0;
@@ -736,10 +729,6 @@ class David : public DavidBase {
     // the reference's refresh (stale off-diagonal vcc entries) for the FP64 iteration; the FP32 stage of a
     // mixed solve always restarts cleanly
     void set_reference_refresh(bool on) override { e64_->ref_refresh = on; }
-    void set_fp32_refresh(int factor) override {
-        B200_CHECK(factor >= 0, kInvalidArgument, "FP32 restart factor must be >= 0");
-        fp32_refresh_ = factor;
-    }
     void set_fp64_gemm(int mode) override {
         B200_CHECK(mode >= 0 && mode <= 3, kInvalidArgument, "FP64 GEMM mode must be 0, 1, 2 or 3");
         fp64_gemm_ = mode;
@@ -753,7 +742,6 @@ class David : public DavidBase {
     double mixed_thr_ = 1e-7;
     int low_ndim_ = 0;
     int fp64_gemm_ = 0;
-    int fp32_refresh_ = 0;
     DeviceArray<double> pc_;
     DeviceArray<float2> psi32_;
     std::unique_ptr<Engine<double2>> e64_;

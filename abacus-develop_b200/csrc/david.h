@@ -59,10 +59,6 @@ struct DavidBase {
     // sweep of a mixed solve; 2 = the int8 emulation in every FP64 stage (1, 2: for the product shapes on
     // which it is faster); 3 = the int8 emulation for every product of every FP64 stage
     virtual void set_fp64_gemm(int mode) = 0;
-    // mixed precision only: the FP32 stage also restarts from its Ritz vectors once at most nband / factor
-    // bands remain unconverged and the basis holds more than factor times their number of extra vectors
-    // (0: restart only when the basis is full, as the reference)
-    virtual void set_fp32_refresh(int factor) = 0;
     virtual int precision() const = 0;
     // 0 = quiet; 1 = one line per Davidson iteration on stderr (iteration, basis size, unconverged bands,
     // largest eigenvalue change), the role of DiagoDavid's test_david levels (diago_david.cpp:53-58)

@@ -603,11 +603,6 @@ class DiagoDavid:
         refinement, 2 in every FP64 iteration (1, 2: on the shapes where it is faster), 3 for every product."""
         call("b200_david_set_fp64_gemm", self._h, int(mode))
 
-    def set_fp32_refresh(self, factor):
-        """Mixed precision: the FP32 stage also restarts once at most nband/factor bands remain unconverged and
-        the basis holds more than factor times their number of extra vectors (0: only when full)."""
-        call("b200_david_set_fp32_refresh", self._h, int(factor))
-
     def set_low_ndim(self, ndim):
         """Mixed precision: david_ndim of the FP32 stage (smaller subspace, smaller FP64 eigensolves)."""
         call("b200_david_set_low_ndim", self._h, int(ndim))

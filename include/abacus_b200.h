@@ -406,12 +406,6 @@ int b200_david_set_mixed_threshold(b200_david* d, double thr);
  * 3 = the int8 emulation for every product of every FP64 iteration.  The emulation's operand residues
  * and products are device workspaces grown at their first use.  No counterpart in the reference. */
 int b200_david_set_fp64_gemm(b200_david* d, int mode);
-/* Mixed precision only: the FP32 stage also restarts from its Ritz vectors (the refresh of
- * diago_david.cpp:797-934) once at most nband / factor bands remain unconverged and the basis holds more
- * than factor times their number of extra vectors, so that its last subspace eigensolves stay small;
- * 0 (the default) restarts only when the basis is full, as the reference.  No counterpart in the
- * reference. */
-int b200_david_set_fp32_refresh(b200_david* d, int factor);
 /* Statistics of the last solve: Davidson iterations in the FP32 stage (mixed only), in FP64,
  * and the number of single-band H applications (all stages). */
 int b200_david_stats(const b200_david* d, int* iters_low, int* iters_fp64, int* hpsi_bands);
