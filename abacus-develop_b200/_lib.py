@@ -70,6 +70,7 @@ _SIGS = {
     "b200_hamilt_autotune": ([vp, i32, i32, i32, vp, vp, vp, pi32, pi32], i32),
     "b200_hamilt_set_plane_variant": ([vp, i32], i32),
     "b200_hamilt_set_band_chunk": ([vp, i32], i32),
+    "b200_server_set_express": ([vp, i32, f64], i32),
     "b200_server_set_policy": ([vp, i32, f64], i32),
     "b200_elecstate_pw_op_f64": ([i32, i32, f64, C.POINTER(vp), vp, vp], i32),
     "b200_elecstate_pw_op_f32": ([i32, i32, f32, C.POINTER(vp), vp, vp], i32),

@@ -120,7 +120,7 @@ class Server {
         B200_CHECK(david_ndim >= 2, kInvalidArgument, "david_ndim must be at least 2");
         B200_CUDA(cudaGetDevice(&dev_));
         t0_ = std::chrono::steady_clock::now();
-        for (int w = 0; w < nworkers; ++w) workers_.emplace_back([this] { worker(); });
+        for (int w = 0; w < nworkers; ++w) workers_.emplace_back([this, w] { worker(w); });
     }
     ~Server() {
         {
@@ -183,7 +183,8 @@ class Server {
             cv_done_.notify_all();
         } else {
             queue_.push_back(p);
-            cv_work_.notify_one();
+            // every worker re-checks: an express worker may not take this request while another could
+            cv_work_.notify_all();
         }
         return p->id;
     }
@@ -228,6 +229,18 @@ class Server {
         std::lock_guard<std::mutex> lk(mu_);
         return shed_count_;
     }
+    // workers 0 .. n-1 take only requests of cells whose mean service time is at most max_service_s (cells
+    // not yet timed included), so that short solves never wait behind a full set of long ones
+    void set_express(int n, double max_service_s) {
+        B200_CHECK(n >= 0 && n < int(workers_.size()), kInvalidArgument, "express workers: 0 .. nworkers-1");
+        B200_CHECK(max_service_s >= 0, kInvalidArgument, "express service bound must be >= 0");
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            n_express_ = n;
+            express_s_ = max_service_s;
+        }
+        cv_work_.notify_all();
+    }
 
     void stats(double* out) {
         std::lock_guard<std::mutex> lk(mu_);
@@ -271,7 +284,7 @@ class Server {
     // oldest, policy 1 the highest response ratio (wait + S_c) / S_c (S_c: running mean service time of the
     // cell; a cell not yet timed counts as the shortest).  With shedding on, requests that waited past
     // shed_factor * S_c are completed as shed first.
-    std::deque<Request*>::iterator next_admissible_locked() {
+    std::deque<Request*>::iterator next_admissible_locked(bool express) {
         const double now = now_s(t0_);
         if (shed_factor_ > 0) {
             bool shed = false;
@@ -299,6 +312,7 @@ class Server {
             const int c = (*it)->cell;
             if (seen[c]) continue;
             seen[c] = 1;
+            if (express && svc_mean_[c] > express_s_) continue;
             if (!(cells_[c].inflight < cells_[c].max_inflight && can_admit_locked(**it))) continue;
             if (policy_ == 0) return it;  // the queue is in arrival order: the first admissible one is the oldest
             const double sc = svc_mean_[c];
@@ -409,14 +423,14 @@ class Server {
         B200_CUDA(cudaStreamSynchronize(s));
     }
 
-    void worker() {
+    void worker(int id) {
         cudaSetDevice(dev_);
         std::unique_lock<std::mutex> lk(mu_);
         for (;;) {
             std::deque<Request*>::iterator pick;
             cv_work_.wait(lk, [&] {
                 if (stop_) return true;
-                pick = next_admissible_locked();
+                pick = next_admissible_locked(id < n_express_);
                 return pick != queue_.end();
             });
             if (stop_) break;
@@ -476,6 +490,8 @@ class Server {
     int ndim_;
     int policy_ = 0;
     double shed_factor_ = 0;
+    int n_express_ = 0;
+    double express_s_ = 0;
     long long shed_count_ = 0;
     std::vector<double> svc_mean_;  // per cell
     int dev_ = 0;
@@ -560,6 +576,13 @@ int b200_server_set_policy(b200_server* s, int policy, double shed_factor) {
     return guarded([&] {
         B200_CHECK(s != nullptr, b200::kInvalidArgument, "NULL argument");
         s->s->set_policy(policy, shed_factor);
+    });
+}
+
+int b200_server_set_express(b200_server* s, int nworkers, double max_service_s) {
+    return guarded([&] {
+        B200_CHECK(s != nullptr, b200::kInvalidArgument, "NULL argument");
+        s->s->set_express(nworkers, max_service_s);
     });
 }
 

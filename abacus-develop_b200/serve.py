@@ -59,6 +59,11 @@ class Server:
         completes requests that waited past shed_factor * S_c with STATUS_SHED (S_c: the cell's mean service)."""
         call("b200_server_set_policy", self._h, int(policy), float(shed_factor))
 
+    def set_express(self, nworkers: int = 0, max_service_s: float = 0.0):
+        """Workers 0..nworkers-1 take only requests of cells whose mean service time is at most max_service_s
+        (cells not yet timed included); 0 turns it off."""
+        call("b200_server_set_express", self._h, int(nworkers), float(max_service_s))
+
     def add_cell(self, hamilt: HamiltPW, max_inflight: int = 2) -> int:
         """Register a resident cell; at most max_inflight of its requests run at once."""
         cid = C.c_int()

@@ -524,6 +524,11 @@ int b200_server_drain(b200_server* s);
  * a queued request that has waited longer than shed_factor * S_c is completed with B200_STATUS_SHED
  * instead of being run (bounded latency under overload); 0 never sheds.  Default: 0 and 0. */
 int b200_server_set_policy(b200_server* s, int policy, double shed_factor);
+/* Express workers (no counterpart in the reference): workers 0 .. nworkers-1 take only requests of cells
+ * whose running mean service time is at most max_service_s (cells not yet timed included), so that short
+ * solves never wait behind a full set of long ones; the other workers serve every cell under the
+ * admission policy.  nworkers in 0 .. (workers of the server) - 1; 0 (the default) turns it off. */
+int b200_server_set_express(b200_server* s, int nworkers, double max_service_s);
 /* out6: pooled slot bytes, peak pooled bytes, peak requests in flight, slots created, slots evicted,
  * seconds since creation. */
 int b200_server_stats(b200_server* s, double* out6);

@@ -89,6 +89,7 @@ def test_solver_entry_points_reject_bad_arguments_without_gpu_calls(pkg):
         (lib.b200_bpcg_set_stream, (None, None), b"NULL"),
         (lib.b200_bpcg_stats, (None, None, None), b"NULL"),
         (lib.b200_david_set_fp64_gemm, (None, 1), b"NULL"),
+        (lib.b200_server_set_express, (None, 1, 0.03), b"NULL"),
     ]
     for fn, args, msg in cases:
         assert fn(*args) == 1, fn.__name__

@@ -87,7 +87,8 @@ def test_budget_too_small_is_rejected(served):
 def test_admission_policy_and_shedding(served):
     """The response-ratio policy serves every request of a burst with the same eigenvalues as first come, first
     served; with shedding on, requests that waited past the bound come back as STATUS_SHED, the others are
-    served correctly and the server keeps serving afterwards."""
+    served correctly and the server keeps serving afterwards; with express workers (reserved for cells of
+    short service) every request is still served, with the results it has alone."""
     S, srv, cells, ids = served
     c = 1
     probe = (ids[c], 2, cells[c].nbands)
@@ -116,7 +117,20 @@ def test_admission_policy_and_shedding(served):
         for r in res:
             if r.status == 0 and r.tag[1] % 4 == 2:
                 assert np.max(np.abs(r.eig - ref.eig)) <= 1e-10
+        # express workers: one that takes no timed cell (bound 1 ns), then two that take every cell; every
+        # request is served with the results it has alone
+        srv.set_policy(1, 0.0)
+        for nexp, bound in ((1, 1e-9), (2, 10.0)):
+            srv.set_express(nexp, bound)
+            for i in range(8):
+                srv.submit(ids[i % 2], i % 4, cells[i % 2].nbands, thr=1e-9, tag=("x", i))
+            srv.submit(*probe, thr=1e-9, tag="probe")
+            res = srv.drain()
+            assert len(res) == 9 and all(r.status == 0 for r in res)
+            got = [r for r in res if r.tag == "probe"][0]
+            assert np.max(np.abs(got.eig - ref.eig)) <= 1e-10
     finally:
+        srv.set_express(0, 0.0)
         srv.set_policy(0, 0.0)
     srv.submit(*probe, thr=1e-9)
     after = srv.drain()
