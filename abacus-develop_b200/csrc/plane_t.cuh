@@ -324,6 +324,19 @@ __global__ void __launch_bounds__(NT, MINB) k_plane_t(PlaneMapView pm, int nz, c
 namespace b200 {
 namespace plane_t {
 
+// One complex value global -> shared memory as an asynchronous copy (cp.async, 8 or 16 bytes): the value does
+// not pass through a register, so a thread has all its copies of a loop in flight at once; cp_async_wait_all
+// then __syncthreads make them visible to the CTA.
+template <typename T> __device__ __forceinline__ void cp_async_value(T* dst_shared, const T* src_global) {
+    static_assert(sizeof(T) == 8 || sizeof(T) == 16, "complex float or double");
+    const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst_shared));
+    if constexpr (sizeof(T) == 16)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src_global) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src_global) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 // ---- z passes on the two-pass transforms (nz = R1 * R2), TS sticks per CTA, NT threads ----
 // The stick buffer keeps the layout of the warp-shuffle z passes: plane slot s holds z = zslot_to_z(s), so
 // the plane passes and psi -> rho see the same buffer whichever z pass wrote it.  In shared memory a stick
@@ -353,10 +366,12 @@ __global__ void __launch_bounds__(NT) k_zinv_t(Src src, int b0, int nbc, const T
     __syncthreads();
     const T* p = reinterpret_cast<const T*>(e.psi) + size_t(b0 + band) * e.ld;
     const int j0 = sm.gofs[s0], j1 = sm.gofs[s0 + ns];
+    // the sphere's values straight into their stick positions, every copy of the loop in flight at once
     for (int j = j0 + tid; j < j1; j += NT) {
         const int pk = sm.gpk[j];
-        A[((pk >> 10) - s0) * LDZ + zpos_natural<R1, R2>(pk & 1023)] = p[sm.glist[j]];
+        cp_async_value(A + ((pk >> 10) - s0) * LDZ + zpos_natural<R1, R2>(pk & 1023), p + sm.glist[j]);
     }
+    cp_async_wait_all();
     __syncthreads();
     for (int i = tid; i < ns * R2; i += NT) {
         const int sl = i / R2, t = i % R2;
@@ -407,11 +422,13 @@ __global__ void __launch_bounds__(NT) k_zfwd_t(Src src, int b0, int nbc, const T
     Twiddles<T, NZ, R1, R2, NT> tw;
     tw.load(roots, tid);
     const T* in = sb + (size_t(blockIdx.z) * nbc + band) * NZ * sm.nst;
+    // the stick planes of this tile (ns sticks of every z slot) as asynchronous copies, all in flight at once
     for (int i = tid; i < ns * NZ; i += NT) {
         const int sz = i / ns;
         const int sl = i - sz * ns;
-        A[sl * LDZ + zpos_output<R1, R2>(zslot_to_z(sz, NZ / 32))] = in[size_t(sz) * sm.nst + s0 + sl];
+        cp_async_value(A + sl * LDZ + zpos_output<R1, R2>(zslot_to_z(sz, NZ / 32)), in + size_t(sz) * sm.nst + s0 + sl);
     }
+    cp_async_wait_all();
     __syncthreads();
     for (int i = tid; i < ns * R1; i += NT) {
         const int sl = i / R1, k1 = i % R1;
