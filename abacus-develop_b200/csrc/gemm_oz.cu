@@ -846,8 +846,8 @@ void oz_zgemm(char opa, int M, int N, int K, double2 alpha, const OzOperand& a, 
 
     // tiles: 128 msub rows of op(A) x BN real columns (BN <= 256, a multiple of 16)
     const int colsB = 2 * N;
-    int tn = (colsB + 255) / 256;
-    int BN = int(round_up((colsB + tn - 1) / tn, 16));
+    const int tn = (colsB + 255) / 256;
+    const int BN = int(round_up((colsB + tn - 1) / tn, 16));
     const int tm128 = (M + 127) / 128;
     const int nk = (a.kr + 127) / 128;
     int sms = 148, dev = 0;
@@ -877,22 +877,10 @@ void oz_zgemm(char opa, int M, int N, int K, double2 alpha, const OzOperand& a, 
     (void)tiles128;
     const int per = (nk + splits - 1) / splits;
     splits = (nk + per - 1) / per;
-    const int fixed = 1024 + 256;  // alignment slack, barriers
-    // a resident B' that leaves fewer than 8 stages of A takes narrower column tiles (down to 64 columns; the
-    // group's CTAs share each A tile through L2): with B' of 160 columns x 1024 K bytes only four 16 KB stages
-    // of A fit, too few to cover the memory latency at the int8 MMA rate (tensor pipe 27 %)
-    if (long(per) * BN * 128 + 3L * kOzATile + fixed <= kOzSmem) {
-        for (int t = tn + 1; t <= 8 && t <= sms; ++t) {
-            if ((kOzSmem - fixed - long(per) * BN * 128) / kOzATile >= 8) break;
-            const int bn = int(round_up((colsB + t - 1) / t, 16));
-            if (bn < 64) break;
-            tn = t;
-            BN = bn;
-        }
-    }
     // B' of one (plane, column tile) resident in shared memory when it leaves room for 3 stages of A; else
     // streamed with A, and long K ranges take 256-row tiles (two accumulators: half the re-reads of B')
     const int b_box = BN * 128;
+    const int fixed = 1024 + 256;  // alignment slack, barriers
     OzSched sc{tm128, tn, a.n * splits, per, nk, 1, 2, false};
     int stages;
     if (tn <= sms && long(per) * b_box + 3L * kOzATile + fixed <= kOzSmem) {
