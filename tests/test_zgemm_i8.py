@@ -129,6 +129,9 @@ CASES = [
     ("N", 100, 40, 37, 0, 1.0, 0.0),
     ("C", 64, 70, 5000, 3, 0.5 - 1.5j, 2.0 + 0.5j),
     ("N", 3000, 160, 512, 0, 1.0, 1.0),
+    # B' resident in shared memory with fewer K blocks; a last column tile partly empty
+    ("N", 1500, 160, 384, 0, 1.0, 0.5),
+    ("N", 1000, 150, 512, 2, 1.0 - 0.5j, 0.0),
     ("C", 512, 160, 51627, 0, 1.0, 0.0),
     ("C", 33, 17, 129, 1, 1.0j, -1.0),
     ("N", 1, 1, 1, 1, 1.0, 0.0),
