@@ -25,6 +25,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <cstring>
 #include <vector>
 
 #include "common.h"
@@ -217,6 +218,9 @@ template <typename T> struct Engine {
     int lwork = 0;
     std::vector<double> eig_h;
     std::vector<int> unconv_h;
+    // page-locked copy of the unconverged-band list: its upload is an asynchronous copy (from pageable
+    // memory the copy would wait for the stream first, one more host round trip per iteration)
+    int* unconv_pin = nullptr;
     bool ref_refresh = true;
     int hpsi_bands = 0;
     int verbosity = 0;
@@ -264,14 +268,14 @@ template <typename T> struct Engine {
         ein.resize(nband);
         pc.resize(dim);
         unconv_d.resize(nband);
-        info.resize(4);
+        info.resize(5);  // eigensolver, Cholesky, cancellation, non-finite flags; the GEMMs' wait error word
         if constexpr (kF32) cn2.resize(nband);
         B200_CUDA(cudaMemsetAsync(hcc.ptr, 0, hcc.n * sizeof(T), s));
         B200_CUDA(cudaMemsetAsync(vcc.ptr, 0, vcc.n * sizeof(T), s));
         B200_CUDA(cudaMemsetAsync(basis.ptr, 0, basis.n * sizeof(T), s));
         B200_CUDA(cudaMemsetAsync(hp.ptr, 0, hp.n * sizeof(T), s));
         B200_CUDA(cudaMemsetAsync(newv.ptr, 0, newv.n * sizeof(T), s));
-        B200_CUDA(cudaMemsetAsync(info.ptr, 0, 4 * sizeof(int), s));
+        B200_CUDA(cudaMemsetAsync(info.ptr, 0, 5 * sizeof(int), s));
         if constexpr (std::is_same<R, double>::value) {
             B200_CUDA(cudaMemcpyAsync(pc.ptr, precond_d, dim * sizeof(double), cudaMemcpyDeviceToDevice, s));
         } else {
@@ -291,6 +295,7 @@ template <typename T> struct Engine {
         work.resize(size_t(lwork > 0 ? lwork : 1));
         eig_h.assign(nbase_x, 0.0);
         unconv_h.assign(nband, 0);
+        B200_CUDA(cudaHostAlloc(&unconv_pin, size_t(nband) * sizeof(int), cudaHostAllocDefault));
         if constexpr (kF32) {
             // tensor-core GEMM workspaces for every subspace product of this engine, so that a solve allocates
             // nothing: split-K partial tiles of up to 16 splits of the largest C (nband x nbase_x), and B split
@@ -319,6 +324,7 @@ template <typename T> struct Engine {
                pc.n * sizeof(R) + tcw.device_bytes() + ozA.device_bytes() + ozw.device_bytes();
     }
     ~Engine() {
+        if (unconv_pin) cudaFreeHost(unconv_pin);
         if (cb) cublasDestroy(cb);
         if (cs) cusolverDnDestroy(cs);
     }
@@ -489,10 +495,24 @@ template <typename T> struct Engine {
             note_launch();
             B200_CUDA(cudaGetLastError());
         }
-        int hinfo[4];
+        // the tensor-core GEMMs' error word travels with the flags: one host round trip for all of them
+        int* gemm_err = nullptr;
+        if constexpr (kF32) gemm_err = tcw.err.ptr;
+        else if (oz) gemm_err = ozw.err.ptr;
+        if (gemm_err)
+            B200_CUDA(cudaMemcpyAsync(info.ptr + 4, gemm_err, sizeof(int), cudaMemcpyDeviceToDevice, s));
+        else
+            B200_CUDA(cudaMemsetAsync(info.ptr + 4, 0, sizeof(int), s));
+        int hinfo[5];
         B200_CUDA(cudaMemcpyAsync(eig_h.data(), w.ptr, nband * sizeof(double), cudaMemcpyDeviceToHost, s));
-        B200_CUDA(cudaMemcpyAsync(hinfo, info.ptr, 4 * sizeof(int), cudaMemcpyDeviceToHost, s));
+        B200_CUDA(cudaMemcpyAsync(hinfo, info.ptr, 5 * sizeof(int), cudaMemcpyDeviceToHost, s));
         B200_CUDA(cudaStreamSynchronize(s));
+        if (hinfo[4] != 0) {
+            B200_CUDA(cudaMemsetAsync(gemm_err, 0, sizeof(int), s));  // read once, then cleared
+            B200_CUDA(cudaStreamSynchronize(s));
+            throw Error(kCudaError, std::string(kF32 ? "tensor-core" : "int8 tensor-core") +
+                                        " GEMM wait ran out (error word " + std::to_string(hinfo[4]) + ")");
+        }
         B200_CHECK(hinfo[3] == 0, kNumericalError,
                    "non-finite entries in the subspace matrix (NaN/Inf in psi, V_eff, D or H|psi>)");
         B200_CHECK(hinfo[1] == 0, kNumericalError,
@@ -501,19 +521,14 @@ template <typename T> struct Engine {
         for (int m = 0; m < nband; ++m)
             B200_CHECK(std::isfinite(eig_h[m]), kNumericalError, "non-finite eigenvalue (NaN/Inf in H|psi> or psi)");
         tock(t_eig);
-        if constexpr (kF32) {
-            const int e = tcw.err.ptr ? tcw.read_error(s) : 0;
-            B200_CHECK(e == 0, kCudaError, "tensor-core GEMM wait ran out (error word " + std::to_string(e) + ")");
-        } else if (oz) {
-            const int e = ozw.err.ptr ? ozw.read_error(s) : 0;
-            B200_CHECK(e == 0, kCudaError, "int8 tensor-core GEMM wait ran out (error word " + std::to_string(e) + ")");
-        }
     }
 
     void cal_grad(const HPsiDevice& f, int nbase, int nc) {
         const T one = cmake<T>(1, 0), zero = cmake<T>(0, 0);
         tick();
-        B200_CUDA(cudaMemcpyAsync(unconv_d.ptr, unconv_h.data(), nc * sizeof(int), cudaMemcpyHostToDevice, s));
+        // the previous upload from unconv_pin completed before the last eigensolve's results were read
+        std::memcpy(unconv_pin, unconv_h.data(), size_t(nc) * sizeof(int));
+        B200_CUDA(cudaMemcpyAsync(unconv_d.ptr, unconv_pin, nc * sizeof(int), cudaMemcpyHostToDevice, s));
         k_gather_cols<T><<<grid_of(long(nbase) * nc), kT, 0, s>>>(nbase, nbase_x, nc, L, unconv_d.ptr, vcc.ptr, w.ptr,
                                                                   vc.ptr, vcl.ptr);
         note_launch();
@@ -550,7 +565,7 @@ template <typename T> struct Engine {
 
     int diag_once(const HPsiDevice& f, int ldpsi, T* psi, double* eig_in, double thr, int maxiter, int& notconv) {
         const T one = cmake<T>(1, 0), zero = cmake<T>(0, 0);
-        B200_CUDA(cudaMemsetAsync(info.ptr, 0, 4 * sizeof(int), s));
+        B200_CUDA(cudaMemsetAsync(info.ptr, 0, 5 * sizeof(int), s));
         B200_CUDA(cudaMemcpy2DAsync(basis.ptr, ld * sizeof(T), psi, size_t(ldpsi) * sizeof(T), dim * sizeof(T), nband,
                                     cudaMemcpyDeviceToDevice, s));
         orth_block(basis.ptr, nband, 0, handover && ntry_ == 0);
