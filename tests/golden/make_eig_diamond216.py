@@ -15,8 +15,8 @@ runs instead; the fixture records which ran.
 Stored: the 480 eigenvalues (Ry), the iteration count, thr, the solver that ran, and the largest residual
 norm |H x - e x| of the returned vectors (a-posteriori bound on each eigenvalue's error).
 
-Run from the repository root:  python tests/golden/make_eig_diamond216.py   (about an hour on 8 cores,
-about 25 GB of host memory)
+Run from the repository root:  python tests/golden/make_eig_diamond216.py   (about 30 minutes on 8 cores,
+about 20 GB of host memory)
 """
 from __future__ import annotations
 
