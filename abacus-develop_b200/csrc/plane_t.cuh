@@ -230,6 +230,31 @@ __global__ void __launch_bounds__(NT, MINB) k_plane_t(PlaneMapView pm, int nz, c
     __syncthreads();
 
     // ---- x: rows of RB positions; inverse, x V_eff, forward ----
+    // FP64: a thread's pass-A items all have t = tid % R2 (NT is a multiple of R2), so its R1 column indices
+    // cmap[R2 n1 + t] are read once, packed one byte each (0xFF: no occupied column), instead of from shared
+    // memory in every pass-A item of every row batch (FP32 CTAs, four per SM, have no registers to spare)
+    static_assert(NT % R2 == 0, "x pass A: one t per thread");
+    constexpr bool kPack = sizeof(T) == 16;
+    constexpr int NPK = kPack ? (R1 + 3) / 4 : 1;
+    unsigned cpk[NPK];
+    if constexpr (kPack) {
+        const int tx = tid % R2;
+#pragma unroll
+        for (int w = 0; w < NPK; ++w) cpk[w] = 0;
+#pragma unroll
+        for (int n1 = 0; n1 < R1; ++n1) {
+            const int cm = cmap[R2 * n1 + tx];
+            cpk[n1 / 4] |= unsigned(cm < 0 ? 0xFF : cm) << (8 * (n1 % 4));
+        }
+    }
+    auto col_of = [&](int n1, int t) -> int {
+        if constexpr (kPack) {
+            const unsigned b = (cpk[n1 / 4] >> (8 * (n1 % 4))) & 0xFFu;
+            return b == 0xFFu ? -1 : int(b);
+        } else {
+            return cmap[R2 * n1 + t];
+        }
+    };
     const R* vz = vt + size_t(zs) * N * N;
     for (int p0 = 0; p0 < N; p0 += RB) {
         for (int i = tid; i < RB * R2; i += NT) {
@@ -238,7 +263,7 @@ __global__ void __launch_bounds__(NT, MINB) k_plane_t(PlaneMapView pm, int nz, c
             T u[R1];
 #pragma unroll
             for (int n1 = 0; n1 < R1; ++n1) {
-                const int cm = cmap[R2 * n1 + t];
+                const int cm = col_of(n1, t);
                 u[n1] = cm >= 0 ? A[cm * LDC + pp] : zero;
             }
             dft<T, +1, R1>(u);
@@ -280,7 +305,7 @@ __global__ void __launch_bounds__(NT, MINB) k_plane_t(PlaneMapView pm, int nz, c
             dft<T, -1, R1>(u);
 #pragma unroll
             for (int n1 = 0; n1 < R1; ++n1) {
-                const int cm = cmap[R2 * n1 + t];
+                const int cm = col_of(n1, t);
                 if (cm >= 0) A[cm * LDC + pp] = u[n1];
             }
         }
