@@ -24,11 +24,16 @@ Compiled from the reference (unchanged, from where they lie):
                                                    the plane-wave basis and its transforms
   source/module_hamilt_pw/hamilt_pwdft/{operator_pw/{operator_pw,ekinetic_pw,veff_pw},kernels/{ekinetic_op,
   veff_op}}.cpp                                    the kinetic and local operators of H|psi>
+  source/module_hamilt_pw/hamilt_pwdft/{operator_pw/nonlocal_pw,kernels/nonlocal_op}.cpp
+                                                   the nonlocal operator of H|psi> (Nonlocal::init / act /
+                                                   add_nonlocal_pp with its functor), compiled against
+                                                   ref/nl_stub/: stand-ins for UnitCell and
+                                                   pseudopot_cell_vnl that declare only the members it reads
 plus this directory's ref/shim.cpp (process-level services: WARNING_QUIT throws, TITLE is silent, the CPU
 device tag, a one-process reduce_pool, NPROC_IN_POOL = 1, diagH_LAPACK on the reference's dngvd_op) and
 ref/david_capi.cpp, ref/dav_subspace_capi.cpp, ref/bpcg_capi.cpp (C entry points with a callback H|psi>),
 ref/occupy_capi.cpp (the occupation functions), ref/pw_basis_capi.cpp (the basis set-up, its transforms
-and the local H|psi> operators).
+and the local H|psi> operators), ref/nonlocal_capi.cpp (the nonlocal operator).
 ref/include/fftw3.h declares the FFTW API names those sources use and ref/fftw_stub.cpp stands in for them
 (FFTW is absent): plans record a batch of 1-D complex transforms that executing runs as mixed-radix FFTs.
 
@@ -96,12 +101,17 @@ SOURCES = [
     "module_hamilt_pw/hamilt_pwdft/operator_pw/veff_pw.cpp",
     "module_hamilt_pw/hamilt_pwdft/kernels/ekinetic_op.cpp",
     "module_hamilt_pw/hamilt_pwdft/kernels/veff_op.cpp",
+    "module_hamilt_pw/hamilt_pwdft/operator_pw/nonlocal_pw.cpp",
+    "module_hamilt_pw/hamilt_pwdft/kernels/nonlocal_op.cpp",
     "module_base/matrix3.cpp",
     "module_base/mymath.cpp",
 ]
 OWN = [HERE / "ref" / "shim.cpp", HERE / "ref" / "david_capi.cpp", HERE / "ref" / "dav_subspace_capi.cpp",
        HERE / "ref" / "bpcg_capi.cpp", HERE / "ref" / "occupy_capi.cpp", HERE / "ref" / "pw_basis_capi.cpp",
-       HERE / "ref" / "fftw_stub.cpp"]
+       HERE / "ref" / "fftw_stub.cpp", HERE / "ref" / "nonlocal_capi.cpp"]
+# compiled with ref/nl_stub/ ahead of the reference tree on the include path (the cell and projector
+# stand-ins the nonlocal operator is built against); every other file sees only the reference's headers
+NL_STUB = {"nonlocal_pw.cpp", "nonlocal_op.cpp", "nonlocal_capi.cpp"}
 
 
 def openblas() -> Path:
@@ -136,7 +146,8 @@ def build(quiet: bool = False, ref: str | os.PathLike | None = None) -> Path | N
     objs = []
     for src in [REF / s for s in SOURCES] + OWN:
         obj = tmp / (src.parent.name + "_" + src.stem + ".o")
-        run(["g++", *flags, "-c", str(src), "-o", str(obj)])
+        extra = [f"-I{HERE / 'ref' / 'nl_stub'}"] if src.name in NL_STUB else []
+        run(["g++", *extra, *flags, "-c", str(src), "-o", str(obj)])
         objs.append(obj)
     # Fortran BLAS / LAPACK references -> scipy_ names
     lib = openblas()

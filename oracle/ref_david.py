@@ -223,3 +223,34 @@ def hpsi_local(lat0, latvec, ecutwfc, kvec_d, ik, veff, psi, nbands, ecutrho=Non
     if rc != 0:
         raise RuntimeError("reference local H|psi> failed: " + lib.ref_pw_basis_last_error().decode())
     return out
+
+
+def nonlocal_act(na, nh, vkb, deeq, psi, npw, hpsi=None):
+    """The nonlocal part of H|psi> by the reference's own Nonlocal operator (operator_pw/nonlocal_pw.cpp:
+    init + act, add_nonlocal_pp with nonlocal_pw_op, gemm_op / gemv_op), compiled against stand-ins for
+    UnitCell and pseudopot_cell_vnl that hold na[it], nh[it], the projectors and D.  vkb: (nkb, npwx) complex;
+    deeq: (nspin, natoms, nhm, nhm) real, spin 0 used; psi: (nbands, ld) complex.  Returns hpsi + V_NL psi
+    (hpsi defaults to zeros), the act() of one k-point with npol = 1."""
+    lib = _load()
+    if not hasattr(lib, "_nl_ready"):
+        pi = C.POINTER(C.c_int)
+        lib.ref_nonlocal_act.argtypes = [C.c_int, pi, pi, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_int,
+                                         C.POINTER(C.c_double), C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p,
+                                         C.c_char_p, C.c_int]
+        lib.ref_nonlocal_act.restype = C.c_int
+        lib._nl_ready = True
+    na_a = np.ascontiguousarray(na, dtype=np.int32)
+    nh_a = np.ascontiguousarray(nh, dtype=np.int32)
+    v = np.ascontiguousarray(vkb, dtype=np.complex128)
+    d = np.ascontiguousarray(deeq, dtype=np.float64)
+    x = np.ascontiguousarray(psi, dtype=np.complex128)
+    out = np.zeros_like(x) if hpsi is None else np.ascontiguousarray(hpsi, dtype=np.complex128).copy()
+    nb, ld = x.shape
+    err = C.create_string_buffer(512)
+    pi = C.POINTER(C.c_int)
+    rc = lib.ref_nonlocal_act(len(na_a), na_a.ctypes.data_as(pi), nh_a.ctypes.data_as(pi), v.shape[0], v.shape[1],
+                              v.ctypes.data, d.shape[0], d.shape[1], d.shape[2], d.ctypes.data_as(C.POINTER(C.c_double)),
+                              nb, int(npw), ld, x.ctypes.data, out.ctypes.data, err, 512)
+    if rc != 0:
+        raise RuntimeError("reference Nonlocal::act failed: " + err.value.decode())
+    return out
